@@ -1,0 +1,476 @@
+"""atomiverse_b200 -- B200-native classical-MD hot path behind a C ABI.
+
+The compute path is libatvb.so (hand-written CUDA for sm_100a, see csrc/);
+this module is a thin ctypes view of its C ABI (include/atvb.h) plus the
+reference-shaped component API (NeighborList, PairLJCut, CoulLong,
+KSpacePME, VelocityVerlet, NoseHoover, FixLangevin, MD) that assembles a
+system description.  There is no CPU fallback: every call goes to the GPU
+library, and importing the package fails loudly if the library is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _abi
+from ._abi import (FP64, LANGEVIN, MIXED, NOSE_HOOVER, NVE, AtvbError,
+                   Scalars, SoaView, SystemDesc, check, load)
+
+__all__ = [
+    "FP64", "MIXED", "NVE", "NOSE_HOOVER", "LANGEVIN", "AtvbError",
+    "Context", "System", "Batch", "Server", "make_desc",
+    "NeighborList", "PairLJCut", "CoulLong", "KSpacePME", "VelocityVerlet",
+    "NoseHoover", "FixLangevin", "MD", "library_path",
+]
+
+FRAME_KEYS = ("x", "y", "z", "vx", "vy", "vz", "fx", "fy", "fz", "mass", "charge")
+
+
+def library_path() -> str:
+    return _abi.LIB_PATH
+
+
+def make_desc(n_atoms, box, **kw) -> SystemDesc:
+    """Flat system record; keywords are the atvb_system_desc field names."""
+    d = SystemDesc()
+    d.n_atoms = int(n_atoms)
+    b = list(box)
+    if len(b) == 3:
+        b = [b[0], 0, 0, 0, b[1], 0, 0, 0, b[2]]
+    for k in range(9):
+        d.box[k] = float(b[k])
+    d.nl_skin = -1.0
+    d.nl_every = 1
+    d.nl_delay = 0
+    d.nl_check = 1
+    d.pme_order = 4
+    d.dt = 1.0
+    for k, v in kw.items():
+        if k == "pme_grid":
+            for i in range(3):
+                d.pme_grid[i] = int(v[i])
+        elif k == "box":
+            continue
+        else:
+            if not hasattr(d, k):
+                raise TypeError(f"unknown system field {k!r}")
+            setattr(d, k, v)
+    return d
+
+
+def _soa(frame: dict, n: int, writable: bool = False) -> tuple[SoaView, list]:
+    """SoaView over numpy arrays in `frame` (float64, contiguous)."""
+    v = SoaView()
+    keep = []
+    for k in FRAME_KEYS:
+        a = frame.get(k)
+        if a is None:
+            continue
+        if writable:
+            if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.c_contiguous):
+                raise TypeError(f"frame[{k!r}] must be a contiguous float64 array")
+        else:
+            a = np.ascontiguousarray(a, dtype=np.float64)
+        if a.shape[0] != n:
+            raise ValueError(f"frame[{k!r}] has {a.shape[0]} rows, expected {n}")
+        keep.append(a)
+        setattr(v, k, a.ctypes.data_as(C.POINTER(C.c_double)))
+    t = frame.get("tag")
+    if t is not None:
+        t = np.ascontiguousarray(t, dtype=np.int64)
+        keep.append(t)
+        v.tag = t.ctypes.data_as(C.POINTER(C.c_int64))
+    return v, keep
+
+
+def scalars_dict(s: Scalars) -> dict:
+    return {
+        "energy": s.energy, "energy_pair": s.energy_pair, "energy_lj": s.energy_lj,
+        "energy_coul": s.energy_coul, "energy_recip": s.energy_recip,
+        "energy_const": s.energy_const, "kinetic": s.kinetic, "conserved": s.conserved,
+        "stress": np.array(list(s.stress)), "nh_xi": s.nh_xi, "step": s.step,
+        "rebuilds": s.rebuilds, "max_neighbors": s.max_neighbors, "status": s.status,
+    }
+
+
+class Context:
+    """One CUDA device (cuda::Context)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load()
+        opts = _abi.DeviceOpts()
+        opts.device = device
+        h = C.c_void_p()
+        check(self.lib.atvb_ctx_create(C.byref(opts), C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.atvb_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
+class System:
+    """One MD system on the device (cuda::md::MD + its components)."""
+
+    def __init__(self, ctx: Context, desc: SystemDesc | dict, frame: dict | None = None):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        if isinstance(desc, dict):
+            desc = make_desc(**desc)
+        self.desc = desc
+        self.n = desc.n_atoms
+        h = C.c_void_p()
+        check(self.lib.atvb_system_create(ctx._h, C.byref(desc), C.byref(h)))
+        self._h = h
+        if frame is not None:
+            self.upload(frame)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.atvb_system_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def upload(self, frame: dict):
+        v, keep = _soa(frame, self.n)
+        check(self.lib.atvb_system_upload(self._h, C.byref(v)))
+        del keep
+
+    def compute_forces(self):
+        check(self.lib.atvb_system_compute_forces(self._h))
+
+    def step(self, n: int):
+        check(self.lib.atvb_system_step(self._h, int(n)))
+
+    def download(self, keys=FRAME_KEYS) -> tuple[dict, dict]:
+        out = {k: np.zeros(self.n) for k in keys}
+        v, keep = _soa(out, self.n, writable=True)
+        s = Scalars()
+        check(self.lib.atvb_system_download(self._h, C.byref(v), C.byref(s)))
+        return out, scalars_dict(s)
+
+    def scalars(self) -> dict:
+        s = Scalars()
+        check(self.lib.atvb_system_scalars(self._h, C.byref(s)))
+        return scalars_dict(s)
+
+    def run(self, frame: dict, n_steps: int) -> dict:
+        """MD::run(frame, n): upload on first use, step, download into frame."""
+        for k in FRAME_KEYS:
+            if k not in frame:
+                frame[k] = np.zeros(self.n)
+            frame[k] = np.ascontiguousarray(frame[k], dtype=np.float64)
+        v, keep = _soa(frame, self.n, writable=True)
+        s = Scalars()
+        check(self.lib.atvb_system_run(self._h, C.byref(v), int(n_steps), C.byref(s)))
+        return scalars_dict(s)
+
+    def history(self, max_steps: int = 4096) -> np.ndarray:
+        buf = np.zeros(3 * max_steps)
+        cnt = C.c_int32()
+        check(self.lib.atvb_system_energy_history(
+            self._h, buf.ctypes.data_as(C.POINTER(C.c_double)), int(max_steps), C.byref(cnt)))
+        return buf[: 3 * cnt.value].reshape(-1, 3)
+
+    def pairs(self) -> tuple[np.ndarray, np.ndarray]:
+        cnt = C.c_int64()
+        check(self.lib.atvb_system_pairs(self._h, None, None, 0, C.byref(cnt)))
+        pi = np.zeros(cnt.value, dtype=np.int32)
+        pj = np.zeros(cnt.value, dtype=np.int32)
+        check(self.lib.atvb_system_pairs(
+            self._h, pi.ctypes.data_as(C.POINTER(C.c_int32)),
+            pj.ctypes.data_as(C.POINTER(C.c_int32)), cnt.value, C.byref(cnt)))
+        return pi, pj
+
+    def set_pair_lanes(self, lanes: int):
+        check(self.lib.atvb_system_set_pair_lanes(self._h, int(lanes)))
+
+    def profile(self, enable: bool):
+        check(self.lib.atvb_system_profile(self._h, 1 if enable else 0))
+
+    def profile_read(self) -> dict:
+        buf = (_abi.KernelTime * 64)()
+        cnt = C.c_int32()
+        check(self.lib.atvb_system_profile_read(self._h, buf, 64, C.byref(cnt)))
+        return {buf[k].name.decode(): (buf[k].total_ms, buf[k].launches) for k in range(cnt.value)}
+
+    def launch_count(self) -> int:
+        n = C.c_int64()
+        check(self.lib.atvb_system_launch_count(self._h, C.byref(n)))
+        return n.value
+
+    def stream(self) -> int:
+        return self.lib.atvb_system_stream(self._h) or 0
+
+
+class Batch:
+    """Many independent systems advanced by one launch per kernel."""
+
+    def __init__(self, ctx: Context, items: list):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        descs = [make_desc(**d) if isinstance(d, dict) else d for d, _ in items]
+        arr = (SystemDesc * len(descs))(*descs)
+        self.sizes = [d.n_atoms for d in descs]
+        h = C.c_void_p()
+        check(self.lib.atvb_batch_create(ctx._h, arr, len(descs), C.byref(h)))
+        self._h = h
+        for k, (_, frame) in enumerate(items):
+            if frame is not None:
+                self.upload(k, frame)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.atvb_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def upload(self, k: int, frame: dict):
+        v, keep = _soa(frame, self.sizes[k])
+        check(self.lib.atvb_batch_upload(self._h, int(k), C.byref(v)))
+
+    def compute_forces(self):
+        check(self.lib.atvb_batch_compute_forces(self._h))
+
+    def step(self, n: int):
+        check(self.lib.atvb_batch_step(self._h, int(n)))
+
+    def download(self, k: int, keys=FRAME_KEYS) -> tuple[dict, dict]:
+        out = {key: np.zeros(self.sizes[k]) for key in keys}
+        v, keep = _soa(out, self.sizes[k], writable=True)
+        s = Scalars()
+        check(self.lib.atvb_batch_download(self._h, int(k), C.byref(v), C.byref(s)))
+        return out, scalars_dict(s)
+
+    def autotune(self) -> int:
+        g = C.c_int32()
+        check(self.lib.atvb_batch_autotune(self._h, C.byref(g)))
+        return g.value
+
+    def launch_count(self) -> int:
+        n = C.c_int64()
+        check(self.lib.atvb_batch_launch_count(self._h, C.byref(n)))
+        return n.value
+
+
+class Server:
+    """Continuous batching of MD segments under a device-memory budget."""
+
+    def __init__(self, ctx: Context, budget_bytes: int, max_active: int = 0):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        h = C.c_void_p()
+        check(self.lib.atvb_server_create(ctx._h, int(budget_bytes), int(max_active), C.byref(h)))
+        self._h = h
+        self.sizes = {}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.atvb_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def submit(self, desc, frame: dict, n_steps: int) -> int:
+        if isinstance(desc, dict):
+            desc = make_desc(**desc)
+        v, keep = _soa(frame, desc.n_atoms)
+        rid = C.c_int64()
+        check(self.lib.atvb_server_submit(self._h, C.byref(desc), C.byref(v), int(n_steps),
+                                          C.byref(rid)))
+        self.sizes[rid.value] = desc.n_atoms
+        return rid.value
+
+    def cancel(self, rid: int):
+        check(self.lib.atvb_server_cancel(self._h, int(rid)))
+
+    def tick(self, chunk: int = 50):
+        check(self.lib.atvb_server_tick(self._h, int(chunk)))
+
+    def poll(self, rid: int) -> dict:
+        r = _abi.RequestResult()
+        check(self.lib.atvb_server_poll(self._h, int(rid), C.byref(r)))
+        return {"id": r.id, "state": r.state, "steps_done": r.steps_done,
+                "t_submit": r.t_submit, "t_start": r.t_start, "t_done": r.t_done,
+                "scalars": scalars_dict(r.scalars)}
+
+    def collect(self, rid: int) -> tuple[dict, dict]:
+        n = self.sizes[rid]
+        out = {k: np.zeros(n) for k in FRAME_KEYS[:9]}
+        v, keep = _soa(out, n, writable=True)
+        r = _abi.RequestResult()
+        check(self.lib.atvb_server_collect(self._h, int(rid), C.byref(v), C.byref(r)))
+        res = {"id": r.id, "state": r.state, "steps_done": r.steps_done,
+               "t_submit": r.t_submit, "t_start": r.t_start, "t_done": r.t_done,
+               "scalars": scalars_dict(r.scalars)}
+        return out, res
+
+    def stats(self) -> dict:
+        q, r, d = C.c_int64(), C.c_int64(), C.c_int64()
+        b = C.c_size_t()
+        check(self.lib.atvb_server_stats(self._h, C.byref(q), C.byref(r), C.byref(d), C.byref(b)))
+        return {"queued": q.value, "running": r.value, "done": d.value, "bytes": b.value}
+
+
+def request_bytes(desc) -> int:
+    if isinstance(desc, dict):
+        desc = make_desc(**desc)
+    b = C.c_size_t()
+    check(load().atvb_request_bytes(C.byref(desc), C.byref(b)))
+    return b.value
+
+
+# ---------------------------------------------------------------------------
+# Reference-shaped component API (cuda::NeighborList, cuda::PairLJCut, ...).
+# Each component only records its constructor arguments; MD.build() folds
+# them into one system description for the fused device step.
+# ---------------------------------------------------------------------------
+
+@dataclass
+class NeighborList:
+    """NeighborList(cutoff, skin=-1 -> 0.3*cutoff, every, delay, check)
+    (neighbor_list.cuh:98; cpu/neighbor/neighbor_list.h:79)."""
+    cutoff: float
+    skin: float = -1.0
+    every: int = 1
+    delay: int = 0
+    check: bool = True
+
+
+@dataclass
+class PairLJCut:
+    """PairLJCut(epsilon, sigma, cutoff) (pair_lj_cut.cuh:25)."""
+    epsilon: float
+    sigma: float
+    cutoff: float
+
+
+@dataclass
+class CoulLong:
+    """CoulLong(alpha, cutoff) (coul_long.cuh:24)."""
+    alpha: float
+    cutoff: float
+
+
+@dataclass
+class KSpacePME:
+    """KSpacePME(alpha, grid_spacing=1.0, order=6) (pme.cuh:26); `grid`
+    fixes the mesh instead of the spacing rule."""
+    alpha: float
+    grid_spacing: float = 1.0
+    order: int = 6
+    grid: tuple | None = None
+
+
+@dataclass
+class VelocityVerlet:
+    dt: float
+
+
+@dataclass
+class NoseHoover:
+    """NoseHoover(T, tau, dt) (nose_hoover.cu:29)."""
+    T: float
+    tau: float
+    dt: float
+
+
+@dataclass
+class FixLangevin:
+    """FixLangevin(T_start, T_stop, damp, dt, seed) (fix_langevin.h)."""
+    T_start: float
+    T_stop: float
+    damp: float
+    dt: float
+    seed: int = 0
+
+
+@dataclass
+class MD:
+    """cuda::md::MD: categorical setters, build(), run(frame, n)
+    (include/atomiverse/cuda/dynamics/md.cuh:118-385)."""
+    ctx: Context | None = None
+    precision: int = FP64
+    _neighbor: NeighborList | None = None
+    _evaluators: list = field(default_factory=list)
+    _integrator: VelocityVerlet | None = None
+    _thermostats: list = field(default_factory=list)
+    _stress: bool = False
+    _system: System | None = None
+
+    def set_neighbor(self, nl: NeighborList):
+        self._neighbor = nl
+        return self
+
+    def set_evaluator(self, ev):
+        self._evaluators.append(ev)
+        return self
+
+    def set_integrator(self, integ: VelocityVerlet):
+        if self._integrator is not None and self._integrator != integ:
+            raise ValueError("set_integrator already configured")
+        self._integrator = integ
+        return self
+
+    def set_thermostat(self, th):
+        self._thermostats.append(th)
+        return self
+
+    def set_stress_required(self, on: bool = True):
+        self._stress = on
+        return self
+
+    def desc(self, n_atoms: int, box) -> SystemDesc:
+        if self._integrator is None:
+            raise ValueError("MD needs an integrator (set_integrator)")
+        if self._neighbor is None and self._evaluators:
+            raise ValueError("a pair evaluator needs a NeighborList: "
+                             "add sim.set_neighbor(NeighborList(cutoff))")
+        kw = dict(precision=self.precision, dt=self._integrator.dt,
+                  stress_required=int(self._stress))
+        nl = self._neighbor
+        kw.update(nl_cutoff=nl.cutoff, nl_skin=nl.skin, nl_every=nl.every,
+                  nl_delay=nl.delay, nl_check=int(nl.check))
+        for ev in self._evaluators:
+            if isinstance(ev, PairLJCut):
+                kw.update(lj_enabled=1, lj_epsilon=ev.epsilon, lj_sigma=ev.sigma,
+                          lj_cutoff=ev.cutoff)
+            elif isinstance(ev, CoulLong):
+                kw.update(coul_enabled=1, coul_alpha=ev.alpha, coul_cutoff=ev.cutoff)
+            elif isinstance(ev, KSpacePME):
+                kw.update(pme_enabled=1, pme_alpha=ev.alpha,
+                          pme_grid_spacing=ev.grid_spacing, pme_order=ev.order)
+                if ev.grid is not None:
+                    kw["pme_grid"] = tuple(ev.grid)
+            else:
+                raise TypeError(f"unsupported evaluator {type(ev).__name__}")
+        for th in self._thermostats:
+            if isinstance(th, NoseHoover):
+                kw.update(thermostat=NOSE_HOOVER, temperature=th.T, tau=th.tau)
+            elif isinstance(th, FixLangevin):
+                if th.T_stop not in (th.T_start, -1.0):
+                    raise ValueError("temperature ramps are not supported")
+                kw.update(thermostat=LANGEVIN, temperature=th.T_start, damp=th.damp,
+                          seed=th.seed)
+            else:
+                raise TypeError(f"unsupported thermostat {type(th).__name__}")
+        return make_desc(n_atoms, box, **kw)
+
+    def run(self, frame: dict, n_steps: int, box=None) -> dict:
+        if self._system is None:
+            if self.ctx is None:
+                self.ctx = Context(0)
+            n = len(frame["x"])
+            self._system = System(self.ctx, self.desc(n, box if box is not None else frame["box"]))
+        return self._system.run(frame, n_steps)

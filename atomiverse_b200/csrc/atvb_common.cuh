@@ -1,0 +1,214 @@
+// atvb_common.cuh -- device-side data model shared by every kernel.
+//
+// One MD system lives in one slot of an Engine.  All per-system device
+// pointers and constants sit in a SysParams record in device memory; every
+// kernel walks a flat list of work items {system, first atom} so that one
+// launch covers any number of systems (the single-system path is a batch of
+// one).  Per-atom master state (x, v, mass, charge, tag) is kept in the
+// caller's original order; the force kernels work on a cell-sorted copy of
+// the positions (pos4) whose order is rebuilt with the neighbour list.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace atvb {
+
+// units.h:138,165,166,173 of the reference (metal units)
+constexpr double kKB = 8.617333262e-5;
+constexpr double kFtm2v = 1.0 / 103.6427;
+constexpr double kMvv2e = 103.6427;
+constexpr double kQqr2e = 14.399645;
+constexpr double kPi = 3.14159265358979323846;
+constexpr double kEwaldF = 1.1283791670955126; // 2/sqrt(pi)
+
+enum Precision : int { kFP64 = 0, kMixed = 1 };
+enum Thermostat : int { kNVE = 0, kNoseHoover = 1, kLangevin = 2 };
+
+// Fixed-point scales.  Energies/virials/KE are accumulated per system as
+// 64-bit integers in units of 2^-32 eV (range +-2.1e9 eV), so their sums are
+// independent of block order; the PME charge grid uses 2^-40 e (FP64) or
+// 2^-32 e (mixed).
+constexpr double kEFix = 4294967296.0;          // 2^32
+constexpr double kEFixInv = 1.0 / 4294967296.0;
+
+// Indices into SysState::acc
+enum Acc : int {
+    kAccELJ = 0,
+    kAccECoul = 1,
+    kAccERecip = 2,
+    kAccVir = 3, // 6 entries: xx yy zz xy xz yz
+    kAccKEA = 9,
+    kAccKEB = 10,
+    kAccCount = 12
+};
+
+struct SysState {
+    unsigned long long acc[kAccCount]; // fixed-point accumulators
+    double xi;         // Nose-Hoover friction
+    double vscale;     // deferred velocity scale (applied by next kick)
+    double s_a;        // scale from the initial-half thermostat
+    double energy, e_lj, e_coul, e_recip, e_const, kinetic, conserved;
+    double virial[6];
+    long long step;
+    long long rebuilds;
+    int ago;           // steps since the last neighbour build
+    int need_rebuild;  // set by the displacement check
+    int rebuild;       // decision for this step
+    int overflow;      // neighbour row overflowed its capacity
+    int max_nnbr;      // largest row seen at the last build
+    int status;        // sticky error bits
+};
+
+struct SysParams {
+    // geometry (orthorhombic)
+    int n;
+    int prec;
+    double L[3], invL[3], halfL[3];
+    float Lf_fix[3]; // L / 2^32 (mixed: fixed-point position step)
+    double fix_scale[3]; // 2^32 / L
+    // neighbour list
+    double rlist2;     // (cutoff + skin)^2, the pair-set test
+    double skin_half2; // (skin/2)^2
+    int nl_every, nl_delay, nl_check;
+    int nc[3], ncell;
+    double cs_inv[3];
+    int alias[3]; // axis has fewer than 2*reach+1 cells: visit every cell
+    int ncol;     // stencil columns
+    int4* cols;   // {dx, dy, zreach(-1 = whole column), 0}
+    int cap;      // neighbour row capacity
+    // LJ
+    int has_lj;
+    double lj_rc2, lj_sig6, lj_eps4, lj_eps24, lj_shift;
+    // real-space Coulomb; erfc(x) = exp(-x^2) * erfcx(x) with erfcx from a
+    // piecewise polynomial fitted on [0, alpha * cutoff] (see erfcx_fit)
+    int has_coul;
+    double coul_rc2, coul_alpha, coul_alpha2;
+    int erfcx_nint;       // intervals (<= kErfcxMaxInt)
+    double erfcx_inv_h;   // intervals per unit of x
+    const double* erfcx_d; // erfcx_nint x kErfcxNd monomial coefficients
+    const float* erfcx_f;  // erfcx_nint x kErfcxNf
+    // PME
+    int has_pme;
+    int K[3], Kh, order;
+    double pme_fscale; // k_e / (pi V)
+    double pme_escale; // k_e / (2 pi V)
+    double pme_alpha2_pi2; // pi^2 / alpha^2
+    double grid_scale, grid_scale_inv; // fixed-point charge scale
+    // integrator / thermostat
+    double dt, dtf; // dtf = dt/2 * ftm2v
+    int thermostat;
+    double T, Q, n_dof_kT, tau;
+    double lang_g1, lang_g2pre; // -1/(damp ftm2v), sqrt(2 kT/(damp dt mvv2e))/ftm2v
+    unsigned int seed;
+    int need_virial;
+    double e_const; // PME self + net-charge energy
+    // per-atom master state (original order)
+    double *x, *y, *z, *vx, *vy, *vz, *mass, *q;
+    long long* tag;
+    double *xr, *yr, *zr; // positions at the last neighbour build
+    // sorted order
+    void* pos4;      // double4 (FP64) or int4 fixed-point + float q (mixed)
+    double4* posd4;  // FP64 sorted positions used by the pair-set test
+    double4* f4;     // forces in sorted order
+    int *perm, *rank, *cell_of, *slot, *cell_count, *cell_start, *cellS;
+    int *nbr, *nnbr;
+    // PME buffers
+    unsigned long long* grid_fix;
+    void* grid_real;  // double or float, K0*K1*K2
+    void* grid_cplx;  // double2 or float2, K0*K1*Kh
+    double* infl;     // H(m) on the half-complex grid
+    // staging for upload / download (original order)
+    double *sx, *sy, *sz;
+    // scalars
+    SysState* st;
+    double* ehist; // energy history ring: 3 doubles per step (E, KE, step)
+    int ehist_cap;
+};
+
+// erfcx tables: erfcx_nint intervals over [0, alpha*rc]; on interval k the
+// local variable is u = x * (2/h) - (2k+1) in [-1, 1].
+constexpr int kErfcxMaxInt = 64;
+constexpr int kErfcxNd = 10; // FP64: degree 9
+constexpr int kErfcxNf = 7;  // FP32: degree 6
+
+// A unit of work: a chunk of atoms (or grid points) of one system.
+struct Item {
+    int sys;
+    int begin;
+};
+
+#define ATVB_DEV __device__ __forceinline__
+
+ATVB_DEV long long to_fix(double v) { return __double2ll_rn(v * kEFix); }
+
+ATVB_DEV void fix_add(unsigned long long* a, double v) {
+    atomicAdd(a, (unsigned long long)to_fix(v));
+}
+
+template <typename T>
+ATVB_DEV T warp_sum(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Block-wide FP64 sum in a fixed order (deterministic for a fixed block
+// shape); result valid in thread 0.  `sh` needs blockDim.x/32 doubles.
+ATVB_DEV double block_sum(double v, double* sh) {
+    v = warp_sum(v);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0)
+        sh[w] = v;
+    __syncthreads();
+    double t = 0.0;
+    if (w == 0) {
+        const int nw = blockDim.x >> 5;
+        t = l < nw ? sh[l] : 0.0;
+        t = warp_sum(t);
+    }
+    return t;
+}
+
+// Block-wide sums of N values at once (one pair of barriers); results valid
+// in thread 0.  `sh` needs 32*N doubles.  Fixed order, so deterministic for
+// a fixed block shape.
+template <int N>
+ATVB_DEV void block_sum_vec(double (&v)[N], double* sh) {
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+#pragma unroll
+    for (int k = 0; k < N; ++k)
+        v[k] = warp_sum(v[k]);
+    __syncthreads();
+    if (l == 0) {
+#pragma unroll
+        for (int k = 0; k < N; ++k)
+            sh[k * 32 + w] = v[k];
+    }
+    __syncthreads();
+    if (w == 0) {
+        const int nw = blockDim.x >> 5;
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            double t = l < nw ? sh[k * 32 + l] : 0.0;
+            v[k] = warp_sum(t);
+        }
+    }
+}
+
+// minimum image used by the force kernels (box.h:123-150 nearbyint form)
+ATVB_DEV double min_img(double d, double L, double invL) {
+    return d - L * rint(d * invL);
+}
+
+// orthorhombic wrap into [0, L) (pbc.h:48-50)
+ATVB_DEV double wrap(double x, double L) { return x - L * floor(x / L); }
+
+ATVB_DEV unsigned int pos_fix(double x, double scale) {
+    // x in [0, L] -> [0, 2^32); L itself folds onto 0
+    return (unsigned int)(unsigned long long)__double2ll_rn(x * scale);
+}
+
+} // namespace atvb

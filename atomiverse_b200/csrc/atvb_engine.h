@@ -1,0 +1,151 @@
+// atvb_engine.h -- host-side engine: systems (slots), work lists, graph.
+#pragma once
+
+#include <cufft.h>
+
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "atvb.h"
+#include "atvb_common.cuh"
+#include "atvb_kernels.cuh"
+
+struct atvb_ctx {
+    int device = 0;
+};
+
+namespace atvb {
+
+extern thread_local std::string g_last_error;
+
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+void cuda_check(cudaError_t e, const char* what);
+int good_fft_size(int n);
+size_t estimate_bytes(const atvb_system_desc& d);
+
+struct Geometry {
+    double L[3];
+    double skin, rlist;
+    int nc[3];
+    double cs[3];
+    int reach[3];
+    int alias[3];
+    std::vector<int4> cols;
+};
+Geometry make_geometry(const atvb_system_desc& d);
+
+// One system's device memory and host mirror of its SysParams.
+class Slot {
+  public:
+    Slot(const atvb_system_desc& d, cudaStream_t stream);
+    ~Slot();
+    Slot(const Slot&) = delete;
+    Slot& operator=(const Slot&) = delete;
+    void alloc_list(int cap);
+
+    atvb_system_desc desc;
+    Geometry geo;
+    SysParams hp;
+    int index = -1;
+    bool uploaded = false;
+    size_t bytes = 0;
+    int max_row = 0;
+    double mean_row = 0.0;
+    double erfcx_err = 0.0; // max relative error of the FP64 erfcx fit
+    cufftHandle plan_f = 0, plan_i = 0;
+    std::vector<double> infl_host;
+
+  private:
+    void* dalloc(size_t b);
+    std::vector<void*> allocs;
+    void* nbr_alloc = nullptr;
+};
+
+struct ProfEntry {
+    std::string name;
+    double ms;
+    long long launches;
+};
+
+class Engine {
+  public:
+    explicit Engine(int device);
+    ~Engine();
+    Engine(const Engine&) = delete;
+    Engine& operator=(const Engine&) = delete;
+
+    int add(const atvb_system_desc& d);
+    void remove(int id);
+    Slot* slot(int id);
+    void upload(int id, const atvb_soa_view& f);
+    void compute_forces();
+    void compute_forces_one(int id);
+    void step(int n);
+    void download(int id, atvb_soa_view* f, atvb_scalars* sc);
+    void scalars(int id, atvb_scalars* out);
+    int64_t pairs(int id, int32_t* pi, int32_t* pj, int64_t capacity);
+    int history(int id, double* out, int max_steps);
+    void set_lanes(int lanes);
+    int autotune();
+    void set_profiling(bool on) { profiling_ = on; }
+    const std::vector<ProfEntry>& profile() const { return prof_acc_; }
+    void clear_profile() { prof_acc_.clear(); }
+    int64_t last_launches() const { return last_launches_; }
+    int64_t kernels_per_step() const;
+    cudaStream_t stream() const { return stream_; }
+    int device() const { return device_; }
+    int lanes() const { return lc_.pair_G; }
+    size_t slot_count() const { return slots_.size(); }
+    bool has(int id) const {
+        return id >= 0 && id < (int)slots_.size() && slots_[id] != nullptr;
+    }
+
+  private:
+    void ensure_table();
+    void push_params(int id);
+    void build_lists();
+    void ensure_ready();
+    int choose_lanes() const;
+    bool check_lists(const LaunchCfg& lc);
+    void sized_rebuild(const LaunchCfg& lc);
+    LaunchCfg restricted_cfg(int id);
+    void enqueue_step(bool profile);
+    void enqueue_forces(const LaunchCfg& lc, const std::vector<int>& pme,
+                        bool profile);
+    void prof_mark(bool profile, const char* next);
+    void collect_profile();
+    void release_graph();
+
+    int device_ = 0;
+    cudaStream_t stream_ = nullptr;
+    int num_sms_ = 148;
+    std::vector<std::unique_ptr<Slot>> slots_;
+    SysParams* d_sp_ = nullptr;
+    int sp_cap_ = 0;
+    std::vector<void*> list_allocs_;
+    LaunchCfg lc_;
+    std::vector<int> pme_slots_;
+    bool dirty_ = true;
+    int list_epoch_ = 0;
+    std::map<int, std::pair<int, LaunchCfg>> single_;
+    cudaGraph_t graph_ = nullptr;
+    cudaGraphExec_t gexec_ = nullptr;
+    int lanes_fixed_ = 0;
+    int64_t last_launches_ = 0;
+    int64_t steps_since_check_ = 0;
+    bool profiling_ = false;
+    std::vector<cudaEvent_t> prof_events_;
+    size_t prof_used_ = 0;
+    std::vector<std::string> prof_seq_;
+    std::vector<ProfEntry> prof_acc_;
+};
+
+} // namespace atvb

@@ -1,0 +1,57 @@
+// atvb_kernels.cuh -- launch configuration shared by the kernel launchers
+// and the engine that captures them into the per-step CUDA graph.
+#pragma once
+
+#include "atvb_common.cuh"
+
+namespace atvb {
+
+constexpr int kChunk = 256;     // atoms per item of the per-atom kernels
+constexpr int kListChunk = 8;   // atoms per item of the list build (warp/atom)
+constexpr int kGridChunk = 4096; // grid points per item of the PME grid kernels
+
+struct ItemList {
+    const Item* d = nullptr; // device array
+    int n = 0;               // number of items
+    int grid = 0;            // blocks to launch (persistent loop covers n)
+};
+
+struct LaunchCfg {
+    const SysParams* sp = nullptr; // device table of every system
+    ItemList atoms;     // kChunk atoms per item (original or sorted order)
+    ItemList list;      // kListChunk atoms per item
+    ItemList pair;      // kChunk / pair_G atoms per item
+    ItemList cells;     // kChunk cells per item
+    ItemList pme_atoms; // kChunk atoms of PME systems
+    ItemList pme_grid;  // kGridChunk half-complex grid points per item
+    ItemList pme_real;  // kGridChunk real grid points per item
+    const int* sys_list = nullptr; // device list of system indices
+    int nsys = 0;
+    int pair_G = 4;     // lanes per atom in the pair kernel
+    int any_mixed = 0, any_fp64 = 0;
+    int pme_order = 4;  // common PME order (the PME kernels are templated)
+    int pme_mixed = 0;
+};
+
+// neighbor.cu
+void launch_rebuild(const LaunchCfg& lc, cudaStream_t s);
+// pair.cu
+void launch_pair(const LaunchCfg& lc, cudaStream_t s);
+// pme.cu
+void launch_pme_spread(const LaunchCfg& lc, cudaStream_t s);
+void launch_pme_convert(const LaunchCfg& lc, cudaStream_t s);
+void launch_pme_influence(const LaunchCfg& lc, cudaStream_t s);
+void launch_pme_gather(const LaunchCfg& lc, cudaStream_t s);
+// integrate.cu
+void launch_integrate_a(const LaunchCfg& lc, cudaStream_t s);
+void launch_sys_a(const LaunchCfg& lc, cudaStream_t s);
+void launch_integrate_b(const LaunchCfg& lc, cudaStream_t s);
+void launch_sys_b(const LaunchCfg& lc, cudaStream_t s);
+void launch_sys_energy(const LaunchCfg& lc, cudaStream_t s);
+void launch_force_rebuild(const LaunchCfg& lc, cudaStream_t s);
+void launch_state_in(const LaunchCfg& lc, cudaStream_t s);
+void launch_wrap_in(const LaunchCfg& lc, cudaStream_t s);
+void launch_state_out(const LaunchCfg& lc, int what, cudaStream_t s);
+void launch_kinetic(const LaunchCfg& lc, cudaStream_t s);
+
+} // namespace atvb

@@ -1,0 +1,317 @@
+// capi.cu -- the extern "C" boundary (include/atvb.h).  Every entry point
+// catches exceptions, records the message for atvb_last_error() and returns
+// a status code; nothing C++ crosses the boundary.
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "atvb.h"
+#include "atvb_engine.h"
+
+using atvb::Engine;
+using atvb::Error;
+
+struct atvb_system {
+    atvb_ctx* ctx = nullptr;
+    std::unique_ptr<Engine> eng;
+    int id = -1;
+    bool uploaded = false;
+};
+
+struct atvb_batch {
+    atvb_ctx* ctx = nullptr;
+    std::unique_ptr<Engine> eng;
+    std::vector<int> ids;
+};
+
+namespace {
+
+template <typename F>
+int guard(F&& f) {
+    try {
+        f();
+        atvb::g_last_error.clear();
+        return ATVB_OK;
+    } catch (const Error& e) {
+        atvb::g_last_error = e.what();
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        atvb::g_last_error = "host allocation failed";
+        return ATVB_ERR_NOMEM;
+    } catch (const std::exception& e) {
+        atvb::g_last_error = e.what();
+        return ATVB_ERR_INVALID;
+    } catch (...) {
+        atvb::g_last_error = "unknown error";
+        return ATVB_ERR_INVALID;
+    }
+}
+
+void need(const void* p, const char* what) {
+    if (!p)
+        throw Error(ATVB_ERR_INVALID, std::string(what) + " is NULL");
+}
+
+} // namespace
+
+extern "C" {
+
+int atvb_abi_version(void) { return ATVB_ABI_VERSION; }
+
+const char* atvb_last_error(void) { return atvb::g_last_error.c_str(); }
+
+int atvb_ctx_create(const atvb_device_opts* opts, atvb_ctx** out) {
+    return guard([&] {
+        need(out, "out");
+        int dev = opts ? opts->device : 0;
+        int count = 0;
+        atvb::cuda_check(cudaGetDeviceCount(&count), "cudaGetDeviceCount");
+        if (dev < 0 || dev >= count)
+            throw Error(ATVB_ERR_INVALID, "no CUDA device " + std::to_string(dev));
+        atvb::cuda_check(cudaSetDevice(dev), "cudaSetDevice");
+        auto* c = new atvb_ctx;
+        c->device = dev;
+        *out = c;
+    });
+}
+
+int atvb_ctx_destroy(atvb_ctx* ctx) {
+    return guard([&] { delete ctx; });
+}
+
+
+// ---- single system ------------------------------------------------------
+
+int atvb_system_create(atvb_ctx* ctx, const atvb_system_desc* desc,
+                       atvb_system** out) {
+    return guard([&] {
+        need(ctx, "ctx");
+        need(desc, "desc");
+        need(out, "out");
+        auto s = std::make_unique<atvb_system>();
+        s->ctx = ctx;
+        s->eng = std::make_unique<Engine>(ctx->device);
+        s->id = s->eng->add(*desc);
+        *out = s.release();
+    });
+}
+
+int atvb_system_destroy(atvb_system* sys) {
+    return guard([&] { delete sys; });
+}
+
+int atvb_system_upload(atvb_system* sys, const atvb_soa_view* frame) {
+    return guard([&] {
+        need(sys, "sys");
+        need(frame, "frame");
+        sys->eng->upload(sys->id, *frame);
+        sys->uploaded = true;
+    });
+}
+
+int atvb_system_compute_forces(atvb_system* sys) {
+    return guard([&] {
+        need(sys, "sys");
+        if (!sys->uploaded)
+            throw Error(ATVB_ERR_STATE, "compute_forces before upload");
+        sys->eng->compute_forces();
+    });
+}
+
+int atvb_system_step(atvb_system* sys, int32_t n_steps) {
+    return guard([&] {
+        need(sys, "sys");
+        if (!sys->uploaded)
+            throw Error(ATVB_ERR_STATE, "step before upload");
+        sys->eng->step(n_steps);
+    });
+}
+
+int atvb_system_download(atvb_system* sys, atvb_soa_view* frame,
+                         atvb_scalars* scalars) {
+    return guard([&] {
+        need(sys, "sys");
+        sys->eng->download(sys->id, frame, scalars);
+    });
+}
+
+int atvb_system_scalars(atvb_system* sys, atvb_scalars* scalars) {
+    return guard([&] {
+        need(sys, "sys");
+        need(scalars, "scalars");
+        sys->eng->scalars(sys->id, scalars);
+    });
+}
+
+int atvb_system_run(atvb_system* sys, atvb_soa_view* frame, int32_t n_steps,
+                    atvb_scalars* scalars) {
+    return guard([&] {
+        need(sys, "sys");
+        need(frame, "frame");
+        if (!sys->uploaded) {
+            sys->eng->upload(sys->id, *frame);
+            sys->uploaded = true;
+        }
+        sys->eng->step(n_steps);
+        sys->eng->download(sys->id, frame, scalars);
+    });
+}
+
+int atvb_system_energy_history(atvb_system* sys, double* out,
+                               int32_t max_steps, int32_t* count) {
+    return guard([&] {
+        need(sys, "sys");
+        need(out, "out");
+        int c = sys->eng->history(sys->id, out, max_steps);
+        if (count)
+            *count = c;
+    });
+}
+
+int atvb_system_pairs(atvb_system* sys, int32_t* pi, int32_t* pj,
+                      int64_t capacity, int64_t* count) {
+    return guard([&] {
+        need(sys, "sys");
+        int64_t c = sys->eng->pairs(sys->id, pi, pj, capacity);
+        if (count)
+            *count = c;
+    });
+}
+
+int atvb_system_profile(atvb_system* sys, int32_t enable) {
+    return guard([&] {
+        need(sys, "sys");
+        sys->eng->set_profiling(enable != 0);
+        if (enable)
+            sys->eng->clear_profile();
+    });
+}
+
+int atvb_system_profile_read(atvb_system* sys, atvb_kernel_time* out,
+                             int32_t capacity, int32_t* count) {
+    return guard([&] {
+        need(sys, "sys");
+        const auto& p = sys->eng->profile();
+        int c = 0;
+        for (const auto& e : p) {
+            if (c >= capacity)
+                break;
+            if (out) {
+                std::memset(&out[c], 0, sizeof(atvb_kernel_time));
+                std::strncpy(out[c].name, e.name.c_str(), sizeof(out[c].name) - 1);
+                out[c].total_ms = e.ms;
+                out[c].launches = e.launches;
+            }
+            ++c;
+        }
+        if (count)
+            *count = c;
+    });
+}
+
+int atvb_system_set_pair_lanes(atvb_system* sys, int32_t lanes) {
+    return guard([&] {
+        need(sys, "sys");
+        sys->eng->set_lanes(lanes);
+    });
+}
+
+int atvb_system_launch_count(atvb_system* sys, int64_t* launches) {
+    return guard([&] {
+        need(sys, "sys");
+        need(launches, "launches");
+        *launches = sys->eng->last_launches();
+    });
+}
+
+void* atvb_system_stream(atvb_system* sys) {
+    return sys ? (void*)sys->eng->stream() : nullptr;
+}
+
+// ---- batch --------------------------------------------------------------
+
+int atvb_batch_create(atvb_ctx* ctx, const atvb_system_desc* descs,
+                      int32_t n_systems, atvb_batch** out) {
+    return guard([&] {
+        need(ctx, "ctx");
+        need(descs, "descs");
+        need(out, "out");
+        if (n_systems < 1)
+            throw Error(ATVB_ERR_INVALID, "n_systems must be >= 1");
+        auto b = std::make_unique<atvb_batch>();
+        b->ctx = ctx;
+        b->eng = std::make_unique<Engine>(ctx->device);
+        for (int k = 0; k < n_systems; ++k)
+            b->ids.push_back(b->eng->add(descs[k]));
+        *out = b.release();
+    });
+}
+
+int atvb_batch_destroy(atvb_batch* b) {
+    return guard([&] { delete b; });
+}
+
+static int batch_id(atvb_batch* b, int32_t index) {
+    if (index < 0 || index >= (int)b->ids.size())
+        throw Error(ATVB_ERR_NOTFOUND, "batch index out of range");
+    return b->ids[index];
+}
+
+int atvb_batch_upload(atvb_batch* b, int32_t index, const atvb_soa_view* frame) {
+    return guard([&] {
+        need(b, "batch");
+        need(frame, "frame");
+        b->eng->upload(batch_id(b, index), *frame);
+    });
+}
+
+int atvb_batch_compute_forces(atvb_batch* b) {
+    return guard([&] {
+        need(b, "batch");
+        b->eng->compute_forces();
+    });
+}
+
+int atvb_batch_step(atvb_batch* b, int32_t n_steps) {
+    return guard([&] {
+        need(b, "batch");
+        b->eng->step(n_steps);
+    });
+}
+
+int atvb_batch_download(atvb_batch* b, int32_t index, atvb_soa_view* frame,
+                        atvb_scalars* scalars) {
+    return guard([&] {
+        need(b, "batch");
+        b->eng->download(batch_id(b, index), frame, scalars);
+    });
+}
+
+int atvb_batch_autotune(atvb_batch* b, int32_t* lanes) {
+    return guard([&] {
+        need(b, "batch");
+        const int g = b->eng->autotune();
+        if (lanes)
+            *lanes = g;
+    });
+}
+
+int atvb_batch_launch_count(atvb_batch* b, int64_t* launches) {
+    return guard([&] {
+        need(b, "batch");
+        need(launches, "launches");
+        *launches = b->eng->last_launches();
+    });
+}
+
+int atvb_request_bytes(const atvb_system_desc* desc, size_t* bytes) {
+    return guard([&] {
+        need(desc, "desc");
+        need(bytes, "bytes");
+        *bytes = atvb::estimate_bytes(*desc);
+    });
+}
+
+} // extern "C"

@@ -1,0 +1,1269 @@
+// engine.cu -- host side of the path: device allocation per system, the
+// system table and work lists, the per-step CUDA graph, and the C ABI.
+//
+// The reference drives one system per cuda::md::MD through Backend::step
+// (src/cuda/driver/driver.cu:123-157), which walks ten phases and launches
+// every component kernel from the host each step.  Here a step is one CUDA
+// graph launch: the phase order is fixed at capture time and the neighbour
+// rebuild decision is taken on the device (k_sys_a), so the loop has no
+// host synchronisation.  An Engine holds any number of systems; the
+// single-system API is an Engine with one slot, the batch API an Engine
+// with many, and the server an Engine whose slots come and go.
+#include <cufft.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "atvb.h"
+#include "atvb_common.cuh"
+#include "atvb_engine.h"
+#include "atvb_kernels.cuh"
+
+namespace atvb {
+
+thread_local std::string g_last_error;
+
+void cuda_check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess)
+        throw Error(ATVB_ERR_CUDA, std::string(what) + ": " +
+                                       cudaGetErrorString(e));
+}
+#define CK(x) cuda_check((x), #x)
+
+static void cufft_check(cufftResult r, const char* what) {
+    if (r != CUFFT_SUCCESS)
+        throw Error(ATVB_ERR_CUDA,
+                    std::string(what) + ": cuFFT error " + std::to_string(r));
+}
+#define CKF(x) cufft_check((x), #x)
+
+// ---------------------------------------------------------------- helpers
+
+static int round_up(long long v, int m) {
+    return (int)(((v + m - 1) / m) * m);
+}
+
+// pme_spline.h:99-111
+int good_fft_size(int n) {
+    if (n < 4)
+        n = 4;
+    for (;; ++n) {
+        int m = n;
+        for (int p : {2, 3, 5, 7})
+            while (m % p == 0)
+                m /= p;
+        if (m == 1)
+            return n;
+    }
+}
+
+// pme_spline.h:32-58 (host copy for the moduli)
+static void bspline_host(double frac, int n, double* th, double* dth) {
+    th[n - 1] = 0.0;
+    th[1] = frac;
+    th[0] = 1.0 - frac;
+    for (int k = 3; k < n; ++k) {
+        const double div = 1.0 / (k - 1);
+        th[k - 1] = div * frac * th[k - 2];
+        for (int j = 1; j < k - 1; ++j)
+            th[k - 1 - j] = div * ((frac + j) * th[k - 2 - j] +
+                                   (k - j - frac) * th[k - 1 - j]);
+        th[0] = div * (1.0 - frac) * th[0];
+    }
+    dth[0] = -th[0];
+    for (int j = 1; j < n; ++j)
+        dth[j] = th[j - 1] - th[j];
+    const double div = 1.0 / (n - 1);
+    th[n - 1] = div * frac * th[n - 2];
+    for (int j = 1; j < n - 1; ++j)
+        th[n - 1 - j] = div * ((frac + j) * th[n - 2 - j] +
+                               (n - j - frac) * th[n - 1 - j]);
+    th[0] = div * (1.0 - frac) * th[0];
+}
+
+// pme_spline.h:67-94
+static std::vector<double> spline_moduli(int K, int n) {
+    std::vector<double> data(n), dd(n), mod(K);
+    bspline_host(0.0, n, data.data(), dd.data());
+    for (int i = 0; i < K; ++i) {
+        double sr = 0, si = 0;
+        for (int k = 0; k < n - 1; ++k) {
+            const double arg = 2.0 * kPi * i * k / K;
+            sr += data[k] * std::cos(arg);
+            si += data[k] * std::sin(arg);
+        }
+        const double den = sr * sr + si * si;
+        mod[i] = den > 1e-12 ? 1.0 / den : 0.0;
+    }
+    for (int i = 0; i < K; ++i)
+        if (mod[i] == 0.0)
+            mod[i] = 0.5 * (mod[(i - 1 + K) % K] + mod[(i + 1) % K]);
+    return mod;
+}
+
+// erfcx(x) = exp(x^2) erfc(x) on [0, xmax]: Chebyshev interpolation on each
+// of `nint` equal intervals (long-double samples of the C library's erfc),
+// converted to monomials in the local variable u in [-1, 1].  Returns the
+// largest relative error of the polynomials against long double on a fine
+// grid.  erfcx is smooth and bounded (1 at x = 0, ~1/(x sqrt(pi)) for large
+// x), so a low degree per short interval reaches double precision.
+static double erfcx_fit(double xmax, int nint, int nc, std::vector<double>& out) {
+    typedef long double LD;
+    const LD pi = 3.141592653589793238462643383279502884L;
+    auto f = [](LD x) { return expl(x * x) * erfcl(x); };
+    out.assign((size_t)nint * nc, 0.0);
+    const LD h = (LD)xmax / nint;
+    std::vector<LD> fx(nc), c(nc), mono(nc), T0(nc), T1(nc), T2(nc);
+    for (int k = 0; k < nint; ++k) {
+        const LD mid = (k + 0.5L) * h, half = 0.5L * h;
+        for (int j = 0; j < nc; ++j)
+            fx[j] = f(mid + half * cosl(pi * (j + 0.5L) / nc));
+        for (int m = 0; m < nc; ++m) {
+            LD acc = 0;
+            for (int j = 0; j < nc; ++j)
+                acc += fx[j] * cosl(pi * m * (j + 0.5L) / nc);
+            c[m] = acc * 2.0L / nc;
+        }
+        c[0] *= 0.5L;
+        // sum_m c_m T_m(u) -> monomials
+        std::fill(mono.begin(), mono.end(), 0.0L);
+        std::fill(T0.begin(), T0.end(), 0.0L);
+        std::fill(T1.begin(), T1.end(), 0.0L);
+        T0[0] = 1.0L;
+        if (nc > 1)
+            T1[1] = 1.0L;
+        for (int m = 0; m < nc; ++m) {
+            const std::vector<LD>& T = m == 0 ? T0 : T1;
+            if (m >= 2) {
+                for (int d = 0; d < nc; ++d)
+                    T2[d] = -T0[d] + (d > 0 ? 2.0L * T1[d - 1] : 0.0L);
+                T0 = T1;
+                T1 = T2;
+            }
+            const std::vector<LD>& Tm = m == 0 ? T0 : T1;
+            (void)T;
+            for (int d = 0; d < nc; ++d)
+                mono[d] += c[m] * Tm[d];
+        }
+        for (int d = 0; d < nc; ++d)
+            out[(size_t)k * nc + d] = (double)mono[d];
+    }
+    double worst = 0.0;
+    for (int t = 0; t <= 20000; ++t) {
+        const LD x = (LD)xmax * t / 20000.0L;
+        int k = (int)(x / h);
+        if (k > nint - 1)
+            k = nint - 1;
+        const LD u = x * (2.0L / h) - (2 * k + 1);
+        LD p = 0;
+        for (int d = nc - 1; d >= 0; --d)
+            p = p * u + (LD)out[(size_t)k * nc + d];
+        const double rel = (double)fabsl(p / f(x) - 1.0L);
+        worst = std::max(worst, rel);
+    }
+    return worst;
+}
+
+// ------------------------------------------------------------ geometry
+
+Geometry make_geometry(const atvb_system_desc& d) {
+    Geometry g;
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c)
+            if (r != c && d.box[3 * r + c] != 0.0)
+                throw Error(ATVB_ERR_INVALID,
+                            "only orthorhombic boxes are supported "
+                            "(off-diagonal cell entries must be 0)");
+    for (int k = 0; k < 3; ++k) {
+        g.L[k] = d.box[4 * k];
+        if (!(g.L[k] > 0.0))
+            throw Error(ATVB_ERR_INVALID, "box edges must be positive");
+    }
+    if (d.n_atoms < 1)
+        throw Error(ATVB_ERR_INVALID, "n_atoms must be >= 1");
+    if (!(d.nl_cutoff > 0.0))
+        throw Error(ATVB_ERR_INVALID, "NeighborList: cutoff must be > 0");
+    // neighbor_list.cuh:98: skin < 0 means 0.3 * cutoff
+    g.skin = d.nl_skin < 0.0 ? 0.3 * d.nl_cutoff : d.nl_skin;
+    g.rlist = d.nl_cutoff + g.skin;
+    for (int k = 0; k < 3; ++k)
+        if (!(g.L[k] > 2.0 * g.rlist))
+            throw Error(ATVB_ERR_INVALID,
+                        "box edge must exceed 2*(cutoff+skin) so that each "
+                        "pair has one minimum image");
+    // cell_list.cpp:112-121 half-reach bins; :186-191 reach
+    for (int k = 0; k < 3; ++k) {
+        int c = (int)std::floor(g.L[k] / (0.5 * g.rlist));
+        g.nc[k] = c < 1 ? 1 : c;
+        g.cs[k] = g.L[k] / g.nc[k];
+        int r = (int)std::ceil(g.rlist / g.cs[k] - 1e-12);
+        g.reach[k] = r < 1 ? 1 : r;
+        g.alias[k] = g.nc[k] < 2 * g.reach[k] + 1;
+    }
+    // Stencil columns: every (dx, dy) whose prism can hold a pair, with the
+    // z reach that the LAMMPS bin-distance rule (cell_list.cpp:199-209)
+    // allows.  An aliased axis visits each of its cells exactly once.
+    const double rl2 = g.rlist * g.rlist;
+    auto axis_offsets = [&](int k) {
+        std::vector<int> o;
+        if (g.alias[k]) {
+            for (int v = 0; v < g.nc[k]; ++v)
+                o.push_back(v);
+        } else {
+            for (int v = -g.reach[k]; v <= g.reach[k]; ++v)
+                o.push_back(v);
+        }
+        return o;
+    };
+    auto gap = [&](int k, int v) -> double {
+        if (g.alias[k])
+            return 0.0;
+        const int a = v < 0 ? -v : v;
+        return a == 0 ? 0.0 : (a - 1) * g.cs[k];
+    };
+    for (int dx : axis_offsets(0))
+        for (int dy : axis_offsets(1)) {
+            const double gx = gap(0, dx), gy = gap(1, dy);
+            if (gx * gx + gy * gy > rl2)
+                continue;
+            int m;
+            if (g.alias[2]) {
+                m = -1;
+            } else {
+                m = 0;
+                for (int dz = 1; dz <= g.reach[2]; ++dz) {
+                    const double gz = gap(2, dz);
+                    if (gx * gx + gy * gy + gz * gz <= rl2)
+                        m = dz;
+                }
+            }
+            g.cols.push_back(make_int4(dx, dy, m, 0));
+        }
+    return g;
+}
+
+static int pme_K(const atvb_system_desc& d, const Geometry& g, int k) {
+    if (d.pme_grid[k] > 0)
+        return d.pme_grid[k];
+    if (!(d.pme_grid_spacing > 0.0))
+        throw Error(ATVB_ERR_INVALID, "KSpacePME: grid_spacing must be > 0");
+    // pme.cpp:69-76
+    int K = good_fft_size((int)std::ceil(g.L[k] / d.pme_grid_spacing));
+    if (K < d.pme_order + 1)
+        K = good_fft_size(d.pme_order + 1);
+    return K;
+}
+
+static int expected_row(const atvb_system_desc& d, const Geometry& g) {
+    const double vol = g.L[0] * g.L[1] * g.L[2];
+    const double rho = d.n_atoms / vol;
+    const double nb = rho * 4.0 / 3.0 * kPi * g.rlist * g.rlist * g.rlist;
+    int cap = round_up((long long)(1.5 * nb + 64.0), 32);
+    const int nmax = round_up(d.n_atoms, 32);
+    return std::min(cap, std::max(nmax, 32));
+}
+
+size_t estimate_bytes(const atvb_system_desc& d) {
+    Geometry g = make_geometry(d);
+    const size_t n = (size_t)d.n_atoms;
+    const int cap = expected_row(d, g);
+    size_t b = n * (14 * 8 + 8 + 32 + 32 + 6 * 4 + (size_t)cap * 4);
+    if (d.precision == ATVB_MIXED)
+        b += n * 16;
+    b += (size_t)(g.nc[0] * g.nc[1] * g.nc[2] + 1) * 8;
+    b += sizeof(SysState) + 3 * 8 * 4096;
+    if (d.pme_enabled) {
+        const size_t K0 = pme_K(d, g, 0), K1 = pme_K(d, g, 1),
+                     K2 = pme_K(d, g, 2);
+        const size_t nt = K0 * K1 * K2, nh = K0 * K1 * (K2 / 2 + 1);
+        const size_t rs = d.precision == ATVB_MIXED ? 4 : 8;
+        b += nt * 8 + nt * rs + nh * 2 * rs + nh * 8;
+        b += 2 * nh * 2 * rs; // cuFFT work areas (upper estimate)
+    }
+    return b;
+}
+
+// --------------------------------------------------------------- Slot
+
+void* Slot::dalloc(size_t b) {
+    void* p = nullptr;
+    if (b == 0)
+        b = 16;
+    cudaError_t e = cudaMalloc(&p, b);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw Error(ATVB_ERR_NOMEM, "cudaMalloc(" + std::to_string(b) +
+                                        " bytes) failed: " +
+                                        cudaGetErrorString(e));
+    }
+    allocs.push_back(p);
+    bytes += b;
+    return p;
+}
+
+Slot::~Slot() {
+    if (plan_f)
+        cufftDestroy(plan_f);
+    if (plan_i)
+        cufftDestroy(plan_i);
+    for (void* p : allocs)
+        cudaFree(p);
+    if (nbr_alloc)
+        cudaFree(nbr_alloc);
+}
+
+void Slot::alloc_list(int new_cap) {
+    if (nbr_alloc)
+        CK(cudaFree(nbr_alloc));
+    nbr_alloc = nullptr;
+    const size_t b = (size_t)hp.n * new_cap * sizeof(int);
+    cudaError_t e = cudaMalloc(&nbr_alloc, b);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw Error(ATVB_ERR_NOMEM, "neighbour list allocation failed");
+    }
+    hp.nbr = (int*)nbr_alloc;
+    hp.cap = new_cap;
+}
+
+Slot::Slot(const atvb_system_desc& d, cudaStream_t stream) : desc(d) {
+    geo = make_geometry(d);
+    std::memset(&hp, 0, sizeof(hp));
+    const int n = d.n_atoms;
+    hp.n = n;
+    hp.prec = d.precision == ATVB_MIXED ? kMixed : kFP64;
+    if (d.precision != ATVB_FP64 && d.precision != ATVB_MIXED)
+        throw Error(ATVB_ERR_INVALID, "unknown precision");
+    for (int k = 0; k < 3; ++k) {
+        hp.L[k] = geo.L[k];
+        hp.invL[k] = 1.0 / geo.L[k];
+        hp.halfL[k] = 0.5 * geo.L[k];
+        hp.Lf_fix[k] = (float)(geo.L[k] / 4294967296.0);
+        hp.fix_scale[k] = 4294967296.0 / geo.L[k];
+        hp.nc[k] = geo.nc[k];
+        hp.cs_inv[k] = 1.0 / geo.cs[k];
+        hp.alias[k] = geo.alias[k];
+    }
+    hp.ncell = geo.nc[0] * geo.nc[1] * geo.nc[2];
+    hp.rlist2 = geo.rlist * geo.rlist;
+    hp.skin_half2 = 0.25 * geo.skin * geo.skin;
+    hp.nl_every = d.nl_every < 1 ? 1 : d.nl_every;
+    hp.nl_delay = d.nl_delay < 0 ? 0 : d.nl_delay;
+    hp.nl_check = d.nl_check ? 1 : 0;
+    hp.ncol = (int)geo.cols.size();
+    // LJ (pair_lj_cut.cpp:30-41)
+    hp.has_lj = d.lj_enabled ? 1 : 0;
+    if (hp.has_lj) {
+        if (!(d.lj_cutoff > 0.0))
+            throw Error(ATVB_ERR_INVALID, "PairLJCut: cutoff must be positive");
+        if (d.lj_cutoff > geo.rlist)
+            throw Error(ATVB_ERR_INVALID,
+                        "PairLJCut cutoff exceeds the neighbour list reach");
+        const double s2 = d.lj_sigma * d.lj_sigma;
+        hp.lj_sig6 = s2 * s2 * s2;
+        hp.lj_rc2 = d.lj_cutoff * d.lj_cutoff;
+        hp.lj_eps4 = 4.0 * d.lj_epsilon;
+        hp.lj_eps24 = 24.0 * d.lj_epsilon;
+        const double r2inv = 1.0 / hp.lj_rc2;
+        const double r6inv = r2inv * r2inv * r2inv * hp.lj_sig6;
+        hp.lj_shift = 4.0 * d.lj_epsilon * (r6inv * r6inv - r6inv);
+    }
+    hp.has_coul = d.coul_enabled ? 1 : 0;
+    if (hp.has_coul) {
+        if (!(d.coul_alpha > 0.0) || !(d.coul_cutoff > 0.0))
+            throw Error(ATVB_ERR_INVALID,
+                        "CoulLong: alpha and cutoff must be positive");
+        if (d.coul_cutoff > geo.rlist)
+            throw Error(ATVB_ERR_INVALID,
+                        "CoulLong cutoff exceeds the neighbour list reach");
+        hp.coul_rc2 = d.coul_cutoff * d.coul_cutoff;
+        hp.coul_alpha = d.coul_alpha;
+        hp.coul_alpha2 = d.coul_alpha * d.coul_alpha;
+        // a hair past alpha*rc so that r^2 < rc^2 never leaves the table
+        const double xmax = d.coul_alpha * d.coul_cutoff * (1.0 + 1e-6);
+        const int nint = std::min(kErfcxMaxInt,
+                                  std::max(16, (int)std::ceil(8.0 * xmax)));
+        hp.erfcx_nint = nint;
+        hp.erfcx_inv_h = nint / xmax;
+        std::vector<double> cd, cf64;
+        const double ed = erfcx_fit(xmax, nint, kErfcxNd, cd);
+        const double ef = erfcx_fit(xmax, nint, kErfcxNf, cf64);
+        if (ed > 1e-15 || ef > 1e-10)
+            throw Error(ATVB_ERR_INVALID,
+                        "erfcx fit failed (alpha*cutoff too large?)");
+        erfcx_err = ed;
+        std::vector<float> cf(cf64.begin(), cf64.end());
+        double* dd_ = (double*)dalloc(cd.size() * sizeof(double));
+        float* df_ = (float*)dalloc(cf.size() * sizeof(float));
+        CK(cudaMemcpyAsync(dd_, cd.data(), cd.size() * sizeof(double),
+                           cudaMemcpyHostToDevice, stream));
+        CK(cudaMemcpyAsync(df_, cf.data(), cf.size() * sizeof(float),
+                           cudaMemcpyHostToDevice, stream));
+        CK(cudaStreamSynchronize(stream));
+        hp.erfcx_d = dd_;
+        hp.erfcx_f = df_;
+    }
+    // integrator / thermostat
+    if (!(d.dt > 0.0))
+        throw Error(ATVB_ERR_INVALID, "VelocityVerlet: dt must be > 0");
+    hp.dt = d.dt;
+    hp.dtf = 0.5 * d.dt * kFtm2v;
+    hp.thermostat = d.thermostat;
+    hp.T = d.temperature;
+    const int ndof = std::max(0, 3 * n - 3);
+    hp.n_dof_kT = (double)ndof * kKB * d.temperature;
+    if (d.thermostat == ATVB_NOSE_HOOVER) {
+        if (!(d.tau > 0.0) || !(d.temperature > 0.0))
+            throw Error(ATVB_ERR_INVALID,
+                        "NoseHoover: temperature and tau must be > 0");
+        hp.tau = d.tau;
+        hp.Q = (double)ndof * kKB * d.temperature * d.tau * d.tau;
+    } else if (d.thermostat == ATVB_LANGEVIN) {
+        if (!(d.damp > 0.0) || d.temperature < 0.0)
+            throw Error(ATVB_ERR_INVALID, "FixLangevin: damp must be > 0");
+        hp.lang_g1 = 1.0 / (d.damp * kFtm2v);
+        hp.lang_g2pre =
+            std::sqrt(2.0 * kKB * d.temperature / (d.damp * d.dt * kMvv2e)) /
+            kFtm2v;
+        hp.seed = d.seed;
+    } else if (d.thermostat != ATVB_NVE) {
+        throw Error(ATVB_ERR_INVALID, "unknown thermostat");
+    }
+    hp.need_virial = d.stress_required ? 1 : 0;
+    // device memory
+    auto dd = [&](size_t cnt) { return (double*)dalloc(cnt * sizeof(double)); };
+    hp.x = dd(n);
+    hp.y = dd(n);
+    hp.z = dd(n);
+    hp.vx = dd(n);
+    hp.vy = dd(n);
+    hp.vz = dd(n);
+    hp.mass = dd(n);
+    hp.q = dd(n);
+    hp.xr = dd(n);
+    hp.yr = dd(n);
+    hp.zr = dd(n);
+    hp.sx = dd(n);
+    hp.sy = dd(n);
+    hp.sz = dd(n);
+    hp.tag = (long long*)dalloc((size_t)n * 8);
+    hp.posd4 = (double4*)dalloc((size_t)n * sizeof(double4));
+    hp.pos4 = hp.prec == kMixed ? dalloc((size_t)n * sizeof(int4))
+                                : (void*)hp.posd4;
+    hp.f4 = (double4*)dalloc((size_t)n * sizeof(double4));
+    auto di = [&](size_t cnt) { return (int*)dalloc(cnt * sizeof(int)); };
+    hp.perm = di(n);
+    hp.rank = di(n);
+    hp.cell_of = di(n);
+    hp.slot = di(n);
+    hp.cellS = di(n);
+    hp.nnbr = di(n);
+    hp.cell_count = di(hp.ncell);
+    hp.cell_start = di(hp.ncell + 1);
+    CK(cudaMemsetAsync(hp.cell_count, 0, sizeof(int) * hp.ncell, stream));
+    hp.cols = (int4*)dalloc(sizeof(int4) * geo.cols.size());
+    CK(cudaMemcpyAsync(hp.cols, geo.cols.data(), sizeof(int4) * geo.cols.size(),
+                       cudaMemcpyHostToDevice, stream));
+    hp.st = (SysState*)dalloc(sizeof(SysState));
+    hp.ehist_cap = d.history_capacity > 0 ? d.history_capacity : 4096;
+    hp.ehist = dd(3 * (size_t)hp.ehist_cap);
+    alloc_list(expected_row(d, geo));
+    // PME
+    hp.has_pme = d.pme_enabled ? 1 : 0;
+    if (hp.has_pme) {
+        if (!(d.pme_alpha > 0.0))
+            throw Error(ATVB_ERR_INVALID, "KSpacePME: alpha must be > 0");
+        if (d.pme_order < 3 || d.pme_order > 8)
+            throw Error(ATVB_ERR_INVALID, "KSpacePME: order must be in [3, 8]");
+        hp.order = d.pme_order;
+        for (int k = 0; k < 3; ++k)
+            hp.K[k] = pme_K(d, geo, k);
+        hp.Kh = hp.K[2] / 2 + 1;
+        const double vol = geo.L[0] * geo.L[1] * geo.L[2];
+        hp.pme_fscale = kQqr2e / (kPi * vol);
+        hp.pme_escale = kQqr2e / (2.0 * kPi * vol);
+        hp.pme_alpha2_pi2 = kPi * kPi / (d.pme_alpha * d.pme_alpha);
+        hp.grid_scale = hp.prec == kMixed ? 4294967296.0 : 1099511627776.0;
+        hp.grid_scale_inv = 1.0 / hp.grid_scale;
+        const size_t K0 = hp.K[0], K1 = hp.K[1], K2 = hp.K[2], Kh = hp.Kh;
+        const size_t nt = K0 * K1 * K2, nh = K0 * K1 * Kh;
+        const size_t rs = hp.prec == kMixed ? 4 : 8;
+        hp.grid_fix = (unsigned long long*)dalloc(nt * 8);
+        CK(cudaMemsetAsync(hp.grid_fix, 0, nt * 8, stream));
+        hp.grid_real = dalloc(nt * rs);
+        hp.grid_cplx = dalloc(nh * 2 * rs);
+        hp.infl = dd(nh);
+        // pme_influence.h:112-155 on the half grid (orthorhombic)
+        std::vector<double> m0 = spline_moduli(hp.K[0], hp.order);
+        std::vector<double> m1 = spline_moduli(hp.K[1], hp.order);
+        std::vector<double> m2 = spline_moduli(hp.K[2], hp.order);
+        infl_host.assign(nh, 0.0);
+        for (size_t a = 0; a < K0; ++a) {
+            const int h0 = a <= K0 / 2 ? (int)a : (int)a - (int)K0;
+            for (size_t b = 0; b < K1; ++b) {
+                const int h1 = b <= K1 / 2 ? (int)b : (int)b - (int)K1;
+                const double bm01 = m0[a] * m1[b];
+                for (size_t c = 0; c < Kh; ++c) {
+                    if (a == 0 && b == 0 && c == 0)
+                        continue;
+                    const int h2 = c <= K2 / 2 ? (int)c : (int)c - (int)K2;
+                    const double mx = h0 * hp.invL[0], my = h1 * hp.invL[1],
+                                 mz = h2 * hp.invL[2];
+                    const double msq = mx * mx + my * my + mz * mz;
+                    infl_host[(a * K1 + b) * Kh + c] =
+                        std::exp(-hp.pme_alpha2_pi2 * msq) / msq * bm01 *
+                        m2[c];
+                }
+            }
+        }
+        CK(cudaMemcpyAsync(hp.infl, infl_host.data(), nh * 8,
+                           cudaMemcpyHostToDevice, stream));
+        const bool mixed = hp.prec == kMixed;
+        CKF(cufftPlan3d(&plan_f, hp.K[0], hp.K[1], hp.K[2],
+                        mixed ? CUFFT_R2C : CUFFT_D2Z));
+        CKF(cufftPlan3d(&plan_i, hp.K[0], hp.K[1], hp.K[2],
+                        mixed ? CUFFT_C2R : CUFFT_Z2D));
+        CKF(cufftSetStream(plan_f, stream));
+        CKF(cufftSetStream(plan_i, stream));
+        size_t ws = 0;
+        if (cufftGetSize(plan_f, &ws) == CUFFT_SUCCESS)
+            bytes += ws;
+        if (cufftGetSize(plan_i, &ws) == CUFFT_SUCCESS)
+            bytes += ws;
+    }
+    CK(cudaStreamSynchronize(stream));
+}
+
+// ------------------------------------------------------------- Engine
+
+Engine::Engine(int device) : device_(device) {
+    CK(cudaSetDevice(device));
+    CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    CK(cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount,
+                              device));
+}
+
+Engine::~Engine() {
+    cudaSetDevice(device_);
+    release_graph();
+    slots_.clear();
+    for (void* p : list_allocs_)
+        cudaFree(p);
+    if (d_sp_)
+        cudaFree(d_sp_);
+    for (auto& e : prof_events_)
+        cudaEventDestroy(e);
+    if (stream_)
+        cudaStreamDestroy(stream_);
+}
+
+void Engine::release_graph() {
+    if (gexec_)
+        cudaGraphExecDestroy(gexec_);
+    if (graph_)
+        cudaGraphDestroy(graph_);
+    gexec_ = nullptr;
+    graph_ = nullptr;
+}
+
+int Engine::add(const atvb_system_desc& d) {
+    CK(cudaSetDevice(device_));
+    auto s = std::make_unique<Slot>(d, stream_);
+    int id = -1;
+    for (size_t k = 0; k < slots_.size(); ++k)
+        if (!slots_[k]) {
+            id = (int)k;
+            break;
+        }
+    if (id < 0) {
+        id = (int)slots_.size();
+        slots_.emplace_back();
+    }
+    s->index = id;
+    slots_[id] = std::move(s);
+    ensure_table();
+    push_params(id);
+    dirty_ = true;
+    return id;
+}
+
+void Engine::remove(int id) {
+    Slot* s = slot(id);
+    (void)s;
+    CK(cudaStreamSynchronize(stream_));
+    slots_[id].reset();
+    dirty_ = true;
+}
+
+Slot* Engine::slot(int id) {
+    if (id < 0 || id >= (int)slots_.size() || !slots_[id])
+        throw Error(ATVB_ERR_NOTFOUND, "no system with id " + std::to_string(id));
+    return slots_[id].get();
+}
+
+void Engine::ensure_table() {
+    if ((int)slots_.size() <= sp_cap_)
+        return;
+    int cap = std::max(8, sp_cap_ * 2);
+    while (cap < (int)slots_.size())
+        cap *= 2;
+    SysParams* nd = nullptr;
+    CK(cudaMalloc(&nd, sizeof(SysParams) * cap));
+    if (d_sp_) {
+        CK(cudaMemcpyAsync(nd, d_sp_, sizeof(SysParams) * sp_cap_,
+                           cudaMemcpyDeviceToDevice, stream_));
+        CK(cudaStreamSynchronize(stream_));
+        CK(cudaFree(d_sp_));
+    }
+    d_sp_ = nd;
+    sp_cap_ = cap;
+    dirty_ = true;
+}
+
+void Engine::push_params(int id) {
+    Slot* s = slot(id);
+    CK(cudaMemcpyAsync(d_sp_ + id, &s->hp, sizeof(SysParams),
+                       cudaMemcpyHostToDevice, stream_));
+}
+
+static ItemList make_list(std::vector<void*>& allocs, const std::vector<Item>& v,
+                          int max_grid, cudaStream_t stream) {
+    ItemList il;
+    il.n = (int)v.size();
+    if (v.empty())
+        return il;
+    void* p = nullptr;
+    CK(cudaMalloc(&p, sizeof(Item) * v.size()));
+    allocs.push_back(p);
+    CK(cudaMemcpyAsync(p, v.data(), sizeof(Item) * v.size(),
+                       cudaMemcpyHostToDevice, stream));
+    il.d = (const Item*)p;
+    il.grid = std::min(il.n, max_grid);
+    return il;
+}
+
+int Engine::choose_lanes() const {
+    if (lanes_fixed_ > 0)
+        return lanes_fixed_;
+    long long n_tot = 0;
+    double row = 0.0;
+    int cnt = 0;
+    for (const auto& s : slots_)
+        if (s && s->uploaded) {
+            n_tot += s->hp.n;
+            row += s->mean_row;
+            ++cnt;
+        }
+    if (cnt == 0)
+        return 4;
+    row /= cnt;
+    const long long target = (long long)num_sms_ * 2048 * 2;
+    int G = 1;
+    while (G < 32 && n_tot * G < target)
+        G *= 2;
+    int gmax = 1;
+    while (gmax < 32 && gmax * 8 <= row)
+        gmax *= 2;
+    return std::max(1, std::min(G, gmax));
+}
+
+void Engine::build_lists() {
+    CK(cudaStreamSynchronize(stream_));
+    for (void* p : list_allocs_)
+        cudaFree(p);
+    list_allocs_.clear();
+    std::vector<Item> atoms, list, pair, cells, patoms, pgrid, preal;
+    std::vector<int> sys;
+    lc_ = LaunchCfg{};
+    lc_.pair_G = choose_lanes();
+    const int pchunk = kChunk / lc_.pair_G;
+    pme_slots_.clear();
+    int pme_prec = -1, pme_order = -1;
+    for (const auto& sp : slots_) {
+        if (!sp || !sp->uploaded)
+            continue;
+        const SysParams& P = sp->hp;
+        const int k = sp->index;
+        sys.push_back(k);
+        for (int b = 0; b < P.n; b += kChunk)
+            atoms.push_back({k, b});
+        for (int b = 0; b < P.n; b += kListChunk)
+            list.push_back({k, b});
+        for (int b = 0; b < P.n; b += pchunk)
+            pair.push_back({k, b});
+        for (int b = 0; b < P.ncell; b += kChunk)
+            cells.push_back({k, b});
+        if (P.prec == kMixed)
+            lc_.any_mixed = 1;
+        else
+            lc_.any_fp64 = 1;
+        if (P.has_pme) {
+            if (pme_prec >= 0 && (pme_prec != P.prec || pme_order != P.order))
+                throw Error(ATVB_ERR_INVALID,
+                            "all PME systems of one engine must share "
+                            "precision and spline order");
+            pme_prec = P.prec;
+            pme_order = P.order;
+            pme_slots_.push_back(k);
+            for (int b = 0; b < P.n; b += kChunk)
+                patoms.push_back({k, b});
+            const long long nh = (long long)P.K[0] * P.K[1] * P.Kh;
+            const long long nt = (long long)P.K[0] * P.K[1] * P.K[2];
+            for (long long b = 0; b < nh; b += kGridChunk)
+                pgrid.push_back({k, (int)b});
+            for (long long b = 0; b < nt; b += kGridChunk)
+                preal.push_back({k, (int)b});
+        }
+    }
+    const int g_light = num_sms_ * 16;
+    lc_.sp = d_sp_;
+    lc_.atoms = make_list(list_allocs_, atoms, g_light, stream_);
+    lc_.list = make_list(list_allocs_, list, num_sms_ * 32, stream_);
+    lc_.pair = make_list(list_allocs_, pair, num_sms_ * 16, stream_);
+    lc_.cells = make_list(list_allocs_, cells, g_light, stream_);
+    lc_.pme_atoms = make_list(list_allocs_, patoms, g_light, stream_);
+    lc_.pme_grid = make_list(list_allocs_, pgrid, g_light, stream_);
+    lc_.pme_real = make_list(list_allocs_, preal, g_light, stream_);
+    lc_.nsys = (int)sys.size();
+    if (!sys.empty()) {
+        void* p = nullptr;
+        CK(cudaMalloc(&p, sizeof(int) * sys.size()));
+        list_allocs_.push_back(p);
+        CK(cudaMemcpyAsync(p, sys.data(), sizeof(int) * sys.size(),
+                           cudaMemcpyHostToDevice, stream_));
+        lc_.sys_list = (const int*)p;
+    }
+    lc_.pme_mixed = pme_prec == kMixed ? 1 : 0;
+    lc_.pme_order = pme_order > 0 ? pme_order : 4;
+    CK(cudaStreamSynchronize(stream_));
+    release_graph();
+    dirty_ = false;
+    ++list_epoch_;
+    single_.clear();
+}
+
+// Kernel launches of one step (cuFFT's own kernels not counted).
+int64_t Engine::kernels_per_step() const {
+    int64_t k = 0;
+    k += 2;                                   // integrate_a, sys_a
+    k += 6;                                   // rebuild pipeline
+    k += (lc_.any_fp64 ? 1 : 0) + (lc_.any_mixed ? 1 : 0); // pair
+    if (!pme_slots_.empty())
+        k += 4;                               // spread, convert, influence, gather
+    k += 2;                                   // integrate_b, sys_b
+    return k;
+}
+
+void Engine::enqueue_forces(const LaunchCfg& lc, const std::vector<int>& pme,
+                            bool profile) {
+    prof_mark(profile, "pair");
+    launch_pair(lc, stream_);
+    if (!pme.empty()) {
+        prof_mark(profile, "pme_spread");
+        launch_pme_spread(lc, stream_);
+        prof_mark(profile, "pme_convert");
+        launch_pme_convert(lc, stream_);
+        prof_mark(profile, "pme_fft_fwd");
+        for (int k : pme) {
+            Slot* s = slots_[k].get();
+            if (s->hp.prec == kMixed)
+                CKF(cufftExecR2C(s->plan_f, (cufftReal*)s->hp.grid_real,
+                                 (cufftComplex*)s->hp.grid_cplx));
+            else
+                CKF(cufftExecD2Z(s->plan_f, (cufftDoubleReal*)s->hp.grid_real,
+                                 (cufftDoubleComplex*)s->hp.grid_cplx));
+        }
+        prof_mark(profile, "pme_influence");
+        launch_pme_influence(lc, stream_);
+        prof_mark(profile, "pme_fft_inv");
+        for (int k : pme) {
+            Slot* s = slots_[k].get();
+            if (s->hp.prec == kMixed)
+                CKF(cufftExecC2R(s->plan_i, (cufftComplex*)s->hp.grid_cplx,
+                                 (cufftReal*)s->hp.grid_real));
+            else
+                CKF(cufftExecZ2D(s->plan_i,
+                                 (cufftDoubleComplex*)s->hp.grid_cplx,
+                                 (cufftDoubleReal*)s->hp.grid_real));
+        }
+        prof_mark(profile, "pme_gather");
+        launch_pme_gather(lc, stream_);
+    }
+}
+
+void Engine::enqueue_step(bool profile) {
+    prof_mark(profile, "integrate_a");
+    launch_integrate_a(lc_, stream_);
+    launch_sys_a(lc_, stream_);
+    prof_mark(profile, "neighbor");
+    launch_rebuild(lc_, stream_);
+    enqueue_forces(lc_, pme_slots_, profile);
+    prof_mark(profile, "integrate_b");
+    launch_integrate_b(lc_, stream_);
+    launch_sys_b(lc_, stream_);
+    prof_mark(profile, nullptr);
+}
+
+void Engine::prof_mark(bool profile, const char* next) {
+    if (!profile)
+        return;
+    cudaEvent_t e;
+    if (prof_used_ < prof_events_.size()) {
+        e = prof_events_[prof_used_];
+    } else {
+        CK(cudaEventCreate(&e));
+        prof_events_.push_back(e);
+    }
+    prof_used_++;
+    CK(cudaEventRecord(e, stream_));
+    prof_seq_.push_back(next ? next : "");
+}
+
+void Engine::ensure_ready() {
+    if (dirty_)
+        build_lists();
+    if (lc_.nsys == 0)
+        throw Error(ATVB_ERR_STATE, "no uploaded system to advance");
+}
+
+void Engine::step(int n) {
+    CK(cudaSetDevice(device_));
+    if (n < 0)
+        throw Error(ATVB_ERR_INVALID, "n_steps must be >= 0");
+    ensure_ready();
+    if (profiling_) {
+        for (int k = 0; k < n; ++k) {
+            enqueue_step(true);
+            CK(cudaGetLastError());
+        }
+        collect_profile();
+    } else {
+        if (!gexec_) {
+            CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+            try {
+                enqueue_step(false);
+            } catch (...) {
+                cudaGraph_t g = nullptr;
+                cudaStreamEndCapture(stream_, &g);
+                if (g)
+                    cudaGraphDestroy(g);
+                throw;
+            }
+            CK(cudaStreamEndCapture(stream_, &graph_));
+            CK(cudaGraphInstantiate(&gexec_, graph_, 0));
+        }
+        for (int k = 0; k < n; ++k)
+            CK(cudaGraphLaunch(gexec_, stream_));
+    }
+    last_launches_ = kernels_per_step() * n;
+    steps_since_check_ += n;
+}
+
+void Engine::collect_profile() {
+    CK(cudaStreamSynchronize(stream_));
+    for (size_t k = 0; k + 1 < prof_used_; ++k) {
+        const std::string& name = prof_seq_[k];
+        if (name.empty())
+            continue;
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, prof_events_[k], prof_events_[k + 1]));
+        auto it = std::find_if(prof_acc_.begin(), prof_acc_.end(),
+                               [&](const ProfEntry& p) { return p.name == name; });
+        if (it == prof_acc_.end()) {
+            prof_acc_.push_back({name, 0.0, 0});
+            it = prof_acc_.end() - 1;
+        }
+        it->ms += ms;
+        it->launches += 1;
+    }
+    prof_used_ = 0;
+    prof_seq_.clear();
+}
+
+void Engine::compute_forces() {
+    CK(cudaSetDevice(device_));
+    ensure_ready();
+    sized_rebuild(lc_);
+    enqueue_forces(lc_, pme_slots_, false);
+    launch_sys_energy(lc_, stream_);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(stream_));
+}
+
+// Force pass of one system only (a request joining a running batch): the
+// other systems' forces, which may carry this step's Langevin kicks, stay.
+void Engine::compute_forces_one(int id) {
+    CK(cudaSetDevice(device_));
+    ensure_ready();
+    const LaunchCfg one = restricted_cfg(id);
+    sized_rebuild(one);
+    std::vector<int> pme;
+    if (slot(id)->hp.has_pme)
+        pme.push_back(id);
+    enqueue_forces(one, pme, false);
+    launch_sys_energy(one, stream_);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(stream_));
+}
+
+// Forced neighbour build of the systems in `lc`, repeated with larger rows
+// until no row overflows.  Outside the step loop only (upload, force pass).
+void Engine::sized_rebuild(const LaunchCfg& lc) {
+    for (int attempt = 0; attempt < 4; ++attempt) {
+        launch_force_rebuild(lc, stream_);
+        launch_rebuild(lc, stream_);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(stream_));
+        if (!check_lists(lc))
+            return;
+    }
+    throw Error(ATVB_ERR_OVERFLOW, "neighbour rows kept overflowing");
+}
+
+// Read each system's largest row of the last build; grow the row capacity
+// of any system that overflowed.  Returns true if a rebuild is needed.
+bool Engine::check_lists(const LaunchCfg& lc) {
+    std::vector<int> ids(lc.nsys);
+    CK(cudaMemcpy(ids.data(), lc.sys_list, sizeof(int) * lc.nsys,
+                  cudaMemcpyDeviceToHost));
+    bool regrow = false;
+    for (int id : ids) {
+        Slot* sp = slot(id);
+        SysState st;
+        CK(cudaMemcpy(&st, sp->hp.st, sizeof(st), cudaMemcpyDeviceToHost));
+        if (st.overflow || st.max_nnbr > sp->hp.cap) {
+            const int cap = round_up((long long)(st.max_nnbr * 1.25) + 32, 32);
+            sp->alloc_list(cap);
+            int zero = 0;
+            CK(cudaMemcpy(&sp->hp.st->overflow, &zero, sizeof(int),
+                          cudaMemcpyHostToDevice));
+            push_params(sp->index);
+            regrow = true;
+        }
+        sp->max_row = st.max_nnbr;
+    }
+    if (regrow) {
+        CK(cudaStreamSynchronize(stream_));
+        release_graph();
+    }
+    return regrow;
+}
+
+// Work lists restricted to one system (upload / download staging).
+LaunchCfg Engine::restricted_cfg(int id) {
+    auto it = single_.find(id);
+    if (it != single_.end() && it->second.first == list_epoch_)
+        return it->second.second;
+    Slot* s = slot(id);
+    const SysParams& P = s->hp;
+    std::vector<Item> atoms, list, cells, pair, patoms, pgrid, preal;
+    for (int b = 0; b < P.n; b += kChunk)
+        atoms.push_back({id, b});
+    for (int b = 0; b < P.n; b += kListChunk)
+        list.push_back({id, b});
+    for (int b = 0; b < P.ncell; b += kChunk)
+        cells.push_back({id, b});
+    const int pchunk = kChunk / lc_.pair_G;
+    for (int b = 0; b < P.n; b += pchunk)
+        pair.push_back({id, b});
+    if (P.has_pme) {
+        for (int b = 0; b < P.n; b += kChunk)
+            patoms.push_back({id, b});
+        const long long nh = (long long)P.K[0] * P.K[1] * P.Kh;
+        const long long nt = (long long)P.K[0] * P.K[1] * P.K[2];
+        for (long long b = 0; b < nh; b += kGridChunk)
+            pgrid.push_back({id, (int)b});
+        for (long long b = 0; b < nt; b += kGridChunk)
+            preal.push_back({id, (int)b});
+    }
+    LaunchCfg c = lc_;
+    c.sp = d_sp_;
+    c.atoms = make_list(list_allocs_, atoms, num_sms_ * 16, stream_);
+    c.list = make_list(list_allocs_, list, num_sms_ * 32, stream_);
+    c.cells = make_list(list_allocs_, cells, num_sms_ * 16, stream_);
+    c.pair = make_list(list_allocs_, pair, num_sms_ * 16, stream_);
+    c.pme_atoms = make_list(list_allocs_, patoms, num_sms_ * 16, stream_);
+    c.pme_grid = make_list(list_allocs_, pgrid, num_sms_ * 16, stream_);
+    c.pme_real = make_list(list_allocs_, preal, num_sms_ * 16, stream_);
+    c.any_mixed = P.prec == kMixed;
+    c.any_fp64 = P.prec != kMixed;
+    if (P.has_pme) {
+        c.pme_mixed = P.prec == kMixed;
+        c.pme_order = P.order;
+    }
+    void* p = nullptr;
+    CK(cudaMalloc(&p, sizeof(int)));
+    list_allocs_.push_back(p);
+    CK(cudaMemcpyAsync(p, &id, sizeof(int), cudaMemcpyHostToDevice, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    c.sys_list = (const int*)p;
+    c.nsys = 1;
+    single_[id] = {list_epoch_, c};
+    return c;
+}
+
+void Engine::upload(int id, const atvb_soa_view& f) {
+    CK(cudaSetDevice(device_));
+    Slot* s = slot(id);
+    const int n = s->hp.n;
+    const size_t b = sizeof(double) * n;
+    std::vector<double> tmp;
+    auto put = [&](double* dst, const double* src, double fill) {
+        if (src) {
+            CK(cudaMemcpyAsync(dst, src, b, cudaMemcpyHostToDevice, stream_));
+        } else {
+            tmp.assign(n, fill);
+            CK(cudaMemcpyAsync(dst, tmp.data(), b, cudaMemcpyHostToDevice,
+                               stream_));
+            CK(cudaStreamSynchronize(stream_));
+        }
+    };
+    if (!f.x || !f.y || !f.z)
+        throw Error(ATVB_ERR_INVALID, "upload needs positions");
+    put(s->hp.x, f.x, 0.0);
+    put(s->hp.y, f.y, 0.0);
+    put(s->hp.z, f.z, 0.0);
+    put(s->hp.vx, f.vx, 0.0);
+    put(s->hp.vy, f.vy, 0.0);
+    put(s->hp.vz, f.vz, 0.0);
+    put(s->hp.mass, f.mass, 1.0);
+    put(s->hp.q, f.charge, 0.0);
+    put(s->hp.sx, f.fx, 0.0);
+    put(s->hp.sy, f.fy, 0.0);
+    put(s->hp.sz, f.fz, 0.0);
+    if (f.mass)
+        for (int i = 0; i < n; ++i)
+            if (!(f.mass[i] > 0.0))
+                throw Error(ATVB_ERR_INVALID, "masses must be positive");
+    std::vector<long long> tag(n);
+    for (int i = 0; i < n; ++i)
+        tag[i] = f.tag ? f.tag[i] : (long long)(i + 1);
+    CK(cudaMemcpyAsync(s->hp.tag, tag.data(), 8 * n, cudaMemcpyHostToDevice,
+                       stream_));
+    // charges: PME self + net-charge constants (pme.cpp:224-252)
+    double qs = 0, q2 = 0;
+    if (f.charge)
+        for (int i = 0; i < n; ++i) {
+            qs += f.charge[i];
+            q2 += f.charge[i] * f.charge[i];
+        }
+    if (s->hp.has_pme) {
+        const double vol = s->hp.L[0] * s->hp.L[1] * s->hp.L[2];
+        const double a = s->desc.pme_alpha;
+        s->hp.e_const = -kQqr2e * a / std::sqrt(kPi) * q2 -
+                        kQqr2e * kPi / (2.0 * vol * a * a) * qs * qs;
+    }
+    SysState st0;
+    std::memset(&st0, 0, sizeof(st0));
+    st0.vscale = 1.0;
+    st0.s_a = 1.0;
+    CK(cudaMemcpyAsync(s->hp.st, &st0, sizeof(st0), cudaMemcpyHostToDevice,
+                       stream_));
+    push_params(id);
+    CK(cudaStreamSynchronize(stream_));
+    s->uploaded = true;
+    dirty_ = true;
+    build_lists();
+    // wrap, first neighbour build, uploaded forces into sorted order, KE --
+    // touching only this system
+    const LaunchCfg one = restricted_cfg(id);
+    launch_wrap_in(one, stream_);
+    sized_rebuild(one);
+    launch_state_in(one, stream_);
+    launch_kinetic(one, stream_);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(stream_));
+    // the forced build counts as the setup build, not a step rebuild
+    long long zero = 0;
+    CK(cudaMemcpy(&s->hp.st->rebuilds, &zero, sizeof(zero),
+                  cudaMemcpyHostToDevice));
+    SysState st;
+    CK(cudaMemcpy(&st, s->hp.st, sizeof(st), cudaMemcpyDeviceToHost));
+    s->mean_row = st.max_nnbr;
+    dirty_ = true; // lane choice may change with the measured row length
+}
+
+void Engine::scalars(int id, atvb_scalars* out) {
+    CK(cudaSetDevice(device_));
+    Slot* s = slot(id);
+    SysState st;
+    CK(cudaStreamSynchronize(stream_));
+    CK(cudaMemcpy(&st, s->hp.st, sizeof(st), cudaMemcpyDeviceToHost));
+    std::memset(out, 0, sizeof(*out));
+    out->energy = st.energy;
+    out->energy_pair = st.energy;
+    out->energy_lj = st.e_lj;
+    out->energy_coul = st.e_coul;
+    out->energy_recip = st.e_recip;
+    out->energy_const = st.e_const;
+    out->kinetic = st.kinetic;
+    out->conserved = st.conserved;
+    for (int k = 0; k < 6; ++k)
+        out->stress[k] = st.virial[k];
+    out->nh_xi = st.xi;
+    out->step = st.step;
+    out->rebuilds = st.rebuilds;
+    out->max_neighbors = st.max_nnbr;
+    out->status = st.overflow ? ATVB_ERR_OVERFLOW : 0;
+}
+
+void Engine::download(int id, atvb_soa_view* f, atvb_scalars* sc) {
+    CK(cudaSetDevice(device_));
+    Slot* s = slot(id);
+    if (!s->uploaded)
+        throw Error(ATVB_ERR_STATE, "download before upload");
+    const int n = s->hp.n;
+    const size_t b = sizeof(double) * n;
+    ensure_ready();
+    const LaunchCfg one = restricted_cfg(id);
+    if (f) {
+        if (f->x)
+            CK(cudaMemcpyAsync(f->x, s->hp.x, b, cudaMemcpyDeviceToHost, stream_));
+        if (f->y)
+            CK(cudaMemcpyAsync(f->y, s->hp.y, b, cudaMemcpyDeviceToHost, stream_));
+        if (f->z)
+            CK(cudaMemcpyAsync(f->z, s->hp.z, b, cudaMemcpyDeviceToHost, stream_));
+        if (f->mass)
+            CK(cudaMemcpyAsync(f->mass, s->hp.mass, b, cudaMemcpyDeviceToHost,
+                               stream_));
+        if (f->charge)
+            CK(cudaMemcpyAsync(f->charge, s->hp.q, b, cudaMemcpyDeviceToHost,
+                               stream_));
+        if (f->fx || f->fy || f->fz) {
+            launch_state_out(one, 0, stream_);
+            if (f->fx)
+                CK(cudaMemcpyAsync(f->fx, s->hp.sx, b, cudaMemcpyDeviceToHost,
+                                   stream_));
+            if (f->fy)
+                CK(cudaMemcpyAsync(f->fy, s->hp.sy, b, cudaMemcpyDeviceToHost,
+                                   stream_));
+            if (f->fz)
+                CK(cudaMemcpyAsync(f->fz, s->hp.sz, b, cudaMemcpyDeviceToHost,
+                                   stream_));
+        }
+        if (f->vx || f->vy || f->vz) {
+            launch_state_out(one, 1, stream_);
+            if (f->vx)
+                CK(cudaMemcpyAsync(f->vx, s->hp.sx, b, cudaMemcpyDeviceToHost,
+                                   stream_));
+            if (f->vy)
+                CK(cudaMemcpyAsync(f->vy, s->hp.sy, b, cudaMemcpyDeviceToHost,
+                                   stream_));
+            if (f->vz)
+                CK(cudaMemcpyAsync(f->vz, s->hp.sz, b, cudaMemcpyDeviceToHost,
+                                   stream_));
+        }
+        if (f->tag) {
+            std::vector<long long> t(n);
+            CK(cudaMemcpyAsync(t.data(), s->hp.tag, 8 * n,
+                               cudaMemcpyDeviceToHost, stream_));
+            CK(cudaStreamSynchronize(stream_));
+            for (int i = 0; i < n; ++i)
+                f->tag[i] = t[i];
+        }
+    }
+    CK(cudaStreamSynchronize(stream_));
+    if (sc)
+        scalars(id, sc);
+}
+
+int64_t Engine::pairs(int id, int32_t* pi, int32_t* pj, int64_t capacity) {
+    CK(cudaSetDevice(device_));
+    Slot* s = slot(id);
+    const int n = s->hp.n, cap = s->hp.cap;
+    std::vector<int> perm(n), nn(n), nbr((size_t)n * cap);
+    CK(cudaStreamSynchronize(stream_));
+    CK(cudaMemcpy(perm.data(), s->hp.perm, 4 * n, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(nn.data(), s->hp.nnbr, 4 * n, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(nbr.data(), s->hp.nbr, 4 * (size_t)n * cap,
+                  cudaMemcpyDeviceToHost));
+    int64_t cnt = 0;
+    for (int a = 0; a < n; ++a)
+        for (int k = 0; k < nn[a]; ++k) {
+            const int i = perm[a], j = perm[nbr[(size_t)a * cap + k]];
+            if (i < j) {
+                if (pi && pj && cnt < capacity) {
+                    pi[cnt] = i;
+                    pj[cnt] = j;
+                }
+                ++cnt;
+            }
+        }
+    return cnt;
+}
+
+int Engine::history(int id, double* out, int max_steps) {
+    Slot* s = slot(id);
+    SysState st;
+    CK(cudaStreamSynchronize(stream_));
+    CK(cudaMemcpy(&st, s->hp.st, sizeof(st), cudaMemcpyDeviceToHost));
+    const int cap = s->hp.ehist_cap;
+    std::vector<double> ring(3 * (size_t)cap);
+    CK(cudaMemcpy(ring.data(), s->hp.ehist, ring.size() * 8,
+                  cudaMemcpyDeviceToHost));
+    const long long total = st.step;
+    const long long avail = std::min<long long>(total, cap);
+    const long long cnt = std::min<long long>(avail, max_steps);
+    for (long long k = 0; k < cnt; ++k) {
+        const long long stepk = total - cnt + k;
+        const long long slotk = stepk % cap;
+        for (int c = 0; c < 3; ++c)
+            out[3 * k + c] = ring[3 * slotk + c];
+    }
+    return (int)cnt;
+}
+
+void Engine::set_lanes(int lanes) {
+    if (lanes != 0 && lanes != 1 && lanes != 2 && lanes != 4 && lanes != 8 &&
+        lanes != 16 && lanes != 32)
+        throw Error(ATVB_ERR_INVALID, "lanes must be 0 or a power of two <= 32");
+    lanes_fixed_ = lanes;
+    dirty_ = true;
+}
+
+// Project-written autotuner: time the pair kernel for every lane count on
+// the engine's own systems and keep the fastest.
+int Engine::autotune() {
+    CK(cudaSetDevice(device_));
+    ensure_ready();
+    const int cands[6] = {1, 2, 4, 8, 16, 32};
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    float best = 1e30f;
+    int best_g = 4;
+    const int saved = lanes_fixed_;
+    for (int g : cands) {
+        lanes_fixed_ = g;
+        build_lists();
+        for (int w = 0; w < 2; ++w)
+            launch_pair(lc_, stream_);
+        CK(cudaEventRecord(e0, stream_));
+        const int reps = 5;
+        for (int r = 0; r < reps; ++r)
+            launch_pair(lc_, stream_);
+        CK(cudaEventRecord(e1, stream_));
+        CK(cudaEventSynchronize(e1));
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        if (ms < best) {
+            best = ms;
+            best_g = g;
+        }
+    }
+    (void)saved;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    lanes_fixed_ = best_g;
+    build_lists();
+    // the timing runs polluted the energy accumulators: recompute
+    compute_forces();
+    return best_g;
+}
+
+} // namespace atvb

@@ -1,0 +1,374 @@
+// integrate.cu -- velocity Verlet, Nose-Hoover, Langevin, kinetic energy and
+// the per-system scalar updates, fused into two atom passes per step.
+//
+// Reference order (src/cpu/driver/runtime.cpp:452-501 with VelocityVerlet at
+// order 0 and the thermostat at +100 in both integrate phases):
+//   initial_integrate: v += dt/2 f/m * ftm2v; x += dt v; wrap   (velocity_verlet.cpp:40-55)
+//                      NH: xi += dt/2 (2KE - Ndf kT)/Q; v *= exp(-dt/2 xi)  (nose_hoover.cpp:104-170)
+//   neighbor decide (neighbor_list.h:128-141), force, post_force Langevin
+//   (fix_langevin.cpp:79-155), final_integrate: v += dt/2 f/m; NH again;
+//   end_of_step: KE (init.cpp:29-45).
+// Fusion: the thermostat scale of each half is a per-system scalar produced
+// by a one-thread-per-system kernel; it is applied to v by the NEXT atom
+// pass (the initial-half scale by the final kick, the final-half scale by
+// the next step's initial kick), so each half step reads and writes v once.
+// The end-of-step kinetic energy is s_B^2 * KE(v) for the deferred scale.
+#include "atvb_common.cuh"
+#include "atvb_kernels.cuh"
+
+namespace atvb {
+
+// splitmix64 stream + Box-Muller with a cached partner
+// (fix_langevin.cpp:37-62); the key mixes seed, step and atom tag
+// (fix_langevin.cpp:112-121).
+struct GaussStream {
+    unsigned long long s;
+    bool has;
+    double cached;
+    ATVB_DEV double u01() {
+        s += 0x9E3779B97F4A7C15ull;
+        unsigned long long z = s;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z = z ^ (z >> 31);
+        return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+    }
+    ATVB_DEV double next() {
+        if (has) {
+            has = false;
+            return cached;
+        }
+        const double u = u01();
+        const double v = u01();
+        const double r = sqrt(-2.0 * log(u > 1e-300 ? u : 1e-300));
+        double sn, cs;
+        sincos(2.0 * kPi * v, &sn, &cs);
+        cached = r * sn;
+        has = true;
+        return r * cs;
+    }
+};
+
+ATVB_DEV double fix_to_d(unsigned long long v) {
+    return (double)(long long)v * kEFixInv;
+}
+
+// Initial half: deferred scale, kick, drift, wrap, sorted repack,
+// displacement check, KE of the kicked velocities (for Nose-Hoover).
+__global__ void __launch_bounds__(kChunk)
+    k_integrate_a(const Item* items, int nitems, const SysParams* sp) {
+    __shared__ double sh[32];
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const Item item = items[it];
+        const SysParams& P = sp[item.sys];
+        const int i = item.begin + threadIdx.x;
+        double ke = 0.0;
+        if (i < P.n) {
+            const double sc = P.st->vscale;
+            const int r = P.rank[i];
+            const double4 f = P.f4[r];
+            const double dtfm = P.dtf / P.mass[i];
+            double v[3] = {P.vx[i], P.vy[i], P.vz[i]};
+            const double fa[3] = {f.x, f.y, f.z};
+            double* const xs[3] = {P.x, P.y, P.z};
+            double x[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                v[d] = __dadd_rn(__dmul_rn(v[d], sc), __dmul_rn(dtfm, fa[d]));
+                double xd = __dadd_rn(xs[d][i], __dmul_rn(P.dt, v[d]));
+                xd = __dadd_rn(xd, -__dmul_rn(P.L[d], floor(xd / P.L[d])));
+                x[d] = xd;
+            }
+            P.vx[i] = v[0];
+            P.vy[i] = v[1];
+            P.vz[i] = v[2];
+            P.x[i] = x[0];
+            P.y[i] = x[1];
+            P.z[i] = x[2];
+            const double q = P.q[i];
+            if (P.prec == kMixed) {
+                int4 p;
+                p.x = (int)pos_fix(x[0], P.fix_scale[0]);
+                p.y = (int)pos_fix(x[1], P.fix_scale[1]);
+                p.z = (int)pos_fix(x[2], P.fix_scale[2]);
+                p.w = __float_as_int((float)q);
+                reinterpret_cast<int4*>(P.pos4)[r] = p;
+            } else {
+                reinterpret_cast<double4*>(P.pos4)[r] =
+                    make_double4(x[0], x[1], x[2], q);
+            }
+            // cell_list.cpp:355-392 with min-image displacement
+            const double ddx = min_img(x[0] - P.xr[i], P.L[0], P.invL[0]);
+            const double ddy = min_img(x[1] - P.yr[i], P.L[1], P.invL[1]);
+            const double ddz = min_img(x[2] - P.zr[i], P.L[2], P.invL[2]);
+            if (ddx * ddx + ddy * ddy + ddz * ddz > P.skin_half2)
+                P.st->need_rebuild = 1;
+            ke = P.mass[i] * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        }
+        if (P.thermostat == kNoseHoover) {
+            const double t = block_sum(ke, sh);
+            if (threadIdx.x == 0)
+                fix_add(&P.st->acc[kAccKEA], 0.5 * kMvv2e * t);
+        }
+    }
+}
+
+// One thread per system: thermostat scalar of the initial half, neighbour
+// decision (every / delay / check), step accumulators reset.
+__global__ void k_sys_a(const int* sys_list, int nsys, const SysParams* sp) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nsys)
+        return;
+    const SysParams& P = sp[sys_list[k]];
+    SysState* st = P.st;
+    st->vscale = 1.0;
+    if (P.thermostat == kNoseHoover) {
+        const double ke = fix_to_d(st->acc[kAccKEA]);
+        st->acc[kAccKEA] = 0ull;
+        st->xi += (P.dt * 0.5) * (2.0 * ke - P.n_dof_kT) / P.Q;
+        st->s_a = exp(-P.dt * 0.5 * st->xi);
+    } else {
+        st->s_a = 1.0;
+    }
+    st->ago += 1;
+    const bool disp = st->need_rebuild != 0;
+    st->need_rebuild = 0;
+    const bool rebuild = st->ago >= P.nl_delay && (st->ago % P.nl_every) == 0 &&
+                         (!P.nl_check || disp);
+    st->rebuild = rebuild ? 1 : 0;
+    if (rebuild) {
+        st->ago = 0;
+        st->rebuilds += 1;
+        st->max_nnbr = 0;
+    }
+}
+
+// Final half: initial-half thermostat scale, Langevin force, kick, KE.
+__global__ void __launch_bounds__(kChunk)
+    k_integrate_b(const Item* items, int nitems, const SysParams* sp) {
+    __shared__ double sh[32];
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const Item item = items[it];
+        const SysParams& P = sp[item.sys];
+        const int i = item.begin + threadIdx.x;
+        double ke = 0.0;
+        if (i < P.n) {
+            const double sc = P.st->s_a;
+            const int r = P.rank[i];
+            double4 f = P.f4[r];
+            const double m = P.mass[i];
+            double v[3] = {__dmul_rn(P.vx[i], sc), __dmul_rn(P.vy[i], sc),
+                           __dmul_rn(P.vz[i], sc)};
+            if (P.thermostat == kLangevin) {
+                const unsigned long long base =
+                    (unsigned long long)P.seed * 0x9E3779B97F4A7C15ull +
+                    (unsigned long long)P.st->step * 0xBF58476D1CE4E5B9ull;
+                GaussStream g{base + (unsigned long long)P.tag[i] *
+                                         0xD6E8FEB86659FD93ull,
+                              false, 0.0};
+                const double g1 = -m * P.lang_g1;
+                const double g2 = P.lang_g2pre * sqrt(m);
+                const double rx = g.next(), ry = g.next(), rz = g.next();
+                f.x += g1 * v[0] + g2 * rx;
+                f.y += g1 * v[1] + g2 * ry;
+                f.z += g1 * v[2] + g2 * rz;
+                P.f4[r] = f;
+            }
+            const double dtfm = P.dtf / m;
+            v[0] = __dadd_rn(v[0], __dmul_rn(dtfm, f.x));
+            v[1] = __dadd_rn(v[1], __dmul_rn(dtfm, f.y));
+            v[2] = __dadd_rn(v[2], __dmul_rn(dtfm, f.z));
+            P.vx[i] = v[0];
+            P.vy[i] = v[1];
+            P.vz[i] = v[2];
+            ke = m * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        }
+        const double t = block_sum(ke, sh);
+        if (threadIdx.x == 0)
+            fix_add(&P.st->acc[kAccKEB], 0.5 * kMvv2e * t);
+    }
+}
+
+ATVB_DEV void finish_energy(const SysParams& P, SysState* st) {
+    st->e_lj = fix_to_d(st->acc[kAccELJ]);
+    st->e_coul = fix_to_d(st->acc[kAccECoul]);
+    st->e_recip = fix_to_d(st->acc[kAccERecip]);
+    st->e_const = P.has_pme ? P.e_const : 0.0;
+    st->energy = st->e_lj + st->e_coul + st->e_recip + st->e_const;
+    for (int k = 0; k < 6; ++k)
+        st->virial[k] = fix_to_d(st->acc[kAccVir + k]);
+    st->acc[kAccELJ] = st->acc[kAccECoul] = st->acc[kAccERecip] = 0ull;
+    for (int k = 0; k < 6; ++k)
+        st->acc[kAccVir + k] = 0ull;
+}
+
+// One thread per system: final-half thermostat, end-of-step scalars,
+// energy history, step counter.
+__global__ void k_sys_b(const int* sys_list, int nsys, const SysParams* sp) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nsys)
+        return;
+    const SysParams& P = sp[sys_list[k]];
+    SysState* st = P.st;
+    const double ke = fix_to_d(st->acc[kAccKEB]);
+    st->acc[kAccKEB] = 0ull;
+    if (P.thermostat == kNoseHoover) {
+        st->xi += (P.dt * 0.5) * (2.0 * ke - P.n_dof_kT) / P.Q;
+        const double s = exp(-P.dt * 0.5 * st->xi);
+        st->vscale = s;
+        st->kinetic = s * s * ke;
+    } else {
+        st->vscale = 1.0;
+        st->kinetic = ke;
+    }
+    finish_energy(P, st);
+    st->conserved = st->energy + st->kinetic;
+    if (P.ehist_cap > 0) {
+        const long long slot = st->step % P.ehist_cap;
+        P.ehist[3 * slot + 0] = st->energy;
+        P.ehist[3 * slot + 1] = st->kinetic;
+        P.ehist[3 * slot + 2] = (double)st->step;
+    }
+    st->step += 1;
+}
+
+// Energies of a force-only evaluation (no step, no thermostat update).
+__global__ void k_sys_energy(const int* sys_list, int nsys,
+                             const SysParams* sp) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nsys)
+        return;
+    const SysParams& P = sp[sys_list[k]];
+    finish_energy(P, P.st);
+    P.st->conserved = P.st->energy + P.st->kinetic;
+}
+
+__global__ void k_force_rebuild(const int* sys_list, int nsys,
+                                const SysParams* sp) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nsys)
+        return;
+    SysState* st = sp[sys_list[k]].st;
+    st->rebuild = 1;
+    st->ago = 0;
+    st->max_nnbr = 0;
+}
+
+// After an upload: wrap positions into [0, L) (pbc.h:48-50) and keep the
+// uploaded forces (staged in sx/sy/sz) in sorted order.  Runs after a
+// forced rebuild, so rank is valid.
+__global__ void k_state_in(const Item* items, int nitems, const SysParams* sp) {
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const Item item = items[it];
+        const SysParams& P = sp[item.sys];
+        const int i = item.begin + threadIdx.x;
+        if (i >= P.n)
+            continue;
+        P.f4[P.rank[i]] = make_double4(P.sx[i], P.sy[i], P.sz[i], 0.0);
+    }
+}
+
+__global__ void k_wrap_in(const Item* items, int nitems, const SysParams* sp) {
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const Item item = items[it];
+        const SysParams& P = sp[item.sys];
+        const int i = item.begin + threadIdx.x;
+        if (i >= P.n)
+            continue;
+        P.x[i] = wrap(P.x[i], P.L[0]);
+        P.y[i] = wrap(P.y[i], P.L[1]);
+        P.z[i] = wrap(P.z[i], P.L[2]);
+    }
+}
+
+// what = 0: forces (original order) into sx/sy/sz;
+// what = 1: velocities with the pending scale applied into sx/sy/sz.
+__global__ void k_state_out(const Item* items, int nitems, const SysParams* sp,
+                            int what) {
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const Item item = items[it];
+        const SysParams& P = sp[item.sys];
+        const int i = item.begin + threadIdx.x;
+        if (i >= P.n)
+            continue;
+        if (what == 0) {
+            const double4 f = P.f4[P.rank[i]];
+            P.sx[i] = f.x;
+            P.sy[i] = f.y;
+            P.sz[i] = f.z;
+        } else {
+            const double s = P.st->vscale;
+            P.sx[i] = P.vx[i] * s;
+            P.sy[i] = P.vy[i] * s;
+            P.sz[i] = P.vz[i] * s;
+        }
+    }
+}
+
+__global__ void k_kinetic(const Item* items, int nitems, const SysParams* sp) {
+    __shared__ double sh[32];
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const Item item = items[it];
+        const SysParams& P = sp[item.sys];
+        const int i = item.begin + threadIdx.x;
+        double ke = 0.0;
+        if (i < P.n)
+            ke = P.mass[i] *
+                 (P.vx[i] * P.vx[i] + P.vy[i] * P.vy[i] + P.vz[i] * P.vz[i]);
+        const double t = block_sum(ke, sh);
+        if (threadIdx.x == 0)
+            fix_add(&P.st->acc[kAccKEB], 0.5 * kMvv2e * t);
+    }
+}
+
+__global__ void k_kinetic_finish(const int* sys_list, int nsys,
+                                 const SysParams* sp) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nsys)
+        return;
+    SysState* st = sp[sys_list[k]].st;
+    st->kinetic = fix_to_d(st->acc[kAccKEB]);
+    st->acc[kAccKEB] = 0ull;
+}
+
+static int sys_blocks(int nsys) { return (nsys + 127) / 128; }
+
+void launch_integrate_a(const LaunchCfg& lc, cudaStream_t s) {
+    k_integrate_a<<<lc.atoms.grid, kChunk, 0, s>>>(lc.atoms.d, lc.atoms.n,
+                                                    lc.sp);
+}
+void launch_sys_a(const LaunchCfg& lc, cudaStream_t s) {
+    k_sys_a<<<sys_blocks(lc.nsys), 128, 0, s>>>(lc.sys_list, lc.nsys, lc.sp);
+}
+void launch_integrate_b(const LaunchCfg& lc, cudaStream_t s) {
+    k_integrate_b<<<lc.atoms.grid, kChunk, 0, s>>>(lc.atoms.d, lc.atoms.n,
+                                                    lc.sp);
+}
+void launch_sys_b(const LaunchCfg& lc, cudaStream_t s) {
+    k_sys_b<<<sys_blocks(lc.nsys), 128, 0, s>>>(lc.sys_list, lc.nsys, lc.sp);
+}
+void launch_sys_energy(const LaunchCfg& lc, cudaStream_t s) {
+    k_sys_energy<<<sys_blocks(lc.nsys), 128, 0, s>>>(lc.sys_list, lc.nsys,
+                                                     lc.sp);
+}
+void launch_force_rebuild(const LaunchCfg& lc, cudaStream_t s) {
+    k_force_rebuild<<<sys_blocks(lc.nsys), 128, 0, s>>>(lc.sys_list, lc.nsys,
+                                                        lc.sp);
+}
+void launch_state_in(const LaunchCfg& lc, cudaStream_t s) {
+    k_state_in<<<lc.atoms.grid, kChunk, 0, s>>>(lc.atoms.d, lc.atoms.n, lc.sp);
+}
+void launch_wrap_in(const LaunchCfg& lc, cudaStream_t s) {
+    k_wrap_in<<<lc.atoms.grid, kChunk, 0, s>>>(lc.atoms.d, lc.atoms.n, lc.sp);
+}
+void launch_state_out(const LaunchCfg& lc, int what, cudaStream_t s) {
+    k_state_out<<<lc.atoms.grid, kChunk, 0, s>>>(lc.atoms.d, lc.atoms.n, lc.sp,
+                                                 what);
+}
+void launch_kinetic(const LaunchCfg& lc, cudaStream_t s) {
+    k_kinetic<<<lc.atoms.grid, kChunk, 0, s>>>(lc.atoms.d, lc.atoms.n, lc.sp);
+    k_kinetic_finish<<<sys_blocks(lc.nsys), 128, 0, s>>>(lc.sys_list, lc.nsys,
+                                                         lc.sp);
+}
+
+} // namespace atvb

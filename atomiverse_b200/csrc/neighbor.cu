@@ -1,0 +1,282 @@
+// neighbor.cu -- cell binning, cell-ordered permutation and the Verlet list.
+//
+// Semantics follow the reference CPU cell list
+// (src/cpu/neighbor/cell_list.cpp:83-314 grid/stencil/binning and :743-895
+// list): a pair {i, j} is listed iff its minimum-image separation, computed
+// in FP64 on the rebuild-time coordinates, satisfies r^2 < (cutoff+skin)^2.
+// Every product and sum of that test is rounded separately (__dmul_rn /
+// __dadd_rn), which is exactly the arithmetic of the FP64 oracle, so the
+// pair set equals the oracle's bit for bit.  The list itself is a FULL list
+// (each pair stored in both rows) in row-major ELL form with a fixed row
+// capacity, so the force kernel needs no atomics and sums every row in a
+// fixed order.
+#include "atvb_common.cuh"
+#include "atvb_kernels.cuh"
+
+namespace atvb {
+
+// Stage 1: cell of every atom (original order) and its arrival slot.
+__global__ void k_cell_count(const Item* items, int nitems,
+                             const SysParams* sp) {
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const Item item = items[it];
+        const SysParams& P = sp[item.sys];
+        if (!P.st->rebuild)
+            continue;
+        const int i = item.begin + threadIdx.x;
+        if (i >= P.n)
+            continue;
+        const double p[3] = {P.x[i], P.y[i], P.z[i]};
+        int c[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            int cd = (int)floor(p[d] * P.cs_inv[d]);
+            cd = cd < 0 ? 0 : (cd > P.nc[d] - 1 ? P.nc[d] - 1 : cd);
+            c[d] = cd;
+        }
+        const int cell = (c[0] * P.nc[1] + c[1]) * P.nc[2] + c[2];
+        P.cell_of[i] = cell;
+        P.slot[i] = atomicAdd(&P.cell_count[cell], 1);
+    }
+}
+
+// Stage 2: exclusive scan of the cell counts, one block per system.
+__global__ void k_cell_scan(const int* sys_list, const SysParams* sp) {
+    const SysParams& P = sp[sys_list[blockIdx.x]];
+    if (!P.st->rebuild)
+        return;
+    __shared__ int warp_tot[32];
+    __shared__ int carry;
+    if (threadIdx.x == 0)
+        carry = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int base = 0; base < P.ncell; base += blockDim.x) {
+        const int c = base + threadIdx.x;
+        const int v = c < P.ncell ? P.cell_count[c] : 0;
+        int incl = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o)
+                incl += t;
+        }
+        if (lane == 31)
+            warp_tot[w] = incl;
+        __syncthreads();
+        if (w == 0) {
+            const int nw = blockDim.x >> 5;
+            int t = lane < nw ? warp_tot[lane] : 0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int u = __shfl_up_sync(0xffffffffu, t, o);
+                if (lane >= o)
+                    t += u;
+            }
+            if (lane < nw)
+                warp_tot[lane] = t; // inclusive over warps
+        }
+        __syncthreads();
+        const int before = (w > 0 ? warp_tot[w - 1] : 0) + carry;
+        if (c < P.ncell) {
+            P.cell_start[c] = before + incl - v;
+            P.cell_count[c] = 0; // ready for the next rebuild
+        }
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1)
+            carry = before + incl;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        P.cell_start[P.ncell] = carry;
+}
+
+// Stage 3: scatter atom ids into their cells.
+__global__ void k_cell_scatter(const Item* items, int nitems,
+                               const SysParams* sp) {
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const Item item = items[it];
+        const SysParams& P = sp[item.sys];
+        if (!P.st->rebuild)
+            continue;
+        const int i = item.begin + threadIdx.x;
+        if (i >= P.n)
+            continue;
+        P.perm[P.cell_start[P.cell_of[i]] + P.slot[i]] = i;
+    }
+}
+
+// Stage 4: order each cell by original index, so the permutation (and with
+// it every later summation order) is independent of atomic arrival order.
+__global__ void k_cell_sort(const Item* citems, int nitems,
+                            const SysParams* sp) {
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const Item item = citems[it];
+        const SysParams& P = sp[item.sys];
+        if (!P.st->rebuild)
+            continue;
+        const int c = item.begin + threadIdx.x;
+        if (c >= P.ncell)
+            continue;
+        const int a = P.cell_start[c], b = P.cell_start[c + 1];
+        for (int k = a + 1; k < b; ++k) {
+            const int v = P.perm[k];
+            int m = k - 1;
+            while (m >= a && P.perm[m] > v) {
+                P.perm[m + 1] = P.perm[m];
+                --m;
+            }
+            P.perm[m + 1] = v;
+        }
+    }
+}
+
+// Stage 5: inverse permutation, sorted positions, reference positions.
+__global__ void k_permute(const Item* items, int nitems, const SysParams* sp) {
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const Item item = items[it];
+        const SysParams& P = sp[item.sys];
+        if (!P.st->rebuild)
+            continue;
+        const int s = item.begin + threadIdx.x;
+        if (s >= P.n)
+            continue;
+        const int i = P.perm[s];
+        P.rank[i] = s;
+        P.cellS[s] = P.cell_of[i];
+        const double x = P.x[i], y = P.y[i], z = P.z[i], q = P.q[i];
+        P.posd4[s] = make_double4(x, y, z, q);
+        if (P.prec == kMixed) {
+            int4 v;
+            v.x = (int)pos_fix(x, P.fix_scale[0]);
+            v.y = (int)pos_fix(y, P.fix_scale[1]);
+            v.z = (int)pos_fix(z, P.fix_scale[2]);
+            v.w = __float_as_int((float)q);
+            reinterpret_cast<int4*>(P.pos4)[s] = v;
+        }
+        P.xr[i] = x;
+        P.yr[i] = y;
+        P.zr[i] = z;
+    }
+}
+
+// Exact FP64 pair-set test (same rounding as the oracle built with
+// -ffp-contract=off): branchy single-wrap minimum image
+// (cell_list.h:214-227), then ((dx*dx + dy*dy) + dz*dz).
+ATVB_DEV double exact_r2(const double4& a, const double4& b, const double* L,
+                         const double* halfL) {
+    double d[3] = {__dadd_rn(a.x, -b.x), __dadd_rn(a.y, -b.y),
+                   __dadd_rn(a.z, -b.z)};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        if (d[k] > halfL[k])
+            d[k] = __dadd_rn(d[k], -L[k]);
+        else if (d[k] < -halfL[k])
+            d[k] = __dadd_rn(d[k], L[k]);
+    }
+    return __dadd_rn(__dadd_rn(__dmul_rn(d[0], d[0]), __dmul_rn(d[1], d[1])),
+                     __dmul_rn(d[2], d[2]));
+}
+
+// Stage 6 (items of kListChunk atoms): one warp per sorted atom walks the
+// stencil columns (contiguous runs of cells along z, hence contiguous runs of
+// sorted atoms), tests 32 candidates per iteration and compacts the hits
+// with a ballot.
+__global__ void __launch_bounds__(256)
+    k_build_list(const Item* items, int nitems, const SysParams* sp) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const Item item = items[it];
+        const SysParams& P = sp[item.sys];
+        if (!P.st->rebuild)
+            continue;
+        const int nc0 = P.nc[0], nc1 = P.nc[1], nc2 = P.nc[2];
+        const double L[3] = {P.L[0], P.L[1], P.L[2]};
+        const double hL[3] = {P.halfL[0], P.halfL[1], P.halfL[2]};
+        const double rl2 = P.rlist2;
+        const int cap = P.cap, ncol = P.ncol;
+        const int4* __restrict__ cols = P.cols;
+        const int* __restrict__ cstart = P.cell_start;
+        const double4* __restrict__ pos = P.posd4;
+        const int s = item.begin + warp;
+        if (s < P.n) {
+            const double4 pi = pos[s];
+            const int c = P.cellS[s];
+            const int cz = c % nc2, cy = (c / nc2) % nc1, cx = c / (nc1 * nc2);
+            int* row = P.nbr + (size_t)s * cap;
+            int cnt = 0;
+            for (int k = 0; k < ncol; ++k) {
+                const int4 col = cols[k];
+                const int xx = (cx + col.x + nc0) % nc0;
+                const int yy = (cy + col.y + nc1) % nc1;
+                const int base = (xx * nc1 + yy) * nc2;
+                int seg_lo[2], seg_hi[2], nseg;
+                if (col.z < 0) {
+                    seg_lo[0] = base;
+                    seg_hi[0] = base + nc2 - 1;
+                    nseg = 1;
+                } else {
+                    const int z0 = cz - col.z, z1 = cz + col.z;
+                    if (z0 < 0) {
+                        seg_lo[0] = base + z0 + nc2;
+                        seg_hi[0] = base + nc2 - 1;
+                        seg_lo[1] = base;
+                        seg_hi[1] = base + z1;
+                        nseg = 2;
+                    } else if (z1 >= nc2) {
+                        seg_lo[0] = base + z0;
+                        seg_hi[0] = base + nc2 - 1;
+                        seg_lo[1] = base;
+                        seg_hi[1] = base + z1 - nc2;
+                        nseg = 2;
+                    } else {
+                        seg_lo[0] = base + z0;
+                        seg_hi[0] = base + z1;
+                        nseg = 1;
+                    }
+                }
+                for (int sg = 0; sg < nseg; ++sg) {
+                    const int a = cstart[seg_lo[sg]];
+                    const int b = cstart[seg_hi[sg] + 1];
+                    for (int j0 = a; j0 < b; j0 += 32) {
+                        const int j = j0 + lane;
+                        bool hit = false;
+                        if (j < b && j != s) {
+                            const double4 pj = pos[j];
+                            hit = exact_r2(pi, pj, L, hL) < rl2;
+                        }
+                        const unsigned m = __ballot_sync(0xffffffffu, hit);
+                        if (hit) {
+                            const int wpos = cnt + __popc(m & lt);
+                            if (wpos < cap)
+                                row[wpos] = j;
+                        }
+                        cnt += __popc(m);
+                    }
+                }
+            }
+            if (lane == 0) {
+                P.nnbr[s] = cnt < cap ? cnt : cap;
+                atomicMax(&P.st->max_nnbr, cnt);
+                if (cnt > cap)
+                    atomicOr(&P.st->overflow, 1);
+            }
+        }
+    }
+}
+
+void launch_rebuild(const LaunchCfg& lc, cudaStream_t s) {
+    k_cell_count<<<lc.atoms.grid, kChunk, 0, s>>>(lc.atoms.d, lc.atoms.n,
+                                                   lc.sp);
+    k_cell_scan<<<lc.nsys, 1024, 0, s>>>(lc.sys_list, lc.sp);
+    k_cell_scatter<<<lc.atoms.grid, kChunk, 0, s>>>(lc.atoms.d, lc.atoms.n,
+                                                     lc.sp);
+    k_cell_sort<<<lc.cells.grid, kChunk, 0, s>>>(lc.cells.d, lc.cells.n,
+                                                  lc.sp);
+    k_permute<<<lc.atoms.grid, kChunk, 0, s>>>(lc.atoms.d, lc.atoms.n, lc.sp);
+    k_build_list<<<lc.list.grid, 32 * kListChunk, 0, s>>>(lc.list.d,
+                                                           lc.list.n, lc.sp);
+}
+
+} // namespace atvb

@@ -1,0 +1,340 @@
+// pme.cu -- smooth-PME reciprocal sum: spread, influence, gather.
+//
+// Math follows the reference's header-only PME
+// (include/atomiverse/cpu/longrange/pme_spline.h:32-58 B-spline recursion,
+// :124-210 fractional coordinates and spreading;
+// include/atomiverse/cpu/longrange/pme_influence.h:159-199 influence with
+// energy and virial, :217-280 force interpolation; src/cpu/longrange/
+// pme.cpp:152-253 driver).  Differences of layout, not of math:
+//  * the charge grid is accumulated in 64-bit fixed point, so the spread is
+//    order-independent and bit-reproducible;
+//  * the transforms are real-to-complex / complex-to-real on the half grid
+//    (K0 x K1 x (K2/2+1)); the half-grid energy and virial weight every
+//    mode with 0 < m2 < K2/2 twice;
+//  * H(m) is tabulated once per box (the CPU-style tables of
+//    pme_influence.h:104-155), and the virial that the reference CUDA PME
+//    omits is produced from the same pass.
+#include "atvb_common.cuh"
+#include "atvb_kernels.cuh"
+
+namespace atvb {
+
+// pme_spline.h:32-58 (Essmann et al. 1995 appendix recursion)
+template <int N, typename T>
+ATVB_DEV void bspline_dev(T frac, T* th, T* dth) {
+    th[N - 1] = T(0);
+    th[1] = frac;
+    th[0] = T(1) - frac;
+#pragma unroll
+    for (int k = 3; k < N; ++k) {
+        const T div = T(1) / T(k - 1);
+        th[k - 1] = div * frac * th[k - 2];
+#pragma unroll
+        for (int j = 1; j < k - 1; ++j)
+            th[k - 1 - j] = div * ((frac + T(j)) * th[k - 2 - j] +
+                                   (T(k - j) - frac) * th[k - 1 - j]);
+        th[0] = div * (T(1) - frac) * th[0];
+    }
+    dth[0] = -th[0];
+#pragma unroll
+    for (int j = 1; j < N; ++j)
+        dth[j] = th[j - 1] - th[j];
+    const T div = T(1) / T(N - 1);
+    th[N - 1] = div * frac * th[N - 2];
+#pragma unroll
+    for (int j = 1; j < N - 1; ++j)
+        th[N - 1 - j] = div * ((frac + T(j)) * th[N - 2 - j] +
+                               (T(N - j) - frac) * th[N - 1 - j]);
+    th[0] = div * (T(1) - frac) * th[0];
+}
+
+ATVB_DEV int gwrap(int g, int K) {
+    if (g >= K)
+        g -= K;
+    if (g < 0)
+        g += K;
+    return g;
+}
+
+// Fractional grid coordinate, base point and B-spline weights of one atom.
+template <bool MIXED, int N, typename T>
+ATVB_DEV void atom_splines(const SysParams& P, int s, T th[3][N], T dth[3][N],
+                           int base[3], double& q) {
+    if (MIXED) {
+        const int4 p = reinterpret_cast<const int4*>(P.pos4)[s];
+        q = (double)__int_as_float(p.w);
+        const unsigned u[3] = {(unsigned)p.x, (unsigned)p.y, (unsigned)p.z};
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            // fixed-point position is the fractional coordinate * 2^32
+            const double uu = (double)u[d] * ((double)P.K[d] * kEFixInv);
+            const double u0 = floor(uu);
+            base[d] = (int)u0;
+            if (base[d] >= P.K[d])
+                base[d] -= P.K[d];
+            bspline_dev<N, T>((T)(uu - u0), th[d], dth[d]);
+        }
+    } else {
+        const double4 p = reinterpret_cast<const double4*>(P.pos4)[s];
+        q = p.w;
+        const double x[3] = {p.x, p.y, p.z};
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            // pme_spline.h:131-141
+            const double sd = P.invL[d] * x[d];
+            double u = sd * P.K[d];
+            u -= floor(u / P.K[d]) * P.K[d];
+            const double u0 = floor(u);
+            base[d] = (int)u0;
+            bspline_dev<N, T>((T)(u - u0), th[d], dth[d]);
+        }
+    }
+}
+
+template <bool MIXED, int N>
+__global__ void __launch_bounds__(256)
+    k_pme_spread(const Item* items, int nitems, const SysParams* sp) {
+    using T = typename std::conditional<MIXED, float, double>::type;
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const Item item = items[it];
+        const SysParams& P = sp[item.sys];
+        if (P.prec != (MIXED ? kMixed : kFP64))
+            continue;
+        const int s = item.begin + threadIdx.x;
+        if (s >= P.n)
+            continue;
+        T th[3][N], dth[3][N];
+        int base[3];
+        double q;
+        atom_splines<MIXED, N, T>(P, s, th, dth, base, q);
+        if (q == 0.0)
+            continue;
+        const int K0 = P.K[0], K1 = P.K[1], K2 = P.K[2];
+        const double gs = P.grid_scale;
+        const int b0 = base[0] - (N - 1), b1 = base[1] - (N - 1),
+                  b2 = base[2] - (N - 1);
+        unsigned long long* __restrict__ grid = P.grid_fix;
+#pragma unroll
+        for (int a = 0; a < N; ++a) {
+            const int g0 = gwrap(b0 + a, K0);
+            const T wa = (T)q * th[0][a];
+#pragma unroll
+            for (int b = 0; b < N; ++b) {
+                const int g1 = gwrap(b1 + b, K1);
+                const T wab = wa * th[1][b];
+                const size_t plane = (size_t)K2 * (g1 + (size_t)K1 * g0);
+#pragma unroll
+                for (int c = 0; c < N; ++c) {
+                    const int g2 = gwrap(b2 + c, K2);
+                    const double w = (double)(wab * th[2][c]);
+                    atomicAdd(grid + plane + g2,
+                              (unsigned long long)__double2ll_rn(w * gs));
+                }
+            }
+        }
+    }
+}
+
+// fixed-point grid -> real grid for the transform; clears the fixed grid
+template <bool MIXED>
+__global__ void k_pme_convert(const Item* items, int nitems,
+                              const SysParams* sp) {
+    using T = typename std::conditional<MIXED, float, double>::type;
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const Item item = items[it];
+        const SysParams& P = sp[item.sys];
+        if (P.prec != (MIXED ? kMixed : kFP64))
+            continue;
+        const size_t ntot = (size_t)P.K[0] * P.K[1] * P.K[2];
+        T* __restrict__ out = reinterpret_cast<T*>(P.grid_real);
+        for (int k = threadIdx.x; k < kGridChunk; k += blockDim.x) {
+            const size_t i = (size_t)item.begin + k;
+            if (i >= ntot)
+                break;
+            const long long v = (long long)P.grid_fix[i];
+            out[i] = (T)((double)v * P.grid_scale_inv);
+            P.grid_fix[i] = 0ull;
+        }
+    }
+}
+
+// pme_influence.h:159-199 on the half-complex grid
+template <bool MIXED>
+__global__ void __launch_bounds__(256)
+    k_pme_influence(const Item* items, int nitems, const SysParams* sp) {
+    using T2 = typename std::conditional<MIXED, float2, double2>::type;
+    __shared__ double sh[32 * 7];
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const Item item = items[it];
+        const SysParams& P = sp[item.sys];
+        if (P.prec != (MIXED ? kMixed : kFP64))
+            continue;
+        const int K0 = P.K[0], K1 = P.K[1], K2 = P.K[2], Kh = P.Kh;
+        const size_t nh = (size_t)K0 * K1 * Kh;
+        T2* __restrict__ grid = reinterpret_cast<T2*>(P.grid_cplx);
+        const bool vir = P.need_virial;
+        double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+        for (int k = threadIdx.x; k < kGridChunk; k += blockDim.x) {
+            const size_t idx = (size_t)item.begin + k;
+            if (idx >= nh)
+                break;
+            const double H = P.infl[idx];
+            T2 Qm = grid[idx];
+            const double re = (double)Qm.x, im = (double)Qm.y;
+            const int m2 = (int)(idx % Kh);
+            const double w = (m2 == 0 || 2 * m2 == K2) ? 1.0 : 2.0;
+            const double ug = w * H * (re * re + im * im);
+            acc[0] += ug;
+            if (vir && H != 0.0) {
+                const size_t r = idx / Kh;
+                const int m1 = (int)(r % K1), m0 = (int)(r / K1);
+                const int h0 = m0 <= K0 / 2 ? m0 : m0 - K0;
+                const int h1 = m1 <= K1 / 2 ? m1 : m1 - K1;
+                const int h2 = m2 <= K2 / 2 ? m2 : m2 - K2;
+                const double mx = h0 * P.invL[0], my = h1 * P.invL[1],
+                             mz = h2 * P.invL[2];
+                const double msq = mx * mx + my * my + mz * mz;
+                const double vt = -2.0 * (1.0 / msq + P.pme_alpha2_pi2);
+                acc[1] += ug * (1.0 + vt * mx * mx);
+                acc[2] += ug * (1.0 + vt * my * my);
+                acc[3] += ug * (1.0 + vt * mz * mz);
+                acc[4] += ug * (vt * mx * my);
+                acc[5] += ug * (vt * mx * mz);
+                acc[6] += ug * (vt * my * mz);
+            }
+            Qm.x = (decltype(Qm.x))(H * re);
+            Qm.y = (decltype(Qm.y))(H * im);
+            grid[idx] = Qm;
+        }
+        // per-item fixed-point flush (independent of batch composition)
+        if (vir) {
+            block_sum_vec<7>(acc, sh);
+            if (threadIdx.x == 0) {
+                fix_add(&P.st->acc[kAccERecip], acc[0] * P.pme_escale);
+                for (int k = 0; k < 6; ++k)
+                    fix_add(&P.st->acc[kAccVir + k], acc[1 + k] * P.pme_escale);
+            }
+        } else {
+            double e1[1] = {acc[0]};
+            block_sum_vec<1>(e1, sh);
+            if (threadIdx.x == 0)
+                fix_add(&P.st->acc[kAccERecip], e1[0] * P.pme_escale);
+        }
+    }
+}
+
+// pme_influence.h:217-280 (orthorhombic: inv_cell is diagonal)
+template <bool MIXED, int N>
+__global__ void __launch_bounds__(256)
+    k_pme_gather(const Item* items, int nitems, const SysParams* sp) {
+    using T = typename std::conditional<MIXED, float, double>::type;
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const Item item = items[it];
+        const SysParams& P = sp[item.sys];
+        if (P.prec != (MIXED ? kMixed : kFP64))
+            continue;
+        const int s = item.begin + threadIdx.x;
+        if (s >= P.n)
+            continue;
+        T th[3][N], dth[3][N];
+        int base[3];
+        double q;
+        atom_splines<MIXED, N, T>(P, s, th, dth, base, q);
+        double fx = 0, fy = 0, fz = 0;
+        if (q != 0.0) {
+            const int K0 = P.K[0], K1 = P.K[1], K2 = P.K[2];
+            const int b0 = base[0] - (N - 1), b1 = base[1] - (N - 1),
+                      b2 = base[2] - (N - 1);
+            const T* __restrict__ grid = reinterpret_cast<const T*>(P.grid_real);
+            T g0s = 0, g1s = 0, g2s = 0;
+#pragma unroll
+            for (int a = 0; a < N; ++a) {
+                const int g0 = gwrap(b0 + a, K0);
+#pragma unroll
+                for (int b = 0; b < N; ++b) {
+                    const int g1 = gwrap(b1 + b, K1);
+                    const size_t plane = (size_t)K2 * (g1 + (size_t)K1 * g0);
+                    const T txy = th[0][a] * th[1][b];
+                    const T dxy = dth[0][a] * th[1][b];
+                    const T xdy = th[0][a] * dth[1][b];
+#pragma unroll
+                    for (int c = 0; c < N; ++c) {
+                        const int g2 = gwrap(b2 + c, K2);
+                        const T cv = __ldg(grid + plane + g2);
+                        g0s += cv * dxy * th[2][c];
+                        g1s += cv * xdy * th[2][c];
+                        g2s += cv * txy * dth[2][c];
+                    }
+                }
+            }
+            const double pref = -P.pme_fscale * q;
+            fx = pref * ((double)g0s * P.K[0] * P.invL[0]);
+            fy = pref * ((double)g1s * P.K[1] * P.invL[1]);
+            fz = pref * ((double)g2s * P.K[2] * P.invL[2]);
+        }
+        // the pair kernel has written f4 for every system this step
+        double4 f = P.f4[s];
+        f.x += fx;
+        f.y += fy;
+        f.z += fz;
+        P.f4[s] = f;
+    }
+}
+
+template <bool MIXED>
+static void spread_order(const LaunchCfg& lc, cudaStream_t s) {
+    const ItemList& il = lc.pme_atoms;
+    switch (lc.pme_order) {
+    case 3: k_pme_spread<MIXED, 3><<<il.grid, kChunk, 0, s>>>(il.d, il.n, lc.sp); break;
+    case 4: k_pme_spread<MIXED, 4><<<il.grid, kChunk, 0, s>>>(il.d, il.n, lc.sp); break;
+    case 5: k_pme_spread<MIXED, 5><<<il.grid, kChunk, 0, s>>>(il.d, il.n, lc.sp); break;
+    case 6: k_pme_spread<MIXED, 6><<<il.grid, kChunk, 0, s>>>(il.d, il.n, lc.sp); break;
+    case 7: k_pme_spread<MIXED, 7><<<il.grid, kChunk, 0, s>>>(il.d, il.n, lc.sp); break;
+    default: k_pme_spread<MIXED, 8><<<il.grid, kChunk, 0, s>>>(il.d, il.n, lc.sp); break;
+    }
+}
+
+template <bool MIXED>
+static void gather_order(const LaunchCfg& lc, cudaStream_t s) {
+    const ItemList& il = lc.pme_atoms;
+    switch (lc.pme_order) {
+    case 3: k_pme_gather<MIXED, 3><<<il.grid, kChunk, 0, s>>>(il.d, il.n, lc.sp); break;
+    case 4: k_pme_gather<MIXED, 4><<<il.grid, kChunk, 0, s>>>(il.d, il.n, lc.sp); break;
+    case 5: k_pme_gather<MIXED, 5><<<il.grid, kChunk, 0, s>>>(il.d, il.n, lc.sp); break;
+    case 6: k_pme_gather<MIXED, 6><<<il.grid, kChunk, 0, s>>>(il.d, il.n, lc.sp); break;
+    case 7: k_pme_gather<MIXED, 7><<<il.grid, kChunk, 0, s>>>(il.d, il.n, lc.sp); break;
+    default: k_pme_gather<MIXED, 8><<<il.grid, kChunk, 0, s>>>(il.d, il.n, lc.sp); break;
+    }
+}
+
+void launch_pme_spread(const LaunchCfg& lc, cudaStream_t s) {
+    if (lc.pme_mixed)
+        spread_order<true>(lc, s);
+    else
+        spread_order<false>(lc, s);
+}
+
+void launch_pme_convert(const LaunchCfg& lc, cudaStream_t s) {
+    const ItemList& il = lc.pme_real;
+    if (lc.pme_mixed)
+        k_pme_convert<true><<<il.grid, 256, 0, s>>>(il.d, il.n, lc.sp);
+    else
+        k_pme_convert<false><<<il.grid, 256, 0, s>>>(il.d, il.n, lc.sp);
+}
+
+void launch_pme_influence(const LaunchCfg& lc, cudaStream_t s) {
+    const ItemList& il = lc.pme_grid;
+    if (lc.pme_mixed)
+        k_pme_influence<true><<<il.grid, 256, 0, s>>>(il.d, il.n, lc.sp);
+    else
+        k_pme_influence<false><<<il.grid, 256, 0, s>>>(il.d, il.n, lc.sp);
+}
+
+void launch_pme_gather(const LaunchCfg& lc, cudaStream_t s) {
+    if (lc.pme_mixed)
+        gather_order<true>(lc, s);
+    else
+        gather_order<false>(lc, s);
+}
+
+} // namespace atvb

@@ -1,0 +1,216 @@
+/* atvb.h -- C ABI of the B200 classical-MD hot path (libatvb.so).
+ *
+ * Plain C types only: pointers, sizes, POD structs.  Every function returns
+ * ATVB_OK (0) or an ATVB_ERR_* code; the message of the last failure on the
+ * calling thread is atvb_last_error().  No exception crosses the boundary.
+ *
+ * Each entry point names the reference interface it replaces (paths within
+ * the Atomiverse source tree).  Units are the reference's metal units:
+ * Angstrom, eV, fs, amu, elementary charge, K (include/atomiverse/core/units.h).
+ */
+#ifndef ATVB_H
+#define ATVB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ATVB_ABI_VERSION 1
+
+#define ATVB_OK 0
+#define ATVB_ERR_INVALID 1  /* bad argument (std::invalid_argument in the reference) */
+#define ATVB_ERR_CUDA 2     /* CUDA runtime / cuFFT failure (ATV_CUDA_CHECK) */
+#define ATVB_ERR_OVERFLOW 3 /* neighbour row capacity exceeded during a step */
+#define ATVB_ERR_STATE 4    /* call out of order (e.g. step before upload) */
+#define ATVB_ERR_NOMEM 5    /* device memory budget exceeded */
+#define ATVB_ERR_NOTFOUND 6 /* unknown request / slot id */
+
+enum atvb_precision {
+    ATVB_FP64 = 0,  /* FP64 pair, PME and integrator (reference ATV_CUDA_PREC_MODE=double) */
+    ATVB_MIXED = 1  /* FP32 pair/PME math, fixed-point grid, FP64 integrator and sums */
+};
+
+enum atvb_thermostat {
+    ATVB_NVE = 0,
+    ATVB_NOSE_HOOVER = 1, /* md::NoseHoover(T, tau, dt): src/cuda/dynamics/nose_hoover.cu:29 */
+    ATVB_LANGEVIN = 2     /* md::FixLangevin(T, T, damp, dt, seed): fix_langevin.cuh */
+};
+
+typedef struct atvb_ctx atvb_ctx;
+typedef struct atvb_system atvb_system;
+typedef struct atvb_batch atvb_batch;
+typedef struct atvb_server atvb_server;
+
+typedef struct atvb_device_opts {
+    int device;          /* CUDA ordinal */
+    int reserved[7];
+} atvb_device_opts;
+
+/* One MD system: the constructor arguments of the reference components the
+ * path binds (NeighborList, PairLJCut, CoulLong, KSpacePME, VelocityVerlet,
+ * NoseHoover / FixLangevin) in one flat record. */
+typedef struct atvb_system_desc {
+    int32_t n_atoms;
+    double box[9];          /* row-major cell [A]; orthorhombic only */
+    int32_t precision;      /* atvb_precision */
+    /* NeighborList(cutoff, skin, every, delay, check): neighbor_list.cuh:98,
+     * cpu/neighbor/neighbor_list.h:79 */
+    double nl_cutoff, nl_skin;
+    int32_t nl_every, nl_delay, nl_check;
+    /* PairLJCut(epsilon, sigma, cutoff): pair_lj_cut.cuh:25 */
+    int32_t lj_enabled;
+    double lj_epsilon, lj_sigma, lj_cutoff;
+    /* CoulLong(alpha, cutoff): coul_long.cuh:24 */
+    int32_t coul_enabled;
+    double coul_alpha, coul_cutoff;
+    /* KSpacePME(alpha, grid_spacing, order): pme.cuh:26; pme_grid[] > 0
+     * overrides the spacing rule */
+    int32_t pme_enabled;
+    double pme_alpha, pme_grid_spacing;
+    int32_t pme_order;
+    int32_t pme_grid[3];
+    /* VelocityVerlet(dt) + thermostat */
+    double dt;
+    int32_t thermostat;     /* atvb_thermostat */
+    double temperature;     /* K */
+    double tau;             /* Nose-Hoover tau [fs] */
+    double damp;            /* Langevin damp [fs] */
+    uint32_t seed;          /* Langevin seed */
+    int32_t stress_required;   /* Component::set_stress_required (component.cuh:131) */
+    int32_t history_capacity;  /* per-step energy ring length (0: default 4096) */
+} atvb_system_desc;
+
+/* Host SoA view of a frame (cuda::Frame::Atoms field names,
+ * include/atomiverse/cuda/frame/frame.cuh:71-96).  Any pointer may be NULL on
+ * upload (zeros / unit mass / tag = index+1) or on download (not copied). */
+typedef struct atvb_soa_view {
+    double *x, *y, *z;
+    double *vx, *vy, *vz;
+    double *fx, *fy, *fz;
+    double *mass, *charge;
+    int32_t* type;
+    int64_t* tag;
+} atvb_soa_view;
+
+/* SystemScalars (include/atomiverse/core/system_scalars.h:17-95) plus the
+ * per-term split of the path and the thermostat state. */
+typedef struct atvb_scalars {
+    double energy;        /* total potential [eV] */
+    double energy_pair;   /* pair + long-range (the reference adds both to energy_pair) */
+    double energy_lj, energy_coul, energy_recip, energy_const;
+    double kinetic, conserved;
+    double stress[6];     /* virial xx yy zz xy xz yz [eV] */
+    double nh_xi;
+    int64_t step;
+    int64_t rebuilds;
+    int32_t max_neighbors;
+    int32_t status;       /* 0 or ATVB_ERR_OVERFLOW */
+} atvb_scalars;
+
+/* Per-kernel-group device time from CUDA events (profiling mode). */
+typedef struct atvb_kernel_time {
+    char name[32];
+    double total_ms;
+    int64_t launches;
+} atvb_kernel_time;
+
+/* ---- library ---------------------------------------------------------- */
+int atvb_abi_version(void);
+/* Thread-local message of the last failing call ("" if none). */
+const char* atvb_last_error(void);
+
+/* ---- context: device + stream (cuda::Context, context.cuh:37-149) ------ */
+int atvb_ctx_create(const atvb_device_opts* opts, atvb_ctx** out);
+int atvb_ctx_destroy(atvb_ctx* ctx);
+
+/* ---- one system: cuda::md::MD (include/atomiverse/cuda/dynamics/md.cuh) ----
+ * create      ~ MD::set_* + MD::build()               (md.cuh:118-178, 285-318)
+ * upload      ~ Backend::materialize, to_cuda          (driver.cu:34-86, transfer.cu:145)
+ * step        ~ MD::run's loop of Backend::step        (driver.cu:123-157)
+ * download    ~ Backend::retrieve, to_cpu              (driver.cu:177)
+ * run         ~ MD::run(cpu::Frame&, n): upload on first use, step, download */
+int atvb_system_create(atvb_ctx* ctx, const atvb_system_desc* desc,
+                       atvb_system** out);
+int atvb_system_destroy(atvb_system* sys);
+int atvb_system_upload(atvb_system* sys, const atvb_soa_view* frame);
+/* Force-only evaluation at the current positions (neighbour build, pair,
+ * PME, energies): the LAMMPS Verlet::setup force pass. */
+int atvb_system_compute_forces(atvb_system* sys);
+int atvb_system_step(atvb_system* sys, int32_t n_steps);
+int atvb_system_download(atvb_system* sys, atvb_soa_view* frame,
+                         atvb_scalars* scalars);
+int atvb_system_scalars(atvb_system* sys, atvb_scalars* scalars);
+int atvb_system_run(atvb_system* sys, atvb_soa_view* frame, int32_t n_steps,
+                    atvb_scalars* scalars);
+/* Energy history ring: 3 doubles per step (potential, kinetic, step).
+ * Writes up to max_steps most recent entries, oldest first; *count gets the
+ * number written. */
+int atvb_system_energy_history(atvb_system* sys, double* out,
+                               int32_t max_steps, int32_t* count);
+/* Pair set of the current neighbour list as unordered pairs (i < j) of
+ * original atom indices: the CSR half list of PairList
+ * (include/atomiverse/core/pair_list.h) flattened.  Call with pi = pj = NULL
+ * to get the count only. */
+int atvb_system_pairs(atvb_system* sys, int32_t* pi, int32_t* pj,
+                      int64_t capacity, int64_t* count);
+/* Profiling: enable per-kernel-group CUDA events on subsequent steps. */
+int atvb_system_profile(atvb_system* sys, int32_t enable);
+int atvb_system_profile_read(atvb_system* sys, atvb_kernel_time* out,
+                             int32_t capacity, int32_t* count);
+/* Lanes per atom in the pair kernel (1,2,4,8,16,32); 0 = autotune. */
+int atvb_system_set_pair_lanes(atvb_system* sys, int32_t lanes);
+/* Kernel launches this library made in the last step() call. */
+int atvb_system_launch_count(atvb_system* sys, int64_t* launches);
+/* The system's CUDA stream (cudaStream_t) for event timing by callers. */
+void* atvb_system_stream(atvb_system* sys);
+
+/* ---- batch: many independent systems in one launch per kernel ---------- */
+int atvb_batch_create(atvb_ctx* ctx, const atvb_system_desc* descs,
+                      int32_t n_systems, atvb_batch** out);
+int atvb_batch_destroy(atvb_batch* b);
+int atvb_batch_upload(atvb_batch* b, int32_t index, const atvb_soa_view* frame);
+int atvb_batch_compute_forces(atvb_batch* b);
+int atvb_batch_step(atvb_batch* b, int32_t n_steps);
+int atvb_batch_download(atvb_batch* b, int32_t index, atvb_soa_view* frame,
+                        atvb_scalars* scalars);
+/* Time candidate pair-kernel shapes on the batch's own size mix and keep
+ * the fastest; *lanes receives the choice. */
+int atvb_batch_autotune(atvb_batch* b, int32_t* lanes);
+int atvb_batch_launch_count(atvb_batch* b, int64_t* launches);
+
+/* ---- server: continuous batching of MD segments ------------------------ */
+typedef struct atvb_request_result {
+    int64_t id;
+    int32_t state;        /* 0 queued, 1 running, 2 done, 3 cancelled, 4 failed */
+    int32_t steps_done;
+    double t_submit, t_start, t_done; /* seconds on the server clock */
+    atvb_scalars scalars;
+} atvb_request_result;
+
+int atvb_server_create(atvb_ctx* ctx, size_t hbm_budget_bytes,
+                       int32_t max_active, atvb_server** out);
+int atvb_server_destroy(atvb_server* srv);
+/* Copies the frame; the request runs n_steps once admitted. */
+int atvb_server_submit(atvb_server* srv, const atvb_system_desc* desc,
+                       const atvb_soa_view* frame, int32_t n_steps,
+                       int64_t* id);
+int atvb_server_cancel(atvb_server* srv, int64_t id);
+/* One scheduling round: admit what fits, advance every running segment by
+ * `chunk` steps in one batched launch sequence, retire finished ones. */
+int atvb_server_tick(atvb_server* srv, int32_t chunk);
+int atvb_server_poll(atvb_server* srv, int64_t id, atvb_request_result* out);
+/* Copy a finished request's frame out and release it. */
+int atvb_server_collect(atvb_server* srv, int64_t id, atvb_soa_view* frame,
+                        atvb_request_result* out);
+int atvb_server_stats(atvb_server* srv, int64_t* queued, int64_t* running,
+                      int64_t* done, size_t* bytes_in_use);
+/* Device bytes one request of this shape holds while resident. */
+int atvb_request_bytes(const atvb_system_desc* desc, size_t* bytes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

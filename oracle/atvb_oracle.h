@@ -1,0 +1,112 @@
+/* atvb_oracle.h -- CPU FP64 restatement of the Atomiverse classical-MD hot
+ * path.  TEST INFRASTRUCTURE ONLY: the parity tests, the smoke check and the
+ * CPU-baseline leg of bench.py call it as the checker.  The product path
+ * (libatvb.so) never links, loads or calls anything in this directory.
+ *
+ * Each function names the reference file:line whose algorithm it restates
+ * (paths are relative to the Atomiverse source tree).  Units are the
+ * reference's "metal" set: Angstrom, eV, fs, amu, e, K.
+ */
+#ifndef ATVB_ORACLE_H
+#define ATVB_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* include/atomiverse/core/units.h:138,165,166,173 */
+#define ORC_KB 8.617333262e-5
+#define ORC_FTM2V (1.0 / 103.6427)
+#define ORC_MVV2E 103.6427
+#define ORC_QQR2E 14.399645
+#define ORC_PI 3.14159265358979323846
+
+enum { ORC_THERMO_NONE = 0, ORC_THERMO_NH = 1, ORC_THERMO_LANGEVIN = 2 };
+
+typedef struct orc_desc {
+    int n;                 /* atoms */
+    double L[3];           /* orthorhombic box edges [A] */
+    double nl_cutoff;      /* NeighborList cutoff [A] */
+    double skin;           /* NeighborList skin [A] */
+    int nl_every, nl_delay, nl_check; /* LAMMPS neigh_modify */
+    int has_lj;
+    double lj_eps, lj_sigma, lj_rc;
+    int has_coul;
+    double coul_alpha, coul_rc;
+    int has_pme;
+    double pme_alpha;
+    int pme_K[3];
+    int pme_order;
+    double dt;             /* fs */
+    int thermostat;        /* ORC_THERMO_* */
+    double T, tau, damp;   /* K, fs (NH tau), fs (Langevin damp) */
+    uint32_t seed;         /* Langevin seed */
+    int need_virial;
+} orc_desc;
+
+typedef struct orc_sys orc_sys;
+
+/* Scalars layout returned by orc_scalars (all eV unless noted):
+ * [0] energy (total potential)  [1] e_lj  [2] e_coul_real  [3] e_recip
+ * [4] e_self+e_net              [5] kinetic
+ * [6..11] virial xx yy zz xy xz yz   [12] NH xi  [13] step  [14] rebuilds */
+#define ORC_NSCALARS 15
+
+orc_sys* orc_create(const orc_desc* d);
+void orc_destroy(orc_sys* s);
+void orc_set_threads(int n);
+int orc_get_threads(void);
+
+/* Host arrays of length n. Positions are wrapped into [0, L) on entry. */
+void orc_set_state(orc_sys* s, const double* x, const double* y,
+                   const double* z, const double* vx, const double* vy,
+                   const double* vz, const double* fx, const double* fy,
+                   const double* fz, const double* mass, const double* q,
+                   const int64_t* tag);
+void orc_get_state(const orc_sys* s, double* x, double* y, double* z,
+                   double* vx, double* vy, double* vz, double* fx, double* fy,
+                   double* fz);
+void orc_scalars(const orc_sys* s, double* out);
+
+/* Half Verlet list at the current positions (cell_list.cpp:743-895
+ * semantics): unordered pairs {i<j} with min-image r^2 < (cutoff+skin)^2.
+ * Returns the pair count. */
+int64_t orc_build_list(orc_sys* s);
+void orc_get_pairs(const orc_sys* s, int32_t* pi, int32_t* pj);
+
+/* Zero forces/energy/virial, then LJ + CoulLong + PME at current positions
+ * over the current list (pre_force + force phases). */
+void orc_compute_forces(orc_sys* s);
+
+/* n MD steps in the LAMMPS Verlet order (runtime.cpp:452-501).  If hist is
+ * non-NULL it receives 2 doubles per step: potential and kinetic energy at
+ * end_of_step.  Returns the number of neighbour rebuilds. */
+int orc_run(orc_sys* s, int n_steps, double* hist);
+
+/* ---- standalone pieces used by the known-answer tests ---- */
+void orc_bspline(double frac, int n, double* theta, double* dtheta);
+int orc_good_fft_size(int n);
+void orc_spline_moduli(int K, int n, double* mod);
+/* in-place 3D complex FFT, data interleaved re/im, layout k2 + K2*(k1+K1*k0);
+ * sign -1 = forward (FFTW_FORWARD), +1 = backward (unnormalised). */
+void orc_fft3d(int K0, int K1, int K2, double* data, int sign);
+/* Reciprocal-space Ewald with self and net-charge terms (ewald_sum.h). */
+void orc_ewald_recip(int n, const double* x, const double* y, const double* z,
+                     const double* q, const double L[3], double alpha,
+                     double accuracy, double* energy, double* fx, double* fy,
+                     double* fz, double* virial);
+/* PME reciprocal + self + net energy/forces/virial (pme.cpp:152-253). */
+void orc_pme(int n, const double* x, const double* y, const double* z,
+             const double* q, const double L[3], double alpha, const int K[3],
+             int order, double* energy, double* fx, double* fy, double* fz,
+             double* virial);
+/* Langevin Gaussian triple for (seed, step, tag): fix_langevin.cpp:37-62,
+ * 112-140. */
+void orc_gauss3(uint32_t seed, int64_t step, int64_t tag, double* out3);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

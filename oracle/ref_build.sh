@@ -1,0 +1,17 @@
+#!/bin/sh
+# Compile the reference's own header-only PME math from the reference tree
+# (never copied into this repository) into oracle/_ref/libref_pme.so.
+# Test infrastructure: the oracle's restatement is checked against it.
+# Usage: oracle/ref_build.sh [REFERENCE_ROOT]   (default /root/reference)
+set -e
+here=$(cd "$(dirname "$0")" && pwd)
+ref=${1:-/root/reference}
+if [ ! -f "$ref/include/atomiverse/cpu/longrange/pme_spline.h" ]; then
+    echo "reference tree not found at $ref; skipping" >&2
+    exit 0
+fi
+mkdir -p "$here/_ref"
+g++ -std=c++20 -O2 -ffp-contract=off -fPIC -shared \
+    -I "$here/ref_shim" -I "$ref/include" \
+    "$here/ref_pme_wrap.cpp" -o "$here/_ref/libref_pme.so"
+echo "built $here/_ref/libref_pme.so"
