@@ -92,6 +92,7 @@ def scalars_dict(s: Scalars) -> dict:
         "energy_const": s.energy_const, "kinetic": s.kinetic, "conserved": s.conserved,
         "stress": np.array(list(s.stress)), "nh_xi": s.nh_xi, "step": s.step,
         "rebuilds": s.rebuilds, "max_neighbors": s.max_neighbors, "status": s.status,
+        "list_pairs": s.list_pairs,
     }
 
 
@@ -149,6 +150,15 @@ class System:
 
     def step(self, n: int):
         check(self.lib.atvb_system_step(self._h, int(n)))
+
+    def step_timed(self, n: int) -> tuple[float, np.ndarray]:
+        """n steps timed with CUDA events on the system's stream: (total
+        ms, per-step ms)."""
+        per = np.zeros(int(n))
+        tot = C.c_double()
+        check(self.lib.atvb_system_step_timed(
+            self._h, int(n), per.ctypes.data_as(C.POINTER(C.c_double)), C.byref(tot)))
+        return tot.value, per
 
     def download(self, keys=FRAME_KEYS) -> tuple[dict, dict]:
         out = {k: np.zeros(self.n) for k in keys}

@@ -86,6 +86,7 @@ class Scalars(C.Structure):
         ("rebuilds", C.c_int64),
         ("max_neighbors", C.c_int32),
         ("status", C.c_int32),
+        ("list_pairs", C.c_int64),
     ]
 
 
@@ -117,6 +118,7 @@ SIGNATURES = {
     "atvb_system_upload": (C.c_int, [_vp, C.POINTER(SoaView)]),
     "atvb_system_compute_forces": (C.c_int, [_vp]),
     "atvb_system_step": (C.c_int, [_vp, C.c_int32]),
+    "atvb_system_step_timed": (C.c_int, [_vp, C.c_int32, _dp, _dp]),
     "atvb_system_download": (C.c_int, [_vp, C.POINTER(SoaView), C.POINTER(Scalars)]),
     "atvb_system_scalars": (C.c_int, [_vp, C.POINTER(Scalars)]),
     "atvb_system_run": (C.c_int, [_vp, C.POINTER(SoaView), C.c_int32, C.POINTER(Scalars)]),

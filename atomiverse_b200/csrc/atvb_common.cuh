@@ -58,6 +58,7 @@ struct SysState {
     int overflow;      // neighbour row overflowed its capacity
     int max_nnbr;      // largest row seen at the last build
     int status;        // sticky error bits
+    unsigned long long list_entries; // row entries of the last build (2 x pairs)
 };
 
 struct SysParams {

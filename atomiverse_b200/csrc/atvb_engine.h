@@ -89,6 +89,7 @@ class Engine {
     void compute_forces();
     void compute_forces_one(int id);
     void step(int n);
+    void step_timed(int n, double* step_ms, double* total_ms);
     void download(int id, atvb_soa_view* f, atvb_scalars* sc);
     void scalars(int id, atvb_scalars* out);
     int64_t pairs(int id, int32_t* pi, int32_t* pj, int64_t capacity);

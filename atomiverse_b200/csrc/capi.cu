@@ -129,6 +129,18 @@ int atvb_system_step(atvb_system* sys, int32_t n_steps) {
     });
 }
 
+int atvb_system_step_timed(atvb_system* sys, int32_t n_steps, double* step_ms,
+                           double* total_ms) {
+    return guard([&] {
+        need(sys, "sys");
+        if (!sys->uploaded)
+            throw Error(ATVB_ERR_STATE, "step before upload");
+        if (n_steps < 1)
+            throw Error(ATVB_ERR_INVALID, "n_steps must be >= 1");
+        sys->eng->step_timed(n_steps, step_ms, total_ms);
+    });
+}
+
 int atvb_system_download(atvb_system* sys, atvb_soa_view* frame,
                          atvb_scalars* scalars) {
     return guard([&] {

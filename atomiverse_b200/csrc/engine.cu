@@ -864,6 +864,35 @@ void Engine::step(int n) {
     steps_since_check_ += n;
 }
 
+void Engine::step_timed(int n, double* step_ms, double* total_ms) {
+    CK(cudaSetDevice(device_));
+    ensure_ready();
+    if (profiling_)
+        throw Error(ATVB_ERR_STATE, "step_timed is not available in profiling mode");
+    step(0); // capture the graph outside the timed span
+    std::vector<cudaEvent_t> ev(n + 1);
+    for (auto& e : ev)
+        CK(cudaEventCreate(&e));
+    CK(cudaEventRecord(ev[0], stream_));
+    for (int k = 0; k < n; ++k) {
+        CK(cudaGraphLaunch(gexec_, stream_));
+        CK(cudaEventRecord(ev[k + 1], stream_));
+    }
+    CK(cudaEventSynchronize(ev[n]));
+    float ms = 0.f;
+    if (step_ms)
+        for (int k = 0; k < n; ++k) {
+            CK(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
+            step_ms[k] = ms;
+        }
+    CK(cudaEventElapsedTime(&ms, ev[0], ev[n]));
+    if (total_ms)
+        *total_ms = ms;
+    for (auto& e : ev)
+        cudaEventDestroy(e);
+    last_launches_ = kernels_per_step() * n;
+}
+
 void Engine::collect_profile() {
     CK(cudaStreamSynchronize(stream_));
     for (size_t k = 0; k + 1 < prof_used_; ++k) {
@@ -1110,6 +1139,7 @@ void Engine::scalars(int id, atvb_scalars* out) {
     out->rebuilds = st.rebuilds;
     out->max_neighbors = st.max_nnbr;
     out->status = st.overflow ? ATVB_ERR_OVERFLOW : 0;
+    out->list_pairs = (int64_t)(st.list_entries / 2);
 }
 
 void Engine::download(int id, atvb_soa_view* f, atvb_scalars* sc) {

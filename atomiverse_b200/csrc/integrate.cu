@@ -140,6 +140,7 @@ __global__ void k_sys_a(const int* sys_list, int nsys, const SysParams* sp) {
         st->ago = 0;
         st->rebuilds += 1;
         st->max_nnbr = 0;
+        st->list_entries = 0ull;
     }
 }
 
@@ -252,6 +253,7 @@ __global__ void k_force_rebuild(const int* sys_list, int nsys,
     st->rebuild = 1;
     st->ago = 0;
     st->max_nnbr = 0;
+    st->list_entries = 0ull;
 }
 
 // After an upload: wrap positions into [0, L) (pbc.h:48-50) and keep the

@@ -259,6 +259,7 @@ __global__ void __launch_bounds__(256)
             if (lane == 0) {
                 P.nnbr[s] = cnt < cap ? cnt : cap;
                 atomicMax(&P.st->max_nnbr, cnt);
+                atomicAdd(&P.st->list_entries, (unsigned long long)cnt);
                 if (cnt > cap)
                     atomicOr(&P.st->overflow, 1);
             }

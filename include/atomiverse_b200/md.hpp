@@ -1,0 +1,229 @@
+// md.hpp -- the reference's CUDA MD surface (cuda::md::MD and its
+// components) as a header-only C++ layer over the C ABI in atvb.h.
+//
+// Component constructors keep the reference signatures:
+//   NeighborList(cutoff, skin = -1, every = 1, delay = 0, check = true)
+//       include/atomiverse/cuda/neighbor/neighbor_list.cuh:98
+//   PairLJCut(epsilon, sigma, cutoff)       cuda/potentials/pair_lj_cut.cuh:25
+//   CoulLong(alpha, cutoff)                 cuda/potentials/coul_long.cuh:24
+//   KSpacePME(alpha, grid_spacing = 1.0, order = 6)  cuda/longrange/pme.cuh:26
+//   md::VelocityVerlet(dt), md::NoseHoover(T, tau, dt),
+//   md::FixLangevin(T_start, T_stop, damp, dt, seed)
+// and MD keeps set_neighbor / set_evaluator / set_integrator /
+// set_thermostat and the continuable run(frame, n_steps)
+// (include/atomiverse/cuda/dynamics/md.cuh:118-385).  Errors surface as
+// std::invalid_argument (bad configuration) or std::runtime_error (CUDA),
+// as in the reference.  The components only record their parameters: the
+// device step is one fused, graph-captured sequence built by the library.
+#pragma once
+
+#include <atvb.h>
+
+#include <cstdint>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace atvb_cpp {
+
+inline void check(int rc) {
+    if (rc == ATVB_OK)
+        return;
+    const std::string msg = atvb_last_error();
+    if (rc == ATVB_ERR_INVALID)
+        throw std::invalid_argument(msg);
+    throw std::runtime_error(msg);
+}
+
+/// Host frame: SoA arrays named like cuda::Frame::Atoms plus the box.
+struct Frame {
+    std::vector<double> x, y, z, vx, vy, vz, fx, fy, fz, mass, charge;
+    std::vector<int64_t> tag;
+    double box[3] = {0, 0, 0};
+    int n() const { return (int)x.size(); }
+    void resize(int n) {
+        for (auto* v : {&x, &y, &z, &vx, &vy, &vz, &fx, &fy, &fz, &mass, &charge})
+            v->resize(n, 0.0);
+        mass.assign(n, 1.0);
+        tag.resize(n);
+        for (int i = 0; i < n; ++i)
+            tag[i] = i + 1;
+    }
+    atvb_soa_view view() {
+        atvb_soa_view v{};
+        v.x = x.data(); v.y = y.data(); v.z = z.data();
+        v.vx = vx.data(); v.vy = vy.data(); v.vz = vz.data();
+        v.fx = fx.data(); v.fy = fy.data(); v.fz = fz.data();
+        v.mass = mass.data(); v.charge = charge.data(); v.tag = tag.data();
+        return v;
+    }
+};
+
+struct NeighborList {
+    double cutoff, skin;
+    int every, delay;
+    bool check;
+    explicit NeighborList(double cutoff_, double skin_ = -1.0, int every_ = 1,
+                          int delay_ = 0, bool check_ = true)
+        : cutoff(cutoff_), skin(skin_), every(every_), delay(delay_), check(check_) {}
+};
+struct PairLJCut {
+    double epsilon, sigma, cutoff;
+    PairLJCut(double e, double s, double c) : epsilon(e), sigma(s), cutoff(c) {
+        if (c <= 0.0)
+            throw std::invalid_argument("PairLJCut: cutoff must be positive");
+    }
+};
+struct CoulLong {
+    double alpha, cutoff;
+    CoulLong(double a, double c) : alpha(a), cutoff(c) {
+        if (a <= 0.0 || c <= 0.0)
+            throw std::invalid_argument("CoulLong: alpha and cutoff must be > 0");
+    }
+};
+struct KSpacePME {
+    double alpha, grid_spacing;
+    int order;
+    int grid[3] = {0, 0, 0};
+    explicit KSpacePME(double a, double spacing = 1.0, int order_ = 6)
+        : alpha(a), grid_spacing(spacing), order(order_) {
+        if (a <= 0.0)
+            throw std::invalid_argument("KSpacePME: alpha must be > 0");
+        if (spacing <= 0.0)
+            throw std::invalid_argument("KSpacePME: grid_spacing must be > 0");
+        if (order_ < 3)
+            throw std::invalid_argument("KSpacePME: order must be >= 3");
+    }
+};
+
+namespace md {
+struct VelocityVerlet {
+    double dt;
+    explicit VelocityVerlet(double dt_) : dt(dt_) {}
+};
+struct NoseHoover {
+    double T, tau, dt;
+    NoseHoover(double T_, double tau_, double dt_) : T(T_), tau(tau_), dt(dt_) {}
+};
+struct FixLangevin {
+    double T_start, T_stop, damp, dt;
+    uint32_t seed;
+    FixLangevin(double t0, double t1, double damp_, double dt_, uint32_t seed_)
+        : T_start(t0), T_stop(t1 < 0 ? t0 : t1), damp(damp_), dt(dt_), seed(seed_) {}
+};
+
+/// cuda::md::MD: categorical setters, then run(frame, n) -- continuable.
+class MD {
+  public:
+    explicit MD(int device = 0, int precision = ATVB_FP64) : precision_(precision) {
+        atvb_device_opts o{};
+        o.device = device;
+        check(atvb_ctx_create(&o, &ctx_));
+        std::memset(&d_, 0, sizeof(d_));
+        d_.nl_skin = -1.0;
+        d_.nl_every = 1;
+        d_.pme_order = 4;
+    }
+    ~MD() {
+        if (sys_)
+            atvb_system_destroy(sys_);
+        if (ctx_)
+            atvb_ctx_destroy(ctx_);
+    }
+    MD(const MD&) = delete;
+    MD& operator=(const MD&) = delete;
+
+    MD& set_neighbor(const NeighborList& nl) {
+        d_.nl_cutoff = nl.cutoff;
+        d_.nl_skin = nl.skin;
+        d_.nl_every = nl.every;
+        d_.nl_delay = nl.delay;
+        d_.nl_check = nl.check ? 1 : 0;
+        have_nl_ = true;
+        return *this;
+    }
+    MD& set_evaluator(const PairLJCut& p) {
+        d_.lj_enabled = 1;
+        d_.lj_epsilon = p.epsilon;
+        d_.lj_sigma = p.sigma;
+        d_.lj_cutoff = p.cutoff;
+        have_pair_ = true;
+        return *this;
+    }
+    MD& set_evaluator(const CoulLong& c) {
+        d_.coul_enabled = 1;
+        d_.coul_alpha = c.alpha;
+        d_.coul_cutoff = c.cutoff;
+        have_pair_ = true;
+        return *this;
+    }
+    MD& set_evaluator(const KSpacePME& k) {
+        d_.pme_enabled = 1;
+        d_.pme_alpha = k.alpha;
+        d_.pme_grid_spacing = k.grid_spacing;
+        d_.pme_order = k.order;
+        for (int i = 0; i < 3; ++i)
+            d_.pme_grid[i] = k.grid[i];
+        return *this;
+    }
+    MD& set_integrator(const VelocityVerlet& v) {
+        if (have_integrator_ && v.dt != d_.dt)
+            throw std::invalid_argument("set_integrator already configured");
+        d_.dt = v.dt;
+        have_integrator_ = true;
+        return *this;
+    }
+    MD& set_thermostat(const NoseHoover& t) {
+        d_.thermostat = ATVB_NOSE_HOOVER;
+        d_.temperature = t.T;
+        d_.tau = t.tau;
+        return *this;
+    }
+    MD& set_thermostat(const FixLangevin& t) {
+        if (t.T_stop != t.T_start)
+            throw std::invalid_argument("FixLangevin: temperature ramps are not supported");
+        d_.thermostat = ATVB_LANGEVIN;
+        d_.temperature = t.T_start;
+        d_.damp = t.damp;
+        d_.seed = t.seed;
+        return *this;
+    }
+    MD& set_stress_required(bool on) {
+        d_.stress_required = on ? 1 : 0;
+        return *this;
+    }
+
+    /// Advance n_steps; the first call uploads `frame`, every call leaves the
+    /// device state in `frame` (MD::run, md.cuh:155-178).
+    atvb_scalars run(Frame& frame, int n_steps) {
+        if (!have_integrator_)
+            throw std::invalid_argument("MD: set_integrator is required");
+        if (have_pair_ && !have_nl_)
+            throw std::invalid_argument(
+                "cuda::md::MD: Add `sim.set_neighbor(cuda::NeighborList{cutoff})`.");
+        if (!sys_) {
+            d_.n_atoms = frame.n();
+            d_.precision = precision_;
+            for (int k = 0; k < 9; ++k)
+                d_.box[k] = 0.0;
+            d_.box[0] = frame.box[0];
+            d_.box[4] = frame.box[1];
+            d_.box[8] = frame.box[2];
+            check(atvb_system_create(ctx_, &d_, &sys_));
+        }
+        atvb_soa_view v = frame.view();
+        atvb_scalars s{};
+        check(atvb_system_run(sys_, &v, n_steps, &s));
+        return s;
+    }
+
+  private:
+    atvb_ctx* ctx_ = nullptr;
+    atvb_system* sys_ = nullptr;
+    atvb_system_desc d_;
+    int precision_;
+    bool have_nl_ = false, have_pair_ = false, have_integrator_ = false;
+};
+} // namespace md
+} // namespace atvb_cpp

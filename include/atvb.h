@@ -108,6 +108,7 @@ typedef struct atvb_scalars {
     int64_t rebuilds;
     int32_t max_neighbors;
     int32_t status;       /* 0 or ATVB_ERR_OVERFLOW */
+    int64_t list_pairs;   /* unordered pairs in the current list (cutoff + skin) */
 } atvb_scalars;
 
 /* Per-kernel-group device time from CUDA events (profiling mode). */
@@ -140,6 +141,11 @@ int atvb_system_upload(atvb_system* sys, const atvb_soa_view* frame);
  * PME, energies): the LAMMPS Verlet::setup force pass. */
 int atvb_system_compute_forces(atvb_system* sys);
 int atvb_system_step(atvb_system* sys, int32_t n_steps);
+/* atvb_system_step with a CUDA event on the system's stream before the
+ * first step and after every step; step_ms (n_steps entries, may be NULL)
+ * gets each step's device time, *total_ms the whole span.  Synchronises. */
+int atvb_system_step_timed(atvb_system* sys, int32_t n_steps, double* step_ms,
+                           double* total_ms);
 int atvb_system_download(atvb_system* sys, atvb_soa_view* frame,
                          atvb_scalars* scalars);
 int atvb_system_scalars(atvb_system* sys, atvb_scalars* scalars);
