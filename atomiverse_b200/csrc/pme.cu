@@ -56,6 +56,18 @@ ATVB_DEV int gwrap(int g, int K) {
     return g;
 }
 
+// Grid base point of a floored fractional coordinate.  The modulo above can
+// round up to exactly K for a coordinate just below zero, and a non-finite
+// position floors to NaN: both map to an in-range point so a corrupted
+// state produces garbage energies, never an out-of-bounds grid access.
+ATVB_DEV int base_index(double u0, int K) {
+    if (!(u0 >= 0.0))
+        return 0;
+    if (u0 >= (double)K)
+        return u0 < 2.0 * K ? (int)(u0 - K) : 0;
+    return (int)u0;
+}
+
 // Fractional grid coordinate, base point and B-spline weights of one atom.
 template <bool MIXED, int N, typename T>
 ATVB_DEV void atom_splines(const SysParams& P, int s, T th[3][N], T dth[3][N],
@@ -85,7 +97,7 @@ ATVB_DEV void atom_splines(const SysParams& P, int s, T th[3][N], T dth[3][N],
             double u = sd * P.K[d];
             u -= floor(u / P.K[d]) * P.K[d];
             const double u0 = floor(u);
-            base[d] = (int)u0;
+            base[d] = base_index(u0, P.K[d]);
             bspline_dev<N, T>((T)(u - u0), th[d], dth[d]);
         }
     }
