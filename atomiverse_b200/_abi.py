@@ -151,6 +151,7 @@ SIGNATURES = {
     "atvb_server_stats": (C.c_int, [_vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64),
                                     C.POINTER(C.c_int64), C.POINTER(C.c_size_t)]),
     "atvb_request_bytes": (C.c_int, [C.POINTER(SystemDesc), C.POINTER(C.c_size_t)]),
+    "atvb_pair_forces_static": (C.c_int, [C.POINTER(SystemDesc)] + [C.c_void_p] * 9),
 }
 
 _lib = None

@@ -216,6 +216,27 @@ int atvb_server_stats(atvb_server* srv, int64_t* queued, int64_t* running,
 /* Device bytes one request of this shape holds while resident. */
 int atvb_request_bytes(const atvb_system_desc* desc, size_t* bytes);
 
+/* ---- allocation-free pair forces -------------------------------------- *
+ * No counterpart in the reference: a stand-alone evaluation of the
+ * short-range pair term (shifted LJ + real-space Ewald erfc Coulomb, FP64)
+ * that allocates nothing.  x, y, z, q (n_atoms each; q may be NULL without
+ * Coulomb) are DEVICE pointers read on `stream` (a cudaStream_t, NULL = the
+ * legacy default stream); fx, fy, fz (device, n_atoms) are overwritten with
+ * the pair forces; energy (device, 2 doubles: LJ, Coulomb real space; may be
+ * NULL) is overwritten.  Only n_atoms, box, precision (ATVB_FP64),
+ * lj_* / coul_* and pme_enabled (must be 0) of the descriptor are read.
+ * Limits: n_atoms <= 65536, at most 65536 cells of edge >= the cutoff,
+ * orthorhombic box with every edge > 2 x cutoff; anything else returns
+ * ATVB_ERR_INVALID before any launch.  Scratch is one fixed device array
+ * per device: calls on the same device must not overlap in time (use one
+ * stream or order the streams).  The first call on a device resolves the
+ * scratch address; make it outside any stream capture.  Asynchronous: no
+ * synchronisation, no host<->device copy. */
+int atvb_pair_forces_static(const atvb_system_desc* desc, const double* x,
+                            const double* y, const double* z, const double* q,
+                            double* fx, double* fy, double* fz, double* energy,
+                            void* stream);
+
 #ifdef __cplusplus
 }
 #endif
