@@ -58,6 +58,7 @@ class Slot {
     bool uploaded = false;
     size_t bytes = 0;
     int max_row = 0;
+    int lanes = 4;  // pair-kernel lanes per atom for this system
     double mean_row = 0.0;
     double erfcx_err = 0.0; // max relative error of the FP64 erfcx fit
     cufftHandle plan_f = 0, plan_i = 0;
@@ -114,7 +115,7 @@ class Engine {
     void push_params(int id);
     void build_lists();
     void ensure_ready();
-    int choose_lanes() const;
+    int lanes_for(const Slot& s) const;
     bool check_lists(const LaunchCfg& lc);
     void sized_rebuild(const LaunchCfg& lc);
     LaunchCfg restricted_cfg(int id);

@@ -9,6 +9,7 @@ namespace atvb {
 constexpr int kChunk = 256;     // atoms per item of the per-atom kernels
 constexpr int kListChunk = 8;   // atoms per item of the list build (warp/atom)
 constexpr int kGridChunk = 4096; // grid points per item of the PME grid kernels
+constexpr int kLaneClasses = 6;  // pair lanes per atom: 1, 2, 4, 8, 16, 32
 
 struct ItemList {
     const Item* d = nullptr; // device array
@@ -20,14 +21,17 @@ struct LaunchCfg {
     const SysParams* sp = nullptr; // device table of every system
     ItemList atoms;     // kChunk atoms per item (original or sorted order)
     ItemList list;      // kListChunk atoms per item
-    ItemList pair;      // kChunk / pair_G atoms per item
+    // pair work by [precision][log2 lanes]: each system has its own lane
+    // count, chosen from that system alone, so its forces and energies do
+    // not depend on which other systems share the engine
+    ItemList pair[2][kLaneClasses];
     ItemList cells;     // kChunk cells per item
     ItemList pme_atoms; // kChunk atoms of PME systems
     ItemList pme_grid;  // kGridChunk half-complex grid points per item
     ItemList pme_real;  // kGridChunk real grid points per item
     const int* sys_list = nullptr; // device list of system indices
     int nsys = 0;
-    int pair_G = 4;     // lanes per atom in the pair kernel
+    int pair_G = 4;     // lanes per atom of the largest system (reported)
     int any_mixed = 0, any_fp64 = 0;
     int pme_order = 4;  // common PME order (the PME kernels are templated)
     int pme_mixed = 0;

@@ -647,29 +647,28 @@ static ItemList make_list(std::vector<void*>& allocs, const std::vector<Item>& v
     return il;
 }
 
-int Engine::choose_lanes() const {
+// Lanes per atom for one system, from that system alone: enough lanes to
+// fill the GPU with this system's atoms, but no more than its rows can keep
+// busy (at least 8 row entries per lane).
+int Engine::lanes_for(const Slot& sl) const {
     if (lanes_fixed_ > 0)
         return lanes_fixed_;
-    long long n_tot = 0;
-    double row = 0.0;
-    int cnt = 0;
-    for (const auto& s : slots_)
-        if (s && s->uploaded) {
-            n_tot += s->hp.n;
-            row += s->mean_row;
-            ++cnt;
-        }
-    if (cnt == 0)
-        return 4;
-    row /= cnt;
+    const long long n = sl.hp.n;
     const long long target = (long long)num_sms_ * 2048 * 2;
     int G = 1;
-    while (G < 32 && n_tot * G < target)
+    while (G < 32 && n * G < target)
         G *= 2;
     int gmax = 1;
-    while (gmax < 32 && gmax * 8 <= row)
+    while (gmax < 32 && gmax * 8 <= sl.mean_row)
         gmax *= 2;
     return std::max(1, std::min(G, gmax));
+}
+
+static int lane_class(int G) {
+    int k = 0;
+    while ((1 << k) < G)
+        ++k;
+    return k;
 }
 
 void Engine::build_lists() {
@@ -677,11 +676,11 @@ void Engine::build_lists() {
     for (void* p : list_allocs_)
         cudaFree(p);
     list_allocs_.clear();
-    std::vector<Item> atoms, list, pair, cells, patoms, pgrid, preal;
+    std::vector<Item> atoms, list, cells, patoms, pgrid, preal;
     std::vector<int> sys;
+    std::vector<Item> pair_by[2][kLaneClasses];
     lc_ = LaunchCfg{};
-    lc_.pair_G = choose_lanes();
-    const int pchunk = kChunk / lc_.pair_G;
+    int largest = -1;
     pme_slots_.clear();
     int pme_prec = -1, pme_order = -1;
     for (const auto& sp : slots_) {
@@ -694,8 +693,16 @@ void Engine::build_lists() {
             atoms.push_back({k, b});
         for (int b = 0; b < P.n; b += kListChunk)
             list.push_back({k, b});
-        for (int b = 0; b < P.n; b += pchunk)
-            pair.push_back({k, b});
+        sp->lanes = lanes_for(*sp);
+        if (P.n > largest) {
+            largest = P.n;
+            lc_.pair_G = sp->lanes;
+        }
+        {
+            std::vector<Item>& pv = pair_by[P.prec == kMixed ? 1 : 0][lane_class(sp->lanes)];
+            for (int b = 0; b < P.n; b += kChunk / sp->lanes)
+                pv.push_back({k, b});
+        }
         for (int b = 0; b < P.ncell; b += kChunk)
             cells.push_back({k, b});
         if (P.prec == kMixed)
@@ -724,7 +731,9 @@ void Engine::build_lists() {
     lc_.sp = d_sp_;
     lc_.atoms = make_list(list_allocs_, atoms, g_light, stream_);
     lc_.list = make_list(list_allocs_, list, num_sms_ * 32, stream_);
-    lc_.pair = make_list(list_allocs_, pair, num_sms_ * 16, stream_);
+    for (int p = 0; p < 2; ++p)
+        for (int c = 0; c < kLaneClasses; ++c)
+            lc_.pair[p][c] = make_list(list_allocs_, pair_by[p][c], num_sms_ * 16, stream_);
     lc_.cells = make_list(list_allocs_, cells, g_light, stream_);
     lc_.pme_atoms = make_list(list_allocs_, patoms, g_light, stream_);
     lc_.pme_grid = make_list(list_allocs_, pgrid, g_light, stream_);
@@ -752,7 +761,9 @@ int64_t Engine::kernels_per_step() const {
     int64_t k = 0;
     k += 2;                                   // integrate_a, sys_a
     k += 6;                                   // rebuild pipeline
-    k += (lc_.any_fp64 ? 1 : 0) + (lc_.any_mixed ? 1 : 0); // pair
+    for (int p = 0; p < 2; ++p)                // pair: one per lane class used
+        for (int c = 0; c < kLaneClasses; ++c)
+            k += lc_.pair[p][c].n ? 1 : 0;
     if (!pme_slots_.empty())
         k += 4;                               // spread, convert, influence, gather
     k += 2;                                   // integrate_b, sys_b
@@ -997,7 +1008,7 @@ LaunchCfg Engine::restricted_cfg(int id) {
         list.push_back({id, b});
     for (int b = 0; b < P.ncell; b += kChunk)
         cells.push_back({id, b});
-    const int pchunk = kChunk / lc_.pair_G;
+    const int pchunk = kChunk / s->lanes;
     for (int b = 0; b < P.n; b += pchunk)
         pair.push_back({id, b});
     if (P.has_pme) {
@@ -1015,7 +1026,11 @@ LaunchCfg Engine::restricted_cfg(int id) {
     c.atoms = make_list(list_allocs_, atoms, num_sms_ * 16, stream_);
     c.list = make_list(list_allocs_, list, num_sms_ * 32, stream_);
     c.cells = make_list(list_allocs_, cells, num_sms_ * 16, stream_);
-    c.pair = make_list(list_allocs_, pair, num_sms_ * 16, stream_);
+    for (int p = 0; p < 2; ++p)
+        for (int k = 0; k < kLaneClasses; ++k)
+            c.pair[p][k] = ItemList{};
+    c.pair[P.prec == kMixed ? 1 : 0][lane_class(s->lanes)] =
+        make_list(list_allocs_, pair, num_sms_ * 16, stream_);
     c.pme_atoms = make_list(list_allocs_, patoms, num_sms_ * 16, stream_);
     c.pme_grid = make_list(list_allocs_, pgrid, num_sms_ * 16, stream_);
     c.pme_real = make_list(list_allocs_, preal, num_sms_ * 16, stream_);

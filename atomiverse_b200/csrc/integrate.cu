@@ -254,6 +254,11 @@ __global__ void k_force_rebuild(const int* sys_list, int nsys,
     st->ago = 0;
     st->max_nnbr = 0;
     st->list_entries = 0ull;
+    // a force pass outside the step loop starts its energy and virial sums
+    // from zero, whatever ran before it (e.g. autotuning launches)
+    st->acc[kAccELJ] = st->acc[kAccECoul] = st->acc[kAccERecip] = 0ull;
+    for (int v = 0; v < 6; ++v)
+        st->acc[kAccVir + v] = 0ull;
 }
 
 // After an upload: wrap positions into [0, L) (pbc.h:48-50) and keep the

@@ -302,34 +302,24 @@ __global__ void __launch_bounds__(256)
 
 template <bool MIXED>
 static void launch_pair_prec(const LaunchCfg& lc, cudaStream_t s) {
-    const int grid = lc.pair.grid;
-    switch (lc.pair_G) {
-    case 1:
-        k_pair<MIXED, 1><<<grid, 256, 0, s>>>(lc.pair.d, lc.pair.n, lc.sp);
-        break;
-    case 2:
-        k_pair<MIXED, 2><<<grid, 256, 0, s>>>(lc.pair.d, lc.pair.n, lc.sp);
-        break;
-    case 4:
-        k_pair<MIXED, 4><<<grid, 256, 0, s>>>(lc.pair.d, lc.pair.n, lc.sp);
-        break;
-    case 8:
-        k_pair<MIXED, 8><<<grid, 256, 0, s>>>(lc.pair.d, lc.pair.n, lc.sp);
-        break;
-    case 16:
-        k_pair<MIXED, 16><<<grid, 256, 0, s>>>(lc.pair.d, lc.pair.n, lc.sp);
-        break;
-    default:
-        k_pair<MIXED, 32><<<grid, 256, 0, s>>>(lc.pair.d, lc.pair.n, lc.sp);
-        break;
-    }
+    const ItemList* L = lc.pair[MIXED ? 1 : 0];
+    if (L[0].n)
+        k_pair<MIXED, 1><<<L[0].grid, 256, 0, s>>>(L[0].d, L[0].n, lc.sp);
+    if (L[1].n)
+        k_pair<MIXED, 2><<<L[1].grid, 256, 0, s>>>(L[1].d, L[1].n, lc.sp);
+    if (L[2].n)
+        k_pair<MIXED, 4><<<L[2].grid, 256, 0, s>>>(L[2].d, L[2].n, lc.sp);
+    if (L[3].n)
+        k_pair<MIXED, 8><<<L[3].grid, 256, 0, s>>>(L[3].d, L[3].n, lc.sp);
+    if (L[4].n)
+        k_pair<MIXED, 16><<<L[4].grid, 256, 0, s>>>(L[4].d, L[4].n, lc.sp);
+    if (L[5].n)
+        k_pair<MIXED, 32><<<L[5].grid, 256, 0, s>>>(L[5].d, L[5].n, lc.sp);
 }
 
 void launch_pair(const LaunchCfg& lc, cudaStream_t s) {
-    if (lc.any_fp64)
-        launch_pair_prec<false>(lc, s);
-    if (lc.any_mixed)
-        launch_pair_prec<true>(lc, s);
+    launch_pair_prec<false>(lc, s);
+    launch_pair_prec<true>(lc, s);
 }
 
 } // namespace atvb

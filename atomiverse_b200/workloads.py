@@ -148,11 +148,13 @@ def ladder(n_systems: int = 512, seed: int = 2029, n_min: int = 256,
     return out
 
 
-def request_stream(n_requests: int = 2000, rate: float = 200.0, seed: int = 2030,
-                   n_min: int = 500, n_max: int = 200000, frac_lj: float = 0.6,
-                   precision: int = 1):
-    """Poisson arrivals of MD segments: (arrival_time_s, desc, frame).  60 %
-    LJ fluids (4 c^3 atoms) and 40 % rock-salt PME melts (n even, n^3 ions),
+def request_specs(n_requests: int = 2000, rate: float = 200.0, seed: int = 2030,
+                  n_min: int = 500, n_max: int = 200000, frac_lj: float = 0.6,
+                  steps: int = 1000):
+    """Poisson arrivals of MD segments as specs (no atoms generated yet):
+    dicts with arrival time [s], kind ("lj" or "pme"), lattice size and
+    seed.  60 % LJ fluids (4 c^3 atoms, as the 4,000-atom fluid rescaled)
+    and 40 % rock-salt PME melts (n even, n^3 ions, grid spacing ~0.94 A),
     sizes log-uniform in [n_min, n_max]."""
     rng = np.random.default_rng(seed)
     t = np.cumsum(rng.exponential(1.0 / rate, n_requests))
@@ -162,15 +164,34 @@ def request_stream(n_requests: int = 2000, rate: float = 200.0, seed: int = 2030
     for k in range(n_requests):
         if kinds[k]:
             c = max(4, round((sizes[k] / 4) ** (1 / 3)))
-            desc, frame = lj_fcc(ncell=c, seed=seed + 1 + k, precision=precision)
+            out.append(dict(t=float(t[k]), kind="lj", cells=int(c), seed=seed + 1 + k,
+                            n_atoms=4 * c ** 3, steps=steps))
         else:
             m = max(8, int(round(sizes[k] ** (1 / 3))))
             m += m % 2
-            L = m * 2.82
-            K = max(8, round(L / 0.94))
-            # small boxes: shrink the real-space cutoff so 2 (rc + skin) < L
-            rc = min(12.0, 0.5 * L - 1.0 - 0.05)
-            desc, frame = rocksalt_melt(ncell=m, seed=seed + 1 + k, grid=(K, K, K),
-                                        precision=precision, rc=rc)
-        out.append((float(t[k]), desc, frame))
+            out.append(dict(t=float(t[k]), kind="pme", cells=int(m), seed=seed + 1 + k,
+                            n_atoms=m ** 3, steps=steps))
     return out
+
+
+def build_request(spec: dict, precision: int = 1):
+    """(desc, frame) of one request spec from ``request_specs``."""
+    if spec["kind"] == "lj":
+        return lj_fcc(ncell=spec["cells"], seed=spec["seed"], precision=precision)
+    m = spec["cells"]
+    L = m * 2.82
+    K = max(8, round(L / 0.94))
+    # small boxes: shrink the real-space cutoff so that 2 (rc + skin) < L
+    rc = min(12.0, 0.5 * L - 1.0 - 0.05)
+    return rocksalt_melt(ncell=m, seed=spec["seed"], grid=(K, K, K), precision=precision,
+                         rc=rc)
+
+
+def request_stream(n_requests: int = 2000, rate: float = 200.0, seed: int = 2030,
+                   n_min: int = 500, n_max: int = 200000, frac_lj: float = 0.6,
+                   precision: int = 1):
+    """Materialised request stream: (arrival_time_s, desc, frame) per
+    request (small streams only; large ones use request_specs and
+    build_request on arrival)."""
+    specs = request_specs(n_requests, rate, seed, n_min, n_max, frac_lj)
+    return [(sp["t"], *build_request(sp, precision)) for sp in specs]
