@@ -42,10 +42,20 @@ struct Geometry {
 };
 Geometry make_geometry(const atvb_system_desc& d);
 
+// Stream-ordered device memory from an engine's own pool.  Frees go back to
+// the pool in stream order (no device-wide synchronisation, no unmapping),
+// so systems can join and leave a running engine without stalling it.
+struct DevMem {
+    cudaMemPool_t pool = nullptr;
+    cudaStream_t stream = nullptr;
+    void* alloc(size_t bytes) const; // throws Error(ATVB_ERR_NOMEM)
+    void free(void* p) const;
+};
+
 // One system's device memory and host mirror of its SysParams.
 class Slot {
   public:
-    Slot(const atvb_system_desc& d, cudaStream_t stream);
+    Slot(const atvb_system_desc& d, const DevMem& mem);
     ~Slot();
     Slot(const Slot&) = delete;
     Slot& operator=(const Slot&) = delete;
@@ -61,11 +71,12 @@ class Slot {
     int lanes = 4;  // pair-kernel lanes per atom for this system
     double mean_row = 0.0;
     double erfcx_err = 0.0; // max relative error of the FP64 erfcx fit
-    cufftHandle plan_f = 0, plan_i = 0;
+    cufftHandle plan_f = 0, plan_i = 0; // borrowed from the engine's plan cache
     std::vector<double> infl_host;
 
   private:
     void* dalloc(size_t b);
+    DevMem mem_;
     std::vector<void*> allocs;
     void* nbr_alloc = nullptr;
 };
@@ -111,6 +122,13 @@ class Engine {
     }
 
   private:
+    struct FftPlans {
+        cufftHandle f = 0, i = 0;
+        int refs = 0;
+        uint64_t last_use = 0;
+    };
+    void acquire_plans(Slot& s);
+    void release_plans(Slot& s);
     void ensure_table();
     void push_params(int id);
     void build_lists();
@@ -128,6 +146,12 @@ class Engine {
 
     int device_ = 0;
     cudaStream_t stream_ = nullptr;
+    DevMem mem_;
+    // cuFFT plans by {K0, K1, K2, precision}, shared by every system of that
+    // grid (their FFTs run one after another on the engine's stream) and kept
+    // after the last user leaves, up to kPlanCacheIdle idle shapes
+    std::map<std::vector<int>, FftPlans> plans_;
+    uint64_t plan_clock_ = 0;
     int num_sms_ = 148;
     std::vector<std::unique_ptr<Slot>> slots_;
     SysParams* d_sp_ = nullptr;

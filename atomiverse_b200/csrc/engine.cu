@@ -290,48 +290,48 @@ size_t estimate_bytes(const atvb_system_desc& d) {
 
 // --------------------------------------------------------------- Slot
 
-void* Slot::dalloc(size_t b) {
+void* DevMem::alloc(size_t b) const {
     void* p = nullptr;
     if (b == 0)
         b = 16;
-    cudaError_t e = cudaMalloc(&p, b);
+    cudaError_t e = cudaMallocFromPoolAsync(&p, b, pool, stream);
     if (e != cudaSuccess) {
         cudaGetLastError();
-        throw Error(ATVB_ERR_NOMEM, "cudaMalloc(" + std::to_string(b) +
-                                        " bytes) failed: " +
-                                        cudaGetErrorString(e));
+        throw Error(ATVB_ERR_NOMEM, "device allocation of " + std::to_string(b) +
+                                        " bytes failed: " + cudaGetErrorString(e));
     }
+    return p;
+}
+
+void DevMem::free(void* p) const {
+    if (p)
+        cudaFreeAsync(p, stream);
+}
+
+void* Slot::dalloc(size_t b) {
+    void* p = mem_.alloc(b);
     allocs.push_back(p);
-    bytes += b;
+    bytes += b == 0 ? 16 : b;
     return p;
 }
 
 Slot::~Slot() {
-    if (plan_f)
-        cufftDestroy(plan_f);
-    if (plan_i)
-        cufftDestroy(plan_i);
     for (void* p : allocs)
-        cudaFree(p);
-    if (nbr_alloc)
-        cudaFree(nbr_alloc);
+        mem_.free(p);
+    mem_.free(nbr_alloc);
 }
 
 void Slot::alloc_list(int new_cap) {
-    if (nbr_alloc)
-        CK(cudaFree(nbr_alloc));
+    mem_.free(nbr_alloc);
     nbr_alloc = nullptr;
     const size_t b = (size_t)hp.n * new_cap * sizeof(int);
-    cudaError_t e = cudaMalloc(&nbr_alloc, b);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        throw Error(ATVB_ERR_NOMEM, "neighbour list allocation failed");
-    }
+    nbr_alloc = mem_.alloc(b);
     hp.nbr = (int*)nbr_alloc;
     hp.cap = new_cap;
 }
 
-Slot::Slot(const atvb_system_desc& d, cudaStream_t stream) : desc(d) {
+Slot::Slot(const atvb_system_desc& d, const DevMem& mem) : desc(d), mem_(mem) {
+    cudaStream_t stream = mem.stream;
     geo = make_geometry(d);
     std::memset(&hp, 0, sizeof(hp));
     const int n = d.n_atoms;
@@ -523,18 +523,6 @@ Slot::Slot(const atvb_system_desc& d, cudaStream_t stream) : desc(d) {
         }
         CK(cudaMemcpyAsync(hp.infl, infl_host.data(), nh * 8,
                            cudaMemcpyHostToDevice, stream));
-        const bool mixed = hp.prec == kMixed;
-        CKF(cufftPlan3d(&plan_f, hp.K[0], hp.K[1], hp.K[2],
-                        mixed ? CUFFT_R2C : CUFFT_D2Z));
-        CKF(cufftPlan3d(&plan_i, hp.K[0], hp.K[1], hp.K[2],
-                        mixed ? CUFFT_C2R : CUFFT_Z2D));
-        CKF(cufftSetStream(plan_f, stream));
-        CKF(cufftSetStream(plan_i, stream));
-        size_t ws = 0;
-        if (cufftGetSize(plan_f, &ws) == CUFFT_SUCCESS)
-            bytes += ws;
-        if (cufftGetSize(plan_i, &ws) == CUFFT_SUCCESS)
-            bytes += ws;
     }
     CK(cudaStreamSynchronize(stream));
 }
@@ -546,6 +534,71 @@ Engine::Engine(int device) : device_(device) {
     CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     CK(cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount,
                               device));
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    CK(cudaMemPoolCreate(&mem_.pool, &props));
+    // keep freed memory in the pool until the engine goes away
+    uint64_t keep = UINT64_MAX;
+    CK(cudaMemPoolSetAttribute(mem_.pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    mem_.stream = stream_;
+}
+
+constexpr int kPlanCacheIdle = 16;
+
+void Engine::acquire_plans(Slot& s) {
+    if (!s.hp.has_pme)
+        return;
+    const bool mixed = s.hp.prec == kMixed;
+    const std::vector<int> key = {s.hp.K[0], s.hp.K[1], s.hp.K[2], mixed ? 1 : 0};
+    FftPlans& p = plans_[key];
+    if (!p.f) {
+        cufftHandle f = 0, i = 0;
+        CKF(cufftPlan3d(&f, key[0], key[1], key[2], mixed ? CUFFT_R2C : CUFFT_D2Z));
+        if (cufftPlan3d(&i, key[0], key[1], key[2], mixed ? CUFFT_C2R : CUFFT_Z2D) !=
+            CUFFT_SUCCESS) {
+            cufftDestroy(f);
+            plans_.erase(key);
+            throw Error(ATVB_ERR_CUDA, "cufftPlan3d failed");
+        }
+        cufftSetStream(f, stream_);
+        cufftSetStream(i, stream_);
+        p.f = f;
+        p.i = i;
+    }
+    ++p.refs;
+    p.last_use = ++plan_clock_;
+    s.plan_f = p.f;
+    s.plan_i = p.i;
+}
+
+void Engine::release_plans(Slot& s) {
+    if (!s.hp.has_pme)
+        return;
+    const std::vector<int> key = {s.hp.K[0], s.hp.K[1], s.hp.K[2],
+                                  s.hp.prec == kMixed ? 1 : 0};
+    auto it = plans_.find(key);
+    if (it != plans_.end() && it->second.refs > 0)
+        --it->second.refs;
+    s.plan_f = s.plan_i = 0;
+    // evict the least recently used idle shapes beyond the cache size
+    for (;;) {
+        int idle = 0;
+        auto lru = plans_.end();
+        for (auto j = plans_.begin(); j != plans_.end(); ++j)
+            if (j->second.refs == 0) {
+                ++idle;
+                if (lru == plans_.end() || j->second.last_use < lru->second.last_use)
+                    lru = j;
+            }
+        if (idle <= kPlanCacheIdle || lru == plans_.end())
+            break;
+        cudaStreamSynchronize(stream_);
+        cufftDestroy(lru->second.f);
+        cufftDestroy(lru->second.i);
+        plans_.erase(lru);
+    }
 }
 
 Engine::~Engine() {
@@ -553,9 +606,15 @@ Engine::~Engine() {
     release_graph();
     slots_.clear();
     for (void* p : list_allocs_)
-        cudaFree(p);
-    if (d_sp_)
-        cudaFree(d_sp_);
+        mem_.free(p);
+    mem_.free(d_sp_);
+    cudaStreamSynchronize(stream_);
+    for (auto& kv : plans_) {
+        cufftDestroy(kv.second.f);
+        cufftDestroy(kv.second.i);
+    }
+    if (mem_.pool)
+        cudaMemPoolDestroy(mem_.pool);
     for (auto& e : prof_events_)
         cudaEventDestroy(e);
     if (stream_)
@@ -573,7 +632,8 @@ void Engine::release_graph() {
 
 int Engine::add(const atvb_system_desc& d) {
     CK(cudaSetDevice(device_));
-    auto s = std::make_unique<Slot>(d, stream_);
+    auto s = std::make_unique<Slot>(d, mem_);
+    acquire_plans(*s);
     int id = -1;
     for (size_t k = 0; k < slots_.size(); ++k)
         if (!slots_[k]) {
@@ -594,9 +654,9 @@ int Engine::add(const atvb_system_desc& d) {
 
 void Engine::remove(int id) {
     Slot* s = slot(id);
-    (void)s;
-    CK(cudaStreamSynchronize(stream_));
-    slots_[id].reset();
+    release_graph(); // the captured step references this system's memory
+    release_plans(*s);
+    slots_[id].reset(); // stream-ordered frees: no wait for the device
     dirty_ = true;
 }
 
@@ -612,14 +672,13 @@ void Engine::ensure_table() {
     int cap = std::max(8, sp_cap_ * 2);
     while (cap < (int)slots_.size())
         cap *= 2;
-    SysParams* nd = nullptr;
-    CK(cudaMalloc(&nd, sizeof(SysParams) * cap));
+    SysParams* nd = (SysParams*)mem_.alloc(sizeof(SysParams) * cap);
     if (d_sp_) {
         CK(cudaMemcpyAsync(nd, d_sp_, sizeof(SysParams) * sp_cap_,
                            cudaMemcpyDeviceToDevice, stream_));
-        CK(cudaStreamSynchronize(stream_));
-        CK(cudaFree(d_sp_));
+        mem_.free(d_sp_);
     }
+    release_graph(); // captured launches point at the old table
     d_sp_ = nd;
     sp_cap_ = cap;
     dirty_ = true;
@@ -632,13 +691,13 @@ void Engine::push_params(int id) {
 }
 
 static ItemList make_list(std::vector<void*>& allocs, const std::vector<Item>& v,
-                          int max_grid, cudaStream_t stream) {
+                          int max_grid, const DevMem& mem) {
+    cudaStream_t stream = mem.stream;
     ItemList il;
     il.n = (int)v.size();
     if (v.empty())
         return il;
-    void* p = nullptr;
-    CK(cudaMalloc(&p, sizeof(Item) * v.size()));
+    void* p = mem.alloc(sizeof(Item) * v.size());
     allocs.push_back(p);
     CK(cudaMemcpyAsync(p, v.data(), sizeof(Item) * v.size(),
                        cudaMemcpyHostToDevice, stream));
@@ -672,9 +731,9 @@ static int lane_class(int G) {
 }
 
 void Engine::build_lists() {
-    CK(cudaStreamSynchronize(stream_));
+    release_graph();
     for (void* p : list_allocs_)
-        cudaFree(p);
+        mem_.free(p);
     list_allocs_.clear();
     std::vector<Item> atoms, list, cells, patoms, pgrid, preal;
     std::vector<int> sys;
@@ -729,19 +788,18 @@ void Engine::build_lists() {
     }
     const int g_light = num_sms_ * 16;
     lc_.sp = d_sp_;
-    lc_.atoms = make_list(list_allocs_, atoms, g_light, stream_);
-    lc_.list = make_list(list_allocs_, list, num_sms_ * 32, stream_);
+    lc_.atoms = make_list(list_allocs_, atoms, g_light, mem_);
+    lc_.list = make_list(list_allocs_, list, num_sms_ * 32, mem_);
     for (int p = 0; p < 2; ++p)
         for (int c = 0; c < kLaneClasses; ++c)
-            lc_.pair[p][c] = make_list(list_allocs_, pair_by[p][c], num_sms_ * 16, stream_);
-    lc_.cells = make_list(list_allocs_, cells, g_light, stream_);
-    lc_.pme_atoms = make_list(list_allocs_, patoms, g_light, stream_);
-    lc_.pme_grid = make_list(list_allocs_, pgrid, g_light, stream_);
-    lc_.pme_real = make_list(list_allocs_, preal, g_light, stream_);
+            lc_.pair[p][c] = make_list(list_allocs_, pair_by[p][c], num_sms_ * 16, mem_);
+    lc_.cells = make_list(list_allocs_, cells, g_light, mem_);
+    lc_.pme_atoms = make_list(list_allocs_, patoms, g_light, mem_);
+    lc_.pme_grid = make_list(list_allocs_, pgrid, g_light, mem_);
+    lc_.pme_real = make_list(list_allocs_, preal, g_light, mem_);
     lc_.nsys = (int)sys.size();
     if (!sys.empty()) {
-        void* p = nullptr;
-        CK(cudaMalloc(&p, sizeof(int) * sys.size()));
+        void* p = mem_.alloc(sizeof(int) * sys.size());
         list_allocs_.push_back(p);
         CK(cudaMemcpyAsync(p, sys.data(), sizeof(int) * sys.size(),
                            cudaMemcpyHostToDevice, stream_));
@@ -1023,25 +1081,24 @@ LaunchCfg Engine::restricted_cfg(int id) {
     }
     LaunchCfg c = lc_;
     c.sp = d_sp_;
-    c.atoms = make_list(list_allocs_, atoms, num_sms_ * 16, stream_);
-    c.list = make_list(list_allocs_, list, num_sms_ * 32, stream_);
-    c.cells = make_list(list_allocs_, cells, num_sms_ * 16, stream_);
+    c.atoms = make_list(list_allocs_, atoms, num_sms_ * 16, mem_);
+    c.list = make_list(list_allocs_, list, num_sms_ * 32, mem_);
+    c.cells = make_list(list_allocs_, cells, num_sms_ * 16, mem_);
     for (int p = 0; p < 2; ++p)
         for (int k = 0; k < kLaneClasses; ++k)
             c.pair[p][k] = ItemList{};
     c.pair[P.prec == kMixed ? 1 : 0][lane_class(s->lanes)] =
-        make_list(list_allocs_, pair, num_sms_ * 16, stream_);
-    c.pme_atoms = make_list(list_allocs_, patoms, num_sms_ * 16, stream_);
-    c.pme_grid = make_list(list_allocs_, pgrid, num_sms_ * 16, stream_);
-    c.pme_real = make_list(list_allocs_, preal, num_sms_ * 16, stream_);
+        make_list(list_allocs_, pair, num_sms_ * 16, mem_);
+    c.pme_atoms = make_list(list_allocs_, patoms, num_sms_ * 16, mem_);
+    c.pme_grid = make_list(list_allocs_, pgrid, num_sms_ * 16, mem_);
+    c.pme_real = make_list(list_allocs_, preal, num_sms_ * 16, mem_);
     c.any_mixed = P.prec == kMixed;
     c.any_fp64 = P.prec != kMixed;
     if (P.has_pme) {
         c.pme_mixed = P.prec == kMixed;
         c.pme_order = P.order;
     }
-    void* p = nullptr;
-    CK(cudaMalloc(&p, sizeof(int)));
+    void* p = mem_.alloc(sizeof(int));
     list_allocs_.push_back(p);
     CK(cudaMemcpyAsync(p, &id, sizeof(int), cudaMemcpyHostToDevice, stream_));
     CK(cudaStreamSynchronize(stream_));
