@@ -70,6 +70,10 @@ struct SysParams {
     double fix_scale[3]; // 2^32 / L
     // neighbour list
     double rlist2;     // (cutoff + skin)^2, the pair-set test
+    // FP32 prefilter of the pair-set test on fixed-point positions: below
+    // lband_lo a candidate is certainly listed, at or above lband_hi it is
+    // certainly not; in between the exact FP64 test decides
+    float lband_lo, lband_hi;
     double skin_half2; // (skin/2)^2
     int nl_every, nl_delay, nl_check;
     int nc[3], ncell;
@@ -81,14 +85,9 @@ struct SysParams {
     // LJ
     int has_lj;
     double lj_rc2, lj_sig6, lj_eps4, lj_eps24, lj_shift;
-    // real-space Coulomb; erfc(x) = exp(-x^2) * erfcx(x) with erfcx from a
-    // piecewise polynomial fitted on [0, alpha * cutoff] (see erfcx_fit)
+    // real-space Coulomb
     int has_coul;
     double coul_rc2, coul_alpha, coul_alpha2;
-    int erfcx_nint;       // intervals (<= kErfcxMaxInt)
-    double erfcx_inv_h;   // intervals per unit of x
-    const double* erfcx_d; // erfcx_nint x kErfcxNd monomial coefficients
-    const float* erfcx_f;  // erfcx_nint x kErfcxNf
     // PME
     int has_pme;
     int K[3], Kh, order;
@@ -111,6 +110,7 @@ struct SysParams {
     // sorted order
     void* pos4;      // double4 (FP64) or int4 fixed-point + float q (mixed)
     double4* posd4;  // FP64 sorted positions used by the pair-set test
+    int4* lpos;      // fixed-point sorted positions at the last build (prefilter)
     double4* f4;     // forces in sorted order
     int *perm, *rank, *cell_of, *slot, *cell_count, *cell_start, *cellS;
     int *nbr, *nnbr;
@@ -126,12 +126,6 @@ struct SysParams {
     double* ehist; // energy history ring: 3 doubles per step (E, KE, step)
     int ehist_cap;
 };
-
-// erfcx tables: erfcx_nint intervals over [0, alpha*rc]; on interval k the
-// local variable is u = x * (2/h) - (2k+1) in [-1, 1].
-constexpr int kErfcxMaxInt = 64;
-constexpr int kErfcxNd = 10; // FP64: degree 9
-constexpr int kErfcxNf = 7;  // FP32: degree 6
 
 // A unit of work: a chunk of atoms (or grid points) of one system.
 struct Item {

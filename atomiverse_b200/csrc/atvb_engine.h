@@ -70,7 +70,6 @@ class Slot {
     int max_row = 0;
     int lanes = 4;  // pair-kernel lanes per atom for this system
     double mean_row = 0.0;
-    double erfcx_err = 0.0; // max relative error of the FP64 erfcx fit
     cufftHandle plan_f = 0, plan_i = 0; // borrowed from the engine's plan cache
     std::vector<double> infl_host;
 

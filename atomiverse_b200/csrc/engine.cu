@@ -22,6 +22,7 @@
 #include "atvb.h"
 #include "atvb_common.cuh"
 #include "atvb_engine.h"
+#include "erfcx_coef.h"
 #include "atvb_kernels.cuh"
 
 namespace atvb {
@@ -106,68 +107,6 @@ static std::vector<double> spline_moduli(int K, int n) {
     return mod;
 }
 
-// erfcx(x) = exp(x^2) erfc(x) on [0, xmax]: Chebyshev interpolation on each
-// of `nint` equal intervals (long-double samples of the C library's erfc),
-// converted to monomials in the local variable u in [-1, 1].  Returns the
-// largest relative error of the polynomials against long double on a fine
-// grid.  erfcx is smooth and bounded (1 at x = 0, ~1/(x sqrt(pi)) for large
-// x), so a low degree per short interval reaches double precision.
-static double erfcx_fit(double xmax, int nint, int nc, std::vector<double>& out) {
-    typedef long double LD;
-    const LD pi = 3.141592653589793238462643383279502884L;
-    auto f = [](LD x) { return expl(x * x) * erfcl(x); };
-    out.assign((size_t)nint * nc, 0.0);
-    const LD h = (LD)xmax / nint;
-    std::vector<LD> fx(nc), c(nc), mono(nc), T0(nc), T1(nc), T2(nc);
-    for (int k = 0; k < nint; ++k) {
-        const LD mid = (k + 0.5L) * h, half = 0.5L * h;
-        for (int j = 0; j < nc; ++j)
-            fx[j] = f(mid + half * cosl(pi * (j + 0.5L) / nc));
-        for (int m = 0; m < nc; ++m) {
-            LD acc = 0;
-            for (int j = 0; j < nc; ++j)
-                acc += fx[j] * cosl(pi * m * (j + 0.5L) / nc);
-            c[m] = acc * 2.0L / nc;
-        }
-        c[0] *= 0.5L;
-        // sum_m c_m T_m(u) -> monomials
-        std::fill(mono.begin(), mono.end(), 0.0L);
-        std::fill(T0.begin(), T0.end(), 0.0L);
-        std::fill(T1.begin(), T1.end(), 0.0L);
-        T0[0] = 1.0L;
-        if (nc > 1)
-            T1[1] = 1.0L;
-        for (int m = 0; m < nc; ++m) {
-            const std::vector<LD>& T = m == 0 ? T0 : T1;
-            if (m >= 2) {
-                for (int d = 0; d < nc; ++d)
-                    T2[d] = -T0[d] + (d > 0 ? 2.0L * T1[d - 1] : 0.0L);
-                T0 = T1;
-                T1 = T2;
-            }
-            const std::vector<LD>& Tm = m == 0 ? T0 : T1;
-            (void)T;
-            for (int d = 0; d < nc; ++d)
-                mono[d] += c[m] * Tm[d];
-        }
-        for (int d = 0; d < nc; ++d)
-            out[(size_t)k * nc + d] = (double)mono[d];
-    }
-    double worst = 0.0;
-    for (int t = 0; t <= 20000; ++t) {
-        const LD x = (LD)xmax * t / 20000.0L;
-        int k = (int)(x / h);
-        if (k > nint - 1)
-            k = nint - 1;
-        const LD u = x * (2.0L / h) - (2 * k + 1);
-        LD p = 0;
-        for (int d = nc - 1; d >= 0; --d)
-            p = p * u + (LD)out[(size_t)k * nc + d];
-        const double rel = (double)fabsl(p / f(x) - 1.0L);
-        worst = std::max(worst, rel);
-    }
-    return worst;
-}
 
 // ------------------------------------------------------------ geometry
 
@@ -196,9 +135,11 @@ Geometry make_geometry(const atvb_system_desc& d) {
             throw Error(ATVB_ERR_INVALID,
                         "box edge must exceed 2*(cutoff+skin) so that each "
                         "pair has one minimum image");
-    // cell_list.cpp:112-121 half-reach bins; :186-191 reach
+    // Bins of at least a third of the list radius (reach 3), finer than the
+    // reference's half-reach bins (cell_list.cpp:112-121, reach :186-191):
+    // fewer candidates per atom.  The pair set does not depend on the bins.
     for (int k = 0; k < 3; ++k) {
-        int c = (int)std::floor(g.L[k] / (0.5 * g.rlist));
+        int c = (int)std::floor(g.L[k] / (g.rlist / 3.0));
         g.nc[k] = c < 1 ? 1 : c;
         g.cs[k] = g.L[k] / g.nc[k];
         int r = (int)std::ceil(g.rlist / g.cs[k] - 1e-12);
@@ -351,6 +292,15 @@ Slot::Slot(const atvb_system_desc& d, const DevMem& mem) : desc(d), mem_(mem) {
     }
     hp.ncell = geo.nc[0] * geo.nc[1] * geo.nc[2];
     hp.rlist2 = geo.rlist * geo.rlist;
+    {
+        // |r2_fp32 - r2_exact| <= 5.4e-7 r2 (three FP32 roundings of each
+        // difference, three of the sum) + 3.6 r q (fixed-point quantum q =
+        // L / 2^32 on both atoms); the band doubles both terms
+        const double q = std::max(geo.L[0], std::max(geo.L[1], geo.L[2])) / 4294967296.0;
+        const double band = 2e-6 * hp.rlist2 + 8.0 * geo.rlist * q + 1e-12;
+        hp.lband_lo = std::nextafter((float)(hp.rlist2 - band), 0.0f);
+        hp.lband_hi = std::nextafter((float)(hp.rlist2 + band), 3.0e38f);
+    }
     hp.skin_half2 = 0.25 * geo.skin * geo.skin;
     hp.nl_every = d.nl_every < 1 ? 1 : d.nl_every;
     hp.nl_delay = d.nl_delay < 0 ? 0 : d.nl_delay;
@@ -384,29 +334,11 @@ Slot::Slot(const atvb_system_desc& d, const DevMem& mem) : desc(d), mem_(mem) {
         hp.coul_rc2 = d.coul_cutoff * d.coul_cutoff;
         hp.coul_alpha = d.coul_alpha;
         hp.coul_alpha2 = d.coul_alpha * d.coul_alpha;
-        // a hair past alpha*rc so that r^2 < rc^2 never leaves the table
-        const double xmax = d.coul_alpha * d.coul_cutoff * (1.0 + 1e-6);
-        const int nint = std::min(kErfcxMaxInt,
-                                  std::max(16, (int)std::ceil(8.0 * xmax)));
-        hp.erfcx_nint = nint;
-        hp.erfcx_inv_h = nint / xmax;
-        std::vector<double> cd, cf64;
-        const double ed = erfcx_fit(xmax, nint, kErfcxNd, cd);
-        const double ef = erfcx_fit(xmax, nint, kErfcxNf, cf64);
-        if (ed > 1e-15 || ef > 1e-10)
+        // the pair kernels' erfcx polynomial covers alpha * r <= kErfcxXmax
+        if (d.coul_alpha * d.coul_cutoff > kErfcxXmax)
             throw Error(ATVB_ERR_INVALID,
-                        "erfcx fit failed (alpha*cutoff too large?)");
-        erfcx_err = ed;
-        std::vector<float> cf(cf64.begin(), cf64.end());
-        double* dd_ = (double*)dalloc(cd.size() * sizeof(double));
-        float* df_ = (float*)dalloc(cf.size() * sizeof(float));
-        CK(cudaMemcpyAsync(dd_, cd.data(), cd.size() * sizeof(double),
-                           cudaMemcpyHostToDevice, stream));
-        CK(cudaMemcpyAsync(df_, cf.data(), cf.size() * sizeof(float),
-                           cudaMemcpyHostToDevice, stream));
-        CK(cudaStreamSynchronize(stream));
-        hp.erfcx_d = dd_;
-        hp.erfcx_f = df_;
+                        "CoulLong: alpha * cutoff must not exceed 6 "
+                        "(erfc(6) = 2e-17 is below double precision)");
     }
     // integrator / thermostat
     if (!(d.dt > 0.0))
@@ -453,6 +385,7 @@ Slot::Slot(const atvb_system_desc& d, const DevMem& mem) : desc(d), mem_(mem) {
     hp.sz = dd(n);
     hp.tag = (long long*)dalloc((size_t)n * 8);
     hp.posd4 = (double4*)dalloc((size_t)n * sizeof(double4));
+    hp.lpos = (int4*)dalloc((size_t)n * sizeof(int4));
     hp.pos4 = hp.prec == kMixed ? dalloc((size_t)n * sizeof(int4))
                                 : (void*)hp.posd4;
     hp.f4 = (double4*)dalloc((size_t)n * sizeof(double4));

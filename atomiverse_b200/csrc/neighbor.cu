@@ -146,11 +146,13 @@ __global__ void k_permute(const Item* items, int nitems, const SysParams* sp) {
         P.cellS[s] = P.cell_of[i];
         const double x = P.x[i], y = P.y[i], z = P.z[i], q = P.q[i];
         P.posd4[s] = make_double4(x, y, z, q);
+        int4 v;
+        v.x = (int)pos_fix(x, P.fix_scale[0]);
+        v.y = (int)pos_fix(y, P.fix_scale[1]);
+        v.z = (int)pos_fix(z, P.fix_scale[2]);
+        v.w = 0;
+        P.lpos[s] = v;
         if (P.prec == kMixed) {
-            int4 v;
-            v.x = (int)pos_fix(x, P.fix_scale[0]);
-            v.y = (int)pos_fix(y, P.fix_scale[1]);
-            v.z = (int)pos_fix(z, P.fix_scale[2]);
             v.w = __float_as_int((float)q);
             reinterpret_cast<int4*>(P.pos4)[s] = v;
         }
@@ -178,12 +180,63 @@ ATVB_DEV double exact_r2(const double4& a, const double4& b, const double* L,
                      __dmul_rn(d[2], d[2]));
 }
 
-// Stage 6 (items of kListChunk atoms): one warp per sorted atom walks the
-// stencil columns (contiguous runs of cells along z, hence contiguous runs of
-// sorted atoms), tests 32 candidates per iteration and compacts the hits
-// with a ballot.
+// The sorted atoms of stencil column `col` around cell (cx, cy, cz): at most
+// two contiguous runs [a0, a0 + l0) and [a1, a1 + l1) (two when the z range
+// wraps).  Offsets along an axis stay within one period of the cell index,
+// so one conditional add or subtract wraps them (also on an aliased axis,
+// whose offsets are absolute cell indices).
+ATVB_DEV void column_runs(const SysParams& P, const int* __restrict__ cstart, int4 col,
+                          int cx, int cy, int cz, int& a0, int& l0, int& a1, int& l1) {
+    const int nc0 = P.nc[0], nc1 = P.nc[1], nc2 = P.nc[2];
+    int xx = cx + col.x;
+    xx += xx < 0 ? nc0 : (xx >= nc0 ? -nc0 : 0);
+    int yy = cy + col.y;
+    yy += yy < 0 ? nc1 : (yy >= nc1 ? -nc1 : 0);
+    const int base = (xx * nc1 + yy) * nc2;
+    int lo0, hi0, lo1 = 0, hi1 = -1;
+    if (col.z < 0) {
+        lo0 = base;
+        hi0 = base + nc2 - 1;
+    } else {
+        const int z0 = cz - col.z, z1 = cz + col.z;
+        if (z0 < 0) {
+            lo0 = base + z0 + nc2;
+            hi0 = base + nc2 - 1;
+            lo1 = base;
+            hi1 = base + z1;
+        } else if (z1 >= nc2) {
+            lo0 = base + z0;
+            hi0 = base + nc2 - 1;
+            lo1 = base;
+            hi1 = base + z1 - nc2;
+        } else {
+            lo0 = base + z0;
+            hi0 = base + z1;
+        }
+    }
+    a0 = cstart[lo0];
+    l0 = cstart[hi0 + 1] - a0;
+    if (hi1 >= lo1) {
+        a1 = cstart[lo1];
+        l1 = cstart[hi1 + 1] - a1;
+    } else {
+        a1 = 0;
+        l1 = 0;
+    }
+}
+
+// Stage 6 (items of kListChunk atoms): one warp per sorted atom.  The lanes
+// first resolve up to 32 stencil columns at once into runs of sorted atoms;
+// a warp prefix sum lays those runs end to end, and the warp then tests 32
+// consecutive candidates per iteration (every lane busy, whatever the column
+// lengths), in column order, compacting hits with a ballot.  Candidates are
+// screened in FP32 on the fixed-point positions (16 bytes per candidate,
+// exact integer minimum image); only those whose FP32 distance lies within
+// the error band of r^2 = (cutoff + skin)^2 take the exact FP64 test, so the
+// listed set is exactly the FP64 one.
 __global__ void __launch_bounds__(256)
     k_build_list(const Item* items, int nitems, const SysParams* sp) {
+    const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
     for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
@@ -191,7 +244,7 @@ __global__ void __launch_bounds__(256)
         const SysParams& P = sp[item.sys];
         if (!P.st->rebuild)
             continue;
-        const int nc0 = P.nc[0], nc1 = P.nc[1], nc2 = P.nc[2];
+        const int nc1 = P.nc[1], nc2 = P.nc[2];
         const double L[3] = {P.L[0], P.L[1], P.L[2]};
         const double hL[3] = {P.halfL[0], P.halfL[1], P.halfL[2]};
         const double rl2 = P.rlist2;
@@ -199,70 +252,75 @@ __global__ void __launch_bounds__(256)
         const int4* __restrict__ cols = P.cols;
         const int* __restrict__ cstart = P.cell_start;
         const double4* __restrict__ pos = P.posd4;
+        const int4* __restrict__ lp = P.lpos;
+        const float sx = P.Lf_fix[0], sy = P.Lf_fix[1], sz = P.Lf_fix[2];
+        const float blo = P.lband_lo, bhi = P.lband_hi;
         const int s = item.begin + warp;
-        if (s < P.n) {
-            const double4 pi = pos[s];
-            const int c = P.cellS[s];
-            const int cz = c % nc2, cy = (c / nc2) % nc1, cx = c / (nc1 * nc2);
-            int* row = P.nbr + (size_t)s * cap;
-            int cnt = 0;
-            for (int k = 0; k < ncol; ++k) {
-                const int4 col = cols[k];
-                const int xx = (cx + col.x + nc0) % nc0;
-                const int yy = (cy + col.y + nc1) % nc1;
-                const int base = (xx * nc1 + yy) * nc2;
-                int seg_lo[2], seg_hi[2], nseg;
-                if (col.z < 0) {
-                    seg_lo[0] = base;
-                    seg_hi[0] = base + nc2 - 1;
-                    nseg = 1;
-                } else {
-                    const int z0 = cz - col.z, z1 = cz + col.z;
-                    if (z0 < 0) {
-                        seg_lo[0] = base + z0 + nc2;
-                        seg_hi[0] = base + nc2 - 1;
-                        seg_lo[1] = base;
-                        seg_hi[1] = base + z1;
-                        nseg = 2;
-                    } else if (z1 >= nc2) {
-                        seg_lo[0] = base + z0;
-                        seg_hi[0] = base + nc2 - 1;
-                        seg_lo[1] = base;
-                        seg_hi[1] = base + z1 - nc2;
-                        nseg = 2;
-                    } else {
-                        seg_lo[0] = base + z0;
-                        seg_hi[0] = base + z1;
-                        nseg = 1;
-                    }
-                }
-                for (int sg = 0; sg < nseg; ++sg) {
-                    const int a = cstart[seg_lo[sg]];
-                    const int b = cstart[seg_hi[sg] + 1];
-                    for (int j0 = a; j0 < b; j0 += 32) {
-                        const int j = j0 + lane;
-                        bool hit = false;
-                        if (j < b && j != s) {
-                            const double4 pj = pos[j];
-                            hit = exact_r2(pi, pj, L, hL) < rl2;
-                        }
-                        const unsigned m = __ballot_sync(0xffffffffu, hit);
-                        if (hit) {
-                            const int wpos = cnt + __popc(m & lt);
-                            if (wpos < cap)
-                                row[wpos] = j;
-                        }
-                        cnt += __popc(m);
-                    }
-                }
+        if (s >= P.n)
+            continue; // warp-uniform
+        const int4 qi = lp[s];
+        const int c = P.cellS[s];
+        const int cz = c % nc2, cy = (c / nc2) % nc1, cx = c / (nc1 * nc2);
+        int* row = P.nbr + (size_t)s * cap;
+        int cnt = 0;
+        for (int c0 = 0; c0 < ncol; c0 += 32) {
+            int a0 = 0, l0 = 0, a1 = 0, l1 = 0;
+            if (c0 + lane < ncol)
+                column_runs(P, cstart, cols[c0 + lane], cx, cy, cz, a0, l0, a1, l1);
+            const int tot = l0 + l1;
+            int incl = tot;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(full, incl, o);
+                if (lane >= o)
+                    incl += t;
             }
-            if (lane == 0) {
-                P.nnbr[s] = cnt < cap ? cnt : cap;
-                atomicMax(&P.st->max_nnbr, cnt);
-                atomicAdd(&P.st->list_entries, (unsigned long long)cnt);
-                if (cnt > cap)
-                    atomicOr(&P.st->overflow, 1);
+            const int excl = incl - tot;
+            const int total = __shfl_sync(full, incl, 31);
+            for (int b = 0; b < total; b += 32) {
+                const int t = b + lane;
+                // owner column: the first lane whose inclusive sum exceeds t
+                int own = 0;
+#pragma unroll
+                for (int step = 16; step > 0; step >>= 1) {
+                    const int probe = __shfl_sync(full, incl, own + step - 1);
+                    if (probe <= t)
+                        own += step;
+                }
+                own &= 31;
+                const int o = t - __shfl_sync(full, excl, own);
+                const int oa0 = __shfl_sync(full, a0, own);
+                const int ol0 = __shfl_sync(full, l0, own);
+                const int oa1 = __shfl_sync(full, a1, own);
+                const int j = o < ol0 ? oa0 + o : oa1 + (o - ol0);
+                bool hit = false;
+                if (t < total && j != s) {
+                    // exact integer minimum image, FP32 distance
+                    const int4 qj = lp[j];
+                    const float dx = (float)(int)((unsigned)qi.x - (unsigned)qj.x) * sx;
+                    const float dy = (float)(int)((unsigned)qi.y - (unsigned)qj.y) * sy;
+                    const float dz = (float)(int)((unsigned)qi.z - (unsigned)qj.z) * sz;
+                    const float r2f = dx * dx + dy * dy + dz * dz;
+                    if (r2f < blo)
+                        hit = true;
+                    else if (r2f < bhi) // within the band: exact test
+                        hit = exact_r2(pos[s], pos[j], L, hL) < rl2;
+                }
+                const unsigned m = __ballot_sync(full, hit);
+                if (hit) {
+                    const int wpos = cnt + __popc(m & lt);
+                    if (wpos < cap)
+                        row[wpos] = j;
+                }
+                cnt += __popc(m);
             }
+        }
+        if (lane == 0) {
+            P.nnbr[s] = cnt < cap ? cnt : cap;
+            atomicMax(&P.st->max_nnbr, cnt);
+            atomicAdd(&P.st->list_entries, (unsigned long long)cnt);
+            if (cnt > cap)
+                atomicOr(&P.st->overflow, 1);
         }
     }
 }

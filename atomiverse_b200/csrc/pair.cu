@@ -16,13 +16,22 @@
 // same on its full list).  Energy/virial block partials are added into the
 // system's 64-bit fixed-point accumulators.
 //
-// FP64 build: positions double4 {x, y, z, q}, all arithmetic in double.
+// erfc: erfc(x) = exp(-x^2) erfcx(x), with erfcx from ONE polynomial in
+// t = 1/(1 + 0.4 x) valid for every system with alpha * cutoff <= 6
+// (erfcx_coef.h, compile-time coefficients: no tables, no shared memory).
+//
+// FP64 build: positions double4 {x, y, z, q}, all arithmetic in double;
+// exp and the reciprocal of the erfcx variable are this file's own FP64
+// routines (Cody-Waite exp, Newton reciprocal), accurate to ~1 ulp.
 // Mixed build: positions int4 {x, y, z fixed point with 2^32 steps per box
 // edge, q as float}; the integer difference is the exact minimum-image
-// separation, converted once to float; pair math in FP32; per-row sums are
-// promoted to FP64 before the lanes are combined.
+// separation, converted once to float; pair math in FP32 with the PTX
+// approximate rsqrt / rcp / ex2; the next two row entries are gathered while
+// the current two are computed; per-row sums are promoted to FP64 before the
+// lanes are combined.
 #include "atvb_common.cuh"
 #include "atvb_kernels.cuh"
+#include "erfcx_coef.h"
 
 namespace atvb {
 
@@ -33,175 +42,246 @@ struct PairAcc {
     double v[6];
 };
 
-// erfcx(x) from the per-system piecewise polynomial held in shared memory
-template <typename T, int NC>
-ATVB_DEV T erfcx_poly(T x, T inv_h, int nint, const T* tab) {
-    int k = (int)(x * inv_h);
-    k = k < nint - 1 ? k : nint - 1;
-    const T u = x * (T(2) * inv_h) - T(2 * k + 1);
-    const T* c = tab + k * NC;
-    T p = c[NC - 1];
+// ---- approximate FP32 special functions (PTX .approx instructions) -------
+ATVB_DEV float ex2_approx(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+ATVB_DEV float rcp_approx(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+ATVB_DEV float rsqrt_approx(float x) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// exp(-z) for z >= 0 in FP64 (Cody-Waite argument reduction): with
+// n = rint(-z / ln 2) and r = -z - n ln 2 (ln 2 split into a 32-bit head,
+// so n * head is exact, and a tail), |r| <= ln(2)/2 and
+// exp(-z) = 2^n exp(r), exp(r) by its Taylor series to degree 12
+// (truncation < 2e-16).  z is clamped at 708 (the result is then ~1e-308,
+// far below anything the callers keep).
+ATVB_DEV double exp_neg64(double z) {
+    const double w = -fmin(z, 708.0);
+    const double n = rint(w * 1.4426950408889634);
+    double r = fma(-n, 0.6931471803691238, w);
+    r = fma(-n, 1.9082149292705877e-10, r);
+    double p = 2.08767569878681e-09;
+    p = fma(p, r, 2.505210838544172e-08);
+    p = fma(p, r, 2.755731922398589e-07);
+    p = fma(p, r, 2.7557319223985893e-06);
+    p = fma(p, r, 2.48015873015873e-05);
+    p = fma(p, r, 0.0001984126984126984);
+    p = fma(p, r, 0.001388888888888889);
+    p = fma(p, r, 0.008333333333333333);
+    p = fma(p, r, 0.041666666666666664);
+    p = fma(p, r, 0.16666666666666666);
+    p = fma(p, r, 0.5);
+    p = fma(p, r, 1.0);
+    p = fma(p, r, 1.0);
+    const long long e = (long long)((int)n + 1023) << 52; // n >= -1022
+    return p * __longlong_as_double(e);
+}
+
+// 1 / v for 1 <= v <= 4 in FP64: FP32 estimate, two Newton steps
+// (relative error 2^-22 -> 2^-44 -> below one FP64 ulp).
+ATVB_DEV double rcp64(double v) {
+    double t = (double)rcp_approx((float)v);
+    t = fma(t, fma(-v, t, 1.0), t);
+    return fma(t, fma(-v, t, 1.0), t);
+}
+
+// erfcx(x) for 0 <= x <= 6 from the universal polynomial of erfcx_coef.h,
+// given t = 1 / (1 + kErfcxP x).  Coefficients are compile-time constants.
+ATVB_DEV double erfcx_of_t(double t) {
+    const double u = fma(kErfcxA, t, kErfcxB);
+    double p = kErfcxD[kErfcxD_N - 1];
 #pragma unroll
-    for (int d = NC - 2; d >= 0; --d)
-        p = p * u + c[d];
+    for (int k = kErfcxD_N - 2; k >= 0; --k)
+        p = fma(p, u, kErfcxD[k]);
+    return p;
+}
+ATVB_DEV float erfcx_of_t(float t) {
+    const float u = fmaf((float)kErfcxA, t, (float)kErfcxB);
+    float p = kErfcxF[kErfcxF_N - 1];
+#pragma unroll
+    for (int k = kErfcxF_N - 2; k >= 0; --k)
+        p = fmaf(p, u, kErfcxF[k]);
     return p;
 }
 
+// Per-row constants of one system, hoisted out of the pair loop.
+template <typename T>
+struct RowConst {
+    T lj_rc2, sig6, eps4, eps24, shift;
+    T c_rc2, alpha, alpha2; // alpha2: alpha^2 (FP64) or alpha^2 log2(e) (FP32)
+    T kqi;
+};
+
+template <typename T>
+struct RowSums {
+    T fx = 0, fy = 0, fz = 0, elj = 0, ec = 0;
+    T v[6] = {0, 0, 0, 0, 0, 0};
+};
+
+// One pair (i, j) at separation (dx, dy, dz), charge product factor qj.
+// Cutoffs are applied by selection, not branches: every lane of a warp runs
+// the same instructions, and a value computed outside its range (including
+// r^2 = 0) is never selected.
+template <bool LJ, bool CO, bool VIR, typename T>
+ATVB_DEV void pair_term(const RowConst<T>& c, T dx, T dy, T dz, T qj,
+                        RowSums<T>& a) {
+    constexpr bool F = sizeof(T) == 4;
+    const T r2 = dx * dx + dy * dy + dz * dz;
+    const bool ok = r2 >= (T)kMinPair2;
+    T rinv;
+    if constexpr (F)
+        rinv = rsqrt_approx(r2);
+    else
+        rinv = rsqrt(r2);
+    const T r2inv = rinv * rinv;
+    T fpair = 0;
+    if (LJ) {
+        const T r6 = r2inv * r2inv * r2inv * c.sig6;
+        const T flj = c.eps24 * r2inv * r6 * (T(2) * r6 - T(1));
+        const T elj = c.eps4 * r6 * (r6 - T(1)) - c.shift;
+        const bool in = ok && r2 < c.lj_rc2;
+        fpair = in ? flj : T(0);
+        a.elj += in ? elj : T(0);
+    }
+    if (CO) {
+        // erfc(x) = exp(-x^2) erfcx(x), x = alpha r
+        const T qq = c.kqi * qj;
+        const T x = c.alpha * (r2 * rinv);
+        T t, e;
+        if constexpr (F) {
+            t = rcp_approx(fmaf((float)kErfcxP, x, 1.0f));
+            e = ex2_approx(-c.alpha2 * r2);
+        } else {
+            t = rcp64(fma(kErfcxP, x, 1.0));
+            e = exp_neg64(c.alpha2 * r2);
+        }
+        const T p = erfcx_of_t(t);
+        const T pref = qq * rinv * e;
+        const bool in = ok && r2 < c.c_rc2;
+        fpair += in ? pref * (p + (T)kEwaldF * x) * r2inv : T(0);
+        a.ec += in ? pref * p : T(0);
+    }
+    const T fxp = fpair * dx, fyp = fpair * dy, fzp = fpair * dz;
+    a.fx += fxp;
+    a.fy += fyp;
+    a.fz += fzp;
+    if (VIR) {
+        a.v[0] += dx * fxp;
+        a.v[1] += dy * fyp;
+        a.v[2] += dz * fzp;
+        a.v[3] += dx * fyp;
+        a.v[4] += dx * fzp;
+        a.v[5] += dy * fzp;
+    }
+}
+
+template <typename T>
+ATVB_DEV void finish_row(const RowSums<T>& r, PairAcc& a, bool vir) {
+    a.fx = (double)r.fx;
+    a.fy = (double)r.fy;
+    a.fz = (double)r.fz;
+    a.elj += (double)r.elj;
+    a.ec += (double)r.ec;
+    if (vir)
+        for (int k = 0; k < 6; ++k)
+            a.v[k] += (double)r.v[k];
+}
+
+template <typename T>
+ATVB_DEV RowConst<T> row_const(const SysParams& P, double qi) {
+    RowConst<T> c;
+    c.lj_rc2 = (T)P.lj_rc2;
+    c.sig6 = (T)P.lj_sig6;
+    c.eps4 = (T)P.lj_eps4;
+    c.eps24 = (T)P.lj_eps24;
+    c.shift = (T)P.lj_shift;
+    c.c_rc2 = (T)P.coul_rc2;
+    c.alpha = (T)P.coul_alpha;
+    c.alpha2 = sizeof(T) == 4 ? (T)(P.coul_alpha2 * 1.4426950408889634) : (T)P.coul_alpha2;
+    c.kqi = (T)(kQqr2e * qi);
+    return c;
+}
+
+// Row of sorted atom s, lanes g, g+G, ...: two entries per iteration so that
+// both index loads and both position gathers are in flight together.
 template <bool LJ, bool CO, bool VIR>
-ATVB_DEV void row_fp64(const SysParams& P, int s, int g, int G, PairAcc& a,
-                       const double* tab) {
+ATVB_DEV void row_fp64(const SysParams& P, int s, int g, int G, PairAcc& acc) {
     const double4* __restrict__ pos = reinterpret_cast<const double4*>(P.pos4);
     const double4 pi = pos[s];
     const int nn = P.nnbr[s];
     const int* __restrict__ row = P.nbr + (size_t)s * P.cap;
     const double L0 = P.L[0], L1 = P.L[1], L2 = P.L[2];
     const double i0 = P.invL[0], i1 = P.invL[1], i2 = P.invL[2];
-    const double lj_rc2 = P.lj_rc2, sig6 = P.lj_sig6, eps4 = P.lj_eps4,
-                 eps24 = P.lj_eps24, shift = P.lj_shift;
-    const double c_rc2 = P.coul_rc2, alpha = P.coul_alpha,
-                 alpha2 = P.coul_alpha2, inv_h = P.erfcx_inv_h;
-    const int nint = P.erfcx_nint;
-    const double kqi = kQqr2e * pi.w;
-    double fx = 0, fy = 0, fz = 0, elj = 0, ec = 0;
-    double v0 = 0, v1 = 0, v2 = 0, v3 = 0, v4 = 0, v5 = 0;
-    for (int k = g; k < nn; k += G) {
-        const int j = __ldg(row + k);
-        const double4 pj = pos[j];
-        const double dx = min_img(pi.x - pj.x, L0, i0);
-        const double dy = min_img(pi.y - pj.y, L1, i1);
-        const double dz = min_img(pi.z - pj.z, L2, i2);
-        const double r2 = dx * dx + dy * dy + dz * dz;
-        if (r2 < kMinPair2)
-            continue;
-        const double rinv = rsqrt(r2);
-        const double r2inv = rinv * rinv;
-        double fpair = 0.0;
-        if (LJ && r2 < lj_rc2) {
-            const double r6inv = r2inv * r2inv * r2inv * sig6;
-            fpair = eps24 * r2inv * (2.0 * r6inv * r6inv - r6inv);
-            elj += eps4 * (r6inv * r6inv - r6inv) - shift;
-        }
-        if (CO && r2 < c_rc2) {
-            const double qq = kqi * pj.w;
-            if (qq != 0.0) {
-                // erfc(x) = exp(-x^2) erfcx(x), x = alpha r
-                const double x = alpha * (r2 * rinv);
-                const double e = exp(-alpha2 * r2);
-                const double ex = erfcx_poly<double, kErfcxNd>(x, inv_h, nint, tab);
-                const double pref = qq * rinv;
-                fpair += pref * e * (ex + kEwaldF * x) * r2inv;
-                ec += pref * e * ex;
-            }
-        }
-        const double fxp = fpair * dx, fyp = fpair * dy, fzp = fpair * dz;
-        fx += fxp;
-        fy += fyp;
-        fz += fzp;
-        if (VIR) {
-            v0 += dx * fxp;
-            v1 += dy * fyp;
-            v2 += dz * fzp;
-            v3 += dx * fyp;
-            v4 += dx * fzp;
-            v5 += dy * fzp;
-        }
+    const RowConst<double> c = row_const<double>(P, pi.w);
+    RowSums<double> a;
+    int k = g;
+    for (; k + G < nn; k += 2 * G) {
+        const int ja = __ldg(row + k), jb = __ldg(row + k + G);
+        const double4 pa = pos[ja], pb = pos[jb];
+        pair_term<LJ, CO, VIR>(c, min_img(pi.x - pa.x, L0, i0), min_img(pi.y - pa.y, L1, i1),
+                               min_img(pi.z - pa.z, L2, i2), pa.w, a);
+        pair_term<LJ, CO, VIR>(c, min_img(pi.x - pb.x, L0, i0), min_img(pi.y - pb.y, L1, i1),
+                               min_img(pi.z - pb.z, L2, i2), pb.w, a);
     }
-    a.fx = fx;
-    a.fy = fy;
-    a.fz = fz;
-    a.elj += elj;
-    a.ec += ec;
-    if (VIR) {
-        a.v[0] += v0;
-        a.v[1] += v1;
-        a.v[2] += v2;
-        a.v[3] += v3;
-        a.v[4] += v4;
-        a.v[5] += v5;
+    if (k < nn) {
+        const double4 pa = pos[__ldg(row + k)];
+        pair_term<LJ, CO, VIR>(c, min_img(pi.x - pa.x, L0, i0), min_img(pi.y - pa.y, L1, i1),
+                               min_img(pi.z - pa.z, L2, i2), pa.w, a);
     }
+    finish_row(a, acc, VIR);
 }
 
 template <bool LJ, bool CO, bool VIR>
-ATVB_DEV void row_mixed(const SysParams& P, int s, int g, int G, PairAcc& a,
-                        const float* tab) {
+ATVB_DEV void row_mixed(const SysParams& P, int s, int g, int G, PairAcc& acc) {
     const int4* __restrict__ pos = reinterpret_cast<const int4*>(P.pos4);
     const int4 pi = pos[s];
-    const float qi = __int_as_float(pi.w);
     const int nn = P.nnbr[s];
     const int* __restrict__ row = P.nbr + (size_t)s * P.cap;
     const float sx = P.Lf_fix[0], sy = P.Lf_fix[1], sz = P.Lf_fix[2];
-    const float lj_rc2 = (float)P.lj_rc2, sig6 = (float)P.lj_sig6,
-                eps4 = (float)P.lj_eps4, eps24 = (float)P.lj_eps24,
-                shift = (float)P.lj_shift;
-    const float c_rc2 = (float)P.coul_rc2, alpha = (float)P.coul_alpha,
-                alpha2 = (float)P.coul_alpha2, inv_h = (float)P.erfcx_inv_h;
-    const int nint = P.erfcx_nint;
-    const float kqi = (float)kQqr2e * qi, kf = (float)kEwaldF;
-    float fx = 0, fy = 0, fz = 0, elj = 0, ec = 0;
-    float v0 = 0, v1 = 0, v2 = 0, v3 = 0, v4 = 0, v5 = 0;
-    for (int k = g; k < nn; k += G) {
-        const int j = __ldg(row + k);
-        const int4 pj = pos[j];
-        const float dx = (float)(int)((unsigned)pi.x - (unsigned)pj.x) * sx;
-        const float dy = (float)(int)((unsigned)pi.y - (unsigned)pj.y) * sy;
-        const float dz = (float)(int)((unsigned)pi.z - (unsigned)pj.z) * sz;
-        const float r2 = dx * dx + dy * dy + dz * dz;
-        if (r2 < 1e-20f)
-            continue;
-        const float r2inv = 1.0f / r2;
-        float fpair = 0.0f;
-        if (LJ && r2 < lj_rc2) {
-            const float r6inv = r2inv * r2inv * r2inv * sig6;
-            fpair = eps24 * r2inv * (2.0f * r6inv * r6inv - r6inv);
-            elj += eps4 * (r6inv * r6inv - r6inv) - shift;
-        }
-        if (CO && r2 < c_rc2) {
-            const float qq = kqi * __int_as_float(pj.w);
-            if (qq != 0.0f) {
-                const float rinv = rsqrtf(r2);
-                const float x = alpha * (r2 * rinv);
-                const float e = expf(-alpha2 * r2);
-                const float ex = erfcx_poly<float, kErfcxNf>(x, inv_h, nint, tab);
-                const float pref = qq * rinv;
-                fpair += pref * e * (ex + kf * x) * r2inv;
-                ec += pref * e * ex;
-            }
-        }
-        const float fxp = fpair * dx, fyp = fpair * dy, fzp = fpair * dz;
-        fx += fxp;
-        fy += fyp;
-        fz += fzp;
-        if (VIR) {
-            v0 += dx * fxp;
-            v1 += dy * fyp;
-            v2 += dz * fzp;
-            v3 += dx * fyp;
-            v4 += dx * fzp;
-            v5 += dy * fzp;
-        }
+    const RowConst<float> c = row_const<float>(P, (double)__int_as_float(pi.w));
+    RowSums<float> a;
+    // the wrapped integer difference is the exact minimum-image separation
+    auto sep = [&](const int4& pj, float& dx, float& dy, float& dz) {
+        dx = (float)(int)((unsigned)pi.x - (unsigned)pj.x) * sx;
+        dy = (float)(int)((unsigned)pi.y - (unsigned)pj.y) * sy;
+        dz = (float)(int)((unsigned)pi.z - (unsigned)pj.z) * sz;
+    };
+    // the next two entries are loaded while the current two are computed;
+    // an entry past the row end is the atom itself (r^2 = 0, never selected)
+    int k = g;
+    int4 pa = pos[k < nn ? __ldg(row + k) : s];
+    int4 pb = pos[k + G < nn ? __ldg(row + k + G) : s];
+    for (; k < nn; k += 2 * G) {
+        const int kn = k + 2 * G;
+        const int4 na = pos[kn < nn ? __ldg(row + kn) : s];
+        const int4 nb = pos[kn + G < nn ? __ldg(row + kn + G) : s];
+        float dx, dy, dz;
+        sep(pa, dx, dy, dz);
+        pair_term<LJ, CO, VIR>(c, dx, dy, dz, __int_as_float(pa.w), a);
+        sep(pb, dx, dy, dz);
+        pair_term<LJ, CO, VIR>(c, dx, dy, dz, __int_as_float(pb.w), a);
+        pa = na;
+        pb = nb;
     }
-    a.fx = fx;
-    a.fy = fy;
-    a.fz = fz;
-    a.elj += elj;
-    a.ec += ec;
-    if (VIR) {
-        a.v[0] += v0;
-        a.v[1] += v1;
-        a.v[2] += v2;
-        a.v[3] += v3;
-        a.v[4] += v4;
-        a.v[5] += v5;
-    }
+    finish_row(a, acc, VIR);
 }
 
 template <bool MIXED, bool LJ, bool CO, bool VIR>
-ATVB_DEV void row(const SysParams& P, int s, int g, int G, PairAcc& a,
-                  const void* tab) {
+ATVB_DEV void row(const SysParams& P, int s, int g, int G, PairAcc& a) {
     if (MIXED)
-        row_mixed<LJ, CO, VIR>(P, s, g, G, a, (const float*)tab);
+        row_mixed<LJ, CO, VIR>(P, s, g, G, a);
     else
-        row_fp64<LJ, CO, VIR>(P, s, g, G, a, (const double*)tab);
+        row_fp64<LJ, CO, VIR>(P, s, g, G, a);
 }
 
 // Per-item flush: every item's energy/virial partial is rounded to fixed
@@ -239,8 +319,6 @@ template <bool MIXED, int G>
 __global__ void __launch_bounds__(256)
     k_pair(const Item* items, int nitems, const SysParams* sp) {
     __shared__ double sh[32 * 8];
-    __shared__ double tab[kErfcxMaxInt * kErfcxNd]; // erfcx of the current system
-    int tab_sys = -1;
     const int g = threadIdx.x % G;
     const int a_off = threadIdx.x / G;
     PairAcc acc;
@@ -252,39 +330,25 @@ __global__ void __launch_bounds__(256)
         const SysParams& P = sp[item.sys];
         if (P.prec != (MIXED ? kMixed : kFP64))
             continue;
-        if (P.has_coul && item.sys != tab_sys) { // block-uniform
-            __syncthreads();
-            const int nt = P.erfcx_nint * (MIXED ? kErfcxNf : kErfcxNd);
-            if (MIXED) {
-                float* tf = reinterpret_cast<float*>(tab);
-                for (int k = threadIdx.x; k < nt; k += blockDim.x)
-                    tf[k] = P.erfcx_f[k];
-            } else {
-                for (int k = threadIdx.x; k < nt; k += blockDim.x)
-                    tab[k] = P.erfcx_d[k];
-            }
-            __syncthreads();
-            tab_sys = item.sys;
-        }
         const int s = item.begin + a_off;
         acc.fx = acc.fy = acc.fz = 0.0;
         if (s < P.n) {
             const bool lj = P.has_lj, co = P.has_coul, vr = P.need_virial;
             if (lj && co) {
                 if (vr)
-                    row<MIXED, true, true, true>(P, s, g, G, acc, tab);
+                    row<MIXED, true, true, true>(P, s, g, G, acc);
                 else
-                    row<MIXED, true, true, false>(P, s, g, G, acc, tab);
+                    row<MIXED, true, true, false>(P, s, g, G, acc);
             } else if (lj) {
                 if (vr)
-                    row<MIXED, true, false, true>(P, s, g, G, acc, tab);
+                    row<MIXED, true, false, true>(P, s, g, G, acc);
                 else
-                    row<MIXED, true, false, false>(P, s, g, G, acc, tab);
+                    row<MIXED, true, false, false>(P, s, g, G, acc);
             } else if (co) {
                 if (vr)
-                    row<MIXED, false, true, true>(P, s, g, G, acc, tab);
+                    row<MIXED, false, true, true>(P, s, g, G, acc);
                 else
-                    row<MIXED, false, true, false>(P, s, g, G, acc, tab);
+                    row<MIXED, false, true, false>(P, s, g, G, acc);
             }
         }
         double fx = acc.fx, fy = acc.fy, fz = acc.fz;

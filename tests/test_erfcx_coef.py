@@ -1,0 +1,62 @@
+"""The compile-time erfcx polynomial used by the pair kernels (CPU only).
+
+erfcx_coef.h holds one polynomial in u = A t + B, t = 1 / (1 + P x), for
+erfcx(x) = exp(x^2) erfc(x) on 0 <= x <= 6.  Evaluated the way the kernels
+do (Horner, in the storage type), it must match SciPy's erfcx within the
+error written in the header, and that error must be small enough for each
+build: ~1 ulp for FP64, below 1e-6 for the FP32 (mixed) build.
+"""
+import os
+import re
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HDR = os.path.join(ROOT, "atomiverse_b200", "csrc", "erfcx_coef.h")
+
+
+def _parse():
+    txt = open(HDR).read()
+    const = {k: float(v) for k, v in re.findall(r"constexpr double (kErfcx[A-Za-z]+) = ([-0-9.e+]+);", txt)}
+    arrays = {}
+    for name, body in re.findall(r"(kErfcx[DF])\[\d+\] = \{(.*?)\};", txt, flags=re.S):
+        arrays[name] = [float(v.rstrip("f")) for v in re.findall(r"[-0-9.e+]+f?", body)]
+    errs = [float(e) for e in re.findall(r"Horner evaluation: ([0-9.e+-]+)", txt)]
+    return const, arrays, errs
+
+
+def _horner(c, x, P, A, B, dtype):
+    t = (1.0 / (1.0 + P * x)).astype(dtype)
+    u = (dtype(A) * t + dtype(B)).astype(dtype)
+    cc = np.array(c, dtype=dtype)
+    acc = np.full_like(u, cc[-1])
+    for k in range(len(cc) - 2, -1, -1):
+        acc = (acc * u + cc[k]).astype(dtype)
+    return acc
+
+
+def test_erfcx_polynomials_match_scipy():
+    special = pytest.importorskip("scipy.special")
+    const, arrays, errs = _parse()
+    assert const["kErfcxXmax"] == 6.0
+    x = np.linspace(0.0, 6.0, 200001)
+    ref = special.erfcx(x)
+    e64 = np.max(np.abs(_horner(arrays["kErfcxD"], x, const["kErfcxP"], const["kErfcxA"],
+                                const["kErfcxB"], np.float64) / ref - 1))
+    e32 = np.max(np.abs(_horner(arrays["kErfcxF"], x, const["kErfcxP"], const["kErfcxA"],
+                                const["kErfcxB"], np.float32) / ref - 1))
+    assert e64 < 4e-15
+    assert e32 < 1e-6
+    # the header states what its generator measured
+    assert errs[0] < 2e-15 and errs[1] < 1e-6
+
+
+def test_erfc_from_erfcx_and_exp():
+    """erfc(x) = exp(-x^2) erfcx(x): the identity the kernels rely on."""
+    special = pytest.importorskip("scipy.special")
+    const, arrays, _ = _parse()
+    x = np.linspace(0.0, 6.0, 5001)
+    got = np.exp(-x * x) * _horner(arrays["kErfcxD"], x, const["kErfcxP"], const["kErfcxA"],
+                                   const["kErfcxB"], np.float64)
+    assert np.max(np.abs(got / special.erfc(x) - 1)) < 1e-13
