@@ -74,6 +74,11 @@ struct SysParams {
     // lband_lo a candidate is certainly listed, at or above lband_hi it is
     // certainly not; in between the exact FP64 test decides
     float lband_lo, lband_hi;
+    // the same screen in a cell-local FP32 frame (coordinates relative to
+    // the first atom of the home cell); usable when every box edge exceeds
+    // 2 (cutoff + skin + 2 cell diagonals), so no fold is needed
+    int lframe_ok;
+    float fband_lo, fband_hi;
     double skin_half2; // (skin/2)^2
     int nl_every, nl_delay, nl_check;
     int nc[3], ncell;
@@ -137,8 +142,14 @@ struct Item {
 
 ATVB_DEV long long to_fix(double v) { return __double2ll_rn(v * kEFix); }
 
+// Fire-and-forget 64-bit integer reduction (no value returned, so the
+// issuing thread never waits for the L2 round trip).
+ATVB_DEV void red_add_u64(unsigned long long* a, unsigned long long v) {
+    asm volatile("red.global.add.u64 [%0], %1;" ::"l"(a), "l"(v) : "memory");
+}
+
 ATVB_DEV void fix_add(unsigned long long* a, double v) {
-    atomicAdd(a, (unsigned long long)to_fix(v));
+    red_add_u64(a, (unsigned long long)to_fix(v));
 }
 
 template <typename T>

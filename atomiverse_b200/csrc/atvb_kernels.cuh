@@ -7,7 +7,7 @@
 namespace atvb {
 
 constexpr int kChunk = 256;     // atoms per item of the per-atom kernels
-constexpr int kListChunk = 8;   // atoms per item of the list build (warp/atom)
+constexpr int kListChunk = 8;   // cells per item of the list build (warp/cell)
 constexpr int kGridChunk = 4096; // grid points per item of the PME grid kernels
 constexpr int kLaneClasses = 6;  // pair lanes per atom: 1, 2, 4, 8, 16, 32
 
@@ -20,7 +20,7 @@ struct ItemList {
 struct LaunchCfg {
     const SysParams* sp = nullptr; // device table of every system
     ItemList atoms;     // kChunk atoms per item (original or sorted order)
-    ItemList list;      // kListChunk atoms per item
+    ItemList list;      // kListChunk cells per item
     // pair work by [precision][log2 lanes]: each system has its own lane
     // count, chosen from that system alone, so its forces and energies do
     // not depend on which other systems share the engine

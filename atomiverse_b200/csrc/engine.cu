@@ -300,6 +300,22 @@ Slot::Slot(const atvb_system_desc& d, const DevMem& mem) : desc(d), mem_(mem) {
         const double band = 2e-6 * hp.rlist2 + 8.0 * geo.rlist * q + 1e-12;
         hp.lband_lo = std::nextafter((float)(hp.rlist2 - band), 0.0f);
         hp.lband_hi = std::nextafter((float)(hp.rlist2 + band), 3.0e38f);
+        // cell-local frame: coordinates up to R = rlist + 2 cell diagonals
+        // from the origin, each carrying <= 3 FP32 roundings (2^-24 R) plus
+        // the fixed-point quantum; the difference one more rounding
+        const double cdiag = std::sqrt(geo.cs[0] * geo.cs[0] + geo.cs[1] * geo.cs[1] +
+                                       geo.cs[2] * geo.cs[2]);
+        const double R = geo.rlist + 2.0 * cdiag;
+        const double u = 1.0 / 16777216.0;
+        const double ec = 3.0 * u * R + 2.0 * q;
+        const double ed = 2.0 * ec + u * geo.rlist;
+        const double fband = 2.0 * (2.0 * std::sqrt(3.0) * geo.rlist * ed + 3.0 * u * hp.rlist2) + 1e-12;
+        hp.fband_lo = std::nextafter((float)(hp.rlist2 - fband), 0.0f);
+        hp.fband_hi = std::nextafter((float)(hp.rlist2 + fband), 3.0e38f);
+        hp.lframe_ok = 1;
+        for (int k = 0; k < 3; ++k)
+            if (!(0.5 * geo.L[k] > R + 1e-9))
+                hp.lframe_ok = 0;
     }
     hp.skin_half2 = 0.25 * geo.skin * geo.skin;
     hp.nl_every = d.nl_every < 1 ? 1 : d.nl_every;
@@ -683,7 +699,7 @@ void Engine::build_lists() {
         sys.push_back(k);
         for (int b = 0; b < P.n; b += kChunk)
             atoms.push_back({k, b});
-        for (int b = 0; b < P.n; b += kListChunk)
+        for (int b = 0; b < P.ncell; b += kListChunk)
             list.push_back({k, b});
         sp->lanes = lanes_for(*sp);
         if (P.n > largest) {
@@ -995,7 +1011,7 @@ LaunchCfg Engine::restricted_cfg(int id) {
     std::vector<Item> atoms, list, cells, pair, patoms, pgrid, preal;
     for (int b = 0; b < P.n; b += kChunk)
         atoms.push_back({id, b});
-    for (int b = 0; b < P.n; b += kListChunk)
+    for (int b = 0; b < P.ncell; b += kListChunk)
         list.push_back({id, b});
     for (int b = 0; b < P.ncell; b += kChunk)
         cells.push_back({id, b});

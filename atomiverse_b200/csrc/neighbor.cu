@@ -225,25 +225,34 @@ ATVB_DEV void column_runs(const SysParams& P, const int* __restrict__ cstart, in
     }
 }
 
-// Stage 6 (items of kListChunk atoms): one warp per sorted atom.  The lanes
-// first resolve up to 32 stencil columns at once into runs of sorted atoms;
-// a warp prefix sum lays those runs end to end, and the warp then tests 32
-// consecutive candidates per iteration (every lane busy, whatever the column
-// lengths), in column order, compacting hits with a ballot.  Candidates are
-// screened in FP32 on the fixed-point positions (16 bytes per candidate,
-// exact integer minimum image); only those whose FP32 distance lies within
-// the error band of r^2 = (cutoff + skin)^2 take the exact FP64 test, so the
-// listed set is exactly the FP64 one.
+// Stage 6 (items of kListChunk cells): one warp per cell.  Every atom of a
+// cell has the same stencil, so the warp resolves the stencil columns once
+// (up to 32 at a time, one per lane, into runs of sorted atoms laid end to
+// end by a warp prefix sum), loads each window of 32 consecutive candidates
+// once, and tests that window against every atom of the cell in turn,
+// appending hits to that atom's row with a ballot.  Rows list candidates in
+// column order.  Candidates are screened in FP32 on the fixed-point
+// positions (16 bytes per candidate, exact integer minimum image); only
+// those whose FP32 distance lies within the error band of
+// r^2 = (cutoff + skin)^2 take the exact FP64 test, so the listed set is
+// exactly the FP64 one.
+constexpr int kCellAtomsWarp = 32; // atoms of one cell handled per pass
+
 __global__ void __launch_bounds__(256)
     k_build_list(const Item* items, int nitems, const SysParams* sp) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
+    __shared__ int4 sq[8][kCellAtomsWarp];
+    __shared__ float4 sr[8][kCellAtomsWarp];
     for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
         const Item item = items[it];
         const SysParams& P = sp[item.sys];
         if (!P.st->rebuild)
             continue;
+        const int c = item.begin + warp;
+        if (c >= P.ncell)
+            continue; // warp-uniform
         const int nc1 = P.nc[1], nc2 = P.nc[2];
         const double L[3] = {P.L[0], P.L[1], P.L[2]};
         const double hL[3] = {P.halfL[0], P.halfL[1], P.halfL[2]};
@@ -255,72 +264,124 @@ __global__ void __launch_bounds__(256)
         const int4* __restrict__ lp = P.lpos;
         const float sx = P.Lf_fix[0], sy = P.Lf_fix[1], sz = P.Lf_fix[2];
         const float blo = P.lband_lo, bhi = P.lband_hi;
-        const int s = item.begin + warp;
-        if (s >= P.n)
-            continue; // warp-uniform
-        const int4 qi = lp[s];
-        const int c = P.cellS[s];
+        const float flo = P.fband_lo, fhi = P.fband_hi;
+        const bool local = P.lframe_ok != 0;
         const int cz = c % nc2, cy = (c / nc2) % nc1, cx = c / (nc1 * nc2);
-        int* row = P.nbr + (size_t)s * cap;
-        int cnt = 0;
-        for (int c0 = 0; c0 < ncol; c0 += 32) {
-            int a0 = 0, l0 = 0, a1 = 0, l1 = 0;
-            if (c0 + lane < ncol)
-                column_runs(P, cstart, cols[c0 + lane], cx, cy, cz, a0, l0, a1, l1);
-            const int tot = l0 + l1;
-            int incl = tot;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int t = __shfl_up_sync(full, incl, o);
-                if (lane >= o)
-                    incl += t;
+        const int cs = cstart[c], ce = cstart[c + 1];
+        for (int i0 = cs; i0 < ce; i0 += kCellAtomsWarp) {
+            const int ni = min(kCellAtomsWarp, ce - i0);
+            const int4 org = lp[i0];
+            __syncwarp();
+            if (lane < ni) {
+                const int4 q = lp[i0 + lane];
+                sq[warp][lane] = q;
+                sr[warp][lane] = make_float4((float)(int)((unsigned)q.x - (unsigned)org.x) * sx,
+                                             (float)(int)((unsigned)q.y - (unsigned)org.y) * sy,
+                                             (float)(int)((unsigned)q.z - (unsigned)org.z) * sz,
+                                             0.0f);
             }
-            const int excl = incl - tot;
-            const int total = __shfl_sync(full, incl, 31);
-            for (int b = 0; b < total; b += 32) {
-                const int t = b + lane;
-                // owner column: the first lane whose inclusive sum exceeds t
-                int own = 0;
+            __syncwarp();
+            int cnt = 0; // row length of atom i0 + lane
+            for (int c0 = 0; c0 < ncol; c0 += 32) {
+                int a0 = 0, l0 = 0, a1 = 0, l1 = 0;
+                if (c0 + lane < ncol)
+                    column_runs(P, cstart, cols[c0 + lane], cx, cy, cz, a0, l0, a1, l1);
+                const int tot = l0 + l1;
+                int incl = tot;
 #pragma unroll
-                for (int step = 16; step > 0; step >>= 1) {
-                    const int probe = __shfl_sync(full, incl, own + step - 1);
-                    if (probe <= t)
-                        own += step;
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int t = __shfl_up_sync(full, incl, o);
+                    if (lane >= o)
+                        incl += t;
                 }
-                own &= 31;
-                const int o = t - __shfl_sync(full, excl, own);
-                const int oa0 = __shfl_sync(full, a0, own);
-                const int ol0 = __shfl_sync(full, l0, own);
-                const int oa1 = __shfl_sync(full, a1, own);
-                const int j = o < ol0 ? oa0 + o : oa1 + (o - ol0);
-                bool hit = false;
-                if (t < total && j != s) {
-                    // exact integer minimum image, FP32 distance
-                    const int4 qj = lp[j];
-                    const float dx = (float)(int)((unsigned)qi.x - (unsigned)qj.x) * sx;
-                    const float dy = (float)(int)((unsigned)qi.y - (unsigned)qj.y) * sy;
-                    const float dz = (float)(int)((unsigned)qi.z - (unsigned)qj.z) * sz;
-                    const float r2f = dx * dx + dy * dy + dz * dz;
-                    if (r2f < blo)
-                        hit = true;
-                    else if (r2f < bhi) // within the band: exact test
-                        hit = exact_r2(pos[s], pos[j], L, hL) < rl2;
+                const int excl = incl - tot;
+                const int total = __shfl_sync(full, incl, 31);
+                for (int b = 0; b < total; b += 32) {
+                    const int t = b + lane;
+                    // owner column: the first lane whose inclusive sum exceeds t
+                    int own = 0;
+#pragma unroll
+                    for (int step = 16; step > 0; step >>= 1) {
+                        const int probe = __shfl_sync(full, incl, own + step - 1);
+                        if (probe <= t)
+                            own += step;
+                    }
+                    own &= 31;
+                    const int o = t - __shfl_sync(full, excl, own);
+                    const int oa0 = __shfl_sync(full, a0, own);
+                    const int ol0 = __shfl_sync(full, l0, own);
+                    const int oa1 = __shfl_sync(full, a1, own);
+                    const bool live = t < total;
+                    const int j = live ? (o < ol0 ? oa0 + o : oa1 + (o - ol0)) : -1;
+                    int4 qj = make_int4(0, 0, 0, 0);
+                    if (live)
+                        qj = lp[j];
+                    if (local) {
+                        // candidate in the cell-local frame (see lframe_ok)
+                        const float rx = (float)(int)((unsigned)qj.x - (unsigned)org.x) * sx;
+                        const float ry = (float)(int)((unsigned)qj.y - (unsigned)org.y) * sy;
+                        const float rz = (float)(int)((unsigned)qj.z - (unsigned)org.z) * sz;
+                        for (int ii = 0; ii < ni; ++ii) {
+                            const float4 ri = sr[warp][ii];
+                            const float dx = ri.x - rx, dy = ri.y - ry, dz = ri.z - rz;
+                            const float r2f = dx * dx + dy * dy + dz * dz;
+                            const bool valid = live && j != i0 + ii;
+                            bool hit = valid && r2f < flo;
+                            const bool amb = valid && !(r2f < flo) && r2f < fhi;
+                            if (__any_sync(full, amb)) { // rare: exact FP64 test
+                                if (amb)
+                                    hit = exact_r2(pos[i0 + ii], pos[j], L, hL) < rl2;
+                            }
+                            const unsigned m = __ballot_sync(full, hit);
+                            if (m) {
+                                const int base = __shfl_sync(full, cnt, ii);
+                                if (hit) {
+                                    const int wpos = base + __popc(m & lt);
+                                    if (wpos < cap)
+                                        P.nbr[(size_t)(i0 + ii) * cap + wpos] = j;
+                                }
+                                if (lane == ii)
+                                    cnt += __popc(m);
+                            }
+                        }
+                    } else {
+                        // exact integer minimum image (small boxes)
+                        for (int ii = 0; ii < ni; ++ii) {
+                            const int4 qi = sq[warp][ii];
+                            const float dx = (float)(int)((unsigned)qi.x - (unsigned)qj.x) * sx;
+                            const float dy = (float)(int)((unsigned)qi.y - (unsigned)qj.y) * sy;
+                            const float dz = (float)(int)((unsigned)qi.z - (unsigned)qj.z) * sz;
+                            const float r2f = dx * dx + dy * dy + dz * dz;
+                            const bool valid = live && j != i0 + ii;
+                            bool hit = valid && r2f < blo;
+                            const bool amb = valid && !(r2f < blo) && r2f < bhi;
+                            if (__any_sync(full, amb)) {
+                                if (amb)
+                                    hit = exact_r2(pos[i0 + ii], pos[j], L, hL) < rl2;
+                            }
+                            const unsigned m = __ballot_sync(full, hit);
+                            if (m) {
+                                const int base = __shfl_sync(full, cnt, ii);
+                                if (hit) {
+                                    const int wpos = base + __popc(m & lt);
+                                    if (wpos < cap)
+                                        P.nbr[(size_t)(i0 + ii) * cap + wpos] = j;
+                                }
+                                if (lane == ii)
+                                    cnt += __popc(m);
+                            }
+                        }
+                    }
                 }
-                const unsigned m = __ballot_sync(full, hit);
-                if (hit) {
-                    const int wpos = cnt + __popc(m & lt);
-                    if (wpos < cap)
-                        row[wpos] = j;
-                }
-                cnt += __popc(m);
             }
-        }
-        if (lane == 0) {
-            P.nnbr[s] = cnt < cap ? cnt : cap;
-            atomicMax(&P.st->max_nnbr, cnt);
-            atomicAdd(&P.st->list_entries, (unsigned long long)cnt);
-            if (cnt > cap)
-                atomicOr(&P.st->overflow, 1);
+            if (lane < ni) {
+                const int i = i0 + lane;
+                P.nnbr[i] = cnt < cap ? cnt : cap;
+                atomicMax(&P.st->max_nnbr, cnt);
+                atomicAdd(&P.st->list_entries, (unsigned long long)cnt);
+                if (cnt > cap)
+                    atomicOr(&P.st->overflow, 1);
+            }
         }
     }
 }

@@ -139,8 +139,8 @@ __global__ void __launch_bounds__(256)
                 for (int c = 0; c < N; ++c) {
                     const int g2 = gwrap(b2 + c, K2);
                     const double w = (double)(wab * th[2][c]);
-                    atomicAdd(grid + plane + g2,
-                              (unsigned long long)__double2ll_rn(w * gs));
+                    red_add_u64(grid + plane + g2,
+                                (unsigned long long)__double2ll_rn(w * gs));
                 }
             }
         }
