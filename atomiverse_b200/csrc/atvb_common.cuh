@@ -68,6 +68,8 @@ struct SysParams {
     double L[3], invL[3], halfL[3];
     float Lf_fix[3]; // L / 2^32 (mixed: fixed-point position step)
     double fix_scale[3]; // 2^32 / L
+    double fix64_scale[3]; // 2^64 / L
+    double Lfix64[3];      // L / 2^64
     // neighbour list
     double rlist2;     // (cutoff + skin)^2, the pair-set test
     // FP32 prefilter of the pair-set test on fixed-point positions: below
@@ -113,7 +115,7 @@ struct SysParams {
     long long* tag;
     double *xr, *yr, *zr; // positions at the last neighbour build
     // sorted order
-    void* pos4;      // double4 (FP64) or int4 fixed-point + float q (mixed)
+    void* pos4;      // FP64: 64-bit fixed-point x, y, z + q (pack_pos64); mixed: int4 fixed-point + float q
     double4* posd4;  // FP64 sorted positions used by the pair-set test
     int4* lpos;      // fixed-point sorted positions at the last build (prefilter)
     double4* f4;     // forces in sorted order
@@ -211,6 +213,23 @@ ATVB_DEV double min_img(double d, double L, double invL) {
 
 // orthorhombic wrap into [0, L) (pbc.h:48-50)
 ATVB_DEV double wrap(double x, double L) { return x - L * floor(x / L); }
+
+// x in [0, L] -> [0, 2^64) (L itself folds onto 0): the FP64 build's sorted
+// positions, so that the minimum image is an exact integer difference
+ATVB_DEV unsigned long long pos_fix64(double x, double scale) {
+    double t = x * scale;
+    if (t >= 18446744073709551616.0)
+        t -= 18446744073709551616.0;
+    return __double2ull_rn(t);
+}
+
+// FP64 sorted position record: three 64-bit fixed-point coordinates (stored
+// as bit patterns in the x, y, z of a double4) and the charge in w
+ATVB_DEV double4 pack_pos64(const double x[3], const double* scale, double q) {
+    return make_double4(__longlong_as_double((long long)pos_fix64(x[0], scale[0])),
+                        __longlong_as_double((long long)pos_fix64(x[1], scale[1])),
+                        __longlong_as_double((long long)pos_fix64(x[2], scale[2])), q);
+}
 
 ATVB_DEV unsigned int pos_fix(double x, double scale) {
     // x in [0, L] -> [0, 2^32); L itself folds onto 0

@@ -10,6 +10,7 @@ constexpr int kChunk = 256;     // atoms per item of the per-atom kernels
 constexpr int kListChunk = 8;   // cells per item of the list build (warp/cell)
 constexpr int kGridChunk = 4096; // grid points per item of the PME grid kernels
 constexpr int kLaneClasses = 6;  // pair lanes per atom: 1, 2, 4, 8, 16, 32
+constexpr int kPairBlock = 256;  // pair-kernel threads per block (atoms per item = this / lanes)
 
 struct ItemList {
     const Item* d = nullptr; // device array

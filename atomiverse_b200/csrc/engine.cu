@@ -286,6 +286,8 @@ Slot::Slot(const atvb_system_desc& d, const DevMem& mem) : desc(d), mem_(mem) {
         hp.halfL[k] = 0.5 * geo.L[k];
         hp.Lf_fix[k] = (float)(geo.L[k] / 4294967296.0);
         hp.fix_scale[k] = 4294967296.0 / geo.L[k];
+        hp.fix64_scale[k] = 18446744073709551616.0 / geo.L[k];
+        hp.Lfix64[k] = geo.L[k] / 18446744073709551616.0;
         hp.nc[k] = geo.nc[k];
         hp.cs_inv[k] = 1.0 / geo.cs[k];
         hp.alias[k] = geo.alias[k];
@@ -403,7 +405,7 @@ Slot::Slot(const atvb_system_desc& d, const DevMem& mem) : desc(d), mem_(mem) {
     hp.posd4 = (double4*)dalloc((size_t)n * sizeof(double4));
     hp.lpos = (int4*)dalloc((size_t)n * sizeof(int4));
     hp.pos4 = hp.prec == kMixed ? dalloc((size_t)n * sizeof(int4))
-                                : (void*)hp.posd4;
+                                : dalloc((size_t)n * sizeof(double4));
     hp.f4 = (double4*)dalloc((size_t)n * sizeof(double4));
     auto di = [&](size_t cnt) { return (int*)dalloc(cnt * sizeof(int)); };
     hp.perm = di(n);
@@ -708,7 +710,7 @@ void Engine::build_lists() {
         }
         {
             std::vector<Item>& pv = pair_by[P.prec == kMixed ? 1 : 0][lane_class(sp->lanes)];
-            for (int b = 0; b < P.n; b += kChunk / sp->lanes)
+            for (int b = 0; b < P.n; b += kPairBlock / sp->lanes)
                 pv.push_back({k, b});
         }
         for (int b = 0; b < P.ncell; b += kChunk)
@@ -1015,7 +1017,7 @@ LaunchCfg Engine::restricted_cfg(int id) {
         list.push_back({id, b});
     for (int b = 0; b < P.ncell; b += kChunk)
         cells.push_back({id, b});
-    const int pchunk = kChunk / s->lanes;
+    const int pchunk = kPairBlock / s->lanes;
     for (int b = 0; b < P.n; b += pchunk)
         pair.push_back({id, b});
     if (P.has_pme) {

@@ -94,8 +94,7 @@ __global__ void __launch_bounds__(kChunk)
                 p.w = __float_as_int((float)q);
                 reinterpret_cast<int4*>(P.pos4)[r] = p;
             } else {
-                reinterpret_cast<double4*>(P.pos4)[r] =
-                    make_double4(x[0], x[1], x[2], q);
+                reinterpret_cast<double4*>(P.pos4)[r] = pack_pos64(x, P.fix64_scale, q);
             }
             // cell_list.cpp:355-392 with min-image displacement
             const double ddx = min_img(x[0] - P.xr[i], P.L[0], P.invL[0]);

@@ -156,6 +156,10 @@ __global__ void k_permute(const Item* items, int nitems, const SysParams* sp) {
             v.w = __float_as_int((float)q);
             reinterpret_cast<int4*>(P.pos4)[s] = v;
         }
+        else {
+            const double xx[3] = {x, y, z};
+            reinterpret_cast<double4*>(P.pos4)[s] = pack_pos64(xx, P.fix64_scale, q);
+        }
         P.xr[i] = x;
         P.yr[i] = y;
         P.zr[i] = z;

@@ -20,7 +20,9 @@
 // t = 1/(1 + 0.4 x) valid for every system with alpha * cutoff <= 6
 // (erfcx_coef.h, compile-time coefficients: no tables, no shared memory).
 //
-// FP64 build: positions double4 {x, y, z, q}, all arithmetic in double;
+// FP64 build: positions as 64-bit fixed point (2^64 steps per box edge,
+// so the wrapped integer difference is the exact minimum image) + FP64 q;
+// all arithmetic in double;
 // exp and the reciprocal of the erfcx variable are this file's own FP64
 // routines (Cody-Waite exp, Newton reciprocal), accurate to ~1 ulp.
 // Mixed build: positions int4 {x, y, z fixed point with 2^32 steps per box
@@ -220,23 +222,30 @@ ATVB_DEV void row_fp64(const SysParams& P, int s, int g, int G, PairAcc& acc) {
     const double4 pi = pos[s];
     const int nn = P.nnbr[s];
     const int* __restrict__ row = P.nbr + (size_t)s * P.cap;
-    const double L0 = P.L[0], L1 = P.L[1], L2 = P.L[2];
-    const double i0 = P.invL[0], i1 = P.invL[1], i2 = P.invL[2];
     const RowConst<double> c = row_const<double>(P, pi.w);
     RowSums<double> a;
+    // the wrapped 64-bit difference is the exact minimum-image separation
+    const double s0 = P.Lfix64[0], s1 = P.Lfix64[1], s2 = P.Lfix64[2];
+    auto sep = [&](const double4& pj, double& dx, double& dy, double& dz) {
+        dx = (double)(__double_as_longlong(pi.x) - __double_as_longlong(pj.x)) * s0;
+        dy = (double)(__double_as_longlong(pi.y) - __double_as_longlong(pj.y)) * s1;
+        dz = (double)(__double_as_longlong(pi.z) - __double_as_longlong(pj.z)) * s2;
+    };
     int k = g;
     for (; k + G < nn; k += 2 * G) {
         const int ja = __ldg(row + k), jb = __ldg(row + k + G);
         const double4 pa = pos[ja], pb = pos[jb];
-        pair_term<LJ, CO, VIR>(c, min_img(pi.x - pa.x, L0, i0), min_img(pi.y - pa.y, L1, i1),
-                               min_img(pi.z - pa.z, L2, i2), pa.w, a);
-        pair_term<LJ, CO, VIR>(c, min_img(pi.x - pb.x, L0, i0), min_img(pi.y - pb.y, L1, i1),
-                               min_img(pi.z - pb.z, L2, i2), pb.w, a);
+        double dx, dy, dz;
+        sep(pa, dx, dy, dz);
+        pair_term<LJ, CO, VIR>(c, dx, dy, dz, pa.w, a);
+        sep(pb, dx, dy, dz);
+        pair_term<LJ, CO, VIR>(c, dx, dy, dz, pb.w, a);
     }
     if (k < nn) {
         const double4 pa = pos[__ldg(row + k)];
-        pair_term<LJ, CO, VIR>(c, min_img(pi.x - pa.x, L0, i0), min_img(pi.y - pa.y, L1, i1),
-                               min_img(pi.z - pa.z, L2, i2), pa.w, a);
+        double dx, dy, dz;
+        sep(pa, dx, dy, dz);
+        pair_term<LJ, CO, VIR>(c, dx, dy, dz, pa.w, a);
     }
     finish_row(a, acc, VIR);
 }
@@ -315,8 +324,9 @@ ATVB_DEV void flush_energy(const SysParams& P, PairAcc& a, double* sh) {
         a.v[k] = 0.0;
 }
 
+// Mixed: at least 4 resident blocks (64 registers); FP64: 2.
 template <bool MIXED, int G>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, MIXED ? 4 : 2)
     k_pair(const Item* items, int nitems, const SysParams* sp) {
     __shared__ double sh[32 * 8];
     const int g = threadIdx.x % G;
@@ -368,17 +378,17 @@ template <bool MIXED>
 static void launch_pair_prec(const LaunchCfg& lc, cudaStream_t s) {
     const ItemList* L = lc.pair[MIXED ? 1 : 0];
     if (L[0].n)
-        k_pair<MIXED, 1><<<L[0].grid, 256, 0, s>>>(L[0].d, L[0].n, lc.sp);
+        k_pair<MIXED, 1><<<L[0].grid, kPairBlock, 0, s>>>(L[0].d, L[0].n, lc.sp);
     if (L[1].n)
-        k_pair<MIXED, 2><<<L[1].grid, 256, 0, s>>>(L[1].d, L[1].n, lc.sp);
+        k_pair<MIXED, 2><<<L[1].grid, kPairBlock, 0, s>>>(L[1].d, L[1].n, lc.sp);
     if (L[2].n)
-        k_pair<MIXED, 4><<<L[2].grid, 256, 0, s>>>(L[2].d, L[2].n, lc.sp);
+        k_pair<MIXED, 4><<<L[2].grid, kPairBlock, 0, s>>>(L[2].d, L[2].n, lc.sp);
     if (L[3].n)
-        k_pair<MIXED, 8><<<L[3].grid, 256, 0, s>>>(L[3].d, L[3].n, lc.sp);
+        k_pair<MIXED, 8><<<L[3].grid, kPairBlock, 0, s>>>(L[3].d, L[3].n, lc.sp);
     if (L[4].n)
-        k_pair<MIXED, 16><<<L[4].grid, 256, 0, s>>>(L[4].d, L[4].n, lc.sp);
+        k_pair<MIXED, 16><<<L[4].grid, kPairBlock, 0, s>>>(L[4].d, L[4].n, lc.sp);
     if (L[5].n)
-        k_pair<MIXED, 32><<<L[5].grid, 256, 0, s>>>(L[5].d, L[5].n, lc.sp);
+        k_pair<MIXED, 32><<<L[5].grid, kPairBlock, 0, s>>>(L[5].d, L[5].n, lc.sp);
 }
 
 void launch_pair(const LaunchCfg& lc, cudaStream_t s) {

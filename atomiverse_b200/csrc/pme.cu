@@ -89,16 +89,16 @@ ATVB_DEV void atom_splines(const SysParams& P, int s, T th[3][N], T dth[3][N],
     } else {
         const double4 p = reinterpret_cast<const double4*>(P.pos4)[s];
         q = p.w;
-        const double x[3] = {p.x, p.y, p.z};
+        const unsigned long long u[3] = {(unsigned long long)__double_as_longlong(p.x),
+                                         (unsigned long long)__double_as_longlong(p.y),
+                                         (unsigned long long)__double_as_longlong(p.z)};
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
-            // pme_spline.h:131-141
-            const double sd = P.invL[d] * x[d];
-            double u = sd * P.K[d];
-            u -= floor(u / P.K[d]) * P.K[d];
-            const double u0 = floor(u);
+            // fixed-point position is the fractional coordinate * 2^64
+            const double uu = (double)u[d] * ((double)P.K[d] * 5.421010862427522e-20);
+            const double u0 = floor(uu);
             base[d] = base_index(u0, P.K[d]);
-            bspline_dev<N, T>((T)(u - u0), th[d], dth[d]);
+            bspline_dev<N, T>((T)(uu - u0), th[d], dth[d]);
         }
     }
 }
