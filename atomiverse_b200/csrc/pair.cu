@@ -128,7 +128,13 @@ template <typename T>
 struct RowSums {
     T fx = 0, fy = 0, fz = 0, elj = 0, ec = 0;
     T v[6] = {0, 0, 0, 0, 0, 0};
+    // mixed build: force components summed in 64-bit fixed point, units of
+    // kForceFix^-1 eV/A (range +-2e9 eV/A), so the row sum is exact and
+    // independent of summation order
+    long long fq[3] = {0, 0, 0};
 };
+constexpr float kForceFix = 4294967296.0f;  // 2^32
+constexpr double kForceFixInv = 1.0 / 4294967296.0;
 
 // One pair (i, j) at separation (dx, dy, dz), charge product factor qj.
 // Cutoffs are applied by selection, not branches: every lane of a warp runs
@@ -174,9 +180,15 @@ ATVB_DEV void pair_term(const RowConst<T>& c, T dx, T dy, T dz, T qj,
         a.ec += in ? pref * p : T(0);
     }
     const T fxp = fpair * dx, fyp = fpair * dy, fzp = fpair * dz;
-    a.fx += fxp;
-    a.fy += fyp;
-    a.fz += fzp;
+    if constexpr (F) {
+        a.fq[0] += __float2ll_rn(fxp * kForceFix);
+        a.fq[1] += __float2ll_rn(fyp * kForceFix);
+        a.fq[2] += __float2ll_rn(fzp * kForceFix);
+    } else {
+        a.fx += fxp;
+        a.fy += fyp;
+        a.fz += fzp;
+    }
     if (VIR) {
         a.v[0] += dx * fxp;
         a.v[1] += dy * fyp;
@@ -189,9 +201,17 @@ ATVB_DEV void pair_term(const RowConst<T>& c, T dx, T dy, T dz, T qj,
 
 template <typename T>
 ATVB_DEV void finish_row(const RowSums<T>& r, PairAcc& a, bool vir) {
-    a.fx = (double)r.fx;
-    a.fy = (double)r.fy;
-    a.fz = (double)r.fz;
+    if constexpr (sizeof(T) == 4) {
+        // multiples of 2^-32 below 2^21 in magnitude: every later FP64 sum of
+        // the lanes' values is exact, so the force is order-independent
+        a.fx = (double)r.fq[0] * kForceFixInv;
+        a.fy = (double)r.fq[1] * kForceFixInv;
+        a.fz = (double)r.fq[2] * kForceFixInv;
+    } else {
+        a.fx = (double)r.fx;
+        a.fy = (double)r.fy;
+        a.fz = (double)r.fz;
+    }
     a.elj += (double)r.elj;
     a.ec += (double)r.ec;
     if (vir)
@@ -324,9 +344,9 @@ ATVB_DEV void flush_energy(const SysParams& P, PairAcc& a, double* sh) {
         a.v[k] = 0.0;
 }
 
-// Mixed: at least 4 resident blocks (64 registers); FP64: 2.
+// Mixed: at least 3 resident blocks (80 registers); FP64: 2.
 template <bool MIXED, int G>
-__global__ void __launch_bounds__(256, MIXED ? 4 : 2)
+__global__ void __launch_bounds__(256, MIXED ? 3 : 2)
     k_pair(const Item* items, int nitems, const SysParams* sp) {
     __shared__ double sh[32 * 8];
     const int g = threadIdx.x % G;

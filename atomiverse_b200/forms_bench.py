@@ -73,6 +73,7 @@ def precision_study(args):
     ctx = A.Context(0)
     desc, frame = W.lj_fcc(ncell=args.ncell, t_star=0.72, seed=2028, precision=A.FP64)
     desc["history_capacity"] = max(args.steps, 16)
+    desc["stress_required"] = 1  # the virial is one of the compared quantities
     n = desc["n_atoms"]
     # the perfect lattice has (numerically) zero forces, so errors are taken
     # on a thermalised snapshot: the FP64 build run `equil` steps from the
@@ -183,12 +184,19 @@ def ladder(args):
         d64 = dict(d, precision=A.FP64)
         s = A.System(ctx, d64, f)
         s.compute_forces()
-        o64, _ = s.download()
         s.step(args.warmup)
         ms, _ = s.step_timed(args.plain_steps)
         t_plain += ms * 1e-3 / args.plain_steps
+        # force error on the thermalised state this run reached (the FCC
+        # start has near-zero forces): both builds from the same snapshot
+        snap, _ = s.download()
         s.close()
-        sm = A.System(ctx, d, f)
+        f2 = dict(f, **{c: snap[c] for c in ("x", "y", "z", "vx", "vy", "vz")})
+        s64 = A.System(ctx, d64, f2)
+        s64.compute_forces()
+        o64, _ = s64.download()
+        s64.close()
+        sm = A.System(ctx, d, f2)
         sm.compute_forces()
         o32, _ = sm.download()
         sm.close()

@@ -145,6 +145,21 @@ def _max_over_ranks(dist, local, v: float) -> float:
     return float(t.item())
 
 
+def pairs_within(system, desc, rc: float):
+    """Unordered pairs closer than rc at the system's current positions
+    (periodic k-d tree count on the host, outside every timed region)."""
+    try:
+        from scipy.spatial import cKDTree
+    except ImportError:
+        return None
+    out, _ = system.download(keys=("x", "y", "z"))
+    L = np.asarray(desc["box"][:3], dtype=np.float64)
+    pts = np.mod(np.stack([out["x"], out["y"], out["z"]], axis=1), L)
+    tree = cKDTree(pts, boxsize=L)
+    ordered = int(tree.count_neighbors(tree, rc))
+    return (ordered - len(pts)) // 2
+
+
 def cpu_baseline(budget_s: float = 20.0, max_steps: int = 5):
     """The oracle (the FP64 CPU restatement of the reference path) on all
     host cores: neighbour list + forces at setup, then timed MD steps until
@@ -250,16 +265,26 @@ def main():
                for k, v in prof.items()}
 
     # ---- mixed-precision leg on the same workload (reported beside)
-    mixed = None
-    if True:
-        d2, f2 = W.rocksalt_melt(precision=A.MIXED)
-        sm = A.System(ctx, d2, f2)
-        sm.compute_forces()
-        sm.step(args.warmup)
-        tm, _ = sm.step_timed(args.steps)
-        tm = _max_over_ranks(dist, local, tm)
-        mixed = ws * args.steps / (tm * 1e-3)
-        del sm
+    d2, f2 = W.rocksalt_melt(precision=A.MIXED)
+    sm = A.System(ctx, d2, f2)
+    sm.compute_forces()
+    sm.step(args.warmup)
+    tm, _ = sm.step_timed(args.steps)
+    tm = _max_over_ranks(dist, local, tm)
+    mixed = ws * args.steps / (tm * 1e-3)
+    sm.profile(True)
+    sm.step(args.steps)
+    mprof = sm.profile_read()
+    sm.profile(False)
+    mpair_ms, mpair_n = mprof.get("pair", (float("nan"), 1))
+    mpair_s = mpair_ms / mpair_n * 1e-3
+    # mixed algorithmic bytes: int4 position + float charge 16 B, force 24 B
+    b_alg_m = n * (16 + 24) + 4 * sm.scalars()["list_pairs"]
+    mixed_roofline = {"bound": "hbm", "achieved": b_alg_m / mpair_s / 1e9, "peak": peak,
+                      "unit": "GB/s", "frac": b_alg_m / mpair_s / 1e9 / peak,
+                      "traffic": _traffic("k_pair_mixed_config1"), "kernel": "k_pair<mixed>",
+                      "algorithmic_bytes": b_alg_m, "pair_launch_ms": mpair_s * 1e3}
+    del sm
 
     # ---- end to end through the C ABI with host buffers: upload from
     # pinned host memory, force pass, K steps, per-step energies (history
@@ -285,6 +310,7 @@ def main():
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         cpu = cpu_baseline()
+    p_rc = pairs_within(sys_, desc, 12.0) if rank == 0 else None
 
     if rank == 0:
         steps_s = value
@@ -301,7 +327,9 @@ def main():
             "ns_per_day_per_replica": ns_day,
             "p50_ms": float(np.percentile(per_step, 50)),
             "p99_ms": float(np.percentile(per_step, 99)),
-            "pair_interactions_per_s": p_half * steps_s,
+            "pair_interactions_per_s": (p_rc if p_rc is not None else p_half) * steps_s,
+            "pairs_within_cutoff": p_rc, "pairs_in_list": p_half,
+            "mixed_roofline": mixed_roofline,
             "neighbor_rebuilds": sc1["rebuilds"] - sc0["rebuilds"],
             "mixed_precision_value": mixed,
             "gpu_launches": launches,
