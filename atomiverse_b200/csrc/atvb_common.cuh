@@ -59,6 +59,8 @@ struct SysState {
     int max_nnbr;      // largest row seen at the last build
     int status;        // sticky error bits
     unsigned long long list_entries; // row entries of the last build (2 x pairs)
+    int nearq_n;       // mixed build: pairs queued this step for an exact LJ cutoff test
+    int nearq_lost;    // pairs that did not fit the queue (decided in FP32)
 };
 
 struct SysParams {
@@ -92,6 +94,11 @@ struct SysParams {
     // LJ
     int has_lj;
     double lj_rc2, lj_sig6, lj_eps4, lj_eps24, lj_shift;
+    // mixed build: FP32 error band of r^2 around the LJ and Coulomb cutoffs,
+    // and the queue of (sorted i, sorted j) pairs found inside the LJ band
+    double mix_band_lj, mix_band_c;
+    int2* nearq;
+    int nearq_cap;
     // real-space Coulomb
     int has_coul;
     double coul_rc2, coul_alpha, coul_alpha2;

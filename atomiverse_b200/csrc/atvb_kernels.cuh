@@ -34,6 +34,7 @@ struct LaunchCfg {
     int nsys = 0;
     int pair_G = 4;     // lanes per atom of the largest system (reported)
     int any_mixed = 0, any_fp64 = 0;
+    int any_near = 0;   // a mixed system settles near-cutoff LJ pairs (k_pair_fix)
     int pme_order = 4;  // common PME order (the PME kernels are templated)
     int pme_mixed = 0;
 };
@@ -42,6 +43,7 @@ struct LaunchCfg {
 void launch_rebuild(const LaunchCfg& lc, cudaStream_t s);
 // pair.cu
 void launch_pair(const LaunchCfg& lc, cudaStream_t s);
+void launch_pair_fix(const LaunchCfg& lc, cudaStream_t s);
 // pme.cu
 void launch_pme_spread(const LaunchCfg& lc, cudaStream_t s);
 void launch_pme_convert(const LaunchCfg& lc, cudaStream_t s);

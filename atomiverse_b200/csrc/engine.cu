@@ -341,6 +341,28 @@ Slot::Slot(const atvb_system_desc& d, const DevMem& mem) : desc(d), mem_(mem) {
         const double r6inv = r2inv * r2inv * r2inv * hp.lj_sig6;
         hp.lj_shift = 4.0 * d.lj_epsilon * (r6inv * r6inv - r6inv);
     }
+    {
+        // |r2_fp32 - r2_fp64| <= 10 2^-24 r2 (conversion, scale, product,
+        // squares and sums) + 2 sqrt(3) r q (32-bit fixed-point quantum q on
+        // both atoms); the band doubles it
+        const double q = std::max(geo.L[0], std::max(geo.L[1], geo.L[2])) / 4294967296.0;
+        auto band = [&](double rc) {
+            return 2.0 * (10.0 / 16777216.0 * rc * rc + 2.0 * std::sqrt(3.0) * rc * q);
+        };
+        hp.mix_band_lj = d.lj_enabled ? band(d.lj_cutoff) : 0.0;
+        // a pair that FP32 rounding moves across the LJ cutoff changes the
+        // forces by the force jump there (the energy is shifted, the force
+        // is not); below 1e-5 eV/A that is negligible and the settling is
+        // off (e.g. LJ cut at 4 sigma under Coulomb: 2.5e-6 eV/A)
+        if (d.lj_enabled) {
+            const double sr2 = d.lj_sigma * d.lj_sigma / (d.lj_cutoff * d.lj_cutoff);
+            const double sr6 = sr2 * sr2 * sr2;
+            const double jump = std::fabs(24.0 * d.lj_epsilon / d.lj_cutoff * (2.0 * sr6 * sr6 - sr6));
+            if (jump < 1e-5)
+                hp.mix_band_lj = 0.0;
+        }
+        hp.mix_band_c = d.coul_enabled ? band(d.coul_cutoff) : 0.0;
+    }
     hp.has_coul = d.coul_enabled ? 1 : 0;
     if (hp.has_coul) {
         if (!(d.coul_alpha > 0.0) || !(d.coul_cutoff > 0.0))
@@ -404,6 +426,10 @@ Slot::Slot(const atvb_system_desc& d, const DevMem& mem) : desc(d), mem_(mem) {
     hp.tag = (long long*)dalloc((size_t)n * 8);
     hp.posd4 = (double4*)dalloc((size_t)n * sizeof(double4));
     hp.lpos = (int4*)dalloc((size_t)n * sizeof(int4));
+    if (hp.prec == kMixed && d.lj_enabled) {
+        hp.nearq_cap = std::max(4096, n / 16);
+        hp.nearq = (int2*)dalloc((size_t)hp.nearq_cap * sizeof(int2));
+    }
     hp.pos4 = hp.prec == kMixed ? dalloc((size_t)n * sizeof(int4))
                                 : dalloc((size_t)n * sizeof(double4));
     hp.f4 = (double4*)dalloc((size_t)n * sizeof(double4));
@@ -717,6 +743,8 @@ void Engine::build_lists() {
             cells.push_back({k, b});
         if (P.prec == kMixed)
             lc_.any_mixed = 1;
+        if (P.prec == kMixed && P.has_lj && P.mix_band_lj > 0.0)
+            lc_.any_near = 1;
         else
             lc_.any_fp64 = 1;
         if (P.has_pme) {
@@ -773,6 +801,7 @@ int64_t Engine::kernels_per_step() const {
     for (int p = 0; p < 2; ++p)                // pair: one per lane class used
         for (int c = 0; c < kLaneClasses; ++c)
             k += lc_.pair[p][c].n ? 1 : 0;
+    k += lc_.any_near ? 1 : 0;                // near-cutoff fix-up (mixed LJ)
     if (!pme_slots_.empty())
         k += 4;                               // spread, convert, influence, gather
     k += 2;                                   // integrate_b, sys_b
@@ -783,6 +812,10 @@ void Engine::enqueue_forces(const LaunchCfg& lc, const std::vector<int>& pme,
                             bool profile) {
     prof_mark(profile, "pair");
     launch_pair(lc, stream_);
+    if (lc.any_near) {
+        prof_mark(profile, "pair_fix");
+        launch_pair_fix(lc, stream_);
+    }
     if (!pme.empty()) {
         prof_mark(profile, "pme_spread");
         launch_pme_spread(lc, stream_);
@@ -1045,6 +1078,7 @@ LaunchCfg Engine::restricted_cfg(int id) {
     c.pme_real = make_list(list_allocs_, preal, num_sms_ * 16, mem_);
     c.any_mixed = P.prec == kMixed;
     c.any_fp64 = P.prec != kMixed;
+    c.any_near = P.prec == kMixed && P.has_lj && P.mix_band_lj > 0.0;
     if (P.has_pme) {
         c.pme_mixed = P.prec == kMixed;
         c.pme_order = P.order;

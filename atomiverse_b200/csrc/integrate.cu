@@ -121,6 +121,7 @@ __global__ void k_sys_a(const int* sys_list, int nsys, const SysParams* sp) {
     const SysParams& P = sp[sys_list[k]];
     SysState* st = P.st;
     st->vscale = 1.0;
+    st->nearq_n = 0; // the previous step's near-cutoff queue has been settled
     if (P.thermostat == kNoseHoover) {
         const double ke = fix_to_d(st->acc[kAccKEA]);
         st->acc[kAccKEA] = 0ull;
@@ -258,6 +259,8 @@ __global__ void k_force_rebuild(const int* sys_list, int nsys,
     st->acc[kAccELJ] = st->acc[kAccECoul] = st->acc[kAccERecip] = 0ull;
     for (int v = 0; v < 6; ++v)
         st->acc[kAccVir + v] = 0ull;
+    st->nearq_n = 0; // nothing queued by launches outside a force pass counts
+    st->nearq_lost = 0;
 }
 
 // After an upload: wrap positions into [0, L) (pbc.h:48-50) and keep the

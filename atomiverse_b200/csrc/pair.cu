@@ -122,6 +122,7 @@ struct RowConst {
     T lj_rc2, sig6, eps4, eps24, shift;
     T c_rc2, alpha, alpha2; // alpha2: alpha^2 (FP64) or alpha^2 log2(e) (FP32)
     T kqi;
+    T band_lj, band_c; // FP32 only: error band of r^2 around each cutoff
 };
 
 template <typename T>
@@ -140,26 +141,45 @@ constexpr double kForceFixInv = 1.0 / 4294967296.0;
 // Cutoffs are applied by selection, not branches: every lane of a warp runs
 // the same instructions, and a value computed outside its range (including
 // r^2 = 0) is never selected.
+//
+// FP32 only: the cutoff tests decide which pairs exist, and the shifted LJ
+// force jumps at its cutoff, so a pair that FP32 rounding moves across a
+// cutoff would cost a whole pair force.  `near` reports an r^2 within the
+// FP32 error band of the LJ cutoff (a ~1e-6-thick shell, ~1e-5 of pairs);
+// such pairs are queued and k_pair_fix settles them on the FP64 positions.
+// `force` >= 0 overrides the decisions (bit 0 LJ, bit 1 Coulomb) and `neg`
+// subtracts the term instead of adding it (k_pair_fix only).
 template <bool LJ, bool CO, bool VIR, typename T>
 ATVB_DEV void pair_term(const RowConst<T>& c, T dx, T dy, T dz, T qj,
-                        RowSums<T>& a) {
+                        RowSums<T>& a, bool& near, int force = -1, bool neg = false) {
     constexpr bool F = sizeof(T) == 4;
     const T r2 = dx * dx + dy * dy + dz * dz;
     const bool ok = r2 >= (T)kMinPair2;
+    bool in_lj = ok && r2 < c.lj_rc2, in_c = ok && r2 < c.c_rc2;
+    if constexpr (F) {
+        // only the LJ cutoff: the real-space Coulomb force at its cutoff is
+        // damped by erfc(alpha rc) (~3e-5 eV/A per pair at alpha rc = 3),
+        // so a flipped Coulomb pair moves the forces by ~1e-7 relative
+        near = LJ && fabsf(r2 - c.lj_rc2) < c.band_lj;
+        if (force >= 0) {
+            in_lj = force & 1;
+            in_c = (force >> 1) & 1;
+        }
+    }
     T rinv;
     if constexpr (F)
         rinv = rsqrt_approx(r2);
     else
         rinv = rsqrt(r2);
     const T r2inv = rinv * rinv;
+    const T sg = neg ? T(-1) : T(1);
     T fpair = 0;
     if (LJ) {
         const T r6 = r2inv * r2inv * r2inv * c.sig6;
         const T flj = c.eps24 * r2inv * r6 * (T(2) * r6 - T(1));
         const T elj = c.eps4 * r6 * (r6 - T(1)) - c.shift;
-        const bool in = ok && r2 < c.lj_rc2;
-        fpair = in ? flj : T(0);
-        a.elj += in ? elj : T(0);
+        fpair = in_lj ? flj : T(0);
+        a.elj += in_lj ? sg * elj : T(0);
     }
     if (CO) {
         // erfc(x) = exp(-x^2) erfcx(x), x = alpha r
@@ -175,27 +195,29 @@ ATVB_DEV void pair_term(const RowConst<T>& c, T dx, T dy, T dz, T qj,
         }
         const T p = erfcx_of_t(t);
         const T pref = qq * rinv * e;
-        const bool in = ok && r2 < c.c_rc2;
-        fpair += in ? pref * (p + (T)kEwaldF * x) * r2inv : T(0);
-        a.ec += in ? pref * p : T(0);
+        fpair += in_c ? pref * (p + (T)kEwaldF * x) * r2inv : T(0);
+        a.ec += in_c ? sg * (pref * p) : T(0);
     }
     const T fxp = fpair * dx, fyp = fpair * dy, fzp = fpair * dz;
     if constexpr (F) {
-        a.fq[0] += __float2ll_rn(fxp * kForceFix);
-        a.fq[1] += __float2ll_rn(fyp * kForceFix);
-        a.fq[2] += __float2ll_rn(fzp * kForceFix);
+        const long long qx = __float2ll_rn(fxp * kForceFix);
+        const long long qy = __float2ll_rn(fyp * kForceFix);
+        const long long qz = __float2ll_rn(fzp * kForceFix);
+        a.fq[0] += neg ? -qx : qx;
+        a.fq[1] += neg ? -qy : qy;
+        a.fq[2] += neg ? -qz : qz;
     } else {
         a.fx += fxp;
         a.fy += fyp;
         a.fz += fzp;
     }
     if (VIR) {
-        a.v[0] += dx * fxp;
-        a.v[1] += dy * fyp;
-        a.v[2] += dz * fzp;
-        a.v[3] += dx * fyp;
-        a.v[4] += dx * fzp;
-        a.v[5] += dy * fzp;
+        a.v[0] += sg * (dx * fxp);
+        a.v[1] += sg * (dy * fyp);
+        a.v[2] += sg * (dz * fzp);
+        a.v[3] += sg * (dx * fyp);
+        a.v[4] += sg * (dx * fzp);
+        a.v[5] += sg * (dy * fzp);
     }
 }
 
@@ -231,6 +253,8 @@ ATVB_DEV RowConst<T> row_const(const SysParams& P, double qi) {
     c.alpha = (T)P.coul_alpha;
     c.alpha2 = sizeof(T) == 4 ? (T)(P.coul_alpha2 * 1.4426950408889634) : (T)P.coul_alpha2;
     c.kqi = (T)(kQqr2e * qi);
+    c.band_lj = (T)P.mix_band_lj;
+    c.band_c = (T)P.mix_band_c;
     return c;
 }
 
@@ -244,6 +268,7 @@ ATVB_DEV void row_fp64(const SysParams& P, int s, int g, int G, PairAcc& acc) {
     const int* __restrict__ row = P.nbr + (size_t)s * P.cap;
     const RowConst<double> c = row_const<double>(P, pi.w);
     RowSums<double> a;
+    bool near;
     // the wrapped 64-bit difference is the exact minimum-image separation
     const double s0 = P.Lfix64[0], s1 = P.Lfix64[1], s2 = P.Lfix64[2];
     auto sep = [&](const double4& pj, double& dx, double& dy, double& dz) {
@@ -257,20 +282,54 @@ ATVB_DEV void row_fp64(const SysParams& P, int s, int g, int G, PairAcc& acc) {
         const double4 pa = pos[ja], pb = pos[jb];
         double dx, dy, dz;
         sep(pa, dx, dy, dz);
-        pair_term<LJ, CO, VIR>(c, dx, dy, dz, pa.w, a);
+        pair_term<LJ, CO, VIR>(c, dx, dy, dz, pa.w, a, near);
         sep(pb, dx, dy, dz);
-        pair_term<LJ, CO, VIR>(c, dx, dy, dz, pb.w, a);
+        pair_term<LJ, CO, VIR>(c, dx, dy, dz, pb.w, a, near);
     }
     if (k < nn) {
         const double4 pa = pos[__ldg(row + k)];
         double dx, dy, dz;
         sep(pa, dx, dy, dz);
-        pair_term<LJ, CO, VIR>(c, dx, dy, dz, pa.w, a);
+        pair_term<LJ, CO, VIR>(c, dx, dy, dz, pa.w, a, near);
     }
     finish_row(a, acc, VIR);
 }
 
-template <bool LJ, bool CO, bool VIR>
+// Cutoff decisions of sorted pair (s, j) from the FP64 master positions,
+// through the same 64-bit fixed-point minimum image as the FP64 build:
+// bit 0 = inside the LJ cutoff, bit 1 = inside the Coulomb cutoff.  Out of
+// line: it runs for ~1e-4 of the pairs and must not cost the hot loop
+// registers.
+__device__ __noinline__ unsigned exact_cutoffs(const SysParams& P, int s, int j) {
+    const int io = P.perm[s], jo = P.perm[j];
+    const double xi[3] = {P.x[io], P.y[io], P.z[io]};
+    const double xj[3] = {P.x[jo], P.y[jo], P.z[jo]};
+    double r2d = 0.0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const long long di = (long long)(pos_fix64(xi[d], P.fix64_scale[d]) -
+                                         pos_fix64(xj[d], P.fix64_scale[d]));
+        const double dd = (double)di * P.Lfix64[d];
+        r2d += dd * dd;
+    }
+    if (!(r2d >= kMinPair2))
+        return 0u;
+    return (r2d < P.lj_rc2 ? 1u : 0u) | (r2d < P.coul_rc2 ? 2u : 0u);
+}
+
+// A lane's share of row s (entries g, g+G, ...) held a pair whose FP32 r^2
+// fell in the LJ cutoff's error band: queued for k_pair_fix, which rescans
+// that share and settles such pairs on the FP64 positions (rare: ~1e-5 of
+// the pairs, one queue entry per affected lane).  code = g | (G << 6).
+ATVB_DEV void queue_near(const SysParams& P, int s, int code) {
+    const int q = atomicAdd(&P.st->nearq_n, 1);
+    if (q < P.nearq_cap)
+        P.nearq[q] = make_int2(s, code);
+    else
+        atomicAdd(&P.st->nearq_lost, 1);
+}
+
+template <bool LJ, bool CO, bool VIR, bool NEAR>
 ATVB_DEV void row_mixed(const SysParams& P, int s, int g, int G, PairAcc& acc) {
     const int4* __restrict__ pos = reinterpret_cast<const int4*>(P.pos4);
     const int4 pi = pos[s];
@@ -287,6 +346,8 @@ ATVB_DEV void row_mixed(const SysParams& P, int s, int g, int G, PairAcc& acc) {
     };
     // the next two entries are loaded while the current two are computed;
     // an entry past the row end is the atom itself (r^2 = 0, never selected)
+    bool near;
+    int n_near = 0;
     int k = g;
     int4 pa = pos[k < nn ? __ldg(row + k) : s];
     int4 pb = pos[k + G < nn ? __ldg(row + k + G) : s];
@@ -296,21 +357,32 @@ ATVB_DEV void row_mixed(const SysParams& P, int s, int g, int G, PairAcc& acc) {
         const int4 nb = pos[kn + G < nn ? __ldg(row + kn + G) : s];
         float dx, dy, dz;
         sep(pa, dx, dy, dz);
-        pair_term<LJ, CO, VIR>(c, dx, dy, dz, __int_as_float(pa.w), a);
+        pair_term<LJ, CO, VIR>(c, dx, dy, dz, __int_as_float(pa.w), a, near);
+        if (NEAR)
+            n_near += near;
         sep(pb, dx, dy, dz);
-        pair_term<LJ, CO, VIR>(c, dx, dy, dz, __int_as_float(pb.w), a);
+        pair_term<LJ, CO, VIR>(c, dx, dy, dz, __int_as_float(pb.w), a, near);
+        if (NEAR)
+            n_near += near;
         pa = na;
         pb = nb;
     }
+    if (NEAR && n_near)
+        queue_near(P, s, g | (G << 6));
     finish_row(a, acc, VIR);
 }
 
 template <bool MIXED, bool LJ, bool CO, bool VIR>
 ATVB_DEV void row(const SysParams& P, int s, int g, int G, PairAcc& a) {
-    if (MIXED)
-        row_mixed<LJ, CO, VIR>(P, s, g, G, a);
-    else
+    if (MIXED) {
+        // near-cutoff settling only where the LJ force jump matters
+        if (LJ && P.mix_band_lj > 0.0)
+            row_mixed<LJ, CO, VIR, true>(P, s, g, G, a);
+        else
+            row_mixed<LJ, CO, VIR, false>(P, s, g, G, a);
+    } else {
         row_fp64<LJ, CO, VIR>(P, s, g, G, a);
+    }
 }
 
 // Per-item flush: every item's energy/virial partial is rounded to fixed
@@ -394,6 +466,82 @@ __global__ void __launch_bounds__(256, MIXED ? 3 : 2)
     }
 }
 
+// Settles the near-cutoff pairs of the queued lane shares (one warp per
+// queue entry, kFixBlocks blocks per system): every entry of the share is
+// recomputed exactly as the pair kernel computed it, and a pair inside the
+// LJ band is subtracted and added back under the FP64 cutoff decisions.
+// Force corrections are whole multiples of 2^-32 eV/A and so are the pair
+// kernel's forces, so the additions are exact and their order does not
+// matter; energy and virial corrections go to the fixed-point accumulators
+// (x 1/2: each pair sits in both of its rows).  Runs after the pair kernel
+// and before the PME gather adds to the same forces.  The queue is emptied
+// at the start of the next step (k_sys_a) or force pass.
+constexpr int kFixBlocks = 16;
+
+template <bool LJ, bool CO, bool VIR>
+ATVB_DEV void fix_share(const SysParams& P, int s, int code, int lane) {
+    const int g = code & 63, G = code >> 6;
+    const int4* __restrict__ pos = reinterpret_cast<const int4*>(P.pos4);
+    const int4 pi = pos[s];
+    const int nn = P.nnbr[s];
+    const int* __restrict__ row = P.nbr + (size_t)s * P.cap;
+    const RowConst<float> c = row_const<float>(P, (double)__int_as_float(pi.w));
+    for (int k = g + G * lane; k < nn; k += 32 * G) {
+        const int j = __ldg(row + k);
+        const int4 pj = pos[j];
+        const float dx = (float)(int)((unsigned)pi.x - (unsigned)pj.x) * P.Lf_fix[0];
+        const float dy = (float)(int)((unsigned)pi.y - (unsigned)pj.y) * P.Lf_fix[1];
+        const float dz = (float)(int)((unsigned)pi.z - (unsigned)pj.z) * P.Lf_fix[2];
+        RowSums<float> d;
+        bool near;
+        pair_term<LJ, CO, VIR>(c, dx, dy, dz, __int_as_float(pj.w), d, near, -1, true);
+        if (!near)
+            continue;
+        const int is = (int)exact_cutoffs(P, s, j);
+        pair_term<LJ, CO, VIR>(c, dx, dy, dz, __int_as_float(pj.w), d, near, is, false);
+        if (d.fq[0] | d.fq[1] | d.fq[2]) {
+            double* f = reinterpret_cast<double*>(P.f4 + s);
+            atomicAdd(f + 0, (double)d.fq[0] * kForceFixInv);
+            atomicAdd(f + 1, (double)d.fq[1] * kForceFixInv);
+            atomicAdd(f + 2, (double)d.fq[2] * kForceFixInv);
+        }
+        if (d.elj != 0.0f)
+            fix_add(&P.st->acc[kAccELJ], 0.5 * (double)d.elj);
+        if (d.ec != 0.0f)
+            fix_add(&P.st->acc[kAccECoul], 0.5 * (double)d.ec);
+        if (VIR)
+            for (int q = 0; q < 6; ++q)
+                if (d.v[q] != 0.0f)
+                    fix_add(&P.st->acc[kAccVir + q], 0.5 * (double)d.v[q]);
+    }
+}
+
+__global__ void __launch_bounds__(256)
+    k_pair_fix(const int* sys_list, int nsys, const SysParams* sp) {
+    const SysParams& P = sp[sys_list[blockIdx.x / kFixBlocks]];
+    if (P.prec != kMixed || !P.has_lj || P.nearq == nullptr || !(P.mix_band_lj > 0.0))
+        return;
+    const int nq = min(P.st->nearq_n, P.nearq_cap);
+    const int lane = threadIdx.x & 31;
+    const int w0 = (blockIdx.x % kFixBlocks) * (blockDim.x / 32) + (threadIdx.x >> 5);
+    const int nw = kFixBlocks * (blockDim.x / 32);
+    const bool co = P.has_coul, vr = P.need_virial;
+    for (int e = w0; e < nq; e += nw) {
+        const int2 q = P.nearq[e];
+        if (co) {
+            if (vr)
+                fix_share<true, true, true>(P, q.x, q.y, lane);
+            else
+                fix_share<true, true, false>(P, q.x, q.y, lane);
+        } else {
+            if (vr)
+                fix_share<true, false, true>(P, q.x, q.y, lane);
+            else
+                fix_share<true, false, false>(P, q.x, q.y, lane);
+        }
+    }
+}
+
 template <bool MIXED>
 static void launch_pair_prec(const LaunchCfg& lc, cudaStream_t s) {
     const ItemList* L = lc.pair[MIXED ? 1 : 0];
@@ -414,6 +562,11 @@ static void launch_pair_prec(const LaunchCfg& lc, cudaStream_t s) {
 void launch_pair(const LaunchCfg& lc, cudaStream_t s) {
     launch_pair_prec<false>(lc, s);
     launch_pair_prec<true>(lc, s);
+}
+
+void launch_pair_fix(const LaunchCfg& lc, cudaStream_t s) {
+    if (lc.any_near && lc.nsys > 0)
+        k_pair_fix<<<lc.nsys * kFixBlocks, 256, 0, s>>>(lc.sys_list, lc.nsys, lc.sp);
 }
 
 } // namespace atvb
