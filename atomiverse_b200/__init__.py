@@ -272,6 +272,15 @@ class Batch:
         check(self.lib.atvb_batch_launch_count(self._h, C.byref(n)))
         return n.value
 
+    def profile(self, enable: bool):
+        check(self.lib.atvb_batch_profile(self._h, int(bool(enable))))
+
+    def profile_read(self) -> dict:
+        buf = (_abi.KernelTime * 64)()
+        cnt = C.c_int32()
+        check(self.lib.atvb_batch_profile_read(self._h, buf, 64, C.byref(cnt)))
+        return {buf[k].name.decode(): (buf[k].total_ms, buf[k].launches) for k in range(cnt.value)}
+
 
 class Server:
     """Continuous batching of MD segments under a device-memory budget."""

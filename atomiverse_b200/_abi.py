@@ -139,6 +139,9 @@ SIGNATURES = {
     "atvb_batch_download": (C.c_int, [_vp, C.c_int32, C.POINTER(SoaView), C.POINTER(Scalars)]),
     "atvb_batch_autotune": (C.c_int, [_vp, C.POINTER(C.c_int32)]),
     "atvb_batch_launch_count": (C.c_int, [_vp, C.POINTER(C.c_int64)]),
+    "atvb_batch_profile": (C.c_int, [_vp, C.c_int32]),
+    "atvb_batch_profile_read": (C.c_int, [_vp, C.POINTER(KernelTime), C.c_int32,
+                                          C.POINTER(C.c_int32)]),
     "atvb_server_create": (C.c_int, [_vp, C.c_size_t, C.c_int32, C.POINTER(_vp)]),
     "atvb_server_destroy": (C.c_int, [_vp]),
     "atvb_server_submit": (C.c_int, [_vp, C.POINTER(SystemDesc), C.POINTER(SoaView),

@@ -70,7 +70,6 @@ class Slot {
     int max_row = 0;
     int lanes = 4;  // pair-kernel lanes per atom for this system
     double mean_row = 0.0;
-    cufftHandle plan_f = 0, plan_i = 0; // borrowed from the engine's plan cache
     std::vector<double> infl_host;
 
   private:
@@ -121,13 +120,20 @@ class Engine {
     }
 
   private:
+    // cuFFT plans of one grid shape: one pair per stream lane (the FFTs of
+    // several systems run concurrently on kFftLanes forked streams; lane
+    // kFftLanes is the engine's own stream, used when one system transforms)
+    static constexpr int kFftLanes = 8;
     struct FftPlans {
-        cufftHandle f = 0, i = 0;
+        cufftHandle f[kFftLanes + 1] = {}, i[kFftLanes + 1] = {};
         int refs = 0;
         uint64_t last_use = 0;
     };
     void acquire_plans(Slot& s);
     void release_plans(Slot& s);
+    FftPlans& shape_plans(const Slot& s);
+    void ensure_lane_plan(const Slot& s, int lane);
+    void exec_fft(const std::vector<int>& pme, bool forward);
     void ensure_table();
     void push_params(int id);
     void build_lists();
@@ -151,6 +157,8 @@ class Engine {
     // after the last user leaves, up to kPlanCacheIdle idle shapes
     std::map<std::vector<int>, FftPlans> plans_;
     uint64_t plan_clock_ = 0;
+    cudaStream_t fft_streams_[kFftLanes] = {};
+    cudaEvent_t fft_fork_ = nullptr, fft_join_[kFftLanes] = {};
     int num_sms_ = 148;
     std::vector<std::unique_ptr<Slot>> slots_;
     SysParams* d_sp_ = nullptr;

@@ -310,6 +310,37 @@ int atvb_batch_autotune(atvb_batch* b, int32_t* lanes) {
     });
 }
 
+int atvb_batch_profile(atvb_batch* b, int32_t enable) {
+    return guard([&] {
+        need(b, "batch");
+        b->eng->set_profiling(enable != 0);
+        if (enable)
+            b->eng->clear_profile();
+    });
+}
+
+int atvb_batch_profile_read(atvb_batch* b, atvb_kernel_time* out, int32_t capacity,
+                            int32_t* count) {
+    return guard([&] {
+        need(b, "batch");
+        const auto& p = b->eng->profile();
+        int c = 0;
+        for (const auto& e : p) {
+            if (c >= capacity)
+                break;
+            if (out) {
+                std::memset(&out[c], 0, sizeof(atvb_kernel_time));
+                std::strncpy(out[c].name, e.name.c_str(), sizeof(out[c].name) - 1);
+                out[c].total_ms = e.ms;
+                out[c].launches = e.launches;
+            }
+            ++c;
+        }
+        if (count)
+            *count = c;
+    });
+}
+
 int atvb_batch_launch_count(atvb_batch* b, int64_t* launches) {
     return guard([&] {
         need(b, "batch");

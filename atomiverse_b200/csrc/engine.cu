@@ -520,45 +520,58 @@ Engine::Engine(int device) : device_(device) {
     uint64_t keep = UINT64_MAX;
     CK(cudaMemPoolSetAttribute(mem_.pool, cudaMemPoolAttrReleaseThreshold, &keep));
     mem_.stream = stream_;
+    for (int l = 0; l < kFftLanes; ++l) {
+        CK(cudaStreamCreateWithFlags(&fft_streams_[l], cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&fft_join_[l], cudaEventDisableTiming));
+    }
+    CK(cudaEventCreateWithFlags(&fft_fork_, cudaEventDisableTiming));
 }
 
 constexpr int kPlanCacheIdle = 16;
 
+static std::vector<int> shape_key(const Slot& s) {
+    return {s.hp.K[0], s.hp.K[1], s.hp.K[2], s.hp.prec == kMixed ? 1 : 0};
+}
+
 void Engine::acquire_plans(Slot& s) {
     if (!s.hp.has_pme)
         return;
-    const bool mixed = s.hp.prec == kMixed;
-    const std::vector<int> key = {s.hp.K[0], s.hp.K[1], s.hp.K[2], mixed ? 1 : 0};
-    FftPlans& p = plans_[key];
-    if (!p.f) {
-        cufftHandle f = 0, i = 0;
-        CKF(cufftPlan3d(&f, key[0], key[1], key[2], mixed ? CUFFT_R2C : CUFFT_D2Z));
-        if (cufftPlan3d(&i, key[0], key[1], key[2], mixed ? CUFFT_C2R : CUFFT_Z2D) !=
-            CUFFT_SUCCESS) {
-            cufftDestroy(f);
-            plans_.erase(key);
-            throw Error(ATVB_ERR_CUDA, "cufftPlan3d failed");
-        }
-        cufftSetStream(f, stream_);
-        cufftSetStream(i, stream_);
-        p.f = f;
-        p.i = i;
-    }
+    FftPlans& p = plans_[shape_key(s)];
     ++p.refs;
     p.last_use = ++plan_clock_;
-    s.plan_f = p.f;
-    s.plan_i = p.i;
+}
+
+Engine::FftPlans& Engine::shape_plans(const Slot& s) {
+    return plans_[shape_key(s)];
+}
+
+// Creates (outside any stream capture) the plan pair of a shape for a lane.
+void Engine::ensure_lane_plan(const Slot& s, int lane) {
+    FftPlans& p = shape_plans(s);
+    if (p.f[lane])
+        return;
+    const std::vector<int> key = shape_key(s);
+    const bool mixed = key[3] == 1;
+    cufftHandle f = 0, i = 0;
+    CKF(cufftPlan3d(&f, key[0], key[1], key[2], mixed ? CUFFT_R2C : CUFFT_D2Z));
+    if (cufftPlan3d(&i, key[0], key[1], key[2], mixed ? CUFFT_C2R : CUFFT_Z2D) !=
+        CUFFT_SUCCESS) {
+        cufftDestroy(f);
+        throw Error(ATVB_ERR_CUDA, "cufftPlan3d failed");
+    }
+    cudaStream_t st = lane == kFftLanes ? stream_ : fft_streams_[lane];
+    cufftSetStream(f, st);
+    cufftSetStream(i, st);
+    p.f[lane] = f;
+    p.i[lane] = i;
 }
 
 void Engine::release_plans(Slot& s) {
     if (!s.hp.has_pme)
         return;
-    const std::vector<int> key = {s.hp.K[0], s.hp.K[1], s.hp.K[2],
-                                  s.hp.prec == kMixed ? 1 : 0};
-    auto it = plans_.find(key);
+    auto it = plans_.find(shape_key(s));
     if (it != plans_.end() && it->second.refs > 0)
         --it->second.refs;
-    s.plan_f = s.plan_i = 0;
     // evict the least recently used idle shapes beyond the cache size
     for (;;) {
         int idle = 0;
@@ -571,10 +584,57 @@ void Engine::release_plans(Slot& s) {
             }
         if (idle <= kPlanCacheIdle || lru == plans_.end())
             break;
+        release_graph();
         cudaStreamSynchronize(stream_);
-        cufftDestroy(lru->second.f);
-        cufftDestroy(lru->second.i);
+        for (int l = 0; l <= kFftLanes; ++l) {
+            if (lru->second.f[l])
+                cufftDestroy(lru->second.f[l]);
+            if (lru->second.i[l])
+                cufftDestroy(lru->second.i[l]);
+        }
         plans_.erase(lru);
+    }
+}
+
+// The forward or inverse FFT of every system in `pme`.  One system: on the
+// engine stream.  Several: forked over the kFftLanes streams (system k of
+// the list on lane k mod kFftLanes, each lane with its own plans) and joined
+// back, so small transforms run side by side; inside a captured step the
+// fork and join become parallel branches of the graph.  Every system keeps
+// its own single-grid plan, so its numbers do not depend on the others.
+void Engine::exec_fft(const std::vector<int>& pme, bool forward) {
+    auto run = [&](const Slot& sl, int lane) {
+        const FftPlans& p = plans_.at(shape_key(sl));
+        const bool mixed = sl.hp.prec == kMixed;
+        if (forward) {
+            if (mixed)
+                CKF(cufftExecR2C(p.f[lane], (cufftReal*)sl.hp.grid_real,
+                                 (cufftComplex*)sl.hp.grid_cplx));
+            else
+                CKF(cufftExecD2Z(p.f[lane], (cufftDoubleReal*)sl.hp.grid_real,
+                                 (cufftDoubleComplex*)sl.hp.grid_cplx));
+        } else {
+            if (mixed)
+                CKF(cufftExecC2R(p.i[lane], (cufftComplex*)sl.hp.grid_cplx,
+                                 (cufftReal*)sl.hp.grid_real));
+            else
+                CKF(cufftExecZ2D(p.i[lane], (cufftDoubleComplex*)sl.hp.grid_cplx,
+                                 (cufftDoubleReal*)sl.hp.grid_real));
+        }
+    };
+    if (pme.size() == 1) {
+        run(*slots_[pme[0]], kFftLanes);
+        return;
+    }
+    const int used = (int)std::min<size_t>(pme.size(), kFftLanes);
+    CK(cudaEventRecord(fft_fork_, stream_));
+    for (int l = 0; l < used; ++l)
+        CK(cudaStreamWaitEvent(fft_streams_[l], fft_fork_, 0));
+    for (size_t q = 0; q < pme.size(); ++q)
+        run(*slots_[pme[q]], (int)(q % kFftLanes));
+    for (int l = 0; l < used; ++l) {
+        CK(cudaEventRecord(fft_join_[l], fft_streams_[l]));
+        CK(cudaStreamWaitEvent(stream_, fft_join_[l], 0));
     }
 }
 
@@ -586,10 +646,21 @@ Engine::~Engine() {
         mem_.free(p);
     mem_.free(d_sp_);
     cudaStreamSynchronize(stream_);
-    for (auto& kv : plans_) {
-        cufftDestroy(kv.second.f);
-        cufftDestroy(kv.second.i);
+    for (auto& kv : plans_)
+        for (int l = 0; l <= kFftLanes; ++l) {
+            if (kv.second.f[l])
+                cufftDestroy(kv.second.f[l]);
+            if (kv.second.i[l])
+                cufftDestroy(kv.second.i[l]);
+        }
+    for (int l = 0; l < kFftLanes; ++l) {
+        if (fft_streams_[l])
+            cudaStreamDestroy(fft_streams_[l]);
+        if (fft_join_[l])
+            cudaEventDestroy(fft_join_[l]);
     }
+    if (fft_fork_)
+        cudaEventDestroy(fft_fork_);
     if (mem_.pool)
         cudaMemPoolDestroy(mem_.pool);
     for (auto& e : prof_events_)
@@ -784,6 +855,15 @@ void Engine::build_lists() {
                            cudaMemcpyHostToDevice, stream_));
         lc_.sys_list = (const int*)p;
     }
+    // plans for this work list, made now (plan creation cannot be captured):
+    // lane q mod kFftLanes for the step, the engine-stream lane for passes
+    // over one system
+    for (size_t q = 0; q < pme_slots_.size(); ++q) {
+        const Slot& sl = *slots_[pme_slots_[q]];
+        ensure_lane_plan(sl, kFftLanes);
+        if (pme_slots_.size() > 1)
+            ensure_lane_plan(sl, (int)(q % kFftLanes));
+    }
     lc_.pme_mixed = pme_prec == kMixed ? 1 : 0;
     lc_.pme_order = pme_order > 0 ? pme_order : 4;
     CK(cudaStreamSynchronize(stream_));
@@ -822,28 +902,11 @@ void Engine::enqueue_forces(const LaunchCfg& lc, const std::vector<int>& pme,
         prof_mark(profile, "pme_convert");
         launch_pme_convert(lc, stream_);
         prof_mark(profile, "pme_fft_fwd");
-        for (int k : pme) {
-            Slot* s = slots_[k].get();
-            if (s->hp.prec == kMixed)
-                CKF(cufftExecR2C(s->plan_f, (cufftReal*)s->hp.grid_real,
-                                 (cufftComplex*)s->hp.grid_cplx));
-            else
-                CKF(cufftExecD2Z(s->plan_f, (cufftDoubleReal*)s->hp.grid_real,
-                                 (cufftDoubleComplex*)s->hp.grid_cplx));
-        }
+        exec_fft(pme, true);
         prof_mark(profile, "pme_influence");
         launch_pme_influence(lc, stream_);
         prof_mark(profile, "pme_fft_inv");
-        for (int k : pme) {
-            Slot* s = slots_[k].get();
-            if (s->hp.prec == kMixed)
-                CKF(cufftExecC2R(s->plan_i, (cufftComplex*)s->hp.grid_cplx,
-                                 (cufftReal*)s->hp.grid_real));
-            else
-                CKF(cufftExecZ2D(s->plan_i,
-                                 (cufftDoubleComplex*)s->hp.grid_cplx,
-                                 (cufftDoubleReal*)s->hp.grid_real));
-        }
+        exec_fft(pme, false);
         prof_mark(profile, "pme_gather");
         launch_pme_gather(lc, stream_);
     }

@@ -27,6 +27,20 @@ def recommend_alpha(cutoff: float, accuracy: float = 1e-5) -> float:
     return (1.35 - 0.15 * math.log(accuracy)) / cutoff
 
 
+def good_fft_size(n: int) -> int:
+    """Smallest 2,3,5,7-smooth integer >= max(n, 4) (the reference's
+    good_fft_size, pme_spline.h:99-111, restated)."""
+    k = max(int(n), 4)
+    while True:
+        m = k
+        for p in (2, 3, 5, 7):
+            while m % p == 0:
+                m //= p
+        if m == 1:
+            return k
+        k += 1
+
+
 def fcc_sites(ncell: int, a: float) -> np.ndarray:
     base = np.array([[0, 0, 0], [0.5, 0.5, 0], [0.5, 0, 0.5], [0, 0.5, 0.5]])
     g = np.arange(ncell)
@@ -125,7 +139,7 @@ def rocksalt_melt(ncell: int = 64, spacing: float = 2.82, jitter: float = 0.2,
     elif grid_spacing is not None:
         desc["pme_grid_spacing"] = grid_spacing
     else:
-        K = round(L / 0.94)
+        K = good_fft_size(math.ceil(L / 0.94))
         desc["pme_grid"] = (K, K, K) if ncell != 64 else (192, 192, 192)
     return desc, _frame(pos, vel, mass, charge)
 
@@ -180,7 +194,7 @@ def build_request(spec: dict, precision: int = 1):
         return lj_fcc(ncell=spec["cells"], seed=spec["seed"], precision=precision)
     m = spec["cells"]
     L = m * 2.82
-    K = max(8, round(L / 0.94))
+    K = good_fft_size(math.ceil(L / 0.94))
     # small boxes: shrink the real-space cutoff so that 2 (rc + skin) < L
     rc = min(12.0, 0.5 * L - 1.0 - 0.05)
     return rocksalt_melt(ncell=m, seed=spec["seed"], grid=(K, K, K), precision=precision,

@@ -186,6 +186,11 @@ int atvb_batch_download(atvb_batch* b, int32_t index, atvb_soa_view* frame,
  * the fastest; *lanes receives the choice. */
 int atvb_batch_autotune(atvb_batch* b, int32_t* lanes);
 int atvb_batch_launch_count(atvb_batch* b, int64_t* launches);
+/* Per-kernel-group CUDA-event times over every system of the batch, as
+ * atvb_system_profile / atvb_system_profile_read. */
+int atvb_batch_profile(atvb_batch* b, int32_t enable);
+int atvb_batch_profile_read(atvb_batch* b, atvb_kernel_time* out,
+                            int32_t capacity, int32_t* count);
 
 /* ---- server: continuous batching of MD segments ------------------------ */
 typedef struct atvb_request_result {
