@@ -314,6 +314,9 @@ class Server:
     def cancel(self, rid: int):
         check(self.lib.atvb_server_cancel(self._h, int(rid)))
 
+    def set_limits(self, max_resident_atoms: int = 0):
+        check(self.lib.atvb_server_set_limits(self._h, int(max_resident_atoms)))
+
     def tick(self, chunk: int = 50):
         check(self.lib.atvb_server_tick(self._h, int(chunk)))
 

@@ -147,6 +147,7 @@ SIGNATURES = {
     "atvb_server_submit": (C.c_int, [_vp, C.POINTER(SystemDesc), C.POINTER(SoaView),
                                      C.c_int32, C.POINTER(C.c_int64)]),
     "atvb_server_cancel": (C.c_int, [_vp, C.c_int64]),
+    "atvb_server_set_limits": (C.c_int, [_vp, C.c_int64]),
     "atvb_server_tick": (C.c_int, [_vp, C.c_int32]),
     "atvb_server_poll": (C.c_int, [_vp, C.c_int64, C.POINTER(RequestResult)]),
     "atvb_server_collect": (C.c_int, [_vp, C.c_int64, C.POINTER(SoaView),

@@ -69,6 +69,8 @@ struct atvb_server {
     size_t budget = 0;
     int max_active = 0;
     size_t in_use = 0;
+    int64_t max_atoms = 0;   // resident-atom cap (0: none)
+    int64_t atoms_in_use = 0;
     int64_t next_id = 1;
     std::map<int64_t, Request> reqs;
     std::deque<int64_t> queue;
@@ -94,7 +96,9 @@ struct atvb_server {
             if ((int)running.size() >= max_active)
                 break;
             Request& r = get(*it);
-            if (in_use + r.bytes > budget) {
+            const bool over_atoms = max_atoms > 0 && !running.empty() &&
+                                    atoms_in_use + r.desc.n_atoms > max_atoms;
+            if (in_use + r.bytes > budget || over_atoms) {
                 if (t - r.t_submit > kMaxSkipWait)
                     break; // hold the line for a request that waited long
                 ++it;
@@ -120,6 +124,7 @@ struct atvb_server {
             r.state = 1;
             r.t_start = now();
             in_use += r.bytes;
+            atoms_in_use += r.desc.n_atoms;
             running.push_back(r.id);
             it = queue.erase(it);
         }
@@ -133,6 +138,7 @@ struct atvb_server {
         eng->remove(r.slot);
         r.slot = -1;
         in_use -= r.bytes;
+        atoms_in_use -= r.desc.n_atoms;
         running.erase(std::remove(running.begin(), running.end(), r.id),
                       running.end());
     }
@@ -245,6 +251,16 @@ int atvb_server_submit(atvb_server* srv, const atvb_system_desc* desc,
         srv->queue.push_back(rid);
         if (id)
             *id = rid;
+    });
+}
+
+int atvb_server_set_limits(atvb_server* srv, int64_t max_resident_atoms) {
+    return sguard([&] {
+        if (!srv)
+            throw Error(ATVB_ERR_INVALID, "server is NULL");
+        if (max_resident_atoms < 0)
+            throw Error(ATVB_ERR_INVALID, "max_resident_atoms must be >= 0");
+        srv->max_atoms = max_resident_atoms;
     });
 }
 

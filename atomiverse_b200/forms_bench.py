@@ -229,6 +229,8 @@ def serve(args):
     th.start()
     budget = int(args.budget_gb * 1e9)
     srv = A.Server(ctx, budget, max_active=args.max_active)
+    if args.max_atoms:
+        srv.set_limits(int(args.max_atoms))
     live = {}        # rid -> spec index
     kept = {}        # spec index -> (desc, frame, served output)
     lat, arrivals, done_at = [], [], []
@@ -272,7 +274,8 @@ def serve(args):
     res = {"form": "serve", "workload": f"{len(specs)} Poisson requests at {args.rate}/s "
            f"(seed 2030), {args.seg_steps}-step segments, 60% LJ / 40% rock-salt PME, "
            "500-200,000 atoms, mixed precision", "requests": len(specs),
-           "budget_bytes": budget, "chunk": args.chunk, "peak_running": peak_running,
+           "budget_bytes": budget, "max_resident_atoms": int(args.max_atoms),
+           "chunk": args.chunk, "peak_running": peak_running,
            "p50_latency_s": float(np.percentile(lat, 50)),
            "p99_latency_s": float(np.percentile(lat, 99)),
            "offered_atom_steps_per_s": offered,
@@ -323,6 +326,8 @@ def main(argv=None):
     ap.add_argument("--budget-gb", type=float, default=120.0)
     ap.add_argument("--max-active", type=int, default=0)
     ap.add_argument("--check", type=int, default=8)
+    ap.add_argument("--max-atoms", type=float, default=4e6,
+                    help="serve: resident-atom admission limit (0 = memory budget only)")
     ap.add_argument("--out", default=None, help="also append the JSON line to this file")
     args = ap.parse_args(argv)
     if args.form == "precision":

@@ -209,6 +209,13 @@ int atvb_server_submit(atvb_server* srv, const atvb_system_desc* desc,
                        const atvb_soa_view* frame, int32_t n_steps,
                        int64_t* id);
 int atvb_server_cancel(atvb_server* srv, int64_t id);
+/* Admission limit besides the device-memory budget: requests are admitted
+ * (in arrival order, smaller ones may pass a larger one that waited less
+ * than half a second) only while the resident atoms stay within
+ * max_resident_atoms; 0 = no limit.  At least one request is always
+ * admitted.  Bounding the resident work keeps each step short, so requests
+ * finish in arrival order instead of all together. */
+int atvb_server_set_limits(atvb_server* srv, int64_t max_resident_atoms);
 /* One scheduling round: admit what fits, advance every running segment by
  * `chunk` steps in one batched launch sequence, retire finished ones. */
 int atvb_server_tick(atvb_server* srv, int32_t chunk);

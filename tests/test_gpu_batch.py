@@ -182,3 +182,23 @@ def test_cpp_md_example(atvb):
     assert step == 100
     assert ke > 0
     assert abs(e2 - e1) <= 1e-3 * abs(e1)          # NVE: total energy conserved
+
+
+@pytest.mark.gpu
+def test_server_resident_atom_limit(atvb, ctx):
+    from atomiverse_b200 import workloads as W
+    reqs = [W.lj_fcc(ncell=c, seed=30 + c, precision=1) for c in (5, 6, 4)]  # 500, 864, 256 atoms
+    srv = atvb.Server(ctx, 1 << 34)
+    srv.set_limits(900)
+    ids = [srv.submit(d, f, 12) for d, f in reqs]
+    sizes = {rid: d["n_atoms"] for rid, (d, _) in zip(ids, reqs)}
+    for _ in range(50):
+        srv.tick(4)
+        running = [rid for rid in ids if srv.poll(rid)["state"] == 1]
+        assert len(running) == 1 or sum(sizes[r] for r in running) <= 900
+        if all(srv.poll(rid)["state"] == 2 for rid in ids):
+            break
+    assert all(srv.poll(rid)["state"] == 2 for rid in ids)
+    with pytest.raises(atvb.AtvbError):
+        srv.set_limits(-1)
+    srv.close()
