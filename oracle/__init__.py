@@ -94,6 +94,9 @@ def lib():
         L.orc_pme.argtypes = [C.c_int, dp, dp, dp, dp, dp, C.c_double,
                               C.POINTER(C.c_int), C.c_int, dp, dp, dp, dp, dp]
         L.orc_gauss3.argtypes = [C.c_uint32, C.c_int64, C.c_int64, dp]
+        L.orc_set_lj_types.restype = C.c_int
+        L.orc_set_lj_types.argtypes = [C.c_void_p, C.c_int, ip, ip, dp, dp, ip]
+        L.orc_set_special.argtypes = [C.c_void_p, C.c_int, ip, ip, dp, dp]
         _lib = L
     return _lib
 
@@ -185,6 +188,34 @@ class OracleSystem:
         d["step"] = int(s[13])
         d["rebuilds"] = int(s[14])
         return d
+
+    def set_lj_types(self, coeffs, types):
+        """coeffs: [(type_i, type_j, eps, sigma), ...]; types: per-atom type."""
+        ti = np.array([c[0] for c in coeffs], dtype=np.int32)
+        tj = np.array([c[1] for c in coeffs], dtype=np.int32)
+        e = np.array([c[2] for c in coeffs], dtype=np.float64)
+        sg = np.array([c[3] for c in coeffs], dtype=np.float64)
+        t = np.ascontiguousarray(types, dtype=np.int32)
+        self._keep_t = (ti, tj, e, sg, t)
+        ip = C.POINTER(C.c_int32)
+        nt = lib().orc_set_lj_types(self._h, len(coeffs), ti.ctypes.data_as(ip),
+                                    tj.ctypes.data_as(ip), _dp(e), _dp(sg),
+                                    t.ctypes.data_as(ip))
+        if nt < 0:
+            raise ValueError("bad LJ type coefficient")
+        return nt
+
+    def set_special(self, pairs, s_lj, s_coul):
+        """pairs: (m, 2) atom indices; s_lj, s_coul: (m,) scales."""
+        p = np.ascontiguousarray(pairs, dtype=np.int32).reshape(-1, 2)
+        a = np.ascontiguousarray(p[:, 0])
+        b = np.ascontiguousarray(p[:, 1])
+        sl = np.ascontiguousarray(s_lj, dtype=np.float64)
+        sc = np.ascontiguousarray(s_coul, dtype=np.float64)
+        self._keep_s = (a, b, sl, sc)
+        ip = C.POINTER(C.c_int32)
+        lib().orc_set_special(self._h, len(a), a.ctypes.data_as(ip), b.ctypes.data_as(ip),
+                              _dp(sl), _dp(sc))
 
     def build_list(self) -> int:
         return int(lib().orc_build_list(self._h))

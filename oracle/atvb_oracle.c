@@ -104,6 +104,14 @@ struct orc_sys {
     double* infl_H;  /* influence tables */
     double *infl_mx, *infl_my, *infl_mz, *infl_inv_msq;
     double inv_pi2_a2;
+    /* per-type LJ tables (ntypes x ntypes) and per-atom types */
+    int ntypes;
+    double *t_sig6, *t_eps, *t_shift;
+    int32_t* type;
+    /* special pairs: per atom, partners sorted by index with scales */
+    int32_t* sp_first; /* n + 1 */
+    int32_t* sp_j;
+    double *sp_lj, *sp_coul;
 };
 
 orc_sys* orc_create(const orc_desc* d) {
@@ -138,6 +146,14 @@ void orc_destroy(orc_sys* s) {
     free(s->first);
     free(s->num);
     free(s->nbr);
+    free(s->t_sig6);
+    free(s->t_eps);
+    free(s->t_shift);
+    free(s->type);
+    free(s->sp_first);
+    free(s->sp_j);
+    free(s->sp_lj);
+    free(s->sp_coul);
     free(s->grid);
     free(s->infl_H);
     free(s->infl_mx);
@@ -430,6 +446,117 @@ static int needs_rebuild(const orc_sys* s) {
 }
 
 /* ------------------------------------------------------------------ */
+/* per-type LJ tables and special pairs                                */
+/* ------------------------------------------------------------------ */
+
+int orc_set_lj_types(orc_sys* s, int ncoef, const int32_t* ti, const int32_t* tj,
+                     const double* eps, const double* sigma, const int32_t* type) {
+    int nt = 0;
+    for (int k = 0; k < ncoef; ++k) {
+        if (ti[k] < 0 || tj[k] < 0 || !(sigma[k] > 0.0))
+            return -1;
+        if (ti[k] + 1 > nt)
+            nt = ti[k] + 1;
+        if (tj[k] + 1 > nt)
+            nt = tj[k] + 1;
+    }
+    const size_t nn = (size_t)nt * nt;
+    double* e = (double*)calloc(nn, sizeof(double));
+    double* sg = (double*)calloc(nn, sizeof(double));
+    char* set = (char*)calloc(nn, 1);
+    for (int k = 0; k < ncoef; ++k) { /* set_type_coeff: symmetric, last wins */
+        const size_t ab = (size_t)ti[k] * nt + tj[k], ba = (size_t)tj[k] * nt + ti[k];
+        e[ab] = e[ba] = eps[k];
+        sg[ab] = sg[ba] = sigma[k];
+        set[ab] = set[ba] = 1;
+    }
+    free(s->t_sig6);
+    free(s->t_eps);
+    free(s->t_shift);
+    s->t_sig6 = (double*)calloc(nn, sizeof(double));
+    s->t_eps = (double*)calloc(nn, sizeof(double));
+    s->t_shift = (double*)calloc(nn, sizeof(double));
+    const double rc = s->d.lj_rc;
+    for (int a = 0; a < nt; ++a)
+        for (int b = 0; b < nt; ++b) {
+            const size_t ab = (size_t)a * nt + b;
+            double ee = e[ab], ss = sg[ab];
+            if (!set[ab]) {
+                const size_t aa = (size_t)a * nt + a, bb = (size_t)b * nt + b;
+                if (set[aa] && set[bb]) {
+                    ee = sqrt(e[aa] * e[bb]);
+                    ss = 0.5 * (sg[aa] + sg[bb]);
+                } else {
+                    ee = 0.0;
+                    ss = 1.0;
+                }
+            }
+            const double s2 = ss * ss, s6 = s2 * s2 * s2;
+            s->t_sig6[ab] = s6;
+            s->t_eps[ab] = ee;
+            const double r2inv = 1.0 / (rc * rc);
+            const double r6inv = r2inv * r2inv * r2inv * s6;
+            s->t_shift[ab] = 4.0 * ee * (r6inv * r6inv - r6inv);
+        }
+    free(e);
+    free(sg);
+    free(set);
+    free(s->type);
+    s->type = (int32_t*)calloc((size_t)(s->n > 0 ? s->n : 1), sizeof(int32_t));
+    for (int i = 0; i < s->n; ++i)
+        s->type[i] = type ? type[i] : 0;
+    s->ntypes = nt;
+    return nt;
+}
+
+void orc_set_special(orc_sys* s, int npairs, const int32_t* pi, const int32_t* pj,
+                     const double* s_lj, const double* s_coul) {
+    const int n = s->n;
+    free(s->sp_first);
+    free(s->sp_j);
+    free(s->sp_lj);
+    free(s->sp_coul);
+    s->sp_first = (int32_t*)calloc((size_t)n + 1, sizeof(int32_t));
+    for (int k = 0; k < npairs; ++k) {
+        s->sp_first[pi[k] + 1]++;
+        s->sp_first[pj[k] + 1]++;
+    }
+    for (int i = 0; i < n; ++i)
+        s->sp_first[i + 1] += s->sp_first[i];
+    const size_t m = (size_t)s->sp_first[n];
+    s->sp_j = (int32_t*)calloc(m ? m : 1, sizeof(int32_t));
+    s->sp_lj = (double*)calloc(m ? m : 1, sizeof(double));
+    s->sp_coul = (double*)calloc(m ? m : 1, sizeof(double));
+    int32_t* fill = (int32_t*)calloc((size_t)n, sizeof(int32_t));
+    for (int k = 0; k < npairs; ++k) {
+        const int a = pi[k], b = pj[k];
+        size_t q = (size_t)s->sp_first[a] + fill[a]++;
+        s->sp_j[q] = b;
+        s->sp_lj[q] = s_lj[k];
+        s->sp_coul[q] = s_coul[k];
+        q = (size_t)s->sp_first[b] + fill[b]++;
+        s->sp_j[q] = a;
+        s->sp_lj[q] = s_lj[k];
+        s->sp_coul[q] = s_coul[k];
+    }
+    free(fill);
+}
+
+/* LJ and Coulomb scale of pair (i, j): 1, 1 unless listed as special */
+static void special_scale(const orc_sys* s, int i, int j, double* sl, double* sc) {
+    *sl = 1.0;
+    *sc = 1.0;
+    if (!s->sp_first)
+        return;
+    for (int q = s->sp_first[i]; q < s->sp_first[i + 1]; ++q)
+        if (s->sp_j[q] == j) {
+            *sl = s->sp_lj[q];
+            *sc = s->sp_coul[q];
+            return;
+        }
+}
+
+/* ------------------------------------------------------------------ */
 /* pair forces: LJ (pair_lj_cut.cpp:723-800) + CoulLong (coul_long.cpp)  */
 /* ------------------------------------------------------------------ */
 
@@ -480,11 +607,21 @@ static void pair_forces(orc_sys* s) {
                 (void)iL2;
                 const double r2 = dx * dx + dy * dy + dz * dz;
                 double fpair = 0.0;
-                if (do_lj && r2 < lj_rc2) {
+                double sl = 1.0, sc = 1.0;
+                special_scale(s, i, j, &sl, &sc);
+                if (do_lj && r2 < lj_rc2 && sl != 0.0) {
+                    double p_sig6 = sig6, p_eps24 = eps24, p_eps4 = eps4, p_shift = vshift;
+                    if (s->ntypes) { /* pair_lj_cut.cpp:760-770 */
+                        const size_t ab = (size_t)s->type[i] * s->ntypes + s->type[j];
+                        p_sig6 = s->t_sig6[ab];
+                        p_eps24 = 24.0 * s->t_eps[ab];
+                        p_eps4 = 4.0 * s->t_eps[ab];
+                        p_shift = s->t_shift[ab];
+                    }
                     const double r2inv = 1.0 / r2;
-                    const double r6inv = r2inv * r2inv * r2inv * sig6;
-                    fpair += eps24 * r2inv * (2.0 * r6inv * r6inv - r6inv);
-                    e_lj += eps4 * (r6inv * r6inv - r6inv) - vshift;
+                    const double r6inv = r2inv * r2inv * r2inv * p_sig6;
+                    fpair += sl * p_eps24 * r2inv * (2.0 * r6inv * r6inv - r6inv);
+                    e_lj += sl * (p_eps4 * (r6inv * r6inv - r6inv) - p_shift);
                 }
                 if (do_coul && r2 < c_rc2 && r2 != 0.0) {
                     const double qj = s->q[j];
@@ -495,10 +632,13 @@ static void pair_forces(orc_sys* s) {
                         const double expm2 = exp(-grij * grij);
                         const double erfcv = erfc(grij);
                         const double prefactor = ORC_QQR2E * qi * qj / r;
-                        const double forcecoul =
+                        double forcecoul =
                             prefactor * (erfcv + kEwaldF * grij * expm2);
+                        if (sc != 1.0)
+                            forcecoul -= (1.0 - sc) * prefactor;
                         fpair += forcecoul * r2inv;
-                        e_c += prefactor * erfcv;
+                        e_c += sc != 1.0 ? prefactor * erfcv - (1.0 - sc) * prefactor
+                                         : prefactor * erfcv;
                     }
                 }
                 if (fpair != 0.0) {

@@ -85,6 +85,24 @@ void orc_compute_forces(orc_sys* s);
  * end_of_step.  Returns the number of neighbour rebuilds. */
 int orc_run(orc_sys* s, int n_steps, double* hist);
 
+/* Per-type LJ (src/cpu/potentials/pair_lj_cut.cpp:44-112 per-type
+ * constructor / set_type_coeff, :255-298 finalize_type_table_): ncoef
+ * explicit (type_i, type_j, eps, sigma) entries, symmetric; an unset cross
+ * term mixes by Lorentz-Berthelot (eps = sqrt(eps_ii eps_jj),
+ * sigma = (sigma_ii + sigma_jj)/2, :246-252) when both diagonals are set,
+ * else the pair does not interact (eps = 0).  Each type pair is shifted at
+ * the common cutoff.  type[n] is the per-atom type.  Returns the number of
+ * types, or -1 on a bad coefficient (type < 0 or sigma <= 0). */
+int orc_set_lj_types(orc_sys* s, int ncoef, const int32_t* ti, const int32_t* tj,
+                     const double* eps, const double* sigma, const int32_t* type);
+/* Special pairs (LAMMPS special_bonds; cpu/potentials/special_scale.h,
+ * pair_lj_cut.cpp:770-800, coul_long.cpp:159-196): npairs unordered (i, j)
+ * atom indices with an LJ scale (multiplies the LJ force and shifted
+ * energy) and a Coulomb scale f (the real-space term keeps erfc and
+ * subtracts (1 - f) k_e q_i q_j / r, the share the reciprocal sum added). */
+void orc_set_special(orc_sys* s, int npairs, const int32_t* pi, const int32_t* pj,
+                     const double* s_lj, const double* s_coul);
+
 /* ---- standalone pieces used by the known-answer tests ---- */
 void orc_bspline(double frac, int n, double* theta, double* dtheta);
 int orc_good_fft_size(int n);
