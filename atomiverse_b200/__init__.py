@@ -82,7 +82,34 @@ def _soa(frame: dict, n: int, writable: bool = False) -> tuple[SoaView, list]:
         t = np.ascontiguousarray(t, dtype=np.int64)
         keep.append(t)
         v.tag = t.ctypes.data_as(C.POINTER(C.c_int64))
+    ty = frame.get("type")
+    if ty is not None and not writable:
+        ty = np.ascontiguousarray(ty, dtype=np.int32)
+        keep.append(ty)
+        v.type = ty.ctypes.data_as(C.POINTER(C.c_int32))
     return v, keep
+
+
+def _lj_type_args(coeffs):
+    """ctypes arguments for (type_i, type_j, epsilon, sigma) coefficients."""
+    ti = np.array([c[0] for c in coeffs], dtype=np.int32)
+    tj = np.array([c[1] for c in coeffs], dtype=np.int32)
+    e = np.array([c[2] for c in coeffs], dtype=np.float64)
+    sg = np.array([c[3] for c in coeffs], dtype=np.float64)
+    ip, dp = C.POINTER(C.c_int32), C.POINTER(C.c_double)
+    return (len(coeffs), ti.ctypes.data_as(ip), tj.ctypes.data_as(ip),
+            e.ctypes.data_as(dp), sg.ctypes.data_as(dp)), (ti, tj, e, sg)
+
+
+def _special_args(special):
+    """ctypes arguments for dict(lj=(s12, s13, s14), coul=(...), bonds=[(tag_a, tag_b)])."""
+    lj = (C.c_double * 3)(*[float(x) for x in special.get("lj", (1.0, 1.0, 1.0))])
+    co = (C.c_double * 3)(*[float(x) for x in special.get("coul", (1.0, 1.0, 1.0))])
+    b = np.asarray(special.get("bonds", []), dtype=np.int64).reshape(-1, 2)
+    a0 = np.ascontiguousarray(b[:, 0])
+    a1 = np.ascontiguousarray(b[:, 1])
+    lp = C.POINTER(C.c_int64)
+    return (lj, co, len(a0), a0.ctypes.data_as(lp), a1.ctypes.data_as(lp)), (lj, co, a0, a1)
 
 
 def scalars_dict(s: Scalars) -> dict:
@@ -119,7 +146,12 @@ class Context:
 class System:
     """One MD system on the device (cuda::md::MD + its components)."""
 
-    def __init__(self, ctx: Context, desc: SystemDesc | dict, frame: dict | None = None):
+    def __init__(self, ctx: Context, desc: SystemDesc | dict, frame: dict | None = None,
+                 lj_types=None, special_bonds=None):
+        """lj_types: [(type_i, type_j, epsilon, sigma), ...] (PairLJCut's
+        per-type form; per-atom types in frame["type"]); special_bonds:
+        dict(lj=(s12, s13, s14), coul=(s12, s13, s14), bonds=[(tag_a, tag_b), ...]).
+        Both are applied before the frame is uploaded."""
         self.ctx = ctx
         self.lib = ctx.lib
         if isinstance(desc, dict):
@@ -129,6 +161,12 @@ class System:
         h = C.c_void_p()
         check(self.lib.atvb_system_create(ctx._h, C.byref(desc), C.byref(h)))
         self._h = h
+        if lj_types is not None:
+            args, keep = _lj_type_args(lj_types)
+            check(self.lib.atvb_system_set_lj_types(self._h, *args))
+        if special_bonds is not None:
+            args, keep = _special_args(special_bonds)
+            check(self.lib.atvb_system_set_special_bonds(self._h, *args))
         if frame is not None:
             self.upload(frame)
 
@@ -225,17 +263,27 @@ class Batch:
     """Many independent systems advanced by one launch per kernel."""
 
     def __init__(self, ctx: Context, items: list):
+        """items: (desc, frame) or (desc, frame, options) with options the
+        System keywords lj_types / special_bonds."""
         self.ctx = ctx
         self.lib = ctx.lib
-        descs = [make_desc(**d) if isinstance(d, dict) else d for d, _ in items]
+        descs = [make_desc(**it[0]) if isinstance(it[0], dict) else it[0] for it in items]
         arr = (SystemDesc * len(descs))(*descs)
         self.sizes = [d.n_atoms for d in descs]
         h = C.c_void_p()
         check(self.lib.atvb_batch_create(ctx._h, arr, len(descs), C.byref(h)))
         self._h = h
-        for k, (_, frame) in enumerate(items):
-            if frame is not None:
-                self.upload(k, frame)
+        for k, it in enumerate(items):
+            opts = it[2] if len(it) > 2 and it[2] else {}
+            if opts.get("lj_types") is not None:
+                args, keep = _lj_type_args(opts["lj_types"])
+                check(self.lib.atvb_batch_set_lj_types(self._h, k, *args))
+            if opts.get("special_bonds") is not None:
+                args, keep = _special_args(opts["special_bonds"])
+                check(self.lib.atvb_batch_set_special_bonds(self._h, k, *args))
+        for k, it in enumerate(items):
+            if it[1] is not None:
+                self.upload(k, it[1])
 
     def close(self):
         if getattr(self, "_h", None):

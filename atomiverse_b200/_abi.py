@@ -139,6 +139,18 @@ SIGNATURES = {
     "atvb_batch_download": (C.c_int, [_vp, C.c_int32, C.POINTER(SoaView), C.POINTER(Scalars)]),
     "atvb_batch_autotune": (C.c_int, [_vp, C.POINTER(C.c_int32)]),
     "atvb_batch_launch_count": (C.c_int, [_vp, C.POINTER(C.c_int64)]),
+    "atvb_batch_set_lj_types": (C.c_int, [_vp, C.c_int32, C.c_int32, C.POINTER(C.c_int32),
+                                          C.POINTER(C.c_int32), C.POINTER(C.c_double),
+                                          C.POINTER(C.c_double)]),
+    "atvb_batch_set_special_bonds": (C.c_int, [_vp, C.c_int32, C.POINTER(C.c_double),
+                                               C.POINTER(C.c_double), C.c_int64,
+                                               C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "atvb_system_set_lj_types": (C.c_int, [_vp, C.c_int32, C.POINTER(C.c_int32),
+                                           C.POINTER(C.c_int32), C.POINTER(C.c_double),
+                                           C.POINTER(C.c_double)]),
+    "atvb_system_set_special_bonds": (C.c_int, [_vp, C.POINTER(C.c_double),
+                                                C.POINTER(C.c_double), C.c_int64,
+                                                C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "atvb_batch_profile": (C.c_int, [_vp, C.c_int32]),
     "atvb_batch_profile_read": (C.c_int, [_vp, C.POINTER(KernelTime), C.c_int32,
                                           C.POINTER(C.c_int32)]),

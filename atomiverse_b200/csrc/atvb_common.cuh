@@ -102,6 +102,18 @@ struct SysParams {
     // real-space Coulomb
     int has_coul;
     double coul_rc2, coul_alpha, coul_alpha2;
+    // per-type LJ and special pairs: such systems take k_pair_general
+    int general;          // 1: pair forces from k_pair_general
+    int ntypes;           // 0: one LJ type (lj_* above)
+    const double* lj_tab; // ntypes^2 x {sig6, eps4, eps24, shift}
+    const float* lj_tabf; // the same in FP32
+    int* type;            // per atom, original order
+    unsigned char* stype; // per atom, sorted order
+    int has_special;
+    const int* sp_first;  // n + 1 (original order): partners of each atom
+    const int* sp_j;      // partner (original index)
+    const unsigned char* sp_cls; // 1: 1-2, 2: 1-3, 3: 1-4
+    double sp_lj[4], sp_coul[4]; // scale per class ([0] = 1: not special)
     // PME
     int has_pme;
     int K[3], Kh, order;
@@ -140,6 +152,11 @@ struct SysParams {
     double* ehist; // energy history ring: 3 doubles per step (E, KE, step)
     int ehist_cap;
 };
+
+// Row entries of the neighbour list: sorted index in the low 30 bits, the
+// special class (0: none, 1: 1-2, 2: 1-3, 3: 1-4) in the top 2 bits.
+constexpr unsigned kRowIdxMask = 0x3fffffffu;
+constexpr int kMaxAtoms = (1 << 30) - 1;
 
 // A unit of work: a chunk of atoms (or grid points) of one system.
 struct Item {

@@ -71,9 +71,19 @@ class Slot {
     int lanes = 4;  // pair-kernel lanes per atom for this system
     double mean_row = 0.0;
     std::vector<double> infl_host;
+    // per-type LJ and special bonds: configured before the first upload
+    int ntypes = 0;          // > 0: per-type LJ (table built at upload)
+    std::vector<int> lj_ti, lj_tj;
+    std::vector<double> lj_eps, lj_sig;
+    void build_lj_tables(const std::vector<int>& types, cudaStream_t stream);
+    bool special_set = false;
+    double sp_lj[3] = {1, 1, 1}, sp_coul[3] = {1, 1, 1};
+    std::vector<long long> bond_a, bond_b;
+    void build_specials(const std::vector<long long>& tags, cudaStream_t stream);
+
+    void* dalloc(size_t b);
 
   private:
-    void* dalloc(size_t b);
     DevMem mem_;
     std::vector<void*> allocs;
     void* nbr_alloc = nullptr;
@@ -96,6 +106,10 @@ class Engine {
     void remove(int id);
     Slot* slot(int id);
     void upload(int id, const atvb_soa_view& f);
+    void set_lj_types(int id, int ncoef, const int32_t* ti, const int32_t* tj,
+                      const double* eps, const double* sigma);
+    void set_special_bonds(int id, const double lj[3], const double coul[3],
+                           int64_t nbonds, const int64_t* a, const int64_t* b);
     void compute_forces();
     void compute_forces_one(int id);
     void step(int n);

@@ -10,6 +10,7 @@ constexpr int kChunk = 256;     // atoms per item of the per-atom kernels
 constexpr int kListChunk = 8;   // cells per item of the list build (warp/cell)
 constexpr int kGridChunk = 4096; // grid points per item of the PME grid kernels
 constexpr int kLaneClasses = 6;  // pair lanes per atom: 1, 2, 4, 8, 16, 32
+constexpr int kGenLanes = 8;      // lanes per atom of k_pair_general
 constexpr int kPairBlock = 256;  // pair-kernel threads per block (atoms per item = this / lanes)
 
 struct ItemList {
@@ -26,6 +27,8 @@ struct LaunchCfg {
     // count, chosen from that system alone, so its forces and energies do
     // not depend on which other systems share the engine
     ItemList pair[2][kLaneClasses];
+    ItemList pair_gen[2]; // [precision]: systems with types or special pairs
+                          // (kChunk / kGenLanes atoms per item)
     ItemList cells;     // kChunk cells per item
     ItemList pme_atoms; // kChunk atoms of PME systems
     ItemList pme_grid;  // kGridChunk half-complex grid points per item
@@ -44,6 +47,8 @@ void launch_rebuild(const LaunchCfg& lc, cudaStream_t s);
 // pair.cu
 void launch_pair(const LaunchCfg& lc, cudaStream_t s);
 void launch_pair_fix(const LaunchCfg& lc, cudaStream_t s);
+// pair_general.cu
+void launch_pair_general(const LaunchCfg& lc, cudaStream_t s);
 // pme.cu
 void launch_pme_spread(const LaunchCfg& lc, cudaStream_t s);
 void launch_pme_convert(const LaunchCfg& lc, cudaStream_t s);

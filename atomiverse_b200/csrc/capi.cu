@@ -192,6 +192,25 @@ int atvb_system_pairs(atvb_system* sys, int32_t* pi, int32_t* pj,
     });
 }
 
+int atvb_system_set_lj_types(atvb_system* sys, int32_t ncoef, const int32_t* type_i,
+                             const int32_t* type_j, const double* epsilon,
+                             const double* sigma) {
+    return guard([&] {
+        need(sys, "sys");
+        sys->eng->set_lj_types(sys->id, ncoef, type_i, type_j, epsilon, sigma);
+    });
+}
+
+int atvb_system_set_special_bonds(atvb_system* sys, const double lj[3], const double coul[3],
+                                  int64_t nbonds, const int64_t* tag_a, const int64_t* tag_b) {
+    return guard([&] {
+        need(sys, "sys");
+        need(lj, "lj");
+        need(coul, "coul");
+        sys->eng->set_special_bonds(sys->id, lj, coul, nbonds, tag_a, tag_b);
+    });
+}
+
 int atvb_system_profile(atvb_system* sys, int32_t enable) {
     return guard([&] {
         need(sys, "sys");
@@ -307,6 +326,30 @@ int atvb_batch_autotune(atvb_batch* b, int32_t* lanes) {
         const int g = b->eng->autotune();
         if (lanes)
             *lanes = g;
+    });
+}
+
+int atvb_batch_set_lj_types(atvb_batch* b, int32_t index, int32_t ncoef,
+                            const int32_t* type_i, const int32_t* type_j,
+                            const double* epsilon, const double* sigma) {
+    return guard([&] {
+        need(b, "batch");
+        if (index < 0 || index >= (int)b->ids.size())
+            throw Error(ATVB_ERR_NOTFOUND, "no system " + std::to_string(index) + " in batch");
+        b->eng->set_lj_types(b->ids[index], ncoef, type_i, type_j, epsilon, sigma);
+    });
+}
+
+int atvb_batch_set_special_bonds(atvb_batch* b, int32_t index, const double lj[3],
+                                 const double coul[3], int64_t nbonds, const int64_t* tag_a,
+                                 const int64_t* tag_b) {
+    return guard([&] {
+        need(b, "batch");
+        need(lj, "lj");
+        need(coul, "coul");
+        if (index < 0 || index >= (int)b->ids.size())
+            throw Error(ATVB_ERR_NOTFOUND, "no system " + std::to_string(index) + " in batch");
+        b->eng->set_special_bonds(b->ids[index], lj, coul, nbonds, tag_a, tag_b);
     });
 }
 

@@ -17,6 +17,7 @@
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "atvb.h"
@@ -276,6 +277,8 @@ Slot::Slot(const atvb_system_desc& d, const DevMem& mem) : desc(d), mem_(mem) {
     geo = make_geometry(d);
     std::memset(&hp, 0, sizeof(hp));
     const int n = d.n_atoms;
+    if (n > kMaxAtoms)
+        throw Error(ATVB_ERR_INVALID, "at most 2^30 - 1 atoms per system");
     hp.n = n;
     hp.prec = d.precision == ATVB_MIXED ? kMixed : kFP64;
     if (d.precision != ATVB_FP64 && d.precision != ATVB_MIXED)
@@ -786,6 +789,7 @@ void Engine::build_lists() {
     std::vector<Item> atoms, list, cells, patoms, pgrid, preal;
     std::vector<int> sys;
     std::vector<Item> pair_by[2][kLaneClasses];
+    std::vector<Item> pair_gen[2];
     lc_ = LaunchCfg{};
     int largest = -1;
     pme_slots_.clear();
@@ -805,7 +809,11 @@ void Engine::build_lists() {
             largest = P.n;
             lc_.pair_G = sp->lanes;
         }
-        {
+        if (P.general) {
+            // per-type LJ or special pairs: the general kernel
+            for (int b = 0; b < P.n; b += kPairBlock / kGenLanes)
+                pair_gen[P.prec == kMixed ? 1 : 0].push_back({k, b});
+        } else {
             std::vector<Item>& pv = pair_by[P.prec == kMixed ? 1 : 0][lane_class(sp->lanes)];
             for (int b = 0; b < P.n; b += kPairBlock / sp->lanes)
                 pv.push_back({k, b});
@@ -814,10 +822,10 @@ void Engine::build_lists() {
             cells.push_back({k, b});
         if (P.prec == kMixed)
             lc_.any_mixed = 1;
-        if (P.prec == kMixed && P.has_lj && P.mix_band_lj > 0.0)
-            lc_.any_near = 1;
         else
             lc_.any_fp64 = 1;
+        if (P.prec == kMixed && P.has_lj && !P.general && P.mix_band_lj > 0.0)
+            lc_.any_near = 1;
         if (P.has_pme) {
             if (pme_prec >= 0 && (pme_prec != P.prec || pme_order != P.order))
                 throw Error(ATVB_ERR_INVALID,
@@ -843,6 +851,8 @@ void Engine::build_lists() {
     for (int p = 0; p < 2; ++p)
         for (int c = 0; c < kLaneClasses; ++c)
             lc_.pair[p][c] = make_list(list_allocs_, pair_by[p][c], num_sms_ * 16, mem_);
+    for (int p = 0; p < 2; ++p)
+        lc_.pair_gen[p] = make_list(list_allocs_, pair_gen[p], num_sms_ * 16, mem_);
     lc_.cells = make_list(list_allocs_, cells, g_light, mem_);
     lc_.pme_atoms = make_list(list_allocs_, patoms, g_light, mem_);
     lc_.pme_grid = make_list(list_allocs_, pgrid, g_light, mem_);
@@ -882,6 +892,7 @@ int64_t Engine::kernels_per_step() const {
         for (int c = 0; c < kLaneClasses; ++c)
             k += lc_.pair[p][c].n ? 1 : 0;
     k += lc_.any_near ? 1 : 0;                // near-cutoff fix-up (mixed LJ)
+    k += (lc_.pair_gen[0].n ? 1 : 0) + (lc_.pair_gen[1].n ? 1 : 0); // general pair
     if (!pme_slots_.empty())
         k += 4;                               // spread, convert, influence, gather
     k += 2;                                   // integrate_b, sys_b
@@ -1113,7 +1124,7 @@ LaunchCfg Engine::restricted_cfg(int id) {
         list.push_back({id, b});
     for (int b = 0; b < P.ncell; b += kChunk)
         cells.push_back({id, b});
-    const int pchunk = kPairBlock / s->lanes;
+    const int pchunk = kPairBlock / (P.general ? kGenLanes : s->lanes);
     for (int b = 0; b < P.n; b += pchunk)
         pair.push_back({id, b});
     if (P.has_pme) {
@@ -1131,17 +1142,22 @@ LaunchCfg Engine::restricted_cfg(int id) {
     c.atoms = make_list(list_allocs_, atoms, num_sms_ * 16, mem_);
     c.list = make_list(list_allocs_, list, num_sms_ * 32, mem_);
     c.cells = make_list(list_allocs_, cells, num_sms_ * 16, mem_);
-    for (int p = 0; p < 2; ++p)
+    for (int p = 0; p < 2; ++p) {
         for (int k = 0; k < kLaneClasses; ++k)
             c.pair[p][k] = ItemList{};
-    c.pair[P.prec == kMixed ? 1 : 0][lane_class(s->lanes)] =
-        make_list(list_allocs_, pair, num_sms_ * 16, mem_);
+        c.pair_gen[p] = ItemList{};
+    }
+    if (P.general)
+        c.pair_gen[P.prec == kMixed ? 1 : 0] = make_list(list_allocs_, pair, num_sms_ * 16, mem_);
+    else
+        c.pair[P.prec == kMixed ? 1 : 0][lane_class(s->lanes)] =
+            make_list(list_allocs_, pair, num_sms_ * 16, mem_);
     c.pme_atoms = make_list(list_allocs_, patoms, num_sms_ * 16, mem_);
     c.pme_grid = make_list(list_allocs_, pgrid, num_sms_ * 16, mem_);
     c.pme_real = make_list(list_allocs_, preal, num_sms_ * 16, mem_);
     c.any_mixed = P.prec == kMixed;
     c.any_fp64 = P.prec != kMixed;
-    c.any_near = P.prec == kMixed && P.has_lj && P.mix_band_lj > 0.0;
+    c.any_near = P.prec == kMixed && P.has_lj && !P.general && P.mix_band_lj > 0.0;
     if (P.has_pme) {
         c.pme_mixed = P.prec == kMixed;
         c.pme_order = P.order;
@@ -1154,6 +1170,194 @@ LaunchCfg Engine::restricted_cfg(int id) {
     c.nsys = 1;
     single_[id] = {list_epoch_, c};
     return c;
+}
+
+// PairLJCut per-type coefficients (src/cpu/potentials/pair_lj_cut.cpp:44-112
+// set_type_coeff): explicit symmetric (type_i, type_j, eps, sigma) entries,
+// checked here, turned into tables at upload (build_lj_tables).
+void Engine::set_lj_types(int id, int ncoef, const int32_t* ti, const int32_t* tj,
+                          const double* eps, const double* sigma) {
+    Slot* sl = slot(id);
+    if (sl->uploaded)
+        throw Error(ATVB_ERR_STATE, "LJ type coefficients must be set before the first upload");
+    if (!sl->hp.has_lj)
+        throw Error(ATVB_ERR_INVALID, "PairLJCut is not enabled for this system");
+    if (ncoef < 1 || !ti || !tj || !eps || !sigma)
+        throw Error(ATVB_ERR_INVALID,
+                    "PairLJCut: the per-type form needs at least one coefficient");
+    int nt = 0;
+    for (int k = 0; k < ncoef; ++k) {
+        if (ti[k] < 0 || tj[k] < 0)
+            throw Error(ATVB_ERR_INVALID, "PairLJCut::set_type_coeff: types must be >= 0");
+        if (!(sigma[k] > 0.0))
+            throw Error(ATVB_ERR_INVALID, "PairLJCut::set_type_coeff: sigma must be > 0");
+        nt = std::max(nt, std::max(ti[k], tj[k]) + 1);
+    }
+    if (nt > 255)
+        throw Error(ATVB_ERR_INVALID, "at most 255 LJ types");
+    sl->lj_ti.assign(ti, ti + ncoef);
+    sl->lj_tj.assign(tj, tj + ncoef);
+    sl->lj_eps.assign(eps, eps + ncoef);
+    sl->lj_sig.assign(sigma, sigma + ncoef);
+    sl->ntypes = nt;
+    sl->hp.general = 1;
+    push_params(id);
+    dirty_ = true;
+}
+
+// The type tables (pair_lj_cut.cpp:255-298 finalize_type_table_), over every
+// type named by a coefficient or carried by an atom: an unset cross term
+// mixes by Lorentz-Berthelot from the two diagonals (sqrt(eps_ii eps_jj),
+// (sigma_ii + sigma_jj) / 2); without both diagonals the pair does not
+// interact (eps = 0), so a type with no coefficient has no LJ site; every
+// type pair is shifted at the common cutoff.
+void Slot::build_lj_tables(const std::vector<int>& types, cudaStream_t stream) {
+    int nt = ntypes;
+    for (int t : types) {
+        if (t < 0 || t > 254)
+            throw Error(ATVB_ERR_INVALID, "atom types must be in [0, 254]");
+        nt = std::max(nt, t + 1);
+    }
+    std::vector<double> e((size_t)nt * nt, 0.0), sg((size_t)nt * nt, 0.0);
+    std::vector<char> set((size_t)nt * nt, 0);
+    for (size_t k = 0; k < lj_ti.size(); ++k) {
+        const size_t ab = (size_t)lj_ti[k] * nt + lj_tj[k], ba = (size_t)lj_tj[k] * nt + lj_ti[k];
+        e[ab] = e[ba] = lj_eps[k];
+        sg[ab] = sg[ba] = lj_sig[k];
+        set[ab] = set[ba] = 1;
+    }
+    const double rc = desc.lj_cutoff;
+    std::vector<double> tab((size_t)nt * nt * 4);
+    std::vector<float> tabf(tab.size());
+    for (int a = 0; a < nt; ++a)
+        for (int b = 0; b < nt; ++b) {
+            const size_t ab = (size_t)a * nt + b;
+            double ee = e[ab], ss = sg[ab];
+            if (!set[ab]) {
+                const size_t aa = (size_t)a * nt + a, bb = (size_t)b * nt + b;
+                if (set[aa] && set[bb]) {
+                    ee = std::sqrt(e[aa] * e[bb]);
+                    ss = 0.5 * (sg[aa] + sg[bb]);
+                } else {
+                    ee = 0.0;
+                    ss = 1.0;
+                }
+            }
+            const double s2 = ss * ss, s6 = s2 * s2 * s2;
+            const double r2inv = 1.0 / (rc * rc);
+            const double r6inv = r2inv * r2inv * r2inv * s6;
+            const double v[4] = {s6, 4.0 * ee, 24.0 * ee, 4.0 * ee * (r6inv * r6inv - r6inv)};
+            for (int q = 0; q < 4; ++q) {
+                tab[ab * 4 + q] = v[q];
+                tabf[ab * 4 + q] = (float)v[q];
+            }
+        }
+    double* dt = (double*)dalloc(tab.size() * sizeof(double));
+    float* dtf = (float*)dalloc(tabf.size() * sizeof(float));
+    int* dtype = (int*)dalloc((size_t)hp.n * sizeof(int));
+    CK(cudaMemcpyAsync(dt, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice,
+                       stream));
+    CK(cudaMemcpyAsync(dtf, tabf.data(), tabf.size() * sizeof(float), cudaMemcpyHostToDevice,
+                       stream));
+    CK(cudaMemcpyAsync(dtype, types.data(), (size_t)hp.n * sizeof(int), cudaMemcpyHostToDevice,
+                       stream));
+    CK(cudaStreamSynchronize(stream));
+    hp.lj_tab = dt;
+    hp.lj_tabf = dtf;
+    hp.type = dtype;
+    hp.stype = (unsigned char*)dalloc((size_t)hp.n);
+    hp.ntypes = nt;
+}
+
+// PairLJCut / CoulLong set_special_bonds(s12, s13, s14) with the bond
+// topology: partners 1, 2 and 3 bonds away (the nearest distance wins) get
+// the scales of their class; built at upload from the tags.
+void Engine::set_special_bonds(int id, const double lj[3], const double coul[3],
+                               int64_t nbonds, const int64_t* a, const int64_t* b) {
+    Slot* sl = slot(id);
+    if (sl->uploaded)
+        throw Error(ATVB_ERR_STATE, "special bonds must be set before the first upload");
+    if (nbonds < 0 || (nbonds > 0 && (!a || !b)))
+        throw Error(ATVB_ERR_INVALID, "special bonds: bad bond list");
+    for (int k = 0; k < 3; ++k) {
+        if (!(lj[k] >= 0.0 && lj[k] <= 1.0) || !(coul[k] >= 0.0 && coul[k] <= 1.0))
+            throw Error(ATVB_ERR_INVALID, "special bond scales must be in [0, 1]");
+        sl->sp_lj[k] = lj[k];
+        sl->sp_coul[k] = coul[k];
+    }
+    sl->bond_a.assign(a, a + nbonds);
+    sl->bond_b.assign(b, b + nbonds);
+    sl->special_set = true;
+    sl->hp.general = 1;
+    push_params(id);
+    dirty_ = true;
+}
+
+void Slot::build_specials(const std::vector<long long>& tags, cudaStream_t stream) {
+    const int n = hp.n;
+    std::unordered_map<long long, int> idx;
+    idx.reserve((size_t)n * 2);
+    for (int i = 0; i < n; ++i)
+        idx[tags[i]] = i;
+    std::vector<std::vector<int>> adj(n);
+    for (size_t k = 0; k < bond_a.size(); ++k) {
+        auto ia = idx.find(bond_a[k]), ib = idx.find(bond_b[k]);
+        if (ia == idx.end() || ib == idx.end() || ia->second == ib->second)
+            throw Error(ATVB_ERR_INVALID, "special bonds: a bond names an unknown atom tag");
+        adj[ia->second].push_back(ib->second);
+        adj[ib->second].push_back(ia->second);
+    }
+    std::vector<int> first(n + 1, 0), js;
+    std::vector<unsigned char> cls;
+    std::vector<int> depth(n, -1), touched;
+    for (int i = 0; i < n; ++i) {
+        first[i] = (int)js.size();
+        std::vector<int> frontier = {i};
+        depth[i] = 0;
+        touched.assign(1, i);
+        std::vector<std::pair<int, int>> found;
+        for (int d = 1; d <= 3; ++d) {
+            std::vector<int> next;
+            for (int u : frontier)
+                for (int v : adj[u])
+                    if (depth[v] < 0) {
+                        depth[v] = d;
+                        touched.push_back(v);
+                        next.push_back(v);
+                        if (sp_lj[d - 1] != 1.0 || sp_coul[d - 1] != 1.0)
+                            found.push_back({v, d});
+                    }
+            frontier.swap(next);
+        }
+        for (int v : touched)
+            depth[v] = -1;
+        std::sort(found.begin(), found.end());
+        for (auto& f : found) {
+            js.push_back(f.first);
+            cls.push_back((unsigned char)f.second);
+        }
+    }
+    first[n] = (int)js.size();
+    int* d_first = (int*)dalloc(first.size() * sizeof(int));
+    int* d_j = (int*)dalloc(std::max<size_t>(js.size(), 1) * sizeof(int));
+    unsigned char* d_c = (unsigned char*)dalloc(std::max<size_t>(cls.size(), 1));
+    CK(cudaMemcpyAsync(d_first, first.data(), first.size() * sizeof(int),
+                       cudaMemcpyHostToDevice, stream));
+    if (!js.empty()) {
+        CK(cudaMemcpyAsync(d_j, js.data(), js.size() * sizeof(int), cudaMemcpyHostToDevice,
+                           stream));
+        CK(cudaMemcpyAsync(d_c, cls.data(), cls.size(), cudaMemcpyHostToDevice, stream));
+    }
+    CK(cudaStreamSynchronize(stream));
+    hp.sp_first = d_first;
+    hp.sp_j = d_j;
+    hp.sp_cls = d_c;
+    hp.has_special = 1;
+    hp.sp_lj[0] = hp.sp_coul[0] = 1.0;
+    for (int k = 0; k < 3; ++k) {
+        hp.sp_lj[k + 1] = sp_lj[k];
+        hp.sp_coul[k + 1] = sp_coul[k];
+    }
 }
 
 void Engine::upload(int id, const atvb_soa_view& f) {
@@ -1194,6 +1398,15 @@ void Engine::upload(int id, const atvb_soa_view& f) {
         tag[i] = f.tag ? f.tag[i] : (long long)(i + 1);
     CK(cudaMemcpyAsync(s->hp.tag, tag.data(), 8 * n, cudaMemcpyHostToDevice,
                        stream_));
+    if (s->ntypes > 0) {
+        std::vector<int> ty(n, 0);
+        if (f.type)
+            for (int i = 0; i < n; ++i)
+                ty[i] = f.type[i];
+        s->build_lj_tables(ty, stream_);
+    }
+    if (s->special_set)
+        s->build_specials(tag, stream_);
     // charges: PME self + net-charge constants (pme.cpp:224-252)
     double qs = 0, q2 = 0;
     if (f.charge)
@@ -1335,7 +1548,7 @@ int64_t Engine::pairs(int id, int32_t* pi, int32_t* pj, int64_t capacity) {
     int64_t cnt = 0;
     for (int a = 0; a < n; ++a)
         for (int k = 0; k < nn[a]; ++k) {
-            const int i = perm[a], j = perm[nbr[(size_t)a * cap + k]];
+            const int i = perm[a], j = perm[nbr[(size_t)a * cap + k] & (int)kRowIdxMask];
             if (i < j) {
                 if (pi && pj && cnt < capacity) {
                     pi[cnt] = i;

@@ -160,6 +160,8 @@ __global__ void k_permute(const Item* items, int nitems, const SysParams* sp) {
             const double xx[3] = {x, y, z};
             reinterpret_cast<double4*>(P.pos4)[s] = pack_pos64(xx, P.fix64_scale, q);
         }
+        if (P.ntypes)
+            P.stype[s] = (unsigned char)P.type[i];
         P.xr[i] = x;
         P.yr[i] = y;
         P.zr[i] = z;
@@ -227,6 +229,16 @@ ATVB_DEV void column_runs(const SysParams& P, const int* __restrict__ cstart, in
         a1 = 0;
         l1 = 0;
     }
+}
+
+// Special class (1: 1-2, 2: 1-3, 3: 1-4, 0: none) of sorted pair (i, j):
+// a scan of i's few special partners, by original index.
+ATVB_DEV unsigned special_class(const SysParams& P, int i, int j) {
+    const int io = P.perm[i], jo = P.perm[j];
+    for (int q = P.sp_first[io]; q < P.sp_first[io + 1]; ++q)
+        if (P.sp_j[q] == jo)
+            return P.sp_cls[q];
+    return 0u;
 }
 
 // Stage 6 (items of kListChunk cells): one warp per cell.  Every atom of a
@@ -341,8 +353,11 @@ __global__ void __launch_bounds__(256)
                                 const int base = __shfl_sync(full, cnt, ii);
                                 if (hit) {
                                     const int wpos = base + __popc(m & lt);
+                                    unsigned e = (unsigned)j;
+                                    if (P.has_special)
+                                        e |= special_class(P, i0 + ii, j) << 30;
                                     if (wpos < cap)
-                                        P.nbr[(size_t)(i0 + ii) * cap + wpos] = j;
+                                        P.nbr[(size_t)(i0 + ii) * cap + wpos] = (int)e;
                                 }
                                 if (lane == ii)
                                     cnt += __popc(m);
@@ -368,8 +383,11 @@ __global__ void __launch_bounds__(256)
                                 const int base = __shfl_sync(full, cnt, ii);
                                 if (hit) {
                                     const int wpos = base + __popc(m & lt);
+                                    unsigned e = (unsigned)j;
+                                    if (P.has_special)
+                                        e |= special_class(P, i0 + ii, j) << 30;
                                     if (wpos < cap)
-                                        P.nbr[(size_t)(i0 + ii) * cap + wpos] = j;
+                                        P.nbr[(size_t)(i0 + ii) * cap + wpos] = (int)e;
                                 }
                                 if (lane == ii)
                                     cnt += __popc(m);

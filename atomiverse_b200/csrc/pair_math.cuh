@@ -1,0 +1,182 @@
+// pair_math.cuh -- numerics shared by the pair kernels (pair.cu and
+// pair_general.cu): approximate FP32 special functions, this library's FP64
+// exp and reciprocal, the erfcx polynomial, per-row constants and sums, and
+// the fixed-point flush of energies and virials.
+#pragma once
+
+#include "atvb_common.cuh"
+#include "atvb_kernels.cuh"
+#include "erfcx_coef.h"
+
+namespace atvb {
+
+constexpr double kMinPair2 = 1e-20; // lj_kernel.cuh:15 kMinPairDist^2
+
+struct PairAcc {
+    double fx, fy, fz, elj, ec;
+    double v[6];
+};
+
+// ---- approximate FP32 special functions (PTX .approx instructions) -------
+ATVB_DEV float ex2_approx(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+ATVB_DEV float rcp_approx(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+ATVB_DEV float rsqrt_approx(float x) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// exp(-z) for z >= 0 in FP64 (Cody-Waite argument reduction): with
+// n = rint(-z / ln 2) and r = -z - n ln 2 (ln 2 split into a 32-bit head,
+// so n * head is exact, and a tail), |r| <= ln(2)/2 and
+// exp(-z) = 2^n exp(r), exp(r) by its Taylor series to degree 12
+// (truncation < 2e-16).  z is clamped at 708 (the result is then ~1e-308,
+// far below anything the callers keep).
+ATVB_DEV double exp_neg64(double z) {
+    const double w = -fmin(z, 708.0);
+    const double n = rint(w * 1.4426950408889634);
+    double r = fma(-n, 0.6931471803691238, w);
+    r = fma(-n, 1.9082149292705877e-10, r);
+    double p = 2.08767569878681e-09;
+    p = fma(p, r, 2.505210838544172e-08);
+    p = fma(p, r, 2.755731922398589e-07);
+    p = fma(p, r, 2.7557319223985893e-06);
+    p = fma(p, r, 2.48015873015873e-05);
+    p = fma(p, r, 0.0001984126984126984);
+    p = fma(p, r, 0.001388888888888889);
+    p = fma(p, r, 0.008333333333333333);
+    p = fma(p, r, 0.041666666666666664);
+    p = fma(p, r, 0.16666666666666666);
+    p = fma(p, r, 0.5);
+    p = fma(p, r, 1.0);
+    p = fma(p, r, 1.0);
+    const long long e = (long long)((int)n + 1023) << 52; // n >= -1022
+    return p * __longlong_as_double(e);
+}
+
+// 1 / v for 1 <= v <= 4 in FP64: FP32 estimate, two Newton steps
+// (relative error 2^-22 -> 2^-44 -> below one FP64 ulp).
+ATVB_DEV double rcp64(double v) {
+    double t = (double)rcp_approx((float)v);
+    t = fma(t, fma(-v, t, 1.0), t);
+    return fma(t, fma(-v, t, 1.0), t);
+}
+
+// erfcx(x) for 0 <= x <= 6 from the universal polynomial of erfcx_coef.h,
+// given t = 1 / (1 + kErfcxP x).  Coefficients are compile-time constants.
+ATVB_DEV double erfcx_of_t(double t) {
+    const double u = fma(kErfcxA, t, kErfcxB);
+    double p = kErfcxD[kErfcxD_N - 1];
+#pragma unroll
+    for (int k = kErfcxD_N - 2; k >= 0; --k)
+        p = fma(p, u, kErfcxD[k]);
+    return p;
+}
+ATVB_DEV float erfcx_of_t(float t) {
+    const float u = fmaf((float)kErfcxA, t, (float)kErfcxB);
+    float p = kErfcxF[kErfcxF_N - 1];
+#pragma unroll
+    for (int k = kErfcxF_N - 2; k >= 0; --k)
+        p = fmaf(p, u, kErfcxF[k]);
+    return p;
+}
+
+// Per-row constants of one system, hoisted out of the pair loop.
+template <typename T>
+struct RowConst {
+    T lj_rc2, sig6, eps4, eps24, shift;
+    T c_rc2, alpha, alpha2; // alpha2: alpha^2 (FP64) or alpha^2 log2(e) (FP32)
+    T kqi;
+    T band_lj, band_c; // FP32 only: error band of r^2 around each cutoff
+};
+
+template <typename T>
+struct RowSums {
+    T fx = 0, fy = 0, fz = 0, elj = 0, ec = 0;
+    T v[6] = {0, 0, 0, 0, 0, 0};
+    // mixed build: force components summed in 64-bit fixed point, units of
+    // kForceFix^-1 eV/A (range +-2e9 eV/A), so the row sum is exact and
+    // independent of summation order
+    long long fq[3] = {0, 0, 0};
+};
+constexpr float kForceFix = 4294967296.0f;  // 2^32
+constexpr double kForceFixInv = 1.0 / 4294967296.0;
+
+template <typename T>
+ATVB_DEV void finish_row(const RowSums<T>& r, PairAcc& a, bool vir) {
+    if constexpr (sizeof(T) == 4) {
+        // multiples of 2^-32 below 2^21 in magnitude: every later FP64 sum of
+        // the lanes' values is exact, so the force is order-independent
+        a.fx = (double)r.fq[0] * kForceFixInv;
+        a.fy = (double)r.fq[1] * kForceFixInv;
+        a.fz = (double)r.fq[2] * kForceFixInv;
+    } else {
+        a.fx = (double)r.fx;
+        a.fy = (double)r.fy;
+        a.fz = (double)r.fz;
+    }
+    a.elj += (double)r.elj;
+    a.ec += (double)r.ec;
+    if (vir)
+        for (int k = 0; k < 6; ++k)
+            a.v[k] += (double)r.v[k];
+}
+
+template <typename T>
+ATVB_DEV RowConst<T> row_const(const SysParams& P, double qi) {
+    RowConst<T> c;
+    c.lj_rc2 = (T)P.lj_rc2;
+    c.sig6 = (T)P.lj_sig6;
+    c.eps4 = (T)P.lj_eps4;
+    c.eps24 = (T)P.lj_eps24;
+    c.shift = (T)P.lj_shift;
+    c.c_rc2 = (T)P.coul_rc2;
+    c.alpha = (T)P.coul_alpha;
+    c.alpha2 = sizeof(T) == 4 ? (T)(P.coul_alpha2 * 1.4426950408889634) : (T)P.coul_alpha2;
+    c.kqi = (T)(kQqr2e * qi);
+    c.band_lj = (T)P.mix_band_lj;
+    c.band_c = (T)P.mix_band_c;
+    return c;
+}
+
+// Per-item flush: every item's energy/virial partial is rounded to fixed
+// point on its own, so a system's sums do not depend on which other systems
+// share the launch (results are identical alone and batched).
+ATVB_DEV void flush_energy(const SysParams& P, PairAcc& a, double* sh) {
+    if (P.need_virial) {
+        double v[8] = {a.elj, a.ec, a.v[0], a.v[1], a.v[2], a.v[3], a.v[4], a.v[5]};
+        block_sum_vec<8>(v, sh);
+        if (threadIdx.x == 0) {
+            if (P.has_lj)
+                fix_add(&P.st->acc[kAccELJ], 0.5 * v[0]);
+            if (P.has_coul)
+                fix_add(&P.st->acc[kAccECoul], 0.5 * v[1]);
+            for (int k = 0; k < 6; ++k)
+                fix_add(&P.st->acc[kAccVir + k], 0.5 * v[2 + k]);
+        }
+    } else {
+        double v[2] = {a.elj, a.ec};
+        block_sum_vec<2>(v, sh);
+        if (threadIdx.x == 0) {
+            // 1/2: every pair is visited from both of its atoms
+            if (P.has_lj)
+                fix_add(&P.st->acc[kAccELJ], 0.5 * v[0]);
+            if (P.has_coul)
+                fix_add(&P.st->acc[kAccECoul], 0.5 * v[1]);
+        }
+    }
+    a.elj = a.ec = 0.0;
+    for (int k = 0; k < 6; ++k)
+        a.v[k] = 0.0;
+}
+
+// Mixed: at least 3 resident blocks (80 registers); FP64: 2.
+} // namespace atvb

@@ -162,6 +162,25 @@ int atvb_system_energy_history(atvb_system* sys, double* out,
  * to get the count only. */
 int atvb_system_pairs(atvb_system* sys, int32_t* pi, int32_t* pj,
                       int64_t capacity, int64_t* count);
+/* Per-type LJ: PairLJCut(std::vector<LJTypeCoeff>, cutoff) / set_type_coeff
+ * (src/cpu/potentials/pair_lj_cut.cpp:44-112; table :255-298).  ncoef
+ * symmetric (type_i, type_j, epsilon, sigma) entries; an unset cross term
+ * mixes by Lorentz-Berthelot from the two diagonals, or does not interact
+ * (epsilon 0) when a diagonal is missing; every type pair is shifted at
+ * lj_cutoff.  Per-atom types come from atvb_soa_view.type at upload.  Call
+ * before the first upload (ATVB_ERR_STATE after); at most 255 types. */
+int atvb_system_set_lj_types(atvb_system* sys, int32_t ncoef, const int32_t* type_i,
+                             const int32_t* type_j, const double* epsilon,
+                             const double* sigma);
+/* Special bonds: PairLJCut::set_special_bonds / CoulLong::set_special_bonds
+ * (s12, s13, s14) (pair_lj_cut.cpp:118-200, coul_long.cpp:34-99) with the
+ * bond topology as pairs of atom tags.  Partners 1, 2 and 3 bonds away
+ * (nearest wins) take the class scales: LJ force and shifted energy times
+ * lj[c]; real-space Coulomb keeps erfc and subtracts (1 - coul[c]) k_e q q / r
+ * (coul_long.cpp:159-196).  Scales in [0, 1].  Call before the first upload. */
+int atvb_system_set_special_bonds(atvb_system* sys, const double lj[3],
+                                  const double coul[3], int64_t nbonds,
+                                  const int64_t* tag_a, const int64_t* tag_b);
 /* Profiling: enable per-kernel-group CUDA events on subsequent steps. */
 int atvb_system_profile(atvb_system* sys, int32_t enable);
 int atvb_system_profile_read(atvb_system* sys, atvb_kernel_time* out,
@@ -182,6 +201,14 @@ int atvb_batch_compute_forces(atvb_batch* b);
 int atvb_batch_step(atvb_batch* b, int32_t n_steps);
 int atvb_batch_download(atvb_batch* b, int32_t index, atvb_soa_view* frame,
                         atvb_scalars* scalars);
+/* atvb_system_set_lj_types / _set_special_bonds for system `index` of a
+ * batch, before that system's first upload. */
+int atvb_batch_set_lj_types(atvb_batch* b, int32_t index, int32_t ncoef,
+                            const int32_t* type_i, const int32_t* type_j,
+                            const double* epsilon, const double* sigma);
+int atvb_batch_set_special_bonds(atvb_batch* b, int32_t index, const double lj[3],
+                                 const double coul[3], int64_t nbonds,
+                                 const int64_t* tag_a, const int64_t* tag_b);
 /* Time candidate pair-kernel shapes on the batch's own size mix and keep
  * the fastest; *lanes receives the choice. */
 int atvb_batch_autotune(atvb_batch* b, int32_t* lanes);

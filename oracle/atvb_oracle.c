@@ -460,6 +460,13 @@ int orc_set_lj_types(orc_sys* s, int ncoef, const int32_t* ti, const int32_t* tj
         if (tj[k] + 1 > nt)
             nt = tj[k] + 1;
     }
+    /* atom types without coefficients have no LJ site (eps = 0) */
+    for (int i = 0; type && i < s->n; ++i) {
+        if (type[i] < 0)
+            return -1;
+        if (type[i] + 1 > nt)
+            nt = type[i] + 1;
+    }
     const size_t nn = (size_t)nt * nt;
     double* e = (double*)calloc(nn, sizeof(double));
     double* sg = (double*)calloc(nn, sizeof(double));

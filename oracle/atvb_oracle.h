@@ -91,8 +91,10 @@ int orc_run(orc_sys* s, int n_steps, double* hist);
  * term mixes by Lorentz-Berthelot (eps = sqrt(eps_ii eps_jj),
  * sigma = (sigma_ii + sigma_jj)/2, :246-252) when both diagonals are set,
  * else the pair does not interact (eps = 0).  Each type pair is shifted at
- * the common cutoff.  type[n] is the per-atom type.  Returns the number of
- * types, or -1 on a bad coefficient (type < 0 or sigma <= 0). */
+ * the common cutoff.  type[n] is the per-atom type; the table covers every
+ * type named by a coefficient or carried by an atom (a type without
+ * coefficients has no LJ site).  Returns the number of types, or -1 on a bad
+ * coefficient (type < 0 or sigma <= 0) or a negative atom type. */
 int orc_set_lj_types(orc_sys* s, int ncoef, const int32_t* ti, const int32_t* tj,
                      const double* eps, const double* sigma, const int32_t* type);
 /* Special pairs (LAMMPS special_bonds; cpu/potentials/special_scale.h,
