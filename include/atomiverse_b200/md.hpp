@@ -5,6 +5,8 @@
 //   NeighborList(cutoff, skin = -1, every = 1, delay = 0, check = true)
 //       include/atomiverse/cuda/neighbor/neighbor_list.cuh:98
 //   PairLJCut(epsilon, sigma, cutoff)       cuda/potentials/pair_lj_cut.cuh:25
+//   PairLJCut({LJTypeCoeff...}, cutoff), set_type_coeff, set_special_bonds
+//       (src/cpu/potentials/pair_lj_cut.cpp:44-200; CoulLong::set_special_bonds)
 //   CoulLong(alpha, cutoff)                 cuda/potentials/coul_long.cuh:24
 //   KSpacePME(alpha, grid_spacing = 1.0, order = 6)  cuda/longrange/pme.cuh:26
 //   md::VelocityVerlet(dt), md::NoseHoover(T, tau, dt),
@@ -23,6 +25,7 @@
 #include <cstring>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 namespace atvb_cpp {
@@ -40,6 +43,8 @@ inline void check(int rc) {
 struct Frame {
     std::vector<double> x, y, z, vx, vy, vz, fx, fy, fz, mass, charge;
     std::vector<int64_t> tag;
+    std::vector<int32_t> type;                      // LJ type per atom (per-type PairLJCut)
+    std::vector<std::pair<int64_t, int64_t>> bonds; // topology (tags) for special bonds
     double box[3] = {0, 0, 0};
     int n() const { return (int)x.size(); }
     void resize(int n) {
@@ -56,6 +61,7 @@ struct Frame {
         v.vx = vx.data(); v.vy = vy.data(); v.vz = vz.data();
         v.fx = fx.data(); v.fy = fy.data(); v.fz = fz.data();
         v.mass = mass.data(); v.charge = charge.data(); v.tag = tag.data();
+        v.type = type.empty() ? nullptr : type.data();
         return v;
     }
 };
@@ -68,18 +74,60 @@ struct NeighborList {
                           int delay_ = 0, bool check_ = true)
         : cutoff(cutoff_), skin(skin_), every(every_), delay(delay_), check(check_) {}
 };
+/// One (type_i, type_j, epsilon, sigma) entry of a per-type PairLJCut.
+struct LJTypeCoeff {
+    int type_i, type_j;
+    double epsilon, sigma;
+};
+/// LAMMPS special_bonds scales for 1-2, 1-3 and 1-4 partners.
+struct SpecialScales {
+    double s12 = 1.0, s13 = 1.0, s14 = 1.0;
+    bool active() const { return s12 != 1.0 || s13 != 1.0 || s14 != 1.0; }
+};
 struct PairLJCut {
-    double epsilon, sigma, cutoff;
+    double epsilon = 0.0, sigma = 0.0, cutoff;
+    std::vector<LJTypeCoeff> coeffs; // non-empty: per-type form
+    SpecialScales special;
     PairLJCut(double e, double s, double c) : epsilon(e), sigma(s), cutoff(c) {
         if (c <= 0.0)
             throw std::invalid_argument("PairLJCut: cutoff must be positive");
     }
+    /// Per-type form (pair_lj_cut.cpp:44-66): unset cross terms mix by
+    /// Lorentz-Berthelot; a type without coefficients has no LJ site.
+    PairLJCut(std::vector<LJTypeCoeff> c, double rc) : cutoff(rc), coeffs(std::move(c)) {
+        if (rc <= 0.0)
+            throw std::invalid_argument("PairLJCut: cutoff must be positive");
+        if (coeffs.empty())
+            throw std::invalid_argument(
+                "PairLJCut: the per-type constructor needs at least one coefficient");
+        epsilon = coeffs[0].epsilon; // scalar fields only carry a valid description
+        sigma = coeffs[0].sigma;
+    }
+    PairLJCut& set_type_coeff(int ti, int tj, double e, double s) {
+        if (coeffs.empty())
+            throw std::logic_error("PairLJCut::set_type_coeff: built with a single epsilon/sigma");
+        if (ti < 0 || tj < 0)
+            throw std::invalid_argument("PairLJCut::set_type_coeff: types must be >= 0");
+        if (s <= 0.0)
+            throw std::invalid_argument("PairLJCut::set_type_coeff: sigma must be > 0");
+        coeffs.push_back({ti, tj, e, s});
+        return *this;
+    }
+    PairLJCut& set_special_bonds(double s12, double s13, double s14) {
+        special = {s12, s13, s14};
+        return *this;
+    }
 };
 struct CoulLong {
     double alpha, cutoff;
+    SpecialScales special;
     CoulLong(double a, double c) : alpha(a), cutoff(c) {
         if (a <= 0.0 || c <= 0.0)
             throw std::invalid_argument("CoulLong: alpha and cutoff must be > 0");
+    }
+    CoulLong& set_special_bonds(double s12, double s13, double s14) {
+        special = {s12, s13, s14};
+        return *this;
     }
 };
 struct KSpacePME {
@@ -148,6 +196,8 @@ class MD {
         d_.lj_epsilon = p.epsilon;
         d_.lj_sigma = p.sigma;
         d_.lj_cutoff = p.cutoff;
+        lj_coeffs_ = p.coeffs;
+        lj_special_ = p.special;
         have_pair_ = true;
         return *this;
     }
@@ -155,6 +205,7 @@ class MD {
         d_.coul_enabled = 1;
         d_.coul_alpha = c.alpha;
         d_.coul_cutoff = c.cutoff;
+        coul_special_ = c.special;
         have_pair_ = true;
         return *this;
     }
@@ -211,6 +262,29 @@ class MD {
             d_.box[4] = frame.box[1];
             d_.box[8] = frame.box[2];
             check(atvb_system_create(ctx_, &d_, &sys_));
+            if (!lj_coeffs_.empty()) {
+                std::vector<int32_t> ti, tj;
+                std::vector<double> e, sg;
+                for (const auto& c : lj_coeffs_) {
+                    ti.push_back(c.type_i);
+                    tj.push_back(c.type_j);
+                    e.push_back(c.epsilon);
+                    sg.push_back(c.sigma);
+                }
+                check(atvb_system_set_lj_types(sys_, (int32_t)ti.size(), ti.data(), tj.data(),
+                                               e.data(), sg.data()));
+            }
+            if (lj_special_.active() || coul_special_.active()) {
+                const double lj[3] = {lj_special_.s12, lj_special_.s13, lj_special_.s14};
+                const double co[3] = {coul_special_.s12, coul_special_.s13, coul_special_.s14};
+                std::vector<int64_t> a, b;
+                for (const auto& bd : frame.bonds) {
+                    a.push_back(bd.first);
+                    b.push_back(bd.second);
+                }
+                check(atvb_system_set_special_bonds(sys_, lj, co, (int64_t)a.size(), a.data(),
+                                                    b.data()));
+            }
         }
         atvb_soa_view v = frame.view();
         atvb_scalars s{};
@@ -224,6 +298,8 @@ class MD {
     atvb_system_desc d_;
     int precision_;
     bool have_nl_ = false, have_pair_ = false, have_integrator_ = false;
+    std::vector<LJTypeCoeff> lj_coeffs_;
+    SpecialScales lj_special_, coul_special_;
 };
 } // namespace md
 } // namespace atvb_cpp

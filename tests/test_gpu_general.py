@@ -178,3 +178,45 @@ def test_configuration_after_upload_is_refused(atvb, ctx):
         atvb.check(s.lib.atvb_system_set_lj_types(s._h, *args))
     assert e.value.code == 4
     s.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [0, 1])
+def test_cpp_water_matches_python(atvb, ctx, tmp_path, precision):
+    """md::MD with per-type PairLJCut, special bonds and PME (C++ mirror)
+    gives bit for bit what the Python layer gives for the same frame."""
+    import os
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    desc, frame, coeffs, special = _water(m=8)  # box 24.8 > 2 (rc + skin)
+    n, bonds = desc["n_atoms"], special["bonds"]
+    path = tmp_path / "water.bin"
+    with open(path, "wb") as fh:
+        fh.write(np.array([n, len(bonds)], dtype=np.int64).tobytes())
+        fh.write(np.array(list(desc["box"]) + [desc["coul_alpha"], desc["coul_cutoff"]]).tobytes())
+        fh.write(np.array([desc["pme_grid"][0]], dtype=np.int64).tobytes())
+        for k in ("x", "y", "z", "charge", "mass"):
+            fh.write(np.ascontiguousarray(frame[k], dtype=np.float64).tobytes())
+        fh.write(frame["type"].astype(np.int32).tobytes())
+        fh.write(np.array(bonds, dtype=np.int64).tobytes())
+    exe = str(tmp_path / "md_water")
+    lib_dir = os.path.join(root, "atomiverse_b200")
+    subprocess.run(["g++", "-std=c++17", "-O2", "-I", os.path.join(root, "include"),
+                    os.path.join(root, "tests", "cpp", "md_water.cpp"), "-o", exe,
+                    "-L", lib_dir, "-latvb", "-Wl,-rpath," + lib_dir], check=True)
+    r = subprocess.run([exe, str(path), "20", str(precision)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    out = r.stdout.split()
+    d = dict(desc, precision=precision, dt=0.5, stress_required=0)
+    s = atvb.System(ctx, d, frame, lj_types=coeffs, special_bonds=special)
+    fr = {k: np.array(v, copy=True) for k, v in frame.items()}
+    sc = s.run(fr, 20)
+    s.close()
+    csum = 0.0
+    for x, y, z in zip(fr["x"].tolist(), fr["y"].tolist(), fr["z"].tolist()):
+        csum += x + 2.0 * y + 3.0 * z
+    assert int(out[0]) == sc["step"] == 20
+    assert float(out[1]) == sc["energy_lj"]
+    assert float(out[2]) == sc["energy_coul"]
+    assert float(out[3]) == sc["energy_recip"]
+    assert float(out[4]) == pytest.approx(csum, rel=1e-15, abs=0)
