@@ -17,8 +17,25 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle.so")
 REF_PME_PATH = os.path.join(HERE, "_ref", "libref_pme.so")
 
-THERMO_NONE, THERMO_NH, THERMO_LANGEVIN = 0, 1, 2
+THERMO_NONE, THERMO_NH, THERMO_LANGEVIN, THERMO_NPT = 0, 1, 2, 3
 NSCALARS = 15
+NPT_NSTATE = 13
+
+
+class OrcNpt(C.Structure):
+    _fields_ = [
+        ("T_start", C.c_double),
+        ("T_stop", C.c_double),
+        ("tau_T", C.c_double),
+        ("P_target", C.c_double),
+        ("tau_P", C.c_double),
+        ("drag", C.c_double),
+        ("mtchain", C.c_int),
+        ("mpchain", C.c_int),
+        ("couple", C.c_int * 3),
+        ("nfirst", C.c_int64),
+        ("nlast", C.c_int64),
+    ]
 
 
 class OrcDesc(C.Structure):
@@ -97,6 +114,9 @@ def lib():
         L.orc_set_lj_types.restype = C.c_int
         L.orc_set_lj_types.argtypes = [C.c_void_p, C.c_int, ip, ip, dp, dp, ip]
         L.orc_set_special.argtypes = [C.c_void_p, C.c_int, ip, ip, dp, dp]
+        L.orc_set_npt.restype = C.c_int
+        L.orc_set_npt.argtypes = [C.c_void_p, C.POINTER(OrcNpt)]
+        L.orc_npt_state.argtypes = [C.c_void_p, dp]
         _lib = L
     return _lib
 
@@ -216,6 +236,23 @@ class OracleSystem:
         ip = C.POINTER(C.c_int32)
         lib().orc_set_special(self._h, len(a), a.ctypes.data_as(ip), b.ctypes.data_as(ip),
                               _dp(sl), _dp(sc))
+
+    def set_npt(self, T, tau_T, P, tau_P, drag=0.0, mtchain=3, mpchain=3,
+                couple=(True, True, True), T_stop=-1.0, span=(0, 0)):
+        """MTK NPT in place of velocity Verlet + thermostat; P in eV/A^3."""
+        p = OrcNpt(float(T), float(T_stop), float(tau_T), float(P), float(tau_P),
+                   float(drag), int(mtchain), int(mpchain),
+                   (C.c_int * 3)(*[int(bool(c)) for c in couple]), int(span[0]),
+                   int(span[1]))
+        if lib().orc_set_npt(self._h, C.byref(p)) != 0:
+            raise ValueError("bad NPT parameters")
+
+    def npt_state(self) -> dict:
+        o = np.zeros(NPT_NSTATE)
+        lib().orc_npt_state(self._h, _dp(o))
+        return {"box": o[0:3].copy(), "conserved": float(o[3]), "eps_dot": o[4:7].copy(),
+                "eta_t": float(o[7]), "eta_t_dot": float(o[8]), "eta_b": float(o[9]),
+                "eta_b_dot": float(o[10]), "T_live": float(o[11]), "KE_global": float(o[12])}
 
     def build_list(self) -> int:
         return int(lib().orc_build_list(self._h))

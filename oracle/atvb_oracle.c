@@ -104,6 +104,7 @@ struct orc_sys {
     double* infl_H;  /* influence tables */
     double *infl_mx, *infl_my, *infl_mz, *infl_inv_msq;
     double inv_pi2_a2;
+    double infl_L[3]; /* box the influence tables were built for */
     /* per-type LJ tables (ntypes x ntypes) and per-atom types */
     int ntypes;
     double *t_sig6, *t_eps, *t_shift;
@@ -112,6 +113,15 @@ struct orc_sys {
     int32_t* sp_first; /* n + 1 */
     int32_t* sp_j;
     double *sp_lj, *sp_coul;
+    /* MTK NPT (nose_hoover_npt.cpp): parameters and extended state */
+    int npt_on;
+    orc_npt np;
+    int pdim;
+    double kT, T_live, W, tdrag, pdrag, KE_global, conserved;
+    double Qt[ORC_MAXCHAIN], Qb[ORC_MAXCHAIN];
+    double eta_t[ORC_MAXCHAIN], eta_t_dot[ORC_MAXCHAIN];
+    double eta_b[ORC_MAXCHAIN], eta_b_dot[ORC_MAXCHAIN];
+    double eps_dot[3];
 };
 
 orc_sys* orc_create(const orc_desc* d) {
@@ -909,17 +919,23 @@ static inline int pme_wrap(int g, int K) {
 
 /* pme.cpp:64-131 ensure_grid + pme_influence.h:112-155 tables */
 static void pme_setup(orc_sys* s) {
-    if (s->grid)
+    /* the tables depend on the cell: rebuilt whenever it changed (NPT) */
+    if (s->grid && s->infl_L[0] == s->d.L[0] && s->infl_L[1] == s->d.L[1] &&
+        s->infl_L[2] == s->d.L[2])
         return;
     for (int d = 0; d < 3; ++d)
         s->K[d] = s->d.pme_K[d];
     const long ntot = (long)s->K[0] * s->K[1] * s->K[2];
-    s->grid = (double*)calloc((size_t)(2 * ntot), sizeof(double));
-    s->infl_H = (double*)calloc((size_t)ntot, sizeof(double));
-    s->infl_mx = (double*)calloc((size_t)ntot, sizeof(double));
-    s->infl_my = (double*)calloc((size_t)ntot, sizeof(double));
-    s->infl_mz = (double*)calloc((size_t)ntot, sizeof(double));
-    s->infl_inv_msq = (double*)calloc((size_t)ntot, sizeof(double));
+    if (!s->grid) {
+        s->grid = (double*)calloc((size_t)(2 * ntot), sizeof(double));
+        s->infl_H = (double*)calloc((size_t)ntot, sizeof(double));
+        s->infl_mx = (double*)calloc((size_t)ntot, sizeof(double));
+        s->infl_my = (double*)calloc((size_t)ntot, sizeof(double));
+        s->infl_mz = (double*)calloc((size_t)ntot, sizeof(double));
+        s->infl_inv_msq = (double*)calloc((size_t)ntot, sizeof(double));
+    }
+    for (int d = 0; d < 3; ++d)
+        s->infl_L[d] = s->d.L[d];
     const int order = s->d.pme_order;
     double* bm[3];
     for (int d = 0; d < 3; ++d) {
@@ -1309,6 +1325,297 @@ static void langevin(orc_sys* s) {
     }
 }
 
+/* ------------------------------------------------------------------ */
+/* MTK NPT (src/cpu/dynamics/nose_hoover_npt.cpp)                      */
+/* ------------------------------------------------------------------ */
+
+/* |eps_dot dt| clamp of the box update (nose_hoover_npt.cpp:44) */
+#define ORC_EPS_DT_MAX 0.005
+
+/* (e^{2x} - 1) / (2x) with the Taylor branch near 0 (nose_hoover_npt.cpp:66-73) */
+static double npt_expm1c(double x) {
+    if (fabs(x) < 1e-6)
+        return 1.0 + x + (2.0 / 3.0) * x * x;
+    return expm1(2.0 * x) / (2.0 * x);
+}
+
+/* build(): chain, barostat masses, drag factors, equipartition KE
+ * (nose_hoover_npt.cpp:87-172) */
+int orc_set_npt(orc_sys* s, const orc_npt* p) {
+    if (p->mtchain < 1 || p->mtchain > ORC_MAXCHAIN || p->mpchain < 1 ||
+        p->mpchain > ORC_MAXCHAIN || !(p->tau_T > 0.0) || !(p->tau_P > 0.0) ||
+        !(p->T_start > 0.0))
+        return -1;
+    s->np = *p;
+    if (s->np.T_stop < 0.0)
+        s->np.T_stop = s->np.T_start;
+    s->npt_on = 1;
+    s->d.thermostat = ORC_THERMO_NPT;
+    s->d.need_virial = 1;
+    s->pdim = (p->couple[0] ? 1 : 0) + (p->couple[1] ? 1 : 0) + (p->couple[2] ? 1 : 0);
+    s->T_live = s->np.T_start;
+    s->kT = ORC_KB * s->np.T_start;
+    const double tT2 = p->tau_T * p->tau_T, tP2 = p->tau_P * p->tau_P;
+    for (int k = 0; k < ORC_MAXCHAIN; ++k) {
+        s->Qt[k] = s->kT * tT2;
+        s->Qb[k] = s->kT * tP2;
+        s->eta_t[k] = s->eta_t_dot[k] = s->eta_b[k] = s->eta_b_dot[k] = 0.0;
+    }
+    s->Qt[0] = (double)s->n_dof * s->kT * tT2;
+    s->W = ((double)s->n_dof + 3.0) * s->kT * tP2;
+    s->tdrag = 1.0 - p->drag * s->d.dt / p->tau_T;
+    s->pdrag = 1.0 - p->drag * s->d.dt / p->tau_P;
+    s->eps_dot[0] = s->eps_dot[1] = s->eps_dot[2] = 0.0;
+    s->KE_global = 0.5 * (double)s->n_dof * s->kT;
+    s->conserved = 0.0;
+    return 0;
+}
+
+void orc_npt_state(const orc_sys* s, double* out) {
+    out[0] = s->d.L[0];
+    out[1] = s->d.L[1];
+    out[2] = s->d.L[2];
+    out[3] = s->conserved;
+    out[4] = s->eps_dot[0];
+    out[5] = s->eps_dot[1];
+    out[6] = s->eps_dot[2];
+    out[7] = s->eta_t[0];
+    out[8] = s->eta_t_dot[0];
+    out[9] = s->eta_b[0];
+    out[10] = s->eta_b_dot[0];
+    out[11] = s->T_live;
+    out[12] = s->KE_global;
+}
+
+/* compute_temp_target (nose_hoover_npt.cpp:192-203) */
+static void npt_temp_target(orc_sys* s, int64_t step) {
+    double delta = 0.0;
+    if (s->np.nlast > s->np.nfirst) {
+        delta = (double)(step - s->np.nfirst) / (double)(s->np.nlast - s->np.nfirst);
+        delta = delta < 0.0 ? 0.0 : (delta > 1.0 ? 1.0 : delta);
+    }
+    s->T_live = s->np.T_start + delta * (s->np.T_stop - s->np.T_start);
+    s->kT = ORC_KB * s->T_live;
+}
+
+static double npt_ke(const orc_sys* s) { return kinetic(s); }
+
+/* compute_axis_KE (nose_hoover_npt.cpp:236-265) */
+static void npt_axis_ke(const orc_sys* s, double ke[3]) {
+    double kx = 0, ky = 0, kz = 0;
+#pragma omp parallel for reduction(+ : kx, ky, kz) schedule(static)
+    for (int i = 0; i < s->n; ++i) {
+        const double m = s->m[i];
+        kx += m * s->vx[i] * s->vx[i];
+        ky += m * s->vy[i] * s->vy[i];
+        kz += m * s->vz[i] * s->vz[i];
+    }
+    ke[0] = 0.5 * ORC_MVV2E * kx;
+    ke[1] = 0.5 * ORC_MVV2E * ky;
+    ke[2] = 0.5 * ORC_MVV2E * kz;
+}
+
+static void npt_scale_v(orc_sys* s, double sx, double sy, double sz) {
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < s->n; ++i) {
+        s->vx[i] *= sx;
+        s->vy[i] *= sy;
+        s->vz[i] *= sz;
+    }
+}
+
+/* nhc_atoms_half (nose_hoover_npt.cpp:267-340): backward sweep with drag at
+ * every link, velocity scale, chain positions, forward sweep without drag */
+static void npt_nhc_atoms(orc_sys* s, double hdt) {
+    const double qdt = 0.5 * hdt, edt = 0.5 * qdt;
+    const int M = s->np.mtchain;
+    for (int pass = 0; pass < 2; ++pass) {
+        for (int j = 0; j < M; ++j) {
+            const int k = pass == 0 ? M - 1 - j : j;
+            const double expfac = k < M - 1 ? exp(-s->eta_t_dot[k + 1] * edt) : 1.0;
+            const double G = k == 0 ? (2.0 * s->KE_global - s->n_dof * s->kT) / s->Qt[0]
+                                    : (s->Qt[k - 1] * s->eta_t_dot[k - 1] * s->eta_t_dot[k - 1] - s->kT) /
+                                          s->Qt[k];
+            s->eta_t_dot[k] *= expfac;
+            s->eta_t_dot[k] += G * qdt;
+            if (pass == 0)
+                s->eta_t_dot[k] *= s->tdrag;
+            s->eta_t_dot[k] *= expfac;
+        }
+        if (pass == 0) {
+            const double sc = exp(-s->eta_t_dot[0] * hdt);
+            npt_scale_v(s, sc, sc, sc);
+            s->KE_global *= sc * sc;
+            for (int k = 0; k < M; ++k)
+                s->eta_t[k] += s->eta_t_dot[k] * hdt;
+        }
+    }
+}
+
+/* nhc_baro_half (nose_hoover_npt.cpp:347-420) */
+static void npt_nhc_baro(orc_sys* s, double hdt) {
+    const double qdt = 0.5 * hdt, edt = 0.5 * qdt;
+    const int M = s->np.mpchain;
+    const double Wa = s->W / 3.0;
+    for (int pass = 0; pass < 2; ++pass) {
+        for (int j = 0; j < M; ++j) {
+            const int k = pass == 0 ? M - 1 - j : j;
+            const double expfac = k < M - 1 ? exp(-s->eta_b_dot[k + 1] * edt) : 1.0;
+            double G;
+            if (k == 0) {
+                double ke2 = 0.0;
+                for (int a = 0; a < 3; ++a)
+                    if (s->np.couple[a])
+                        ke2 += Wa * s->eps_dot[a] * s->eps_dot[a];
+                G = (ke2 - s->kT) / s->Qb[0];
+            } else {
+                G = (s->Qb[k - 1] * s->eta_b_dot[k - 1] * s->eta_b_dot[k - 1] - s->kT) / s->Qb[k];
+            }
+            s->eta_b_dot[k] *= expfac;
+            s->eta_b_dot[k] += G * qdt;
+            if (pass == 0)
+                s->eta_b_dot[k] *= s->pdrag;
+            s->eta_b_dot[k] *= expfac;
+        }
+        if (pass == 0) {
+            const double bs = exp(-s->eta_b_dot[0] * hdt);
+            for (int a = 0; a < 3; ++a)
+                if (s->np.couple[a])
+                    s->eps_dot[a] *= bs;
+            for (int k = 0; k < M; ++k)
+                s->eta_b[k] += s->eta_b_dot[k] * hdt;
+        }
+    }
+}
+
+/* update_eps_dot (nose_hoover_npt.cpp:422-560) with the isotropic couple()
+ * average when all three axes are barostatted */
+static void npt_update_eps(orc_sys* s, double hdt) {
+    const double V = s->d.L[0] * s->d.L[1] * s->d.L[2];
+    if (V <= 0.0)
+        return;
+    double ke[3];
+    npt_axis_ke(s, ke);
+    double diag[3] = {s->vir[0] + 2.0 * ke[0], s->vir[1] + 2.0 * ke[1],
+                      s->vir[2] + 2.0 * ke[2]};
+    if (s->pdim == 3) {
+        const double ave = (1.0 / 3.0) * (diag[0] + diag[1] + diag[2]);
+        diag[0] = diag[1] = diag[2] = ave;
+    }
+    double mtk_ke = 0.0;
+    for (int a = 0; a < 3; ++a)
+        if (s->np.couple[a])
+            mtk_ke += ke[a];
+    const int n_atoms = (s->n_dof + 3) / 3;
+    const double mtk = s->pdim > 0 ? 6.0 * mtk_ke / ((double)s->pdim * n_atoms) : 0.0;
+    for (int a = 0; a < 3; ++a) {
+        if (!s->np.couple[a])
+            continue;
+        const double Pa = diag[a] / V;
+        const double G = (3.0 * V * (Pa - s->np.P_target) + mtk) / s->W;
+        s->eps_dot[a] += G * hdt;
+    }
+}
+
+/* scale_v_by_baro (nose_hoover_npt.cpp:580-630) */
+static void npt_scale_baro(orc_sys* s, double hdt) {
+    double sum = 0.0;
+    for (int a = 0; a < 3; ++a)
+        if (s->np.couple[a])
+            sum += s->eps_dot[a];
+    const int n_atoms = (s->n_dof + 3) / 3;
+    const double mtk2 = s->pdim > 0 ? sum / ((double)s->pdim * n_atoms) : 0.0;
+    const double sx = exp(-(s->eps_dot[0] + mtk2) * hdt);
+    const double sy = exp(-(s->eps_dot[1] + mtk2) * hdt);
+    const double sz = exp(-(s->eps_dot[2] + mtk2) * hdt);
+    npt_scale_v(s, sx, sy, sz);
+    if (sx == sy && sy == sz)
+        s->KE_global *= sx * sx;
+    else
+        s->KE_global = npt_ke(s);
+}
+
+static void npt_kick(orc_sys* s) {
+    const double dtf = 0.5 * s->d.dt * ORC_FTM2V;
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < s->n; ++i) {
+        const double dtfm = dtf / s->m[i];
+        s->vx[i] += dtfm * s->fx[i];
+        s->vy[i] += dtfm * s->fy[i];
+        s->vz[i] += dtfm * s->fz[i];
+    }
+}
+
+/* propagate_x_and_box (nose_hoover_npt.cpp:650-760): closed-form drift,
+ * box scaled per axis, wrap */
+static void npt_propagate(orc_sys* s) {
+    const double dt = s->d.dt;
+    double a[3], dr[3];
+    for (int d = 0; d < 3; ++d) {
+        double e = s->eps_dot[d] * dt;
+        e = e < -ORC_EPS_DT_MAX ? -ORC_EPS_DT_MAX : (e > ORC_EPS_DT_MAX ? ORC_EPS_DT_MAX : e);
+        a[d] = exp(e);
+        dr[d] = npt_expm1c(e * 0.5);
+    }
+    for (int d = 0; d < 3; ++d)
+        s->d.L[d] *= a[d];
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < s->n; ++i) {
+        s->x[i] = wrap_coord(s->x[i] * a[0] + s->vx[i] * dt * dr[0], s->d.L[0]);
+        s->y[i] = wrap_coord(s->y[i] * a[1] + s->vy[i] * dt * dr[1], s->d.L[1]);
+        s->z[i] = wrap_coord(s->z[i] * a[2] + s->vz[i] * dt * dr[2], s->d.L[2]);
+    }
+}
+
+/* extended_hamiltonian (nose_hoover_npt.cpp:770-805) */
+static double npt_hamiltonian(const orc_sys* s) {
+    double H = s->ke + (s->e_lj + s->e_coul + s->e_recip + s->e_const);
+    const double Wa = s->W / 3.0;
+    for (int a = 0; a < 3; ++a)
+        if (s->np.couple[a])
+            H += 0.5 * Wa * s->eps_dot[a] * s->eps_dot[a];
+    for (int k = 0; k < s->np.mtchain; ++k)
+        H += 0.5 * s->Qt[k] * s->eta_t_dot[k] * s->eta_t_dot[k];
+    for (int k = 0; k < s->np.mpchain; ++k)
+        H += 0.5 * s->Qb[k] * s->eta_b_dot[k] * s->eta_b_dot[k];
+    H += (double)s->n_dof * s->kT * s->eta_t[0];
+    for (int k = 1; k < s->np.mtchain; ++k)
+        H += s->kT * s->eta_t[k];
+    for (int k = 0; k < s->np.mpchain; ++k)
+        H += s->kT * s->eta_b[k];
+    H += s->np.P_target * s->d.L[0] * s->d.L[1] * s->d.L[2];
+    return H;
+}
+
+/* One MTK step (nose_hoover_npt.cpp:812-885 launch: P1-P6 at
+ * initial_integrate, P7 at final_integrate, P8-P11 at end_of_step).  The
+ * list is rebuilt every step: the cell changes every step. */
+static void npt_step(orc_sys* s) {
+    const double hdt = 0.5 * s->d.dt;
+    npt_temp_target(s, s->step);
+    const double tT2 = s->np.tau_T * s->np.tau_T;
+    s->Qt[0] = (double)s->n_dof * s->kT * tT2;
+    for (int k = 1; k < s->np.mtchain; ++k)
+        s->Qt[k] = s->kT * tT2;
+    npt_nhc_baro(s, hdt);   /* P1 */
+    npt_nhc_atoms(s, hdt);  /* P2 */
+    npt_update_eps(s, hdt); /* P3: the virial of the last force evaluation */
+    npt_scale_baro(s, hdt); /* P4 */
+    npt_kick(s);            /* P5 */
+    npt_propagate(s);       /* P6 */
+    orc_build_list(s);
+    ++s->rebuilds;
+    orc_compute_forces(s);
+    npt_kick(s); /* P7 */
+    s->KE_global = npt_ke(s);
+    npt_scale_baro(s, hdt); /* P8 */
+    npt_update_eps(s, hdt); /* P9 */
+    npt_nhc_atoms(s, hdt);  /* P10 */
+    npt_nhc_baro(s, hdt);   /* P11 */
+    s->ke = s->KE_global;
+    s->conserved = npt_hamiltonian(s);
+}
+
 /* runtime.cpp:452-501 step order with VelocityVerlet (velocity_verlet.cpp)
  * at order 0 and the thermostat at +100 in both integrate phases. */
 int orc_run(orc_sys* s, int n_steps, double* hist) {
@@ -1319,6 +1626,18 @@ int orc_run(orc_sys* s, int n_steps, double* hist) {
     int rebuilds = 0;
     if (s->npairs == 0 && s->nbr == NULL)
         orc_build_list(s);
+    if (s->npt_on) {
+        for (int st = 0; st < n_steps; ++st) {
+            npt_step(s);
+            ++rebuilds;
+            if (hist) {
+                hist[2 * st] = s->e_lj + s->e_coul + s->e_recip + s->e_const;
+                hist[2 * st + 1] = s->ke;
+            }
+            s->step++;
+        }
+        return rebuilds;
+    }
     for (int st = 0; st < n_steps; ++st) {
         /* initial_integrate */
 #pragma omp parallel for schedule(static)

@@ -23,7 +23,20 @@ extern "C" {
 #define ORC_QQR2E 14.399645
 #define ORC_PI 3.14159265358979323846
 
-enum { ORC_THERMO_NONE = 0, ORC_THERMO_NH = 1, ORC_THERMO_LANGEVIN = 2 };
+enum { ORC_THERMO_NONE = 0, ORC_THERMO_NH = 1, ORC_THERMO_LANGEVIN = 2, ORC_THERMO_NPT = 3 };
+
+#define ORC_MAXCHAIN 10
+
+/* MTK NPT parameters: NoseHooverNPT(T_target, tau_T, P_target, tau_P, dt,
+ * drag, mtchain, mpchain, couple_axis, T_stop) + set_run_span(nfirst, nlast)
+ * (include/atomiverse/cpu/dynamics/nose_hoover_npt.h:180-215).  P_target in
+ * eV/A^3 (positive compressive), T_stop < 0: no ramp. */
+typedef struct orc_npt {
+    double T_start, T_stop, tau_T, P_target, tau_P, drag;
+    int mtchain, mpchain;
+    int couple[3];
+    int64_t nfirst, nlast;
+} orc_npt;
 
 typedef struct orc_desc {
     int n;                 /* atoms */
@@ -104,6 +117,16 @@ int orc_set_lj_types(orc_sys* s, int ncoef, const int32_t* ti, const int32_t* tj
  * subtracts (1 - f) k_e q_i q_j / r, the share the reciprocal sum added). */
 void orc_set_special(orc_sys* s, int npairs, const int32_t* pi, const int32_t* pj,
                      const double* s_lj, const double* s_coul);
+
+/* Switch the system's integrator to MTK NPT (replaces velocity Verlet and
+ * the thermostat; nose_hoover_npt.cpp:87-172 build).  Returns 0, or -1 on a
+ * bad parameter (chain length outside [1, ORC_MAXCHAIN], tau <= 0). */
+int orc_set_npt(orc_sys* s, const orc_npt* p);
+/* NPT state: [0..2] box edges, [3] conserved extended Hamiltonian,
+ * [4..6] eps_dot, [7] eta_t[0], [8] eta_t_dot[0], [9] eta_b[0],
+ * [10] eta_b_dot[0], [11] live temperature setpoint, [12] KE_global. */
+#define ORC_NPT_NSTATE 13
+void orc_npt_state(const orc_sys* s, double* out);
 
 /* ---- standalone pieces used by the known-answer tests ---- */
 void orc_bspline(double frac, int n, double* theta, double* dtheta);
