@@ -119,8 +119,28 @@ def scalars_dict(s: Scalars) -> dict:
         "energy_const": s.energy_const, "kinetic": s.kinetic, "conserved": s.conserved,
         "stress": np.array(list(s.stress)), "nh_xi": s.nh_xi, "step": s.step,
         "rebuilds": s.rebuilds, "max_neighbors": s.max_neighbors, "status": s.status,
-        "list_pairs": s.list_pairs,
+        "list_pairs": s.list_pairs, "box": np.array(list(s.box)), "pressure": s.pressure,
     }
+
+
+def _npt_desc(npt) -> "_abi.NptDesc":
+    """NoseHooverNPT (or a dict of its fields) -> atvb_npt_desc."""
+    if isinstance(npt, dict):
+        npt = NoseHooverNPT(**npt)
+    d = _abi.NptDesc()
+    d.T_start = float(npt.T_target)
+    d.T_stop = float(npt.T_stop)
+    d.tau_T = float(npt.tau_T)
+    d.P_target = float(npt.P_target)
+    d.tau_P = float(npt.tau_P)
+    d.drag = float(npt.drag)
+    d.mtchain = int(npt.mtchain)
+    d.mpchain = int(npt.mpchain)
+    for a in range(3):
+        d.couple[a] = 1 if npt.couple_axis[a] else 0
+    d.nfirst = int(npt.nfirst)
+    d.nlast = int(npt.nlast)
+    return d
 
 
 class Context:
@@ -147,11 +167,12 @@ class System:
     """One MD system on the device (cuda::md::MD + its components)."""
 
     def __init__(self, ctx: Context, desc: SystemDesc | dict, frame: dict | None = None,
-                 lj_types=None, special_bonds=None):
+                 lj_types=None, special_bonds=None, npt=None):
         """lj_types: [(type_i, type_j, epsilon, sigma), ...] (PairLJCut's
         per-type form; per-atom types in frame["type"]); special_bonds:
-        dict(lj=(s12, s13, s14), coul=(s12, s13, s14), bonds=[(tag_a, tag_b), ...]).
-        Both are applied before the frame is uploaded."""
+        dict(lj=(s12, s13, s14), coul=(s12, s13, s14), bonds=[(tag_a, tag_b), ...]);
+        npt: a NoseHooverNPT (MTK NPT in place of velocity Verlet, desc NVE).
+        All are applied before the frame is uploaded."""
         self.ctx = ctx
         self.lib = ctx.lib
         if isinstance(desc, dict):
@@ -167,6 +188,8 @@ class System:
         if special_bonds is not None:
             args, keep = _special_args(special_bonds)
             check(self.lib.atvb_system_set_special_bonds(self._h, *args))
+        if npt is not None:
+            check(self.lib.atvb_system_set_npt(self._h, C.byref(_npt_desc(npt))))
         if frame is not None:
             self.upload(frame)
 
@@ -264,7 +287,7 @@ class Batch:
 
     def __init__(self, ctx: Context, items: list):
         """items: (desc, frame) or (desc, frame, options) with options the
-        System keywords lj_types / special_bonds."""
+        System keywords lj_types / special_bonds / npt."""
         self.ctx = ctx
         self.lib = ctx.lib
         descs = [make_desc(**it[0]) if isinstance(it[0], dict) else it[0] for it in items]
@@ -281,6 +304,8 @@ class Batch:
             if opts.get("special_bonds") is not None:
                 args, keep = _special_args(opts["special_bonds"])
                 check(self.lib.atvb_batch_set_special_bonds(self._h, k, *args))
+            if opts.get("npt") is not None:
+                check(self.lib.atvb_batch_set_npt(self._h, k, C.byref(_npt_desc(opts["npt"]))))
         for k, it in enumerate(items):
             if it[1] is not None:
                 self.upload(k, it[1])
@@ -467,6 +492,30 @@ class FixLangevin:
 
 
 @dataclass
+class NoseHooverNPT:
+    """NoseHooverNPT(T_target, tau_T, P_target, tau_P, dt, drag=0, mtchain=3,
+    mpchain=3, couple_axis=(True, True, True), T_stop=-1) + set_run_span
+    (cuda/dynamics/nose_hoover_npt.cuh:60-70): MTK NPT, P_target in eV/A^3.
+    An integrator: it replaces VelocityVerlet and the thermostat."""
+    T_target: float
+    tau_T: float
+    P_target: float
+    tau_P: float
+    dt: float
+    drag: float = 0.0
+    mtchain: int = 3
+    mpchain: int = 3
+    couple_axis: tuple = (True, True, True)
+    T_stop: float = -1.0
+    nfirst: int = 0
+    nlast: int = 0
+
+    def set_run_span(self, nfirst: int, nlast: int):
+        self.nfirst, self.nlast = int(nfirst), int(nlast)
+        return self
+
+
+@dataclass
 class MD:
     """cuda::md::MD: categorical setters, build(), run(frame, n)
     (include/atomiverse/cuda/dynamics/md.cuh:118-385)."""
@@ -487,7 +536,7 @@ class MD:
         self._evaluators.append(ev)
         return self
 
-    def set_integrator(self, integ: VelocityVerlet):
+    def set_integrator(self, integ):
         if self._integrator is not None and self._integrator != integ:
             raise ValueError("set_integrator already configured")
         self._integrator = integ
@@ -542,5 +591,9 @@ class MD:
             if self.ctx is None:
                 self.ctx = Context(0)
             n = len(frame["x"])
-            self._system = System(self.ctx, self.desc(n, box if box is not None else frame["box"]))
-        return self._system.run(frame, n_steps)
+            npt = self._integrator if isinstance(self._integrator, NoseHooverNPT) else None
+            self._system = System(self.ctx, self.desc(n, box if box is not None else frame["box"]),
+                                  npt=npt)
+        sc = self._system.run(frame, n_steps)
+        frame["box"] = tuple(sc["box"])   # the cell moves under NPT
+        return sc

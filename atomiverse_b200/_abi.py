@@ -87,6 +87,25 @@ class Scalars(C.Structure):
         ("max_neighbors", C.c_int32),
         ("status", C.c_int32),
         ("list_pairs", C.c_int64),
+        ("box", C.c_double * 3),
+        ("pressure", C.c_double),
+    ]
+
+
+class NptDesc(C.Structure):
+    """atvb_npt_desc: md::NoseHooverNPT parameters."""
+    _fields_ = [
+        ("T_start", C.c_double),
+        ("T_stop", C.c_double),
+        ("tau_T", C.c_double),
+        ("P_target", C.c_double),
+        ("tau_P", C.c_double),
+        ("drag", C.c_double),
+        ("mtchain", C.c_int32),
+        ("mpchain", C.c_int32),
+        ("couple", C.c_int32 * 3),
+        ("nfirst", C.c_int64),
+        ("nlast", C.c_int64),
     ]
 
 
@@ -145,6 +164,8 @@ SIGNATURES = {
     "atvb_batch_set_special_bonds": (C.c_int, [_vp, C.c_int32, C.POINTER(C.c_double),
                                                C.POINTER(C.c_double), C.c_int64,
                                                C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "atvb_system_set_npt": (C.c_int, [_vp, C.POINTER(NptDesc)]),
+    "atvb_batch_set_npt": (C.c_int, [_vp, C.c_int32, C.POINTER(NptDesc)]),
     "atvb_system_set_lj_types": (C.c_int, [_vp, C.c_int32, C.POINTER(C.c_int32),
                                            C.POINTER(C.c_int32), C.POINTER(C.c_double),
                                            C.POINTER(C.c_double)]),

@@ -23,7 +23,13 @@ constexpr double kPi = 3.14159265358979323846;
 constexpr double kEwaldF = 1.1283791670955126; // 2/sqrt(pi)
 
 enum Precision : int { kFP64 = 0, kMixed = 1 };
-enum Thermostat : int { kNVE = 0, kNoseHoover = 1, kLangevin = 2 };
+enum Thermostat : int { kNVE = 0, kNoseHoover = 1, kLangevin = 2, kNPT = 3 };
+
+// longest Nose-Hoover chain of the MTK NPT integrator
+constexpr int kMaxChain = 10;
+
+// SysState::status bits
+constexpr int kStatusBoxRange = 1; // NPT cell left the range its grid was planned for
 
 // Fixed-point scales.  Energies/virials/KE are accumulated per system as
 // 64-bit integers in units of 2^-32 eV (range +-2.1e9 eV), so their sums are
@@ -40,7 +46,8 @@ enum Acc : int {
     kAccVir = 3, // 6 entries: xx yy zz xy xz yz
     kAccKEA = 9,
     kAccKEB = 10,
-    kAccCount = 12
+    kAccKEX = 12, // 3 entries: per-axis kinetic energy (NPT)
+    kAccCount = 15
 };
 
 struct SysState {
@@ -61,6 +68,23 @@ struct SysState {
     unsigned long long list_entries; // row entries of the last build (2 x pairs)
     int nearq_n;       // mixed build: pairs queued this step for an exact LJ cutoff test
     int nearq_lost;    // pairs that did not fit the queue (decided in FP32)
+    double box[3];     // current cell edges
+    double pressure;   // (2 KE + trace W) / (3 V) [eV/A^3]
+    // MTK NPT extended state (nose_hoover_npt.cpp): chains, strain rates and
+    // the factors of the next initial half step, prepared at the end of the
+    // previous step by k_sys_b (or by k_npt_prep before the first step)
+    double eta_t[kMaxChain], eta_t_dot[kMaxChain];
+    double eta_b[kMaxChain], eta_b_dot[kMaxChain];
+    double eps_dot[3];
+    double ke_global, kT, T_live, Qt0, Qt1;
+    double vs[3];      // per-axis velocity scale applied by the next initial kick
+    double vs_out[3];  // the part of vs that belongs to the finished step
+    double npt_a[3], npt_drift[3]; // exp(eps_dot dt) and the drift factor
+    double Lnext[3];   // cell after the next drift
+    double fixn_scale[3], fixn64_scale[3]; // 2^32 / Lnext, 2^64 / Lnext
+    double Lb[3], Lb_inv[3]; // cell at the last neighbour build
+    double ub[3];      // Lb / Lnext: next positions mapped into the build cell
+    double disp_thr2;  // squared displacement that forces a rebuild
 };
 
 struct SysParams {
@@ -84,6 +108,8 @@ struct SysParams {
     int lframe_ok;
     float fband_lo, fband_hi;
     double skin_half2; // (skin/2)^2
+    double rlist;      // cutoff + skin
+    double nl_cut;     // NeighborList cutoff (the largest interaction cutoff)
     int nl_every, nl_delay, nl_check;
     int nc[3], ncell;
     double cs_inv[3];
@@ -121,6 +147,8 @@ struct SysParams {
     double pme_escale; // k_e / (2 pi V)
     double pme_alpha2_pi2; // pi^2 / alpha^2
     double grid_scale, grid_scale_inv; // fixed-point charge scale
+    const double* bmod;    // B-spline moduli |b(m)|^2 per axis: K0 + K1 + K2
+    double pme_alpha, pme_eself, pme_qsum2; // e_const = eself - k_e pi qsum2 / (2 V alpha^2)
     // integrator / thermostat
     double dt, dtf; // dtf = dt/2 * ftm2v
     int thermostat;
@@ -129,6 +157,13 @@ struct SysParams {
     unsigned int seed;
     int need_virial;
     double e_const; // PME self + net-charge energy
+    // MTK NPT (thermostat == kNPT; nose_hoover_npt.cpp)
+    double npt_T0, npt_T1, npt_tauT, npt_P, npt_tdrag, npt_pdrag, npt_W, npt_Qb;
+    int npt_mt, npt_mp, npt_pdim, n_dof;
+    int npt_couple[3];
+    long long npt_nfirst, npt_nlast;
+    double npt_Lmin[3]; // smallest cell the neighbour grid is valid for
+    double npt_cut;     // largest interaction cutoff (rebuild rule)
     // per-atom master state (original order)
     double *x, *y, *z, *vx, *vy, *vz, *mass, *q;
     long long* tag;
@@ -144,7 +179,6 @@ struct SysParams {
     unsigned long long* grid_fix;
     void* grid_real;  // double or float, K0*K1*K2
     void* grid_cplx;  // double2 or float2, K0*K1*Kh
-    double* infl;     // H(m) on the half-complex grid
     // staging for upload / download (original order)
     double *sx, *sy, *sz;
     // scalars

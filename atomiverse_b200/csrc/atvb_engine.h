@@ -33,6 +33,7 @@ size_t estimate_bytes(const atvb_system_desc& d);
 
 struct Geometry {
     double L[3];
+    double Lmin[3]; // smallest cell the bins and stencil are valid for
     double skin, rlist;
     int nc[3];
     double cs[3];
@@ -40,7 +41,7 @@ struct Geometry {
     int alias[3];
     std::vector<int4> cols;
 };
-Geometry make_geometry(const atvb_system_desc& d);
+Geometry make_geometry(const atvb_system_desc& d, double shrink = 0.0);
 
 // Stream-ordered device memory from an engine's own pool.  Frees go back to
 // the pool in stream order (no device-wide synchronisation, no unmapping),
@@ -70,7 +71,6 @@ class Slot {
     int max_row = 0;
     int lanes = 4;  // pair-kernel lanes per atom for this system
     double mean_row = 0.0;
-    std::vector<double> infl_host;
     // per-type LJ and special bonds: configured before the first upload
     int ntypes = 0;          // > 0: per-type LJ (table built at upload)
     std::vector<int> lj_ti, lj_tj;
@@ -82,6 +82,9 @@ class Slot {
     void build_specials(const std::vector<long long>& tags, cudaStream_t stream);
 
     void* dalloc(size_t b);
+    void free_alloc(void* p);
+    void replan_cells(double shrink);
+    bool npt = false; // MTK NPT configured (atvb_system_set_npt)
 
   private:
     DevMem mem_;
@@ -110,6 +113,7 @@ class Engine {
                       const double* eps, const double* sigma);
     void set_special_bonds(int id, const double lj[3], const double coul[3],
                            int64_t nbonds, const int64_t* a, const int64_t* b);
+    void set_npt(int id, const atvb_npt_desc& p);
     void compute_forces();
     void compute_forces_one(int id);
     void step(int n);

@@ -64,6 +64,7 @@ void launch_force_rebuild(const LaunchCfg& lc, cudaStream_t s);
 void launch_state_in(const LaunchCfg& lc, cudaStream_t s);
 void launch_wrap_in(const LaunchCfg& lc, cudaStream_t s);
 void launch_state_out(const LaunchCfg& lc, int what, cudaStream_t s);
+void launch_npt_prep(const LaunchCfg& lc, cudaStream_t s);
 void launch_kinetic(const LaunchCfg& lc, cudaStream_t s);
 
 } // namespace atvb

@@ -192,6 +192,14 @@ int atvb_system_pairs(atvb_system* sys, int32_t* pi, int32_t* pj,
     });
 }
 
+int atvb_system_set_npt(atvb_system* sys, const atvb_npt_desc* npt) {
+    return guard([&] {
+        need(sys, "sys");
+        need(npt, "npt");
+        sys->eng->set_npt(sys->id, *npt);
+    });
+}
+
 int atvb_system_set_lj_types(atvb_system* sys, int32_t ncoef, const int32_t* type_i,
                              const int32_t* type_j, const double* epsilon,
                              const double* sigma) {
@@ -337,6 +345,16 @@ int atvb_batch_set_lj_types(atvb_batch* b, int32_t index, int32_t ncoef,
         if (index < 0 || index >= (int)b->ids.size())
             throw Error(ATVB_ERR_NOTFOUND, "no system " + std::to_string(index) + " in batch");
         b->eng->set_lj_types(b->ids[index], ncoef, type_i, type_j, epsilon, sigma);
+    });
+}
+
+int atvb_batch_set_npt(atvb_batch* b, int32_t index, const atvb_npt_desc* npt) {
+    return guard([&] {
+        need(b, "batch");
+        need(npt, "npt");
+        if (index < 0 || index >= (int)b->ids.size())
+            throw Error(ATVB_ERR_NOTFOUND, "no system " + std::to_string(index) + " in batch");
+        b->eng->set_npt(b->ids[index], *npt);
     });
 }
 

@@ -23,6 +23,7 @@
 #include "atvb.h"
 #include "atvb_common.cuh"
 #include "atvb_engine.h"
+#include "box.cuh"
 #include "erfcx_coef.h"
 #include "atvb_kernels.cuh"
 
@@ -111,7 +112,10 @@ static std::vector<double> spline_moduli(int K, int n) {
 
 // ------------------------------------------------------------ geometry
 
-Geometry make_geometry(const atvb_system_desc& d) {
+// `shrink` > 0 (MTK NPT): plan the bins and stencil for every cell down to
+// L (1 - shrink) per axis, so that the grid stays valid while the cell
+// breathes; the bins then grow with the cell (bin count fixed).
+Geometry make_geometry(const atvb_system_desc& d, double shrink) {
     Geometry g;
     for (int r = 0; r < 3; ++r)
         for (int c = 0; c < 3; ++c)
@@ -136,13 +140,18 @@ Geometry make_geometry(const atvb_system_desc& d) {
             throw Error(ATVB_ERR_INVALID,
                         "box edge must exceed 2*(cutoff+skin) so that each "
                         "pair has one minimum image");
+    double Lp[3];
+    for (int k = 0; k < 3; ++k) {
+        Lp[k] = g.L[k] * (1.0 - shrink);
+        g.Lmin[k] = Lp[k];
+    }
     // Bins of at least a third of the list radius (reach 3), finer than the
     // reference's half-reach bins (cell_list.cpp:112-121, reach :186-191):
     // fewer candidates per atom.  The pair set does not depend on the bins.
     for (int k = 0; k < 3; ++k) {
-        int c = (int)std::floor(g.L[k] / (g.rlist / 3.0));
+        int c = (int)std::floor(Lp[k] / (g.rlist / 3.0));
         g.nc[k] = c < 1 ? 1 : c;
-        g.cs[k] = g.L[k] / g.nc[k];
+        g.cs[k] = Lp[k] / g.nc[k];
         int r = (int)std::ceil(g.rlist / g.cs[k] - 1e-12);
         g.reach[k] = r < 1 ? 1 : r;
         g.alias[k] = g.nc[k] < 2 * g.reach[k] + 1;
@@ -257,6 +266,39 @@ void* Slot::dalloc(size_t b) {
     return p;
 }
 
+void Slot::free_alloc(void* p) {
+    auto it = std::find(allocs.begin(), allocs.end(), p);
+    if (it != allocs.end()) {
+        allocs.erase(it);
+        mem_.free(p);
+    }
+}
+
+// Re-plan the bins and stencil for cells down to L (1 - shrink) per axis
+// (MTK NPT): new bin arrays and columns, box-dependent fields recomputed.
+void Slot::replan_cells(double shrink) {
+    cudaStream_t stream = mem_.stream;
+    geo = make_geometry(desc, shrink);
+    free_alloc(hp.cell_count);
+    free_alloc(hp.cell_start);
+    free_alloc(hp.cols);
+    for (int k = 0; k < 3; ++k) {
+        hp.nc[k] = geo.nc[k];
+        hp.alias[k] = geo.alias[k];
+        hp.npt_Lmin[k] = geo.Lmin[k];
+    }
+    hp.ncell = geo.nc[0] * geo.nc[1] * geo.nc[2];
+    hp.ncol = (int)geo.cols.size();
+    hp.cell_count = (int*)dalloc(sizeof(int) * hp.ncell);
+    hp.cell_start = (int*)dalloc(sizeof(int) * (hp.ncell + 1));
+    CK(cudaMemsetAsync(hp.cell_count, 0, sizeof(int) * hp.ncell, stream));
+    hp.cols = (int4*)dalloc(sizeof(int4) * geo.cols.size());
+    CK(cudaMemcpyAsync(hp.cols, geo.cols.data(), sizeof(int4) * geo.cols.size(),
+                       cudaMemcpyHostToDevice, stream));
+    apply_box(hp, geo.L, false);
+    CK(cudaStreamSynchronize(stream));
+}
+
 Slot::~Slot() {
     for (void* p : allocs)
         mem_.free(p);
@@ -284,44 +326,14 @@ Slot::Slot(const atvb_system_desc& d, const DevMem& mem) : desc(d), mem_(mem) {
     if (d.precision != ATVB_FP64 && d.precision != ATVB_MIXED)
         throw Error(ATVB_ERR_INVALID, "unknown precision");
     for (int k = 0; k < 3; ++k) {
-        hp.L[k] = geo.L[k];
-        hp.invL[k] = 1.0 / geo.L[k];
-        hp.halfL[k] = 0.5 * geo.L[k];
-        hp.Lf_fix[k] = (float)(geo.L[k] / 4294967296.0);
-        hp.fix_scale[k] = 4294967296.0 / geo.L[k];
-        hp.fix64_scale[k] = 18446744073709551616.0 / geo.L[k];
-        hp.Lfix64[k] = geo.L[k] / 18446744073709551616.0;
         hp.nc[k] = geo.nc[k];
-        hp.cs_inv[k] = 1.0 / geo.cs[k];
         hp.alias[k] = geo.alias[k];
+        hp.npt_Lmin[k] = geo.Lmin[k];
     }
     hp.ncell = geo.nc[0] * geo.nc[1] * geo.nc[2];
+    hp.rlist = geo.rlist;
     hp.rlist2 = geo.rlist * geo.rlist;
-    {
-        // |r2_fp32 - r2_exact| <= 5.4e-7 r2 (three FP32 roundings of each
-        // difference, three of the sum) + 3.6 r q (fixed-point quantum q =
-        // L / 2^32 on both atoms); the band doubles both terms
-        const double q = std::max(geo.L[0], std::max(geo.L[1], geo.L[2])) / 4294967296.0;
-        const double band = 2e-6 * hp.rlist2 + 8.0 * geo.rlist * q + 1e-12;
-        hp.lband_lo = std::nextafter((float)(hp.rlist2 - band), 0.0f);
-        hp.lband_hi = std::nextafter((float)(hp.rlist2 + band), 3.0e38f);
-        // cell-local frame: coordinates up to R = rlist + 2 cell diagonals
-        // from the origin, each carrying <= 3 FP32 roundings (2^-24 R) plus
-        // the fixed-point quantum; the difference one more rounding
-        const double cdiag = std::sqrt(geo.cs[0] * geo.cs[0] + geo.cs[1] * geo.cs[1] +
-                                       geo.cs[2] * geo.cs[2]);
-        const double R = geo.rlist + 2.0 * cdiag;
-        const double u = 1.0 / 16777216.0;
-        const double ec = 3.0 * u * R + 2.0 * q;
-        const double ed = 2.0 * ec + u * geo.rlist;
-        const double fband = 2.0 * (2.0 * std::sqrt(3.0) * geo.rlist * ed + 3.0 * u * hp.rlist2) + 1e-12;
-        hp.fband_lo = std::nextafter((float)(hp.rlist2 - fband), 0.0f);
-        hp.fband_hi = std::nextafter((float)(hp.rlist2 + fband), 3.0e38f);
-        hp.lframe_ok = 1;
-        for (int k = 0; k < 3; ++k)
-            if (!(0.5 * geo.L[k] > R + 1e-9))
-                hp.lframe_ok = 0;
-    }
+    hp.nl_cut = d.nl_cutoff;
     hp.skin_half2 = 0.25 * geo.skin * geo.skin;
     hp.nl_every = d.nl_every < 1 ? 1 : d.nl_every;
     hp.nl_delay = d.nl_delay < 0 ? 0 : d.nl_delay;
@@ -344,27 +356,18 @@ Slot::Slot(const atvb_system_desc& d, const DevMem& mem) : desc(d), mem_(mem) {
         const double r6inv = r2inv * r2inv * r2inv * hp.lj_sig6;
         hp.lj_shift = 4.0 * d.lj_epsilon * (r6inv * r6inv - r6inv);
     }
-    {
-        // |r2_fp32 - r2_fp64| <= 10 2^-24 r2 (conversion, scale, product,
-        // squares and sums) + 2 sqrt(3) r q (32-bit fixed-point quantum q on
-        // both atoms); the band doubles it
-        const double q = std::max(geo.L[0], std::max(geo.L[1], geo.L[2])) / 4294967296.0;
-        auto band = [&](double rc) {
-            return 2.0 * (10.0 / 16777216.0 * rc * rc + 2.0 * std::sqrt(3.0) * rc * q);
-        };
-        hp.mix_band_lj = d.lj_enabled ? band(d.lj_cutoff) : 0.0;
-        // a pair that FP32 rounding moves across the LJ cutoff changes the
-        // forces by the force jump there (the energy is shifted, the force
-        // is not); below 1e-5 eV/A that is negligible and the settling is
-        // off (e.g. LJ cut at 4 sigma under Coulomb: 2.5e-6 eV/A)
-        if (d.lj_enabled) {
-            const double sr2 = d.lj_sigma * d.lj_sigma / (d.lj_cutoff * d.lj_cutoff);
-            const double sr6 = sr2 * sr2 * sr2;
-            const double jump = std::fabs(24.0 * d.lj_epsilon / d.lj_cutoff * (2.0 * sr6 * sr6 - sr6));
-            if (jump < 1e-5)
-                hp.mix_band_lj = 0.0;
-        }
-        hp.mix_band_c = d.coul_enabled ? band(d.coul_cutoff) : 0.0;
+    // mixed build: settle pairs near the LJ cutoff (band set by apply_box).
+    // A pair that FP32 rounding moves across the LJ cutoff changes the
+    // forces by the force jump there (the energy is shifted, the force is
+    // not); below 1e-5 eV/A that is negligible and the settling is off
+    // (e.g. LJ cut at 4 sigma under Coulomb: 2.5e-6 eV/A)
+    hp.mix_band_lj = d.lj_enabled ? 1.0 : 0.0;
+    if (d.lj_enabled) {
+        const double sr2 = d.lj_sigma * d.lj_sigma / (d.lj_cutoff * d.lj_cutoff);
+        const double sr6 = sr2 * sr2 * sr2;
+        const double jump = std::fabs(24.0 * d.lj_epsilon / d.lj_cutoff * (2.0 * sr6 * sr6 - sr6));
+        if (jump < 1e-5)
+            hp.mix_band_lj = 0.0;
     }
     hp.has_coul = d.coul_enabled ? 1 : 0;
     if (hp.has_coul) {
@@ -464,9 +467,7 @@ Slot::Slot(const atvb_system_desc& d, const DevMem& mem) : desc(d), mem_(mem) {
         for (int k = 0; k < 3; ++k)
             hp.K[k] = pme_K(d, geo, k);
         hp.Kh = hp.K[2] / 2 + 1;
-        const double vol = geo.L[0] * geo.L[1] * geo.L[2];
-        hp.pme_fscale = kQqr2e / (kPi * vol);
-        hp.pme_escale = kQqr2e / (2.0 * kPi * vol);
+        hp.pme_alpha = d.pme_alpha;
         hp.pme_alpha2_pi2 = kPi * kPi / (d.pme_alpha * d.pme_alpha);
         hp.grid_scale = hp.prec == kMixed ? 4294967296.0 : 1099511627776.0;
         hp.grid_scale_inv = 1.0 / hp.grid_scale;
@@ -477,33 +478,19 @@ Slot::Slot(const atvb_system_desc& d, const DevMem& mem) : desc(d), mem_(mem) {
         CK(cudaMemsetAsync(hp.grid_fix, 0, nt * 8, stream));
         hp.grid_real = dalloc(nt * rs);
         hp.grid_cplx = dalloc(nh * 2 * rs);
-        hp.infl = dd(nh);
-        // pme_influence.h:112-155 on the half grid (orthorhombic)
-        std::vector<double> m0 = spline_moduli(hp.K[0], hp.order);
-        std::vector<double> m1 = spline_moduli(hp.K[1], hp.order);
-        std::vector<double> m2 = spline_moduli(hp.K[2], hp.order);
-        infl_host.assign(nh, 0.0);
-        for (size_t a = 0; a < K0; ++a) {
-            const int h0 = a <= K0 / 2 ? (int)a : (int)a - (int)K0;
-            for (size_t b = 0; b < K1; ++b) {
-                const int h1 = b <= K1 / 2 ? (int)b : (int)b - (int)K1;
-                const double bm01 = m0[a] * m1[b];
-                for (size_t c = 0; c < Kh; ++c) {
-                    if (a == 0 && b == 0 && c == 0)
-                        continue;
-                    const int h2 = c <= K2 / 2 ? (int)c : (int)c - (int)K2;
-                    const double mx = h0 * hp.invL[0], my = h1 * hp.invL[1],
-                                 mz = h2 * hp.invL[2];
-                    const double msq = mx * mx + my * my + mz * mz;
-                    infl_host[(a * K1 + b) * Kh + c] =
-                        std::exp(-hp.pme_alpha2_pi2 * msq) / msq * bm01 *
-                        m2[c];
-                }
-            }
+        // B-spline moduli per axis (pme_spline.h:67-94); the influence
+        // function H(m) itself is evaluated on the fly from the current cell
+        std::vector<double> bm;
+        for (int k = 0; k < 3; ++k) {
+            const std::vector<double> m = spline_moduli(hp.K[k], hp.order);
+            bm.insert(bm.end(), m.begin(), m.end());
         }
-        CK(cudaMemcpyAsync(hp.infl, infl_host.data(), nh * 8,
-                           cudaMemcpyHostToDevice, stream));
+        double* dbm = dd(bm.size());
+        CK(cudaMemcpyAsync(dbm, bm.data(), bm.size() * 8, cudaMemcpyHostToDevice, stream));
+        hp.bmod = dbm;
+        CK(cudaStreamSynchronize(stream));
     }
+    apply_box(hp, geo.L, false);
     CK(cudaStreamSynchronize(stream));
 }
 
@@ -737,6 +724,15 @@ void Engine::ensure_table() {
 
 void Engine::push_params(int id) {
     Slot* s = slot(id);
+    if (s->npt && s->uploaded) {
+        // the device owns an NPT system's cell: keep it
+        SysParams dev;
+        CK(cudaMemcpyAsync(&dev, d_sp_ + id, sizeof(SysParams), cudaMemcpyDeviceToHost,
+                           stream_));
+        CK(cudaStreamSynchronize(stream_));
+        s->hp.e_const = dev.e_const;
+        apply_box(s->hp, dev.L, true);
+    }
     CK(cudaMemcpyAsync(d_sp_ + id, &s->hp, sizeof(SysParams),
                        cudaMemcpyHostToDevice, stream_));
 }
@@ -1047,6 +1043,7 @@ void Engine::compute_forces() {
     sized_rebuild(lc_);
     enqueue_forces(lc_, pme_slots_, false);
     launch_sys_energy(lc_, stream_);
+    launch_npt_prep(lc_, stream_);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(stream_));
 }
@@ -1063,6 +1060,7 @@ void Engine::compute_forces_one(int id) {
         pme.push_back(id);
     enqueue_forces(one, pme, false);
     launch_sys_energy(one, stream_);
+    launch_npt_prep(one, stream_);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(stream_));
 }
@@ -1170,6 +1168,62 @@ LaunchCfg Engine::restricted_cfg(int id) {
     c.nsys = 1;
     single_[id] = {list_epoch_, c};
     return c;
+}
+
+// md::NoseHooverNPT (nose_hoover_npt.cpp:76-172): parameters checked, the
+// system switched from velocity Verlet to MTK NPT, the neighbour bins
+// re-planned for a breathing cell (down to 90 % of each edge, or as far as
+// the minimum-image limit 2 (cutoff + skin) allows).
+void Engine::set_npt(int id, const atvb_npt_desc& p) {
+    Slot* sl = slot(id);
+    if (sl->uploaded)
+        throw Error(ATVB_ERR_STATE, "NoseHooverNPT must be set before the first upload");
+    if (sl->desc.thermostat != ATVB_NVE)
+        throw Error(ATVB_ERR_INVALID,
+                    "NoseHooverNPT replaces the thermostat: the system must be NVE");
+    if (p.mtchain < 1 || p.mtchain > kMaxChain || p.mpchain < 1 || p.mpchain > kMaxChain)
+        throw Error(ATVB_ERR_INVALID, "NoseHooverNPT: chain lengths must be in [1, 10]");
+    if (!(p.tau_T > 0.0) || !(p.tau_P > 0.0) || !(p.T_start > 0.0))
+        throw Error(ATVB_ERR_INVALID, "NoseHooverNPT: T, tau_T and tau_P must be > 0");
+    if (!std::isfinite(p.P_target) || !(p.drag >= 0.0))
+        throw Error(ATVB_ERR_INVALID, "NoseHooverNPT: bad P_target or drag");
+    SysParams& h = sl->hp;
+    double shrink = 0.1;
+    for (int k = 0; k < 3; ++k)
+        shrink = std::min(shrink, 1.0 - 2.0 * sl->geo.rlist * (1.0 + 1e-9) / sl->geo.L[k]);
+    if (shrink < 0.0)
+        shrink = 0.0;
+    sl->replan_cells(shrink);
+    h.thermostat = kNPT;
+    h.need_virial = 1; // requires_system_stress (nose_hoover_npt.cuh:79-82)
+    h.n_dof = std::max(0, 3 * h.n - 3);
+    h.npt_T0 = p.T_start;
+    h.npt_T1 = p.T_stop < 0.0 ? p.T_start : p.T_stop;
+    h.npt_tauT = p.tau_T;
+    h.npt_P = p.P_target;
+    h.npt_mt = p.mtchain;
+    h.npt_mp = p.mpchain;
+    h.npt_pdim = 0;
+    for (int a = 0; a < 3; ++a) {
+        h.npt_couple[a] = p.couple[a] ? 1 : 0;
+        h.npt_pdim += h.npt_couple[a];
+    }
+    h.npt_nfirst = p.nfirst;
+    h.npt_nlast = p.nlast;
+    const double kT = kKB * p.T_start;
+    h.npt_Qb = kT * p.tau_P * p.tau_P;
+    h.npt_W = ((double)h.n_dof + 3.0) * kT * p.tau_P * p.tau_P;
+    h.npt_tdrag = 1.0 - p.drag * h.dt / p.tau_T;
+    h.npt_pdrag = 1.0 - p.drag * h.dt / p.tau_P;
+    double cut = sl->desc.nl_cutoff;
+    if (h.has_lj)
+        cut = std::max(cut, sl->desc.lj_cutoff);
+    if (h.has_coul)
+        cut = std::max(cut, sl->desc.coul_cutoff);
+    h.npt_cut = cut;
+    sl->npt = true;
+    push_params(id);
+    dirty_ = true;
 }
 
 // PairLJCut per-type coefficients (src/cpu/potentials/pair_lj_cut.cpp:44-112
@@ -1419,11 +1473,19 @@ void Engine::upload(int id, const atvb_soa_view& f) {
         const double a = s->desc.pme_alpha;
         s->hp.e_const = -kQqr2e * a / std::sqrt(kPi) * q2 -
                         kQqr2e * kPi / (2.0 * vol * a * a) * qs * qs;
+        s->hp.pme_eself = -kQqr2e * a / std::sqrt(kPi) * q2;
+        s->hp.pme_qsum2 = qs * qs;
     }
     SysState st0;
     std::memset(&st0, 0, sizeof(st0));
     st0.vscale = 1.0;
     st0.s_a = 1.0;
+    for (int k = 0; k < 3; ++k) {
+        st0.box[k] = s->hp.L[k];
+        st0.Lb[k] = st0.Lnext[k] = s->hp.L[k];
+        st0.Lb_inv[k] = 1.0 / s->hp.L[k];
+        st0.vs[k] = st0.vs_out[k] = 1.0;
+    }
     CK(cudaMemcpyAsync(s->hp.st, &st0, sizeof(st0), cudaMemcpyHostToDevice,
                        stream_));
     push_params(id);
@@ -1438,6 +1500,7 @@ void Engine::upload(int id, const atvb_soa_view& f) {
     sized_rebuild(one);
     launch_state_in(one, stream_);
     launch_kinetic(one, stream_);
+    launch_npt_prep(one, stream_);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(stream_));
     // the forced build counts as the setup build, not a step rebuild
@@ -1471,8 +1534,12 @@ void Engine::scalars(int id, atvb_scalars* out) {
     out->step = st.step;
     out->rebuilds = st.rebuilds;
     out->max_neighbors = st.max_nnbr;
-    out->status = st.overflow ? ATVB_ERR_OVERFLOW : 0;
+    out->status = st.overflow ? ATVB_ERR_OVERFLOW
+                              : ((st.status & kStatusBoxRange) ? ATVB_ERR_STATE : 0);
     out->list_pairs = (int64_t)(st.list_entries / 2);
+    for (int k = 0; k < 3; ++k)
+        out->box[k] = st.box[k];
+    out->pressure = st.pressure;
 }
 
 void Engine::download(int id, atvb_soa_view* f, atvb_scalars* sc) {

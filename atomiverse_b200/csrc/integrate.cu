@@ -15,6 +15,8 @@
 // The end-of-step kinetic energy is s_B^2 * KE(v) for the deferred scale.
 #include "atvb_common.cuh"
 #include "atvb_kernels.cuh"
+#include "box.cuh"
+#include "npt.cuh"
 
 namespace atvb {
 
@@ -53,6 +55,55 @@ ATVB_DEV double fix_to_d(unsigned long long v) {
     return (double)(long long)v * kEFixInv;
 }
 
+// MTK NPT initial half for atom i (nose_hoover_npt.cpp:812-850 P2-P6): the
+// pending per-axis velocity scale (end-of-step chain and barostat factors of
+// the previous step, initial-half ones of this step), the force kick, the
+// closed-form drift x e^{eps dt} + v dt drift into the next cell, wrap,
+// sorted repack with the next cell's scales, displacement check in the
+// build cell.
+ATVB_DEV void npt_drift_atom(const SysParams& P, int i) {
+    const SysState* st = P.st;
+    const int r = P.rank[i];
+    const double4 f = P.f4[r];
+    const double dtfm = P.dtf / P.mass[i];
+    double v[3] = {P.vx[i], P.vy[i], P.vz[i]};
+    const double fa[3] = {f.x, f.y, f.z};
+    double* const xs[3] = {P.x, P.y, P.z};
+    double x[3];
+    double d2 = 0.0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        v[d] = __dadd_rn(__dmul_rn(v[d], st->vs[d]), __dmul_rn(dtfm, fa[d]));
+        const double Ln = st->Lnext[d];
+        double xd = __dadd_rn(__dmul_rn(xs[d][i], st->npt_a[d]),
+                              __dmul_rn(__dmul_rn(v[d], P.dt), st->npt_drift[d]));
+        xd = __dadd_rn(xd, -__dmul_rn(Ln, floor(xd / Ln)));
+        x[d] = xd;
+        const double* xr = d == 0 ? P.xr : (d == 1 ? P.yr : P.zr);
+        const double du = min_img(xd * st->ub[d] - xr[i], st->Lb[d], st->Lb_inv[d]);
+        d2 += du * du;
+    }
+    P.vx[i] = v[0];
+    P.vy[i] = v[1];
+    P.vz[i] = v[2];
+    P.x[i] = x[0];
+    P.y[i] = x[1];
+    P.z[i] = x[2];
+    const double q = P.q[i];
+    if (P.prec == kMixed) {
+        int4 p;
+        p.x = (int)pos_fix(x[0], st->fixn_scale[0]);
+        p.y = (int)pos_fix(x[1], st->fixn_scale[1]);
+        p.z = (int)pos_fix(x[2], st->fixn_scale[2]);
+        p.w = __float_as_int((float)q);
+        reinterpret_cast<int4*>(P.pos4)[r] = p;
+    } else {
+        reinterpret_cast<double4*>(P.pos4)[r] = pack_pos64(x, st->fixn64_scale, q);
+    }
+    if (d2 > st->disp_thr2)
+        P.st->need_rebuild = 1;
+}
+
 // Initial half: deferred scale, kick, drift, wrap, sorted repack,
 // displacement check, KE of the kicked velocities (for Nose-Hoover).
 __global__ void __launch_bounds__(kChunk)
@@ -63,7 +114,9 @@ __global__ void __launch_bounds__(kChunk)
         const SysParams& P = sp[item.sys];
         const int i = item.begin + threadIdx.x;
         double ke = 0.0;
-        if (i < P.n) {
+        if (i < P.n && P.thermostat == kNPT) {
+            npt_drift_atom(P, i);
+        } else if (i < P.n) {
             const double sc = P.st->vscale;
             const int r = P.rank[i];
             const double4 f = P.f4[r];
@@ -120,6 +173,13 @@ __global__ void k_sys_a(const int* sys_list, int nsys, const SysParams* sp) {
         return;
     const SysParams& P = sp[sys_list[k]];
     SysState* st = P.st;
+    if (P.thermostat == kNPT) {
+        // commit the cell of this step's drift: every later kernel of the
+        // step (neighbour build, forces, PME) reads it from SysParams
+        apply_box(const_cast<SysParams&>(sp[sys_list[k]]), st->Lnext, true);
+        for (int d = 0; d < 3; ++d)
+            st->box[d] = st->Lnext[d];
+    }
     st->vscale = 1.0;
     st->nearq_n = 0; // the previous step's near-cutoff queue has been settled
     if (P.thermostat == kNoseHoover) {
@@ -137,6 +197,10 @@ __global__ void k_sys_a(const int* sys_list, int nsys, const SysParams* sp) {
                          (!P.nl_check || disp);
     st->rebuild = rebuild ? 1 : 0;
     if (rebuild) {
+        for (int d = 0; d < 3; ++d) {
+            st->Lb[d] = P.L[d];
+            st->Lb_inv[d] = 1.0 / P.L[d];
+        }
         st->ago = 0;
         st->rebuilds += 1;
         st->max_nnbr = 0;
@@ -148,11 +212,13 @@ __global__ void k_sys_a(const int* sys_list, int nsys, const SysParams* sp) {
 __global__ void __launch_bounds__(kChunk)
     k_integrate_b(const Item* items, int nitems, const SysParams* sp) {
     __shared__ double sh[32];
+    __shared__ double sh3[32 * 3];
     for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
         const Item item = items[it];
         const SysParams& P = sp[item.sys];
         const int i = item.begin + threadIdx.x;
         double ke = 0.0;
+        double kax[3] = {0.0, 0.0, 0.0};
         if (i < P.n) {
             const double sc = P.st->s_a;
             const int r = P.rank[i];
@@ -183,10 +249,20 @@ __global__ void __launch_bounds__(kChunk)
             P.vy[i] = v[1];
             P.vz[i] = v[2];
             ke = m * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+            kax[0] = m * v[0] * v[0];
+            kax[1] = m * v[1] * v[1];
+            kax[2] = m * v[2] * v[2];
         }
-        const double t = block_sum(ke, sh);
-        if (threadIdx.x == 0)
-            fix_add(&P.st->acc[kAccKEB], 0.5 * kMvv2e * t);
+        if (P.thermostat == kNPT) {
+            block_sum_vec<3>(kax, sh3);
+            if (threadIdx.x == 0)
+                for (int d = 0; d < 3; ++d)
+                    fix_add(&P.st->acc[kAccKEX + d], 0.5 * kMvv2e * kax[d]);
+        } else {
+            const double t = block_sum(ke, sh);
+            if (threadIdx.x == 0)
+                fix_add(&P.st->acc[kAccKEB], 0.5 * kMvv2e * t);
+        }
     }
 }
 
@@ -203,6 +279,51 @@ ATVB_DEV void finish_energy(const SysParams& P, SysState* st) {
         st->acc[kAccVir + k] = 0ull;
 }
 
+// Cell edges and the scalar pressure (2 KE + W_xx + W_yy + W_zz) / (3 V)
+ATVB_DEV void cell_scalars(const SysParams& P, SysState* st) {
+    for (int d = 0; d < 3; ++d)
+        st->box[d] = P.L[d];
+    const double V = P.L[0] * P.L[1] * P.L[2];
+    st->pressure =
+        (2.0 * st->kinetic + st->virial[0] + st->virial[1] + st->virial[2]) / (3.0 * V);
+}
+
+ATVB_DEV void record_history(const SysParams& P, SysState* st) {
+    if (P.ehist_cap > 0) {
+        const long long slot = st->step % P.ehist_cap;
+        P.ehist[3 * slot + 0] = st->energy;
+        P.ehist[3 * slot + 1] = st->kinetic;
+        P.ehist[3 * slot + 2] = (double)st->step;
+    }
+}
+
+// MTK NPT end of step (nose_hoover_npt.cpp:855-885, P8-P11) from the
+// per-axis kinetic energies of the kicked velocities, then the scalars of
+// the next step's initial half (npt_prepare).
+ATVB_DEV void npt_end_of_step(const SysParams& P, SysState* st) {
+    const double hdt = 0.5 * P.dt;
+    double ke[3];
+    for (int d = 0; d < 3; ++d) {
+        ke[d] = fix_to_d(st->acc[kAccKEX + d]);
+        st->acc[kAccKEX + d] = 0ull;
+    }
+    finish_energy(P, st); // energies and the virial of this step's forces
+    st->ke_global = ke[0] + ke[1] + ke[2];
+    double s8[3];
+    npt_scale_baro(P, st, hdt, ke, s8);                 // P8
+    npt_update_eps(P, st, hdt, ke);                     // P9
+    const double s10 = npt_nhc_atoms(P, st, hdt, ke);   // P10
+    npt_nhc_baro(P, st, hdt);                           // P11
+    st->kinetic = st->ke_global;
+    st->conserved = npt_hamiltonian(P, st);
+    st->vscale = 1.0;
+    cell_scalars(P, st);
+    record_history(P, st);
+    st->step += 1;
+    const double vs_out[3] = {s8[0] * s10, s8[1] * s10, s8[2] * s10};
+    npt_prepare(P, st, ke, vs_out);
+}
+
 // One thread per system: final-half thermostat, end-of-step scalars,
 // energy history, step counter.
 __global__ void k_sys_b(const int* sys_list, int nsys, const SysParams* sp) {
@@ -211,6 +332,10 @@ __global__ void k_sys_b(const int* sys_list, int nsys, const SysParams* sp) {
         return;
     const SysParams& P = sp[sys_list[k]];
     SysState* st = P.st;
+    if (P.thermostat == kNPT) {
+        npt_end_of_step(P, st);
+        return;
+    }
     const double ke = fix_to_d(st->acc[kAccKEB]);
     st->acc[kAccKEB] = 0ull;
     if (P.thermostat == kNoseHoover) {
@@ -224,6 +349,7 @@ __global__ void k_sys_b(const int* sys_list, int nsys, const SysParams* sp) {
     }
     finish_energy(P, st);
     st->conserved = st->energy + st->kinetic;
+    cell_scalars(P, st);
     if (P.ehist_cap > 0) {
         const long long slot = st->step % P.ehist_cap;
         P.ehist[3 * slot + 0] = st->energy;
@@ -242,6 +368,7 @@ __global__ void k_sys_energy(const int* sys_list, int nsys,
     const SysParams& P = sp[sys_list[k]];
     finish_energy(P, P.st);
     P.st->conserved = P.st->energy + P.st->kinetic;
+    cell_scalars(P, P.st);
 }
 
 __global__ void k_force_rebuild(const int* sys_list, int nsys,
@@ -305,6 +432,11 @@ __global__ void k_state_out(const Item* items, int nitems, const SysParams* sp,
             P.sx[i] = f.x;
             P.sy[i] = f.y;
             P.sz[i] = f.z;
+        } else if (P.thermostat == kNPT) {
+            const double* s = P.st->vs_out;
+            P.sx[i] = P.vx[i] * s[0];
+            P.sy[i] = P.vy[i] * s[1];
+            P.sz[i] = P.vz[i] * s[2];
         } else {
             const double s = P.st->vscale;
             P.sx[i] = P.vx[i] * s;
@@ -340,7 +472,63 @@ __global__ void k_kinetic_finish(const int* sys_list, int nsys,
     st->acc[kAccKEB] = 0ull;
 }
 
+// Per-axis kinetic energy of MTK NPT systems that have not stepped yet (the
+// input of their first initial half).
+__global__ void k_npt_kinetic(const Item* items, int nitems, const SysParams* sp) {
+    __shared__ double sh[32 * 3];
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const Item item = items[it];
+        const SysParams& P = sp[item.sys];
+        if (P.thermostat != kNPT || P.st->step != 0)
+            continue;
+        const int i = item.begin + threadIdx.x;
+        double k[3] = {0.0, 0.0, 0.0};
+        if (i < P.n) {
+            const double m = P.mass[i];
+            k[0] = m * P.vx[i] * P.vx[i];
+            k[1] = m * P.vy[i] * P.vy[i];
+            k[2] = m * P.vz[i] * P.vz[i];
+        }
+        block_sum_vec<3>(k, sh);
+        if (threadIdx.x == 0)
+            for (int d = 0; d < 3; ++d)
+                fix_add(&P.st->acc[kAccKEX + d], 0.5 * kMvv2e * k[d]);
+    }
+}
+
+// Before the first step of an MTK NPT system: the extended state of the
+// reference's build() (chains and strain rates at rest, KE_global at
+// equipartition, nose_hoover_npt.cpp:87-172), then the scalars of step 0's
+// initial half from the virial of the last force evaluation (zero before
+// any).  Idempotent while no step has run.
+__global__ void k_npt_prep(const int* sys_list, int nsys, const SysParams* sp) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nsys)
+        return;
+    const SysParams& P = sp[sys_list[k]];
+    SysState* st = P.st;
+    if (P.thermostat != kNPT || st->step != 0)
+        return;
+    double ke[3];
+    for (int d = 0; d < 3; ++d) {
+        ke[d] = fix_to_d(st->acc[kAccKEX + d]);
+        st->acc[kAccKEX + d] = 0ull;
+    }
+    for (int c = 0; c < kMaxChain; ++c)
+        st->eta_t[c] = st->eta_t_dot[c] = st->eta_b[c] = st->eta_b_dot[c] = 0.0;
+    for (int d = 0; d < 3; ++d)
+        st->eps_dot[d] = 0.0;
+    st->ke_global = 0.5 * (double)P.n_dof * kKB * P.npt_T0;
+    const double one[3] = {1.0, 1.0, 1.0};
+    npt_prepare(P, st, ke, one);
+}
+
 static int sys_blocks(int nsys) { return (nsys + 127) / 128; }
+
+void launch_npt_prep(const LaunchCfg& lc, cudaStream_t s) {
+    k_npt_kinetic<<<lc.atoms.grid, kChunk, 0, s>>>(lc.atoms.d, lc.atoms.n, lc.sp);
+    k_npt_prep<<<sys_blocks(lc.nsys), 128, 0, s>>>(lc.sys_list, lc.nsys, lc.sp);
+}
 
 void launch_integrate_a(const LaunchCfg& lc, cudaStream_t s) {
     k_integrate_a<<<lc.atoms.grid, kChunk, 0, s>>>(lc.atoms.d, lc.atoms.n,

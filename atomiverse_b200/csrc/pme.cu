@@ -190,23 +190,27 @@ __global__ void __launch_bounds__(256)
             const size_t idx = (size_t)item.begin + k;
             if (idx >= nh)
                 break;
-            const double H = P.infl[idx];
             T2 Qm = grid[idx];
             const double re = (double)Qm.x, im = (double)Qm.y;
             const int m2 = (int)(idx % Kh);
+            const size_t r = idx / Kh;
+            const int m1 = (int)(r % K1), m0 = (int)(r / K1);
+            const int h0 = m0 <= K0 / 2 ? m0 : m0 - K0;
+            const int h1 = m1 <= K1 / 2 ? m1 : m1 - K1;
+            const int h2 = m2 <= K2 / 2 ? m2 : m2 - K2;
+            const double mx = h0 * P.invL[0], my = h1 * P.invL[1], mz = h2 * P.invL[2];
+            const double msq = mx * mx + my * my + mz * mz;
+            // H(m) = exp(-pi^2 m^2 / alpha^2) / m^2 * B(m), zero mode
+            // cleared (pme_influence.h:112-155), from the current cell
+            const double imsq = idx == 0 ? 0.0 : 1.0 / msq;
+            const double H = idx == 0 ? 0.0
+                                      : exp(-P.pme_alpha2_pi2 * msq) * imsq *
+                                            (P.bmod[m0] * P.bmod[K0 + m1]) * P.bmod[K0 + K1 + m2];
             const double w = (m2 == 0 || 2 * m2 == K2) ? 1.0 : 2.0;
             const double ug = w * H * (re * re + im * im);
             acc[0] += ug;
             if (vir && H != 0.0) {
-                const size_t r = idx / Kh;
-                const int m1 = (int)(r % K1), m0 = (int)(r / K1);
-                const int h0 = m0 <= K0 / 2 ? m0 : m0 - K0;
-                const int h1 = m1 <= K1 / 2 ? m1 : m1 - K1;
-                const int h2 = m2 <= K2 / 2 ? m2 : m2 - K2;
-                const double mx = h0 * P.invL[0], my = h1 * P.invL[1],
-                             mz = h2 * P.invL[2];
-                const double msq = mx * mx + my * my + mz * mz;
-                const double vt = -2.0 * (1.0 / msq + P.pme_alpha2_pi2);
+                const double vt = -2.0 * (imsq + P.pme_alpha2_pi2);
                 acc[1] += ug * (1.0 + vt * mx * mx);
                 acc[2] += ug * (1.0 + vt * my * my);
                 acc[3] += ug * (1.0 + vt * mz * mz);

@@ -36,7 +36,8 @@ enum atvb_precision {
 enum atvb_thermostat {
     ATVB_NVE = 0,
     ATVB_NOSE_HOOVER = 1, /* md::NoseHoover(T, tau, dt): src/cuda/dynamics/nose_hoover.cu:29 */
-    ATVB_LANGEVIN = 2     /* md::FixLangevin(T, T, damp, dt, seed): fix_langevin.cuh */
+    ATVB_LANGEVIN = 2,    /* md::FixLangevin(T, T, damp, dt, seed): fix_langevin.cuh */
+    ATVB_NPT = 3          /* md::NoseHooverNPT: set by atvb_system_set_npt */
 };
 
 typedef struct atvb_ctx atvb_ctx;
@@ -83,6 +84,22 @@ typedef struct atvb_system_desc {
     int32_t history_capacity;  /* per-step energy ring length (0: default 4096) */
 } atvb_system_desc;
 
+/* md::NoseHooverNPT(T_target, tau_T, P_target, tau_P, dt, drag, mtchain,
+ * mpchain, couple_axis, T_stop) + set_run_span(nfirst, nlast)
+ * (include/atomiverse/cuda/dynamics/nose_hoover_npt.cuh:60-70,
+ * src/cpu/dynamics/nose_hoover_npt.cpp:76-172): Martyna-Tobias-Klein NPT with
+ * Nose-Hoover chains on the atoms and on the barostat.  P_target in eV/A^3
+ * (LAMMPS sign: positive compresses); T_stop < 0: constant setpoint; dt is
+ * the system's dt.  couple[a] != 0: axis a is barostatted (all three: the
+ * axis pressures are averaged, isotropic cell). */
+typedef struct atvb_npt_desc {
+    double T_start, T_stop, tau_T;   /* K, K, fs */
+    double P_target, tau_P, drag;    /* eV/A^3, fs, - */
+    int32_t mtchain, mpchain;        /* chain lengths, 1..10 */
+    int32_t couple[3];
+    int64_t nfirst, nlast;           /* temperature ramp span (steps) */
+} atvb_npt_desc;
+
 /* Host SoA view of a frame (cuda::Frame::Atoms field names,
  * include/atomiverse/cuda/frame/frame.cuh:71-96).  Any pointer may be NULL on
  * upload (zeros / unit mass / tag = index+1) or on download (not copied). */
@@ -107,8 +124,11 @@ typedef struct atvb_scalars {
     int64_t step;
     int64_t rebuilds;
     int32_t max_neighbors;
-    int32_t status;       /* 0 or ATVB_ERR_OVERFLOW */
+    int32_t status;       /* 0, ATVB_ERR_OVERFLOW, or ATVB_ERR_STATE (an NPT cell
+                             left the range its neighbour grid was planned for) */
     int64_t list_pairs;   /* unordered pairs in the current list (cutoff + skin) */
+    double box[3];        /* current cell edges [A] (change under NPT) */
+    double pressure;      /* (2 KE + W_xx + W_yy + W_zz) / (3 V) [eV/A^3] */
 } atvb_scalars;
 
 /* Per-kernel-group device time from CUDA events (profiling mode). */
@@ -181,6 +201,14 @@ int atvb_system_set_lj_types(atvb_system* sys, int32_t ncoef, const int32_t* typ
 int atvb_system_set_special_bonds(atvb_system* sys, const double lj[3],
                                   const double coul[3], int64_t nbonds,
                                   const int64_t* tag_a, const int64_t* tag_b);
+/* MTK NPT in place of velocity Verlet + thermostat (NoseHooverNPT
+ * "replaces VelocityVerlet + NoseHoover + Barostat", nose_hoover_npt.cuh:15):
+ * desc.thermostat must be ATVB_NVE; stress is then always computed.  Before
+ * the first upload.  The neighbour bins are planned for cells down to 90 %
+ * of the initial edge (less when the box is barely larger than 2 (cutoff +
+ * skin)); a cell that shrinks further is held and flagged in
+ * atvb_scalars.status (re-create the system from the current frame). */
+int atvb_system_set_npt(atvb_system* sys, const atvb_npt_desc* npt);
 /* Profiling: enable per-kernel-group CUDA events on subsequent steps. */
 int atvb_system_profile(atvb_system* sys, int32_t enable);
 int atvb_system_profile_read(atvb_system* sys, atvb_kernel_time* out,
@@ -203,6 +231,8 @@ int atvb_batch_download(atvb_batch* b, int32_t index, atvb_soa_view* frame,
                         atvb_scalars* scalars);
 /* atvb_system_set_lj_types / _set_special_bonds for system `index` of a
  * batch, before that system's first upload. */
+/* atvb_system_set_npt for system `index` of a batch, before its first upload. */
+int atvb_batch_set_npt(atvb_batch* b, int32_t index, const atvb_npt_desc* npt);
 int atvb_batch_set_lj_types(atvb_batch* b, int32_t index, int32_t ncoef,
                             const int32_t* type_i, const int32_t* type_j,
                             const double* epsilon, const double* sigma);

@@ -1,0 +1,141 @@
+"""MTK NPT on the GPU (md::NoseHooverNPT) against the oracle:
+
+- the reference's npt_lj_mtk regression (216 LJ atoms, 80 steps, no force
+  pass before the first step): cell volume, positions and the conserved
+  extended Hamiltonian match the oracle, and the volume is the reference's
+  own V = 269.425432;
+- a charged LJ melt with PME under 16 kbar: the cell, PME prefactors and
+  neighbour bins follow the cell every step;
+- one uncoupled axis keeps its edge;
+- an NPT system batched with a Nose-Hoover one gives what each gives alone.
+"""
+import numpy as np
+import pytest
+
+from conftest import oracle_system
+
+KB = 8.617333262e-5
+
+
+def _lj_cube(n_side=6, rho=0.8):
+    n = n_side ** 3
+    L = (n / rho) ** (1.0 / 3.0)
+    a = L / n_side
+    idx = np.array([(ix, iy, iz) for ix in range(n_side) for iy in range(n_side)
+                    for iz in range(n_side)])
+    pos = (idx + 0.5) * a
+    ix, iy, iz = idx[:, 0], idx[:, 1], idx[:, 2]
+    desc = dict(n_atoms=n, box=(L, L, L), nl_cutoff=2.5, nl_skin=0.3, lj_enabled=1,
+                lj_epsilon=1.0, lj_sigma=1.0, lj_cutoff=2.5, dt=0.005)
+    frame = dict(x=pos[:, 0].copy(), y=pos[:, 1].copy(), z=pos[:, 2].copy(),
+                 vx=0.02 * ((ix + iy + iz) % 3 - 1.0), vy=0.02 * ((ix + 2 * iy) % 3 - 1.0),
+                 vz=0.02 * ((2 * ix + iz) % 3 - 1.0), mass=np.ones(n))
+    return desc, frame
+
+
+def _melt(ncell=6):
+    from atomiverse_b200 import workloads as W
+    desc, frame = W.rocksalt_melt(ncell=ncell, rc=5.5, grid=(20, 20, 20))
+    desc = dict(desc, thermostat=0, stress_required=1)
+    return desc, frame
+
+
+def _pos(out):
+    return np.stack([out["x"], out["y"], out["z"]], axis=1)
+
+
+def _oracle_npt(orc, desc, frame, npt, steps, setup=False):
+    o = oracle_system(orc, desc, frame)
+    o.set_npt(npt["T_target"], npt["tau_T"], npt["P_target"], npt["tau_P"],
+              couple=npt.get("couple_axis", (True, True, True)))
+    if setup:
+        o.build_list()
+        o.compute_forces()
+    o.run(steps)
+    return o
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision,tol", [(0, 1e-10), (1, 1e-6)])
+def test_npt_lj_regression_matches_oracle(atvb, ctx, orc, precision, tol):
+    desc, frame = _lj_cube()
+    npt = dict(T_target=1.0 / KB, tau_T=0.1, P_target=0.0, tau_P=1.0, dt=0.005)
+    s = atvb.System(ctx, dict(desc, precision=precision), frame, npt=npt)
+    s.step(80)
+    out, sc = s.download()
+    s.close()
+    o = _oracle_npt(orc, desc, frame, npt, 80)
+    ost = o.npt_state()
+    V, Vo = float(np.prod(sc["box"])), float(np.prod(ost["box"]))
+    assert V == pytest.approx(Vo, rel=tol)
+    assert V == pytest.approx(269.425432, abs=max(1e-6, tol * V))
+    assert sc["conserved"] == pytest.approx(ost["conserved"], rel=10 * tol)
+    d = _pos(out) - _pos(o.state())
+    d -= np.rint(d / sc["box"]) * sc["box"]
+    assert np.abs(d).max() < 1e3 * tol * sc["box"][0]
+    assert sc["status"] == 0 and sc["step"] == 80
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision,tol", [(0, 1e-9), (1, 2e-6)])
+def test_npt_pme_melt_matches_oracle(atvb, ctx, orc, precision, tol):
+    desc, frame = _melt()
+    npt = dict(T_target=1200.0, tau_T=100.0, P_target=1e-5, tau_P=1000.0, dt=2.0)
+    s = atvb.System(ctx, dict(desc, precision=precision), frame, npt=npt)
+    s.compute_forces()
+    s.step(20)
+    out, sc = s.download()
+    s.close()
+    o = _oracle_npt(orc, desc, frame, npt, 20, setup=True)
+    ost, osc = o.npt_state(), o.scalars()
+    assert sc["box"][0] != desc["box"][0]
+    assert np.allclose(sc["box"], ost["box"], rtol=tol, atol=0)
+    assert sc["conserved"] == pytest.approx(ost["conserved"], rel=10 * tol)
+    assert sc["energy_recip"] + sc["energy_const"] == pytest.approx(
+        osc["e_recip"] + osc["e_const"], rel=100 * tol)
+    d = _pos(out) - _pos(o.state())
+    d -= np.rint(d / sc["box"]) * sc["box"]
+    assert np.abs(d).max() < 1e3 * tol * sc["box"][0]
+
+
+@pytest.mark.gpu
+def test_npt_uncoupled_axis_keeps_edge(atvb, ctx, orc):
+    desc, frame = _lj_cube()
+    npt = dict(T_target=1.0 / KB, tau_T=0.1, P_target=0.0, tau_P=1.0, dt=0.005,
+               couple_axis=(True, True, False))
+    s = atvb.System(ctx, desc, frame, npt=npt)
+    s.compute_forces()
+    s.step(30)
+    _, sc = s.download()
+    s.close()
+    assert sc["box"][2] == desc["box"][2]
+    assert sc["box"][0] != desc["box"][0]
+    o = _oracle_npt(orc, desc, frame, npt, 30, setup=True)
+    assert np.allclose(sc["box"], o.npt_state()["box"], rtol=1e-10, atol=0)
+
+
+@pytest.mark.gpu
+def test_npt_batch_equals_alone(atvb, ctx):
+    from atomiverse_b200 import workloads as W
+    d1, f1 = _lj_cube()
+    npt = dict(T_target=1.0 / KB, tau_T=0.1, P_target=0.0, tau_P=1.0, dt=0.005)
+    d2, f2 = _melt()
+    npt2 = dict(T_target=1200.0, tau_T=100.0, P_target=1e-5, tau_P=1000.0, dt=2.0)
+    d3, f3 = W.lj_fcc(ncell=5, seed=3)
+    items = [(d1, f1, dict(npt=npt)), (d2, f2, dict(npt=npt2)), (d3, f3)]
+    b = atvb.Batch(ctx, items)
+    b.compute_forces()
+    b.step(15)
+    for k, it in enumerate(items):
+        ob, sb = b.download(k)
+        opts = it[2] if len(it) > 2 else {}
+        s = atvb.System(ctx, it[0], it[1], **opts)
+        s.compute_forces()
+        s.step(15)
+        oa, sa = s.download()
+        s.close()
+        for key in ("x", "y", "z", "vx", "vy", "vz"):
+            assert np.array_equal(ob[key], oa[key]), (k, key)
+        assert np.array_equal(sb["box"], sa["box"])
+        assert sb["conserved"] == sa["conserved"]
+    b.close()
