@@ -22,7 +22,7 @@ __all__ = [
     "FP64", "MIXED", "NVE", "NOSE_HOOVER", "LANGEVIN", "AtvbError",
     "Context", "System", "Batch", "Server", "make_desc",
     "NeighborList", "PairLJCut", "CoulLong", "KSpacePME", "VelocityVerlet",
-    "NoseHoover", "FixLangevin", "MD", "library_path",
+    "NoseHoover", "FixLangevin", "NoseHooverNPT", "MD", "library_path",
 ]
 
 FRAME_KEYS = ("x", "y", "z", "vx", "vy", "vz", "fx", "fy", "fz", "mass", "charge")

@@ -233,7 +233,7 @@ size_t estimate_bytes(const atvb_system_desc& d) {
                      K2 = pme_K(d, g, 2);
         const size_t nt = K0 * K1 * K2, nh = K0 * K1 * (K2 / 2 + 1);
         const size_t rs = d.precision == ATVB_MIXED ? 4 : 8;
-        b += nt * 8 + nt * rs + nh * 2 * rs + nh * 8;
+        b += nt * 8 + nt * rs + nh * 2 * rs + (K0 + K1 + K2) * 8;
         b += 2 * nh * 2 * rs; // cuFFT work areas (upper estimate)
     }
     return b;

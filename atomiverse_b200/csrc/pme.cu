@@ -16,6 +16,7 @@
 //    omits is produced from the same pass.
 #include "atvb_common.cuh"
 #include "atvb_kernels.cuh"
+#include "pair_math.cuh"
 
 namespace atvb {
 
@@ -192,9 +193,10 @@ __global__ void __launch_bounds__(256)
                 break;
             T2 Qm = grid[idx];
             const double re = (double)Qm.x, im = (double)Qm.y;
-            const int m2 = (int)(idx % Kh);
-            const size_t r = idx / Kh;
-            const int m1 = (int)(r % K1), m0 = (int)(r / K1);
+            // half grids stay below 2^31 points: 32-bit index arithmetic
+            const unsigned ui = (unsigned)idx, ur = ui / (unsigned)Kh;
+            const int m2 = (int)(ui - ur * (unsigned)Kh);
+            const int m1 = (int)(ur % (unsigned)K1), m0 = (int)(ur / (unsigned)K1);
             const int h0 = m0 <= K0 / 2 ? m0 : m0 - K0;
             const int h1 = m1 <= K1 / 2 ? m1 : m1 - K1;
             const int h2 = m2 <= K2 / 2 ? m2 : m2 - K2;
@@ -202,9 +204,9 @@ __global__ void __launch_bounds__(256)
             const double msq = mx * mx + my * my + mz * mz;
             // H(m) = exp(-pi^2 m^2 / alpha^2) / m^2 * B(m), zero mode
             // cleared (pme_influence.h:112-155), from the current cell
-            const double imsq = idx == 0 ? 0.0 : 1.0 / msq;
+            const double imsq = idx == 0 ? 0.0 : rcp64(msq);
             const double H = idx == 0 ? 0.0
-                                      : exp(-P.pme_alpha2_pi2 * msq) * imsq *
+                                      : exp_neg64(P.pme_alpha2_pi2 * msq) * imsq *
                                             (P.bmod[m0] * P.bmod[K0 + m1]) * P.bmod[K0 + K1 + m2];
             const double w = (m2 == 0 || 2 * m2 == K2) ? 1.0 : 2.0;
             const double ug = w * H * (re * re + im * im);

@@ -21,6 +21,7 @@
 
 #include <atvb.h>
 
+#include <array>
 #include <cstdint>
 #include <cstring>
 #include <stdexcept>
@@ -160,6 +161,35 @@ struct FixLangevin {
     FixLangevin(double t0, double t1, double damp_, double dt_, uint32_t seed_)
         : T_start(t0), T_stop(t1 < 0 ? t0 : t1), damp(damp_), dt(dt_), seed(seed_) {}
 };
+/// cuda::md::NoseHooverNPT(T_target, tau_T, P_target, tau_P, dt, drag,
+/// mtchain, mpchain, couple_axis, T_stop) + set_run_span
+/// (cuda/dynamics/nose_hoover_npt.cuh:60-70).  An integrator: it replaces
+/// VelocityVerlet and the thermostat.  P_target in eV/A^3.
+struct NoseHooverNPT {
+    atvb_npt_desc p{};
+    double dt;
+    NoseHooverNPT(double T_target, double tau_T, double P_target, double tau_P, double dt_,
+                  double drag = 0.0, int mtchain = 3, int mpchain = 3,
+                  std::array<bool, 3> couple_axis = {true, true, true}, double T_stop = -1.0)
+        : dt(dt_) {
+        p.T_start = T_target;
+        p.T_stop = T_stop;
+        p.tau_T = tau_T;
+        p.P_target = P_target;
+        p.tau_P = tau_P;
+        p.drag = drag;
+        p.mtchain = mtchain;
+        p.mpchain = mpchain;
+        for (int a = 0; a < 3; ++a)
+            p.couple[a] = couple_axis[a] ? 1 : 0;
+    }
+    NoseHooverNPT& set_run_span(int64_t nfirst, int64_t nlast) {
+        p.nfirst = nfirst;
+        p.nlast = nlast;
+        return *this;
+    }
+    double T_target() const { return p.T_start; }
+};
 
 /// cuda::md::MD: categorical setters, then run(frame, n) -- continuable.
 class MD {
@@ -225,6 +255,15 @@ class MD {
         have_integrator_ = true;
         return *this;
     }
+    MD& set_integrator(const NoseHooverNPT& v) {
+        if (have_integrator_)
+            throw std::invalid_argument("set_integrator already configured");
+        d_.dt = v.dt;
+        npt_ = v.p;
+        have_npt_ = true;
+        have_integrator_ = true;
+        return *this;
+    }
     MD& set_thermostat(const NoseHoover& t) {
         d_.thermostat = ATVB_NOSE_HOOVER;
         d_.temperature = t.T;
@@ -262,6 +301,8 @@ class MD {
             d_.box[4] = frame.box[1];
             d_.box[8] = frame.box[2];
             check(atvb_system_create(ctx_, &d_, &sys_));
+            if (have_npt_)
+                check(atvb_system_set_npt(sys_, &npt_));
             if (!lj_coeffs_.empty()) {
                 std::vector<int32_t> ti, tj;
                 std::vector<double> e, sg;
@@ -289,6 +330,8 @@ class MD {
         atvb_soa_view v = frame.view();
         atvb_scalars s{};
         check(atvb_system_run(sys_, &v, n_steps, &s));
+        for (int k = 0; k < 3; ++k) // the cell moves under NPT
+            frame.box[k] = s.box[k];
         return s;
     }
 
@@ -299,6 +342,8 @@ class MD {
     int precision_;
     bool have_nl_ = false, have_pair_ = false, have_integrator_ = false;
     std::vector<LJTypeCoeff> lj_coeffs_;
+    atvb_npt_desc npt_{};
+    bool have_npt_ = false;
     SpecialScales lj_special_, coul_special_;
 };
 } // namespace md

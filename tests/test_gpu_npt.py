@@ -139,3 +139,35 @@ def test_npt_batch_equals_alone(atvb, ctx):
         assert np.array_equal(sb["box"], sa["box"])
         assert sb["conserved"] == sa["conserved"]
     b.close()
+
+
+@pytest.mark.gpu
+def test_cpp_npt_regression(atvb, tmp_path):
+    """The reference's npt_lj_mtk case through the C++ mirror
+    (md::NoseHooverNPT): the reference CPU build's V = 269.425432."""
+    import os
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    exe = str(tmp_path / "md_npt")
+    lib_dir = os.path.join(root, "atomiverse_b200")
+    subprocess.run(["g++", "-std=c++17", "-O2", "-I", os.path.join(root, "include"),
+                    os.path.join(root, "tests", "cpp", "md_npt.cpp"), "-o", exe,
+                    "-L", lib_dir, "-latvb", "-Wl,-rpath," + lib_dir], check=True)
+    r = subprocess.run([exe], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    V, H, status = r.stdout.split()
+    assert float(V) == pytest.approx(269.425432, abs=1e-6)
+    assert np.isfinite(float(H)) and int(status) == 0
+
+
+@pytest.mark.gpu
+def test_python_md_mirror_npt(atvb, ctx):
+    """md.MD with NoseHooverNPT as its integrator moves frame["box"]."""
+    desc, frame = _lj_cube()
+    fr = dict(frame, box=desc["box"])
+    sim = atvb.MD(ctx=ctx)
+    sim.set_neighbor(atvb.NeighborList(2.5, 0.3)).set_evaluator(atvb.PairLJCut(1.0, 1.0, 2.5))
+    sim.set_integrator(atvb.NoseHooverNPT(1.0 / KB, 0.1, 0.0, 1.0, 0.005))
+    sim.run(fr, 40)
+    sim.run(fr, 40)
+    assert float(np.prod(fr["box"])) == pytest.approx(269.425432, abs=1e-6)
