@@ -209,6 +209,40 @@ class System:
     def compute_forces(self):
         check(self.lib.atvb_system_compute_forces(self._h))
 
+    def set_snapshots(self, every: int, depth: int = 8):
+        """Publish positions/velocities every `every` steps into a host ring."""
+        check(self.lib.atvb_system_set_snapshots(self._h, int(every), int(depth)))
+
+    def poll_snapshots(self, max_frames: int = 64) -> tuple[list, int]:
+        """Frames published since the last poll (no device sync):
+        [(step, box, {x, y, z, vx, vy, vz})], dropped."""
+        n, m = self.n, int(max_frames)
+        arrs = [np.zeros(m * n) for _ in range(6)]
+        steps = np.zeros(m, dtype=np.int64)
+        box = np.zeros(3 * m)
+        cnt, drop = C.c_int32(), C.c_int64()
+        dp = C.POINTER(C.c_double)
+        check(self.lib.atvb_system_snapshot_poll(
+            self._h, m, steps.ctypes.data_as(C.POINTER(C.c_int64)), box.ctypes.data_as(dp),
+            *[a.ctypes.data_as(dp) for a in arrs], C.byref(cnt), C.byref(drop)))
+        keys = ("x", "y", "z", "vx", "vy", "vz")
+        frames = [(int(steps[f]), box[3 * f:3 * f + 3].copy(),
+                   {k: arrs[j][f * n:(f + 1) * n].copy() for j, k in enumerate(keys)})
+                  for f in range(cnt.value)]
+        return frames, int(drop.value)
+
+    def save(self) -> bytes:
+        """Checkpoint: the whole resumable state as bytes."""
+        nb = C.c_int64()
+        check(self.lib.atvb_system_checkpoint_size(self._h, C.byref(nb)))
+        buf = C.create_string_buffer(nb.value)
+        check(self.lib.atvb_system_save(self._h, buf, nb.value))
+        return buf.raw
+
+    def restore(self, blob: bytes):
+        """Resume from save()'s bytes, in place of the first upload."""
+        check(self.lib.atvb_system_restore(self._h, blob, len(blob)))
+
     def step(self, n: int):
         check(self.lib.atvb_system_step(self._h, int(n)))
 
@@ -324,6 +358,16 @@ class Batch:
 
     def compute_forces(self):
         check(self.lib.atvb_batch_compute_forces(self._h))
+
+    def save(self, k: int) -> bytes:
+        nb = C.c_int64()
+        check(self.lib.atvb_batch_checkpoint_size(self._h, int(k), C.byref(nb)))
+        buf = C.create_string_buffer(nb.value)
+        check(self.lib.atvb_batch_save(self._h, int(k), buf, nb.value))
+        return buf.raw
+
+    def restore(self, k: int, blob: bytes):
+        check(self.lib.atvb_batch_restore(self._h, int(k), blob, len(blob)))
 
     def step(self, n: int):
         check(self.lib.atvb_batch_step(self._h, int(n)))

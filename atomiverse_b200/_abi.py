@@ -165,6 +165,16 @@ SIGNATURES = {
                                                C.POINTER(C.c_double), C.c_int64,
                                                C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "atvb_system_set_npt": (C.c_int, [_vp, C.POINTER(NptDesc)]),
+    "atvb_system_set_snapshots": (C.c_int, [_vp, C.c_int32, C.c_int32]),
+    "atvb_system_snapshot_poll": (C.c_int, [_vp, C.c_int32, C.POINTER(C.c_int64)] +
+                                  [C.POINTER(C.c_double)] * 7 +
+                                  [C.POINTER(C.c_int32), C.POINTER(C.c_int64)]),
+    "atvb_system_checkpoint_size": (C.c_int, [_vp, C.POINTER(C.c_int64)]),
+    "atvb_system_save": (C.c_int, [_vp, _vp, C.c_int64]),
+    "atvb_system_restore": (C.c_int, [_vp, _vp, C.c_int64]),
+    "atvb_batch_checkpoint_size": (C.c_int, [_vp, C.c_int32, C.POINTER(C.c_int64)]),
+    "atvb_batch_save": (C.c_int, [_vp, C.c_int32, _vp, C.c_int64]),
+    "atvb_batch_restore": (C.c_int, [_vp, C.c_int32, _vp, C.c_int64]),
     "atvb_batch_set_npt": (C.c_int, [_vp, C.c_int32, C.POINTER(NptDesc)]),
     "atvb_system_set_lj_types": (C.c_int, [_vp, C.c_int32, C.POINTER(C.c_int32),
                                            C.POINTER(C.c_int32), C.POINTER(C.c_double),

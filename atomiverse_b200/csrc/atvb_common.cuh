@@ -85,6 +85,19 @@ struct SysState {
     double Lb[3], Lb_inv[3]; // cell at the last neighbour build
     double ub[3];      // Lb / Lnext: next positions mapped into the build cell
     double disp_thr2;  // squared displacement that forces a rebuild
+    // trajectory snapshots published so far, and the ring slot being
+    // written this step (-1: none)
+    long long snap_count;
+    int snap_slot;
+};
+
+// Header of one trajectory snapshot slot in host-mapped memory (seqlock:
+// `begin` is raised before the payload is written, `end` after it and a
+// system-scope fence; a reader that sees begin == end == its sequence number
+// around its copy has an untorn frame).
+struct SnapHeader {
+    long long begin, end, step, pad;
+    double box[3], pad2;
 };
 
 struct SysParams {
@@ -164,6 +177,11 @@ struct SysParams {
     long long npt_nfirst, npt_nlast;
     double npt_Lmin[3]; // smallest cell the neighbour grid is valid for
     double npt_cut;     // largest interaction cutoff (rebuild rule)
+    // trajectory snapshots: every `snap_every` steps positions and
+    // velocities go to a ring of `snap_depth` slots in host-mapped memory
+    char* snap_ring;    // device view of the ring (null: off)
+    int snap_every, snap_depth;
+    long long snap_slot_bytes;
     // per-atom master state (original order)
     double *x, *y, *z, *vx, *vy, *vz, *mass, *q;
     long long* tag;

@@ -85,6 +85,8 @@ class Slot {
     void free_alloc(void* p);
     void replan_cells(double shrink);
     bool npt = false; // MTK NPT configured (atvb_system_set_npt)
+    char* snap_host = nullptr; // trajectory snapshot ring (host-mapped)
+    long long snap_read = 0;   // snapshots consumed by the host
 
   private:
     DevMem mem_;
@@ -114,6 +116,12 @@ class Engine {
     void set_special_bonds(int id, const double lj[3], const double coul[3],
                            int64_t nbonds, const int64_t* a, const int64_t* b);
     void set_npt(int id, const atvb_npt_desc& p);
+    void set_snapshots(int id, int every, int depth);
+    int poll_snapshots(int id, int max_frames, int64_t* steps, double* box,
+                       double* const out[6], int64_t* dropped);
+    size_t checkpoint_bytes(int id);
+    void save(int id, void* buf, size_t cap);
+    void restore(int id, const void* buf, size_t size);
     void compute_forces();
     void compute_forces_one(int id);
     void step(int n);

@@ -37,6 +37,7 @@ struct LaunchCfg {
     int nsys = 0;
     int pair_G = 4;     // lanes per atom of the largest system (reported)
     int any_mixed = 0, any_fp64 = 0;
+    int any_snap = 0;   // a system publishes trajectory snapshots
     int any_near = 0;   // a mixed system settles near-cutoff LJ pairs (k_pair_fix)
     int pme_order = 4;  // common PME order (the PME kernels are templated)
     int pme_mixed = 0;
@@ -65,6 +66,8 @@ void launch_state_in(const LaunchCfg& lc, cudaStream_t s);
 void launch_wrap_in(const LaunchCfg& lc, cudaStream_t s);
 void launch_state_out(const LaunchCfg& lc, int what, cudaStream_t s);
 void launch_npt_prep(const LaunchCfg& lc, cudaStream_t s);
+void launch_repack(const LaunchCfg& lc, cudaStream_t s);
+void launch_snapshots(const LaunchCfg& lc, cudaStream_t s);
 void launch_kinetic(const LaunchCfg& lc, cudaStream_t s);
 
 } // namespace atvb

@@ -192,6 +192,82 @@ int atvb_system_pairs(atvb_system* sys, int32_t* pi, int32_t* pj,
     });
 }
 
+int atvb_system_set_snapshots(atvb_system* sys, int32_t every, int32_t depth) {
+    return guard([&] {
+        need(sys, "sys");
+        sys->eng->set_snapshots(sys->id, every, depth);
+    });
+}
+
+int atvb_system_snapshot_poll(atvb_system* sys, int32_t max_frames, int64_t* steps,
+                              double* box, double* x, double* y, double* z, double* vx,
+                              double* vy, double* vz, int32_t* count, int64_t* dropped) {
+    return guard([&] {
+        need(sys, "sys");
+        if (max_frames < 0)
+            throw Error(ATVB_ERR_INVALID, "max_frames must be >= 0");
+        double* const out[6] = {x, y, z, vx, vy, vz};
+        const int c = sys->eng->poll_snapshots(sys->id, max_frames, steps, box, out, dropped);
+        if (count)
+            *count = c;
+    });
+}
+
+int atvb_system_checkpoint_size(atvb_system* sys, int64_t* bytes) {
+    return guard([&] {
+        need(sys, "sys");
+        need(bytes, "bytes");
+        *bytes = (int64_t)sys->eng->checkpoint_bytes(sys->id);
+    });
+}
+
+int atvb_system_save(atvb_system* sys, void* buf, int64_t capacity) {
+    return guard([&] {
+        need(sys, "sys");
+        need(buf, "buf");
+        sys->eng->save(sys->id, buf, capacity < 0 ? 0 : (size_t)capacity);
+    });
+}
+
+int atvb_system_restore(atvb_system* sys, const void* buf, int64_t size) {
+    return guard([&] {
+        need(sys, "sys");
+        need(buf, "buf");
+        sys->eng->restore(sys->id, buf, size < 0 ? 0 : (size_t)size);
+        sys->uploaded = true;
+    });
+}
+
+int atvb_batch_checkpoint_size(atvb_batch* b, int32_t index, int64_t* bytes) {
+    return guard([&] {
+        need(b, "batch");
+        need(bytes, "bytes");
+        if (index < 0 || index >= (int)b->ids.size())
+            throw Error(ATVB_ERR_NOTFOUND, "no system " + std::to_string(index) + " in batch");
+        *bytes = (int64_t)b->eng->checkpoint_bytes(b->ids[index]);
+    });
+}
+
+int atvb_batch_save(atvb_batch* b, int32_t index, void* buf, int64_t capacity) {
+    return guard([&] {
+        need(b, "batch");
+        need(buf, "buf");
+        if (index < 0 || index >= (int)b->ids.size())
+            throw Error(ATVB_ERR_NOTFOUND, "no system " + std::to_string(index) + " in batch");
+        b->eng->save(b->ids[index], buf, capacity < 0 ? 0 : (size_t)capacity);
+    });
+}
+
+int atvb_batch_restore(atvb_batch* b, int32_t index, const void* buf, int64_t size) {
+    return guard([&] {
+        need(b, "batch");
+        need(buf, "buf");
+        if (index < 0 || index >= (int)b->ids.size())
+            throw Error(ATVB_ERR_NOTFOUND, "no system " + std::to_string(index) + " in batch");
+        b->eng->restore(b->ids[index], buf, size < 0 ? 0 : (size_t)size);
+    });
+}
+
 int atvb_system_set_npt(atvb_system* sys, const atvb_npt_desc* npt) {
     return guard([&] {
         need(sys, "sys");

@@ -12,6 +12,7 @@
 #include <cufft.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -300,6 +301,10 @@ void Slot::replan_cells(double shrink) {
 }
 
 Slot::~Slot() {
+    if (snap_host) {
+        cudaStreamSynchronize(mem_.stream); // no snapshot kernel still writing
+        cudaFreeHost(snap_host);
+    }
     for (void* p : allocs)
         mem_.free(p);
     mem_.free(nbr_alloc);
@@ -822,6 +827,8 @@ void Engine::build_lists() {
             lc_.any_fp64 = 1;
         if (P.prec == kMixed && P.has_lj && !P.general && P.mix_band_lj > 0.0)
             lc_.any_near = 1;
+        if (P.snap_ring)
+            lc_.any_snap = 1;
         if (P.has_pme) {
             if (pme_prec >= 0 && (pme_prec != P.prec || pme_order != P.order))
                 throw Error(ATVB_ERR_INVALID,
@@ -892,6 +899,7 @@ int64_t Engine::kernels_per_step() const {
     if (!pme_slots_.empty())
         k += 4;                               // spread, convert, influence, gather
     k += 2;                                   // integrate_b, sys_b
+    k += lc_.any_snap ? 3 : 0;                // trajectory snapshots
     return k;
 }
 
@@ -929,6 +937,10 @@ void Engine::enqueue_step(bool profile) {
     prof_mark(profile, "integrate_b");
     launch_integrate_b(lc_, stream_);
     launch_sys_b(lc_, stream_);
+    if (lc_.any_snap) {
+        prof_mark(profile, "snapshot");
+        launch_snapshots(lc_, stream_);
+    }
     prof_mark(profile, nullptr);
 }
 
@@ -1491,6 +1503,7 @@ void Engine::upload(int id, const atvb_soa_view& f) {
     push_params(id);
     CK(cudaStreamSynchronize(stream_));
     s->uploaded = true;
+    s->snap_read = 0; // the published snapshot count restarts with the state
     dirty_ = true;
     build_lists();
     // wrap, first neighbour build, uploaded forces into sorted order, KE --
@@ -1694,6 +1707,278 @@ int Engine::autotune() {
     // the timing runs polluted the energy accumulators: recompute
     compute_forces();
     return best_g;
+}
+
+} // namespace atvb
+
+// ------------------------------------------------------------ checkpoints
+//
+// A checkpoint is the whole resumable state of one system: the master atom
+// arrays (original order, raw velocities), the forces of the last force
+// pass, the positions and cell of the last neighbour build, and the
+// device-side SysState (thermostat / barostat chains, pending velocity
+// scales, step and list counters).  Restoring rebuilds the neighbour list
+// from the positions of the last build, so the rows, their order and the
+// lane count are those of the saved run: continuing gives the same
+// trajectory, bit for bit, as never stopping.
+
+namespace atvb {
+
+namespace {
+constexpr char kCkptMagic[8] = {'A', 'T', 'V', 'B', 'C', 'K', 'P', '1'};
+constexpr uint32_t kCkptVersion = 1;
+
+struct CkptHeader {
+    char magic[8];
+    uint32_t version;
+    uint32_t header_bytes;
+    int32_t n;
+    int32_t precision;
+    int32_t thermostat;
+    int32_t ntypes;
+    int64_t state_bytes;
+    double mean_row;
+    double reserved[4];
+};
+
+// per-atom double arrays: x y z vx vy vz fx fy fz xr yr zr mass q
+constexpr int kCkptArrays = 14;
+} // namespace
+
+size_t Engine::checkpoint_bytes(int id) {
+    Slot* s = slot(id);
+    const size_t n = (size_t)s->hp.n;
+    return sizeof(CkptHeader) + sizeof(SysState) + n * (kCkptArrays * 8 + 8) +
+           (s->ntypes > 0 ? n * 4 : 0);
+}
+
+void Engine::save(int id, void* buf, size_t cap) {
+    CK(cudaSetDevice(device_));
+    Slot* s = slot(id);
+    if (!s->uploaded)
+        throw Error(ATVB_ERR_STATE, "checkpoint before upload");
+    const size_t need = checkpoint_bytes(id);
+    if (!buf || cap < need)
+        throw Error(ATVB_ERR_INVALID, "checkpoint buffer smaller than atvb_*_checkpoint_size");
+    ensure_ready();
+    const LaunchCfg one = restricted_cfg(id);
+    const SysParams& P = s->hp;
+    const size_t n = (size_t)P.n, b = n * 8;
+    char* p = (char*)buf;
+    CkptHeader h;
+    std::memset(&h, 0, sizeof(h));
+    std::memcpy(h.magic, kCkptMagic, 8);
+    h.version = kCkptVersion;
+    h.header_bytes = sizeof(CkptHeader);
+    h.n = P.n;
+    h.precision = P.prec;
+    h.thermostat = P.thermostat;
+    h.ntypes = s->ntypes;
+    h.state_bytes = sizeof(SysState);
+    h.mean_row = s->mean_row;
+    std::memcpy(p, &h, sizeof(h));
+    p += sizeof(h);
+    CK(cudaMemcpyAsync(p, P.st, sizeof(SysState), cudaMemcpyDeviceToHost, stream_));
+    p += sizeof(SysState);
+    const double* src[6] = {P.x, P.y, P.z, P.vx, P.vy, P.vz};
+    for (const double* a : src) {
+        CK(cudaMemcpyAsync(p, a, b, cudaMemcpyDeviceToHost, stream_));
+        p += b;
+    }
+    launch_state_out(one, 0, stream_); // forces, original order
+    for (const double* a : {P.sx, P.sy, P.sz}) {
+        CK(cudaMemcpyAsync(p, a, b, cudaMemcpyDeviceToHost, stream_));
+        p += b;
+    }
+    for (const double* a : {P.xr, P.yr, P.zr, P.mass, P.q}) {
+        CK(cudaMemcpyAsync(p, a, b, cudaMemcpyDeviceToHost, stream_));
+        p += b;
+    }
+    CK(cudaMemcpyAsync(p, P.tag, b, cudaMemcpyDeviceToHost, stream_));
+    p += b;
+    if (s->ntypes > 0)
+        CK(cudaMemcpyAsync(p, P.type, n * 4, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(stream_));
+}
+
+void Engine::restore(int id, const void* buf, size_t size) {
+    CK(cudaSetDevice(device_));
+    Slot* s = slot(id);
+    if (s->uploaded)
+        throw Error(ATVB_ERR_STATE, "restore into a system that was already uploaded");
+    if (!buf || size < sizeof(CkptHeader))
+        throw Error(ATVB_ERR_INVALID, "checkpoint too short");
+    CkptHeader h;
+    std::memcpy(&h, buf, sizeof(h));
+    if (std::memcmp(h.magic, kCkptMagic, 8) != 0 || h.version != kCkptVersion ||
+        h.header_bytes != sizeof(CkptHeader) || h.state_bytes != (int64_t)sizeof(SysState))
+        throw Error(ATVB_ERR_INVALID, "not a checkpoint of this library version");
+    SysParams& P = s->hp;
+    if (h.n != P.n || h.precision != P.prec || h.thermostat != P.thermostat ||
+        h.ntypes != s->ntypes)
+        throw Error(ATVB_ERR_INVALID,
+                    "checkpoint does not match the system (atoms, precision, "
+                    "integrator or LJ types)");
+    if (size < checkpoint_bytes(id))
+        throw Error(ATVB_ERR_INVALID, "checkpoint too short");
+    const size_t n = (size_t)P.n;
+    const char* p = (const char*)buf + sizeof(CkptHeader);
+    SysState st;
+    std::memcpy(&st, p, sizeof(st));
+    p += sizeof(SysState);
+    st.snap_count = 0; // snapshot rings belong to the running process
+    st.snap_slot = -1;
+    const double* a[kCkptArrays];
+    for (int k = 0; k < kCkptArrays; ++k) {
+        a[k] = (const double*)p;
+        p += n * 8;
+    }
+    const int64_t* tag = (const int64_t*)p;
+    p += n * 8;
+    std::vector<int32_t> type;
+    if (s->ntypes > 0) {
+        type.resize(n);
+        std::memcpy(type.data(), p, n * 4);
+    }
+    // 1. the positions and cell of the last neighbour build: the upload's
+    //    list build then reproduces the saved run's list
+    if (s->npt)
+        apply_box(P, st.Lb, true);
+    atvb_soa_view v;
+    std::memset(&v, 0, sizeof(v));
+    v.x = const_cast<double*>(a[9]);
+    v.y = const_cast<double*>(a[10]);
+    v.z = const_cast<double*>(a[11]);
+    v.vx = const_cast<double*>(a[3]);
+    v.vy = const_cast<double*>(a[4]);
+    v.vz = const_cast<double*>(a[5]);
+    v.fx = const_cast<double*>(a[6]);
+    v.fy = const_cast<double*>(a[7]);
+    v.fz = const_cast<double*>(a[8]);
+    v.mass = const_cast<double*>(a[12]);
+    v.charge = const_cast<double*>(a[13]);
+    v.tag = const_cast<int64_t*>(tag);
+    v.type = type.empty() ? nullptr : type.data();
+    upload(id, v);
+    // 2. the current cell, positions and state
+    if (s->npt) {
+        apply_box(P, st.box, true);
+        CK(cudaMemcpyAsync(d_sp_ + id, &P, sizeof(SysParams), cudaMemcpyHostToDevice,
+                           stream_));
+    }
+    const size_t b = n * 8;
+    CK(cudaMemcpyAsync(P.x, a[0], b, cudaMemcpyHostToDevice, stream_));
+    CK(cudaMemcpyAsync(P.y, a[1], b, cudaMemcpyHostToDevice, stream_));
+    CK(cudaMemcpyAsync(P.z, a[2], b, cudaMemcpyHostToDevice, stream_));
+    CK(cudaMemcpyAsync(P.xr, a[9], b, cudaMemcpyHostToDevice, stream_));
+    CK(cudaMemcpyAsync(P.yr, a[10], b, cudaMemcpyHostToDevice, stream_));
+    CK(cudaMemcpyAsync(P.zr, a[11], b, cudaMemcpyHostToDevice, stream_));
+    const LaunchCfg one = restricted_cfg(id);
+    launch_repack(one, stream_);
+    CK(cudaMemcpyAsync(P.st, &st, sizeof(st), cudaMemcpyHostToDevice, stream_));
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(stream_));
+    s->mean_row = h.mean_row;
+    dirty_ = true;
+}
+
+} // namespace atvb
+
+// ------------------------------------------------------ trajectory snapshots
+
+namespace atvb {
+
+void Engine::set_snapshots(int id, int every, int depth) {
+    CK(cudaSetDevice(device_));
+    Slot* s = slot(id);
+    if (every < 0 || (every > 0 && (depth < 1 || depth > 4096)))
+        throw Error(ATVB_ERR_INVALID, "snapshots: every >= 0 and depth in [1, 4096]");
+    CK(cudaStreamSynchronize(stream_));
+    release_graph();
+    if (s->snap_host) {
+        CK(cudaFreeHost(s->snap_host));
+        s->snap_host = nullptr;
+    }
+    SysParams& P = s->hp;
+    P.snap_ring = nullptr;
+    P.snap_every = 0;
+    P.snap_depth = 0;
+    if (every > 0) {
+        const size_t slot_bytes = sizeof(SnapHeader) + (size_t)P.n * 6 * sizeof(double);
+        void* h = nullptr;
+        CK(cudaHostAlloc(&h, slot_bytes * depth, cudaHostAllocMapped));
+        std::memset(h, 0, slot_bytes * depth);
+        void* d = nullptr;
+        CK(cudaHostGetDevicePointer(&d, h, 0));
+        s->snap_host = (char*)h;
+        P.snap_ring = (char*)d;
+        P.snap_every = every;
+        P.snap_depth = depth;
+        P.snap_slot_bytes = (long long)slot_bytes;
+    }
+    // the published count restarts with the ring
+    s->snap_read = 0;
+    if (s->uploaded) {
+        const long long zero = 0;
+        CK(cudaMemcpy(&P.st->snap_count, &zero, sizeof(zero), cudaMemcpyHostToDevice));
+    }
+    push_params(id);
+    dirty_ = true;
+}
+
+// Frames published since the last poll, oldest first, without waiting for
+// the device: a slot is taken when its seqlock shows the expected sequence
+// number before and after the copy; frames overwritten before they were
+// read are counted as dropped.
+int Engine::poll_snapshots(int id, int max_frames, int64_t* steps, double* box,
+                           double* const out[6], int64_t* dropped) {
+    Slot* s = slot(id);
+    if (!s->snap_host)
+        throw Error(ATVB_ERR_STATE, "snapshots are not enabled for this system");
+    const SysParams& P = s->hp;
+    const size_t n = (size_t)P.n, sb = (size_t)P.snap_slot_bytes;
+    int got = 0;
+    int64_t lost = 0;
+    while (got < max_frames) {
+        const long long want = s->snap_read + 1;
+        const char* base = s->snap_host + (size_t)((want - 1) % P.snap_depth) * sb;
+        const volatile SnapHeader* h = (const volatile SnapHeader*)base;
+        const long long end = h->end;
+        if (end < want)
+            break; // not published yet
+        if (end > want) {
+            // overwritten: skip to the oldest frame the ring still holds
+            const long long oldest = std::max(want + 1, end - P.snap_depth + 1);
+            lost += oldest - want;
+            s->snap_read = oldest - 1;
+            continue;
+        }
+        std::atomic_thread_fence(std::memory_order_acquire);
+        const int64_t step = h->step;
+        double bx[3] = {h->box[0], h->box[1], h->box[2]};
+        const double* d = (const double*)(base + sizeof(SnapHeader));
+        for (int f = 0; f < 6; ++f)
+            if (out[f])
+                std::memcpy(out[f] + (size_t)got * n, d + (size_t)f * n, n * sizeof(double));
+        std::atomic_thread_fence(std::memory_order_acquire);
+        if (h->begin != want) {
+            // overwritten while copying
+            lost += 1;
+            s->snap_read = want;
+            continue;
+        }
+        if (steps)
+            steps[got] = step;
+        if (box)
+            for (int a = 0; a < 3; ++a)
+                box[3 * got + a] = bx[a];
+        ++got;
+        s->snap_read = want;
+    }
+    if (dropped)
+        *dropped = lost;
+    return got;
 }
 
 } // namespace atvb

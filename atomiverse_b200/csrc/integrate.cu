@@ -523,7 +523,112 @@ __global__ void k_npt_prep(const int* sys_list, int nsys, const SysParams* sp) {
     npt_prepare(P, st, ke, one);
 }
 
+// Sorted position records from the master positions with the committed
+// cell's scales (a restored checkpoint: the list was rebuilt from the
+// positions of the last build, the atoms have moved on since).
+__global__ void k_repack(const Item* items, int nitems, const SysParams* sp) {
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const Item item = items[it];
+        const SysParams& P = sp[item.sys];
+        const int i = item.begin + threadIdx.x;
+        if (i >= P.n)
+            continue;
+        const int r = P.rank[i];
+        const double x[3] = {P.x[i], P.y[i], P.z[i]};
+        const double q = P.q[i];
+        if (P.prec == kMixed) {
+            int4 p;
+            p.x = (int)pos_fix(x[0], P.fix_scale[0]);
+            p.y = (int)pos_fix(x[1], P.fix_scale[1]);
+            p.z = (int)pos_fix(x[2], P.fix_scale[2]);
+            p.w = __float_as_int((float)q);
+            reinterpret_cast<int4*>(P.pos4)[r] = p;
+        } else {
+            reinterpret_cast<double4*>(P.pos4)[r] = pack_pos64(x, P.fix64_scale, q);
+        }
+    }
+}
+
+// Trajectory snapshots (the device-ordered freeze of
+// cuda/asynchronous/async_bridge.cuh, written straight into host-mapped
+// memory): after a step whose count is a multiple of snap_every, open a
+// ring slot, copy positions and velocities (with the pending scale, as a
+// download sees them), close the slot.  Kernel boundaries order the three
+// phases; the fences make each phase visible to the host before the next.
+__global__ void k_snap_open(const int* sys_list, int nsys, const SysParams* sp) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nsys)
+        return;
+    const SysParams& P = sp[sys_list[k]];
+    SysState* st = P.st;
+    st->snap_slot = -1;
+    if (!P.snap_ring || st->step % P.snap_every != 0)
+        return;
+    const int slot = (int)(st->snap_count % P.snap_depth);
+    SnapHeader* h = reinterpret_cast<SnapHeader*>(P.snap_ring + (size_t)slot * P.snap_slot_bytes);
+    *(volatile long long*)&h->begin = st->snap_count + 1;
+    __threadfence_system();
+    st->snap_slot = slot;
+}
+
+__global__ void k_snap_data(const Item* items, int nitems, const SysParams* sp) {
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const Item item = items[it];
+        const SysParams& P = sp[item.sys];
+        if (!P.snap_ring)
+            continue;
+        const SysState* st = P.st;
+        const int slot = st->snap_slot;
+        const int i = item.begin + threadIdx.x;
+        if (slot < 0 || i >= P.n)
+            continue;
+        double* d = reinterpret_cast<double*>(P.snap_ring + (size_t)slot * P.snap_slot_bytes +
+                                              sizeof(SnapHeader));
+        const size_t n = (size_t)P.n;
+        double s[3];
+        for (int a = 0; a < 3; ++a)
+            s[a] = P.thermostat == kNPT ? st->vs_out[a] : st->vscale;
+        d[i] = P.x[i];
+        d[n + i] = P.y[i];
+        d[2 * n + i] = P.z[i];
+        d[3 * n + i] = P.vx[i] * s[0];
+        d[4 * n + i] = P.vy[i] * s[1];
+        d[5 * n + i] = P.vz[i] * s[2];
+        __threadfence_system(); // payload visible to the host before the close
+    }
+}
+
+__global__ void k_snap_close(const int* sys_list, int nsys, const SysParams* sp) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nsys)
+        return;
+    const SysParams& P = sp[sys_list[k]];
+    SysState* st = P.st;
+    if (!P.snap_ring || st->snap_slot < 0)
+        return;
+    SnapHeader* h =
+        reinterpret_cast<SnapHeader*>(P.snap_ring + (size_t)st->snap_slot * P.snap_slot_bytes);
+    h->step = st->step;
+    for (int a = 0; a < 3; ++a)
+        h->box[a] = P.L[a];
+    __threadfence_system();
+    *(volatile long long*)&h->end = st->snap_count + 1;
+    __threadfence_system();
+    st->snap_count += 1;
+    st->snap_slot = -1;
+}
+
 static int sys_blocks(int nsys) { return (nsys + 127) / 128; }
+
+void launch_snapshots(const LaunchCfg& lc, cudaStream_t s) {
+    k_snap_open<<<sys_blocks(lc.nsys), 128, 0, s>>>(lc.sys_list, lc.nsys, lc.sp);
+    k_snap_data<<<lc.atoms.grid, kChunk, 0, s>>>(lc.atoms.d, lc.atoms.n, lc.sp);
+    k_snap_close<<<sys_blocks(lc.nsys), 128, 0, s>>>(lc.sys_list, lc.nsys, lc.sp);
+}
+
+void launch_repack(const LaunchCfg& lc, cudaStream_t s) {
+    k_repack<<<lc.atoms.grid, kChunk, 0, s>>>(lc.atoms.d, lc.atoms.n, lc.sp);
+}
 
 void launch_npt_prep(const LaunchCfg& lc, cudaStream_t s) {
     k_npt_kinetic<<<lc.atoms.grid, kChunk, 0, s>>>(lc.atoms.d, lc.atoms.n, lc.sp);

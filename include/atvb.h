@@ -209,6 +209,36 @@ int atvb_system_set_special_bonds(atvb_system* sys, const double lj[3],
  * skin)); a cell that shrinks further is held and flagged in
  * atvb_scalars.status (re-create the system from the current frame). */
 int atvb_system_set_npt(atvb_system* sys, const atvb_npt_desc* npt);
+/* Checkpoints (state I/O; the reference's resumable record is
+ * cpu/record/mrec.h MrecWriter::flush, a molrs Zarr store, and
+ * cpu/io/frame_writer.h write_frame_zarr): the whole resumable state of a
+ * system in one self-describing byte blob -- atom arrays, forces of the last
+ * force pass, positions and cell of the last neighbour build, thermostat /
+ * barostat chains, pending velocity scales, step and list counters.
+ * Restore into a freshly created system with the same description and the
+ * same set_lj_types / set_special_bonds / set_npt configuration, in place of
+ * its first upload; stepping on gives the same trajectory, bit for bit, as
+ * the saved run.  Layout: header (magic "ATVBCKP1", version, sizes), the
+ * state record, 14 arrays of n doubles (x y z vx vy vz fx fy fz, positions
+ * at the last build, mass, charge), n int64 tags, n int32 types if per-type
+ * LJ. */
+int atvb_system_checkpoint_size(atvb_system* sys, int64_t* bytes);
+int atvb_system_save(atvb_system* sys, void* buf, int64_t capacity);
+int atvb_system_restore(atvb_system* sys, const void* buf, int64_t size);
+/* Trajectory snapshots (the async snapshot ring of
+ * cuda/asynchronous/async_bridge.cuh; a recorder such as MrecRecorder or the
+ * XYZ writer consumes the frames): every `every` steps (0: off) the step
+ * graph writes positions and velocities (as a download reports them) into
+ * a ring of `depth` frames in host-mapped memory, behind a per-slot seqlock;
+ * the step stream never waits for the host.  atvb_system_snapshot_poll
+ * returns the frames published since the last poll, oldest first, without
+ * synchronising: each array holds max_frames x n doubles (frame-major, any
+ * may be NULL), steps[max_frames], box[3 * max_frames]; frames overwritten
+ * before they were polled are counted in *dropped. */
+int atvb_system_set_snapshots(atvb_system* sys, int32_t every, int32_t depth);
+int atvb_system_snapshot_poll(atvb_system* sys, int32_t max_frames, int64_t* steps,
+                              double* box, double* x, double* y, double* z, double* vx,
+                              double* vy, double* vz, int32_t* count, int64_t* dropped);
 /* Profiling: enable per-kernel-group CUDA events on subsequent steps. */
 int atvb_system_profile(atvb_system* sys, int32_t enable);
 int atvb_system_profile_read(atvb_system* sys, atvb_kernel_time* out,
@@ -232,6 +262,10 @@ int atvb_batch_download(atvb_batch* b, int32_t index, atvb_soa_view* frame,
 /* atvb_system_set_lj_types / _set_special_bonds for system `index` of a
  * batch, before that system's first upload. */
 /* atvb_system_set_npt for system `index` of a batch, before its first upload. */
+/* Checkpoints of system `index` of a batch (restore before its first upload). */
+int atvb_batch_checkpoint_size(atvb_batch* b, int32_t index, int64_t* bytes);
+int atvb_batch_save(atvb_batch* b, int32_t index, void* buf, int64_t capacity);
+int atvb_batch_restore(atvb_batch* b, int32_t index, const void* buf, int64_t size);
 int atvb_batch_set_npt(atvb_batch* b, int32_t index, const atvb_npt_desc* npt);
 int atvb_batch_set_lj_types(atvb_batch* b, int32_t index, int32_t ncoef,
                             const int32_t* type_i, const int32_t* type_j,

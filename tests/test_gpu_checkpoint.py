@@ -1,0 +1,95 @@
+"""Checkpoints (state I/O): save a system mid-run, restore it into a fresh
+system, step on -- the trajectory equals the one that never stopped, bit for
+bit, for every integrator and both precisions (neighbour rows, their order
+and the lane count are those of the saved run).  Bad blobs are refused."""
+import numpy as np
+import pytest
+
+KB = 8.617333262e-5
+KEYS = ("x", "y", "z", "vx", "vy", "vz", "fx", "fy", "fz")
+
+
+def _cases():
+    from atomiverse_b200 import workloads as W
+    from test_gpu_general import _water
+    out = []
+    d, f = W.rocksalt_melt(ncell=6, rc=5.5, grid=(20, 20, 20))          # NH + PME
+    out.append(("pme_nh_fp64", d, f, {}))
+    out.append(("pme_nh_mixed", dict(d, precision=1), f, {}))
+    d, f = W.lj_fcc(ncell=6, precision=1, thermostat=2, t_star=1.0)     # Langevin
+    out.append(("lj_langevin_mixed", d, f, {}))
+    d, f = W.lj_fcc(ncell=5, seed=11)    # hot enough for list rebuilds in 40 steps
+    npt = dict(T_target=1.44 / KB, tau_T=5.0, P_target=0.0, tau_P=50.0, dt=d["dt"])
+    out.append(("lj_npt_fp64", d, f, dict(npt=npt)))
+    out.append(("lj_npt_mixed", dict(d, precision=1), f, dict(npt=npt)))
+    d, f, coeffs, special = _water(m=8)
+    out.append(("water_general_fp64", dict(d, dt=0.5), f,
+                dict(lj_types=coeffs, special_bonds=special)))
+    return out
+
+
+CASES = _cases()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,desc,frame,opts", CASES, ids=[c[0] for c in CASES])
+def test_restore_continues_bit_for_bit(atvb, ctx, name, desc, frame, opts):
+    a = atvb.System(ctx, desc, frame, **opts)
+    a.compute_forces()
+    a.step(40)
+    oa, sa = a.download()
+    a.close()
+    b = atvb.System(ctx, desc, frame, **opts)
+    b.compute_forces()
+    b.step(15)
+    blob = b.save()
+    b.close()
+    c = atvb.System(ctx, desc, None, **opts)
+    c.restore(blob)
+    c.step(25)
+    oc, sc = c.download()
+    c.close()
+    for k in KEYS:
+        assert np.array_equal(oa[k], oc[k]), (name, k)
+    for k in ("step", "energy", "kinetic", "conserved", "rebuilds"):
+        assert sa[k] == sc[k], (name, k)
+    assert np.array_equal(sa["box"], sc["box"])
+    assert sa["rebuilds"] > 0
+
+
+@pytest.mark.gpu
+def test_batch_restore_and_bad_blobs(atvb, ctx):
+    from atomiverse_b200 import workloads as W
+    d1, f1 = W.lj_fcc(ncell=5, seed=7)
+    d2, f2 = W.rocksalt_melt(ncell=6, rc=5.5, grid=(20, 20, 20), precision=1)
+    s = atvb.System(ctx, d2, f2)
+    s.compute_forces()
+    s.step(10)
+    blob = s.save()
+    s.step(10)
+    want, _ = s.download()
+    s.close()
+    b = atvb.Batch(ctx, [(d1, f1), (d2, None)])
+    b.restore(1, blob)
+    b.step(10)
+    got, _ = b.download(1)
+    for k in KEYS:
+        assert np.array_equal(want[k], got[k]), k
+    with pytest.raises(atvb.AtvbError) as e:
+        b.restore(1, blob)                         # already running
+    assert e.value.code == 4
+    b.close()
+    other = atvb.System(ctx, d1)                   # different system
+    with pytest.raises(atvb.AtvbError) as e:
+        other.restore(blob)
+    assert e.value.code == 1
+    with pytest.raises(atvb.AtvbError):
+        other.restore(blob[:100])                  # truncated
+    bad = bytearray(blob)
+    bad[0:8] = b"NOTACKPT"
+    same = atvb.System(ctx, d2)
+    with pytest.raises(atvb.AtvbError):
+        same.restore(bytes(bad))
+    same.restore(blob)                             # the good one still works
+    other.close()
+    same.close()

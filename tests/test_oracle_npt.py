@@ -129,4 +129,5 @@ def test_pme_tables_follow_the_cell(orc):
     f1 = fresh.state()
     for k in ("fx", "fy", "fz"):
         assert np.array_equal(st[k], f1[k])
-    assert fresh.scalars()["e_recip"] == s.scalars()["e_recip"]
+    # energies: OpenMP reduction order may differ in the last bit
+    assert fresh.scalars()["e_recip"] == pytest.approx(s.scalars()["e_recip"], rel=1e-14)
