@@ -455,6 +455,31 @@ class Server:
                "scalars": scalars_dict(r.scalars)}
         return out, res
 
+    def keep_checkpoints(self, on: bool = True):
+        check(self.lib.atvb_server_keep_checkpoints(self._h, int(bool(on))))
+
+    def suspend(self, rid: int):
+        check(self.lib.atvb_server_suspend(self._h, int(rid)))
+
+    def resume(self, rid: int, more_steps: int):
+        check(self.lib.atvb_server_resume(self._h, int(rid), int(more_steps)))
+
+    def checkpoint(self, rid: int) -> bytes:
+        nb = C.c_int64()
+        check(self.lib.atvb_server_checkpoint(self._h, int(rid), None, 0, C.byref(nb)))
+        buf = C.create_string_buffer(nb.value)
+        check(self.lib.atvb_server_checkpoint(self._h, int(rid), buf, nb.value, C.byref(nb)))
+        return buf.raw
+
+    def submit_checkpoint(self, desc, blob: bytes, n_steps: int) -> int:
+        if isinstance(desc, dict):
+            desc = make_desc(**desc)
+        rid = C.c_int64()
+        check(self.lib.atvb_server_submit_checkpoint(self._h, C.byref(desc), blob, len(blob),
+                                                     int(n_steps), C.byref(rid)))
+        self.sizes[rid.value] = desc.n_atoms
+        return rid.value
+
     def stats(self) -> dict:
         q, r, d = C.c_int64(), C.c_int64(), C.c_int64()
         b = C.c_size_t()

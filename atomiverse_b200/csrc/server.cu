@@ -13,6 +13,7 @@
 // fixed-point sums flushed per work item), so a request's result is the same
 // alone and in the mix.
 #include <algorithm>
+#include <cstring>
 #include <chrono>
 #include <deque>
 #include <map>
@@ -37,7 +38,9 @@ struct Request {
     std::vector<int64_t> tag;
     int n_steps = 0;
     int steps_done = 0;
-    int state = 0; // 0 queued, 1 running, 2 done, 3 cancelled, 4 failed
+    int state = 0; // 0 queued, 1 running, 2 done, 3 cancelled, 4 failed, 5 suspended
+    std::vector<char> ckpt; // resumable state (suspended, kept, or submitted)
+    bool resume = false;    // admit from ckpt instead of the frame
     int slot = -1;
     size_t bytes = 0;
     double t_submit = 0, t_start = 0, t_done = 0;
@@ -70,6 +73,7 @@ struct atvb_server {
     int max_active = 0;
     size_t in_use = 0;
     int64_t max_atoms = 0;   // resident-atom cap (0: none)
+    bool keep_ckpt = false;  // finished requests keep a checkpoint (resumable)
     int64_t atoms_in_use = 0;
     int64_t next_id = 1;
     std::map<int64_t, Request> reqs;
@@ -106,8 +110,12 @@ struct atvb_server {
             }
             try {
                 r.slot = eng->add(r.desc);
-                eng->upload(r.slot, r.view());
-                eng->compute_forces_one(r.slot);
+                if (r.resume) {
+                    eng->restore(r.slot, r.ckpt.data(), r.ckpt.size());
+                } else {
+                    eng->upload(r.slot, r.view());
+                    eng->compute_forces_one(r.slot);
+                }
             } catch (const Error& e) {
                 if (r.slot >= 0 && eng->has(r.slot))
                     eng->remove(r.slot);
@@ -130,7 +138,14 @@ struct atvb_server {
         }
     }
 
-    void retire(Request& r, bool keep_frame) {
+    void save(Request& r) {
+        r.ckpt.resize(eng->checkpoint_bytes(r.slot));
+        eng->save(r.slot, r.ckpt.data(), r.ckpt.size());
+    }
+
+    void retire(Request& r, bool keep_frame, bool keep_state = false) {
+        if (keep_state)
+            save(r);
         if (keep_frame) {
             atvb_soa_view v = r.view();
             eng->download(r.slot, &v, &r.sc);
@@ -163,7 +178,7 @@ struct atvb_server {
         }
         for (int64_t id : done) {
             Request& r = get(id);
-            retire(r, true);
+            retire(r, true, keep_ckpt);
             r.state = 2;
             r.t_done = now();
         }
@@ -314,8 +329,8 @@ int atvb_server_collect(atvb_server* srv, int64_t id, atvb_soa_view* frame,
         if (!srv)
             throw Error(ATVB_ERR_INVALID, "server is NULL");
         Request& r = srv->get(id);
-        if (r.state != 2)
-            throw Error(ATVB_ERR_STATE, "request not finished");
+        if (r.state != 2 && r.state != 5)
+            throw Error(ATVB_ERR_STATE, "request not finished or suspended");
         const size_t n = r.x.size();
         auto cp = [&](double* dst, const std::vector<double>& src) {
             if (dst)
@@ -335,6 +350,103 @@ int atvb_server_collect(atvb_server* srv, int64_t id, atvb_soa_view* frame,
         if (out)
             fill_result(r, out);
         srv->reqs.erase(id);
+    });
+}
+
+int atvb_server_keep_checkpoints(atvb_server* srv, int32_t on) {
+    return sguard([&] {
+        if (!srv)
+            throw Error(ATVB_ERR_INVALID, "server is NULL");
+        srv->keep_ckpt = on != 0;
+    });
+}
+
+int atvb_server_suspend(atvb_server* srv, int64_t id) {
+    return sguard([&] {
+        if (!srv)
+            throw Error(ATVB_ERR_INVALID, "server is NULL");
+        Request& r = srv->get(id);
+        if (r.state != 1)
+            throw Error(ATVB_ERR_STATE, "only a running request can be suspended");
+        srv->retire(r, true, true);
+        r.state = 5;
+        r.t_done = srv->now();
+    });
+}
+
+int atvb_server_resume(atvb_server* srv, int64_t id, int32_t more_steps) {
+    return sguard([&] {
+        if (!srv)
+            throw Error(ATVB_ERR_INVALID, "server is NULL");
+        if (more_steps < 0)
+            throw Error(ATVB_ERR_INVALID, "more_steps must be >= 0");
+        Request& r = srv->get(id);
+        if (!((r.state == 5 || r.state == 2) && !r.ckpt.empty()))
+            throw Error(ATVB_ERR_STATE,
+                        "only a suspended request, or a finished one that kept its "
+                        "checkpoint, can be resumed");
+        r.n_steps = r.steps_done + more_steps;
+        r.resume = true;
+        r.state = 0;
+        r.t_submit = srv->now();
+        srv->queue.push_back(id);
+    });
+}
+
+int atvb_server_checkpoint(atvb_server* srv, int64_t id, void* buf, int64_t capacity,
+                           int64_t* size) {
+    return sguard([&] {
+        if (!srv)
+            throw Error(ATVB_ERR_INVALID, "server is NULL");
+        Request& r = srv->get(id);
+        size_t need;
+        if (r.state == 1)
+            need = srv->eng->checkpoint_bytes(r.slot);
+        else if (!r.ckpt.empty())
+            need = r.ckpt.size();
+        else
+            throw Error(ATVB_ERR_STATE, "request holds no state to checkpoint");
+        if (size)
+            *size = (int64_t)need;
+        if (!buf)
+            return;
+        if (capacity < (int64_t)need)
+            throw Error(ATVB_ERR_INVALID, "checkpoint buffer too small");
+        if (r.state == 1)
+            srv->eng->save(r.slot, buf, need);
+        else
+            std::memcpy(buf, r.ckpt.data(), need);
+    });
+}
+
+int atvb_server_submit_checkpoint(atvb_server* srv, const atvb_system_desc* desc,
+                                  const void* buf, int64_t size, int32_t n_steps,
+                                  int64_t* id) {
+    return sguard([&] {
+        if (!srv || !desc || !buf || size <= 0)
+            throw Error(ATVB_ERR_INVALID, "server/desc/checkpoint is NULL");
+        if (n_steps < 0)
+            throw Error(ATVB_ERR_INVALID, "n_steps must be >= 0");
+        atvb::make_geometry(*desc);
+        Request r;
+        r.id = srv->next_id++;
+        r.desc = *desc;
+        const int n = desc->n_atoms;
+        for (auto* v : {&r.x, &r.y, &r.z, &r.vx, &r.vy, &r.vz, &r.fx, &r.fy, &r.fz, &r.m, &r.q})
+            v->assign(n, 0.0);
+        r.tag.assign(n, 0);
+        r.ckpt.assign((const char*)buf, (const char*)buf + size);
+        r.resume = true;
+        r.n_steps = n_steps;
+        r.bytes = atvb::estimate_bytes(*desc);
+        if (r.bytes > srv->budget)
+            throw Error(ATVB_ERR_NOMEM, "request needs more than the whole budget");
+        r.t_submit = srv->now();
+        const int64_t rid = r.id;
+        srv->reqs.emplace(rid, std::move(r));
+        srv->queue.push_back(rid);
+        if (id)
+            *id = rid;
     });
 }
 

@@ -286,7 +286,8 @@ int atvb_batch_profile_read(atvb_batch* b, atvb_kernel_time* out,
 /* ---- server: continuous batching of MD segments ------------------------ */
 typedef struct atvb_request_result {
     int64_t id;
-    int32_t state;        /* 0 queued, 1 running, 2 done, 3 cancelled, 4 failed */
+    int32_t state;        /* 0 queued, 1 running, 2 done, 3 cancelled, 4 failed,
+                             5 suspended */
     int32_t steps_done;
     double t_submit, t_start, t_done; /* seconds on the server clock */
     atvb_scalars scalars;
@@ -316,6 +317,22 @@ int atvb_server_collect(atvb_server* srv, int64_t id, atvb_soa_view* frame,
                         atvb_request_result* out);
 int atvb_server_stats(atvb_server* srv, int64_t* queued, int64_t* running,
                       int64_t* done, size_t* bytes_in_use);
+/* Resumable segments (checkpoints, see atvb_system_save).  suspend: stop a
+ * running request, keep its state and frame (collect works), free its
+ * device memory.  resume: queue a suspended request -- or a finished one
+ * when keep_checkpoints is on -- for more_steps further steps; it continues
+ * bit for bit where it stopped.  checkpoint: the blob of a running,
+ * suspended or kept request (buf NULL: size only).  submit_checkpoint: a
+ * new request that resumes from a blob, e.g. one taken on another GPU or
+ * process (the desc must match the saved system). */
+int atvb_server_keep_checkpoints(atvb_server* srv, int32_t on);
+int atvb_server_suspend(atvb_server* srv, int64_t id);
+int atvb_server_resume(atvb_server* srv, int64_t id, int32_t more_steps);
+int atvb_server_checkpoint(atvb_server* srv, int64_t id, void* buf, int64_t capacity,
+                           int64_t* size);
+int atvb_server_submit_checkpoint(atvb_server* srv, const atvb_system_desc* desc,
+                                  const void* buf, int64_t size, int32_t n_steps,
+                                  int64_t* id);
 /* Device bytes one request of this shape holds while resident. */
 int atvb_request_bytes(const atvb_system_desc* desc, size_t* bytes);
 

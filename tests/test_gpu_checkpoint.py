@@ -93,3 +93,57 @@ def test_batch_restore_and_bad_blobs(atvb, ctx):
     same.restore(blob)                             # the good one still works
     other.close()
     same.close()
+
+
+@pytest.mark.gpu
+def test_server_resumable_segments(atvb, ctx):
+    """Serve a request in segments -- run, suspend, resume; keep a finished
+    request's state and extend it; move a running request to a second
+    server by checkpoint -- every path ends where one uninterrupted run of
+    the same steps ends, bit for bit."""
+    from atomiverse_b200 import workloads as W
+    d1, f1 = W.lj_fcc(ncell=5, seed=21, precision=1)
+    d2, f2 = W.rocksalt_melt(ncell=6, rc=5.5, grid=(20, 20, 20), precision=1)
+    ref = {}
+    for key, (d, f) in {"lj": (d1, f1), "melt": (d2, f2)}.items():
+        s = atvb.System(ctx, d, f)
+        s.compute_forces()
+        s.step(30)
+        ref[key] = s.download()[0]
+        s.close()
+    srv = atvb.Server(ctx, 1 << 34)
+    srv.keep_checkpoints(True)
+    a = srv.submit(d1, f1, 30)                    # one segment of 30
+    b = srv.submit(d2, f2, 12)                    # 12, then 18 more
+    c = srv.submit(d2, f2, 30)                    # suspended at 10, resumed
+    srv.tick(10)
+    srv.suspend(c)
+    assert srv.poll(c)["state"] == 5
+    srv.tick(2)
+    assert srv.poll(b)["state"] == 2
+    srv.resume(b, 18)
+    srv.resume(c, 20)
+    blob, done_at = None, 0
+    for _ in range(20):
+        srv.tick(6)
+        pa = srv.poll(a)
+        if blob is None and pa["state"] == 1 and pa["steps_done"] >= 15:
+            blob, done_at = srv.checkpoint(a), pa["steps_done"]   # a running request
+        if all(srv.poll(r)["state"] == 2 for r in (a, b, c)):
+            break
+    for rid, key in ((a, "lj"), (b, "melt"), (c, "melt")):
+        out, res = srv.collect(rid)
+        for k in KEYS:
+            assert np.array_equal(out[k], ref[key][k]), (rid, k)
+    assert blob is not None
+    srv2 = atvb.Server(ctx, 1 << 34)               # migrate: finish a's copy elsewhere
+    m = srv2.submit_checkpoint(d1, blob, 30 - done_at)
+    for _ in range(10):
+        srv2.tick(6)
+        if srv2.poll(m)["state"] == 2:
+            break
+    out, _ = srv2.collect(m)
+    for k in KEYS:
+        assert np.array_equal(out[k], ref["lj"][k]), k
+    srv.close()
+    srv2.close()
