@@ -137,18 +137,32 @@ ATVB_DEV void row_fp64(const SysParams& P, int s, int g, int G, PairAcc& acc) {
         dy = (double)(__double_as_longlong(pi.y) - __double_as_longlong(pj.y)) * s1;
         dz = (double)(__double_as_longlong(pi.z) - __double_as_longlong(pj.z)) * s2;
     };
+    // software pipeline: the positions of the next two entries and the row
+    // indices of the two after them are in flight while the current pair
+    // computes (the kernel waits on the gather, not on the FP64 pipe)
     int k = g;
+    int ja = k < nn ? __ldg(row + k) : 0;
+    int jb = k + G < nn ? __ldg(row + k + G) : 0;
+    double4 pa = pos[ja], pb = pos[jb];
+    {
+        const int kn = k + 2 * G;
+        ja = kn < nn ? __ldg(row + kn) : 0;
+        jb = kn + G < nn ? __ldg(row + kn + G) : 0;
+    }
     for (; k + G < nn; k += 2 * G) {
-        const int ja = __ldg(row + k), jb = __ldg(row + k + G);
-        const double4 pa = pos[ja], pb = pos[jb];
+        const double4 ca = pa, cb = pb;
+        pa = pos[ja];
+        pb = pos[jb];
+        const int kn = k + 4 * G;
+        ja = kn < nn ? __ldg(row + kn) : 0;
+        jb = kn + G < nn ? __ldg(row + kn + G) : 0;
         double dx, dy, dz;
-        sep(pa, dx, dy, dz);
-        pair_term<LJ, CO, VIR>(c, dx, dy, dz, pa.w, a, near);
-        sep(pb, dx, dy, dz);
-        pair_term<LJ, CO, VIR>(c, dx, dy, dz, pb.w, a, near);
+        sep(ca, dx, dy, dz);
+        pair_term<LJ, CO, VIR>(c, dx, dy, dz, ca.w, a, near);
+        sep(cb, dx, dy, dz);
+        pair_term<LJ, CO, VIR>(c, dx, dy, dz, cb.w, a, near);
     }
     if (k < nn) {
-        const double4 pa = pos[__ldg(row + k)];
         double dx, dy, dz;
         sep(pa, dx, dy, dz);
         pair_term<LJ, CO, VIR>(c, dx, dy, dz, pa.w, a, near);
@@ -205,17 +219,23 @@ ATVB_DEV void row_mixed(const SysParams& P, int s, int g, int G, PairAcc& acc) {
         dy = (float)(int)((unsigned)pi.y - (unsigned)pj.y) * sy;
         dz = (float)(int)((unsigned)pi.z - (unsigned)pj.z) * sz;
     };
-    // the next two entries are loaded while the current two are computed;
-    // an entry past the row end is the atom itself (r^2 = 0, never selected)
+    // software pipeline: the positions of the next two entries and the row
+    // indices of the two after them are loaded while the current two are
+    // computed; an entry past the row end is the atom itself (r^2 = 0,
+    // never selected)
     bool near;
     int n_near = 0;
     int k = g;
     int4 pa = pos[k < nn ? __ldg(row + k) : s];
     int4 pb = pos[k + G < nn ? __ldg(row + k + G) : s];
+    int ia = k + 2 * G < nn ? __ldg(row + k + 2 * G) : s;
+    int ib = k + 3 * G < nn ? __ldg(row + k + 3 * G) : s;
     for (; k < nn; k += 2 * G) {
-        const int kn = k + 2 * G;
-        const int4 na = pos[kn < nn ? __ldg(row + kn) : s];
-        const int4 nb = pos[kn + G < nn ? __ldg(row + kn + G) : s];
+        const int4 na = pos[ia];
+        const int4 nb = pos[ib];
+        const int kn = k + 4 * G;
+        ia = kn < nn ? __ldg(row + kn) : s;
+        ib = kn + G < nn ? __ldg(row + kn + G) : s;
         float dx, dy, dz;
         sep(pa, dx, dy, dz);
         pair_term<LJ, CO, VIR>(c, dx, dy, dz, __int_as_float(pa.w), a, near);

@@ -56,24 +56,36 @@ ATVB_DEV void row_general(const SysParams& P, int s, int g, PairAcc& acc) {
     c.alpha2 = MIXED ? (T)(P.coul_alpha2 * 1.4426950408889634) : (T)P.coul_alpha2;
     c.kqi = (T)(kQqr2e * qi);
     RowSums<T> a;
-    for (int k = g; k < nn; k += kGenLanes) {
-        const unsigned raw = __ldg(row + k);
+    // software pipeline: the position of the next entry and the row entry
+    // after it are loaded while the current pair computes (an entry past
+    // the row end is the atom itself, never computed)
+    using Pos = typename std::conditional<MIXED, int4, double4>::type;
+    const Pos* __restrict__ pos = reinterpret_cast<const Pos*>(P.pos4);
+    int k = g;
+    unsigned raw = k < nn ? __ldg(row + k) : (unsigned)s;
+    unsigned rawn = k + kGenLanes < nn ? __ldg(row + k + kGenLanes) : (unsigned)s;
+    Pos pj = pos[raw & kRowIdxMask];
+    for (; k < nn; k += kGenLanes) {
+        const Pos pn = pos[rawn & kRowIdxMask];
+        const unsigned rawnn =
+            k + 2 * kGenLanes < nn ? __ldg(row + k + 2 * kGenLanes) : (unsigned)s;
         const int j = (int)(raw & kRowIdxMask);
         const int cls = (int)(raw >> 30);
         T dx, dy, dz, qj;
-        if (MIXED) {
-            const int4 pj = reinterpret_cast<const int4*>(P.pos4)[j];
+        if constexpr (MIXED) {
             dx = (T)((float)(int)((unsigned)qi4.x - (unsigned)pj.x) * P.Lf_fix[0]);
             dy = (T)((float)(int)((unsigned)qi4.y - (unsigned)pj.y) * P.Lf_fix[1]);
             dz = (T)((float)(int)((unsigned)qi4.z - (unsigned)pj.z) * P.Lf_fix[2]);
             qj = (T)__int_as_float(pj.w);
         } else {
-            const double4 pj = reinterpret_cast<const double4*>(P.pos4)[j];
             dx = (T)((double)(__double_as_longlong(pi8.x) - __double_as_longlong(pj.x)) * P.Lfix64[0]);
             dy = (T)((double)(__double_as_longlong(pi8.y) - __double_as_longlong(pj.y)) * P.Lfix64[1]);
             dz = (T)((double)(__double_as_longlong(pi8.z) - __double_as_longlong(pj.z)) * P.Lfix64[2]);
             qj = (T)pj.w;
         }
+        raw = rawn;
+        rawn = rawnn;
+        pj = pn;
         const T r2 = dx * dx + dy * dy + dz * dz;
         const bool ok = r2 >= (T)kMinPair2;
         T rinv;

@@ -72,13 +72,21 @@ ATVB_DEV double rcp64(double v) {
 
 // erfcx(x) for 0 <= x <= 6 from the universal polynomial of erfcx_coef.h,
 // given t = 1 / (1 + kErfcxP x).  Coefficients are compile-time constants.
+// FP64: the even and odd coefficients as two Horner chains in u^2 (half
+// the dependency depth of one chain, one more operation), p = E + u O
 ATVB_DEV double erfcx_of_t(double t) {
     const double u = fma(kErfcxA, t, kErfcxB);
-    double p = kErfcxD[kErfcxD_N - 1];
+    const double v = u * u;
+    constexpr int NE = (kErfcxD_N + 1) / 2, NO = kErfcxD_N / 2;
+    double e = kErfcxD[2 * (NE - 1)];
+    double o = kErfcxD[2 * (NO - 1) + 1];
 #pragma unroll
-    for (int k = kErfcxD_N - 2; k >= 0; --k)
-        p = fma(p, u, kErfcxD[k]);
-    return p;
+    for (int k = NE - 2; k >= 0; --k)
+        e = fma(e, v, kErfcxD[2 * k]);
+#pragma unroll
+    for (int k = NO - 2; k >= 0; --k)
+        o = fma(o, v, kErfcxD[2 * k + 1]);
+    return fma(u, o, e);
 }
 ATVB_DEV float erfcx_of_t(float t) {
     const float u = fmaf((float)kErfcxA, t, (float)kErfcxB);
