@@ -34,32 +34,29 @@ ATVB_DEV float rsqrt_approx(float x) {
     return y;
 }
 
-// exp(-z) for z >= 0 in FP64 (Cody-Waite argument reduction): with
-// n = rint(-z / ln 2) and r = -z - n ln 2 (ln 2 split into a 32-bit head,
-// so n * head is exact, and a tail), |r| <= ln(2)/2 and
-// exp(-z) = 2^n exp(r), exp(r) by its Taylor series to degree 12
-// (truncation < 2e-16).  z is clamped at 708 (the result is then ~1e-308,
-// far below anything the callers keep).
+// exp(-z) for z >= 0 in FP64, table-driven (P. T. P. Tang, "Table-driven
+// implementation of the exponential function in IEEE floating-point
+// arithmetic", ACM TOMS 15 (1989) 144-157): n = rint(-z 64/ln2), r =
+// -z - n ln2/64 (ln2/64 split into a head whose products with n are exact
+// and a tail), |r| <= ln2/128, and exp(-z) = 2^(n div 64) 2^((n mod 64)/64)
+// exp(r) with 2^(j/64) from a 64-entry table and exp(r) by its Taylor
+// series to degree 5 (truncation < 4e-17).  z is clamped at 708 (the result
+// is then ~1e-308, far below anything the callers keep).
 ATVB_DEV double exp_neg64(double z) {
     const double w = -fmin(z, 708.0);
-    const double n = rint(w * 1.4426950408889634);
-    double r = fma(-n, 0.6931471803691238, w);
-    r = fma(-n, 1.9082149292705877e-10, r);
-    double p = 2.08767569878681e-09;
-    p = fma(p, r, 2.505210838544172e-08);
-    p = fma(p, r, 2.755731922398589e-07);
-    p = fma(p, r, 2.7557319223985893e-06);
-    p = fma(p, r, 2.48015873015873e-05);
-    p = fma(p, r, 0.0001984126984126984);
-    p = fma(p, r, 0.001388888888888889);
-    p = fma(p, r, 0.008333333333333333);
-    p = fma(p, r, 0.041666666666666664);
-    p = fma(p, r, 0.16666666666666666);
+    const double n = rint(w * kExp64ByLn2);
+    double r = fma(-n, kExpLn2By64Hi, w);
+    r = fma(-n, kExpLn2By64Lo, r);
+    double p = 1.0 / 120.0;
+    p = fma(p, r, 1.0 / 24.0);
+    p = fma(p, r, 1.0 / 6.0);
     p = fma(p, r, 0.5);
     p = fma(p, r, 1.0);
     p = fma(p, r, 1.0);
-    const long long e = (long long)((int)n + 1023) << 52; // n >= -1022
-    return p * __longlong_as_double(e);
+    const int ni = (int)n;
+    const double t = __ldg(kExp2Tab + (ni & 63));
+    const long long e = (long long)((ni >> 6) + 1023) << 52; // ni >> 6 >= -1022
+    return (t * p) * __longlong_as_double(e);
 }
 
 // 1 / v for 1 <= v <= 4 in FP64: FP32 estimate, two Newton steps

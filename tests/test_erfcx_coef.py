@@ -60,3 +60,30 @@ def test_erfc_from_erfcx_and_exp():
     got = np.exp(-x * x) * _horner(arrays["kErfcxD"], x, const["kErfcxP"], const["kErfcxA"],
                                    const["kErfcxB"], np.float64)
     assert np.max(np.abs(got / special.erfc(x) - 1)) < 1e-13
+
+
+def test_table_driven_exp_constants():
+    """exp_neg64's table (2^(j/64)) and split ln2/64, evaluated the way the
+    kernel does (Tang's table-driven reduction, degree-5 Taylor), stay
+    within 2 ulp of exp(-z) on [0, 708]; the head of ln2/64 has enough
+    trailing zero bits that n * head is exact."""
+    txt = open(HDR).read()
+    c = {k: float(v) for k, v in re.findall(r"constexpr double (kExp[A-Za-z0-9]+) = ([-0-9.e+]+);", txt)}
+    body = re.search(r"kExp2Tab\[64\] = \{(.*?)\};", txt, flags=re.S).group(1)
+    tab = np.array([float(v) for v in re.findall(r"[-0-9.e+]+", body)])
+    assert len(tab) == 64
+    assert np.allclose(tab, 2.0 ** (np.arange(64) / 64.0), rtol=2e-16, atol=0)
+    hi, lo, inv = c["kExpLn2By64Hi"], c["kExpLn2By64Lo"], c["kExp64ByLn2"]
+    m, _ = np.frexp(hi)
+    assert float(m * 2 ** 29).is_integer()           # <= 29 significant bits
+    assert abs((hi + lo) - np.log(2) / 64) < 1e-18
+    z = np.concatenate([np.linspace(0.0, 40.0, 200001), np.linspace(40.0, 700.0, 20001)])
+    w = -z
+    n = np.rint(w * inv)
+    r = (w - n * hi) - n * lo
+    p = np.full_like(r, 1.0 / 120.0)
+    for k in (1.0 / 24.0, 1.0 / 6.0, 0.5, 1.0, 1.0):
+        p = p * r + k
+    ni = n.astype(np.int64)
+    val = tab[ni & 63] * p * np.ldexp(1.0, ni >> 6)
+    assert np.max(np.abs(val / np.exp(-z) - 1.0)) < 5e-16   # 2 ulp incl. numpy's own exp
