@@ -141,6 +141,7 @@ struct SysParams {
     // real-space Coulomb
     int has_coul;
     double coul_rc2, coul_alpha, coul_alpha2;
+    int coul_short; // alpha * cutoff <= kErfcxSXmax: the short FP64 erfcx set
     // per-type LJ and special pairs: such systems take k_pair_general
     int general;          // 1: pair forces from k_pair_general
     int ntypes;           // 0: one LJ type (lj_* above)

@@ -385,6 +385,7 @@ Slot::Slot(const atvb_system_desc& d, const DevMem& mem) : desc(d), mem_(mem) {
         hp.coul_rc2 = d.coul_cutoff * d.coul_cutoff;
         hp.coul_alpha = d.coul_alpha;
         hp.coul_alpha2 = d.coul_alpha * d.coul_alpha;
+        hp.coul_short = d.coul_alpha * d.coul_cutoff <= kErfcxSXmax ? 1 : 0;
         // the pair kernels' erfcx polynomial covers alpha * r <= kErfcxXmax
         if (d.coul_alpha * d.coul_cutoff > kErfcxXmax)
             throw Error(ATVB_ERR_INVALID,

@@ -23,8 +23,9 @@
 // FP64 build: positions as 64-bit fixed point (2^64 steps per box edge,
 // so the wrapped integer difference is the exact minimum image) + FP64 q;
 // all arithmetic in double;
-// exp and the reciprocal of the erfcx variable are this file's own FP64
-// routines (Cody-Waite exp, Newton reciprocal), accurate to ~1 ulp.
+// exp and the reciprocal of the erfcx variable are this library's own FP64
+// routines (table-driven exp, Newton reciprocal), accurate to ~1 ulp;
+// systems with alpha * cutoff <= 3.2 take a shorter erfcx polynomial.
 // Mixed build: positions int4 {x, y, z fixed point with 2^32 steps per box
 // edge, q as float}; the integer difference is the exact minimum-image
 // separation, converted once to float; pair math in FP32 with the PTX
@@ -47,7 +48,7 @@ namespace atvb {
 // such pairs are queued and k_pair_fix settles them on the FP64 positions.
 // `force` >= 0 overrides the decisions (bit 0 LJ, bit 1 Coulomb) and `neg`
 // subtracts the term instead of adding it (k_pair_fix only).
-template <bool LJ, bool CO, bool VIR, typename T>
+template <bool LJ, bool CO, bool VIR, bool SHORT = false, typename T>
 ATVB_DEV void pair_term(const RowConst<T>& c, T dx, T dy, T dz, T qj,
                         RowSums<T>& a, bool& near, int force = -1, bool neg = false) {
     constexpr bool F = sizeof(T) == 4;
@@ -88,10 +89,14 @@ ATVB_DEV void pair_term(const RowConst<T>& c, T dx, T dy, T dz, T qj,
             t = rcp_approx(fmaf((float)kErfcxP, x, 1.0f));
             e = ex2_approx(-c.alpha2 * r2);
         } else {
-            t = rcp64(fma(kErfcxP, x, 1.0));
+            t = rcp64(fma(SHORT ? kErfcxSP : kErfcxP, x, 1.0));
             e = exp_neg64(c.alpha2 * r2);
         }
-        const T p = erfcx_of_t(t);
+        T p;
+        if constexpr (!F && SHORT)
+            p = erfcx_short_of_t(t);
+        else
+            p = erfcx_of_t(t);
         const T pref = qq * rinv * e;
         fpair += in_c ? pref * (p + (T)kEwaldF * x) * r2inv : T(0);
         a.ec += in_c ? sg * (pref * p) : T(0);
@@ -121,7 +126,7 @@ ATVB_DEV void pair_term(const RowConst<T>& c, T dx, T dy, T dz, T qj,
 
 // Row of sorted atom s, lanes g, g+G, ...: two entries per iteration so that
 // both index loads and both position gathers are in flight together.
-template <bool LJ, bool CO, bool VIR>
+template <bool LJ, bool CO, bool VIR, bool SHORT>
 ATVB_DEV void row_fp64(const SysParams& P, int s, int g, int G, PairAcc& acc) {
     const double4* __restrict__ pos = reinterpret_cast<const double4*>(P.pos4);
     const double4 pi = pos[s];
@@ -158,14 +163,14 @@ ATVB_DEV void row_fp64(const SysParams& P, int s, int g, int G, PairAcc& acc) {
         jb = kn + G < nn ? __ldg(row + kn + G) : 0;
         double dx, dy, dz;
         sep(ca, dx, dy, dz);
-        pair_term<LJ, CO, VIR>(c, dx, dy, dz, ca.w, a, near);
+        pair_term<LJ, CO, VIR, SHORT>(c, dx, dy, dz, ca.w, a, near);
         sep(cb, dx, dy, dz);
-        pair_term<LJ, CO, VIR>(c, dx, dy, dz, cb.w, a, near);
+        pair_term<LJ, CO, VIR, SHORT>(c, dx, dy, dz, cb.w, a, near);
     }
     if (k < nn) {
         double dx, dy, dz;
         sep(pa, dx, dy, dz);
-        pair_term<LJ, CO, VIR>(c, dx, dy, dz, pa.w, a, near);
+        pair_term<LJ, CO, VIR, SHORT>(c, dx, dy, dz, pa.w, a, near);
     }
     finish_row(a, acc, VIR);
 }
@@ -261,8 +266,10 @@ ATVB_DEV void row(const SysParams& P, int s, int g, int G, PairAcc& a) {
             row_mixed<LJ, CO, VIR, true>(P, s, g, G, a);
         else
             row_mixed<LJ, CO, VIR, false>(P, s, g, G, a);
+    } else if (CO && P.coul_short) {
+        row_fp64<LJ, CO, VIR, true>(P, s, g, G, a);
     } else {
-        row_fp64<LJ, CO, VIR>(P, s, g, G, a);
+        row_fp64<LJ, CO, VIR, false>(P, s, g, G, a);
     }
 }
 

@@ -85,6 +85,22 @@ ATVB_DEV double erfcx_of_t(double t) {
         o = fma(o, v, kErfcxD[2 * k + 1]);
     return fma(u, o, e);
 }
+// the short-range FP64 set (systems with alpha * cutoff <= kErfcxSXmax):
+// t = 1 / (1 + kErfcxSP x), five fewer terms
+ATVB_DEV double erfcx_short_of_t(double t) {
+    const double u = fma(kErfcxSA, t, kErfcxSB);
+    const double v = u * u;
+    constexpr int NE = (kErfcxS_N + 1) / 2, NO = kErfcxS_N / 2;
+    double e = kErfcxS[2 * (NE - 1)];
+    double o = kErfcxS[2 * (NO - 1) + 1];
+#pragma unroll
+    for (int k = NE - 2; k >= 0; --k)
+        e = fma(e, v, kErfcxS[2 * k]);
+#pragma unroll
+    for (int k = NO - 2; k >= 0; --k)
+        o = fma(o, v, kErfcxS[2 * k + 1]);
+    return fma(u, o, e);
+}
 ATVB_DEV float erfcx_of_t(float t) {
     const float u = fmaf((float)kErfcxA, t, (float)kErfcxB);
     float p = kErfcxF[kErfcxF_N - 1];

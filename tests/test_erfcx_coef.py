@@ -87,3 +87,27 @@ def test_table_driven_exp_constants():
     ni = n.astype(np.int64)
     val = tab[ni & 63] * p * np.ldexp(1.0, ni >> 6)
     assert np.max(np.abs(val / np.exp(-z) - 1.0)) < 5e-16   # 2 ulp incl. numpy's own exp
+
+
+def test_short_range_erfcx_set_matches_scipy():
+    """The short FP64 set (alpha * cutoff <= 3.2) evaluated as the kernel
+    does (even/odd Horner chains in u^2) stays within 2e-15 of SciPy."""
+    special = pytest.importorskip("scipy.special")
+    txt = open(HDR).read()
+    c = {k: float(v) for k, v in re.findall(r"constexpr double (kErfcxS[A-Za-z]+) = ([-0-9.e+]+);", txt)}
+    body = re.search(r"kErfcxS\[\d+\] = \{(.*?)\};", txt, flags=re.S).group(1)
+    cs = np.array([float(v) for v in re.findall(r"[-0-9.e+]+", body)])
+    x = np.linspace(0.0, c["kErfcxSXmax"], 50001)
+    t = 1.0 / (1.0 + c["kErfcxSP"] * x)
+    u = c["kErfcxSA"] * t + c["kErfcxSB"]
+    v = u * u
+    ce, co = cs[0::2], cs[1::2]
+    e = np.full_like(u, ce[-1])
+    for k in range(len(ce) - 2, -1, -1):
+        e = e * v + ce[k]
+    o = np.full_like(u, co[-1])
+    for k in range(len(co) - 2, -1, -1):
+        o = o * v + co[k]
+    got = e + u * o
+    assert np.max(np.abs(got / special.erfcx(x) - 1.0)) < 2e-15
+    assert len(cs) < 20                      # shorter than the full-range set
