@@ -74,9 +74,17 @@ ATVB_DEV void pair_term(const RowConst<T>& c, T dx, T dy, T dz, T qj,
     const T sg = neg ? T(-1) : T(1);
     T fpair = 0;
     if (LJ) {
-        const T r6 = r2inv * r2inv * r2inv * c.sig6;
-        const T flj = c.eps24 * r2inv * r6 * (T(2) * r6 - T(1));
-        const T elj = c.eps4 * r6 * (r6 - T(1)) - c.shift;
+        T flj, elj;
+        if constexpr (F) {
+            const T r6 = r2inv * r2inv * r2inv * c.sig6;
+            flj = c.eps24 * r2inv * r6 * (T(2) * r6 - T(1));
+            elj = c.eps4 * r6 * (r6 - T(1)) - c.shift;
+        } else {
+            // folded constants: four fewer FP64 operations
+            const T r6 = r2inv * r2inv * r2inv;
+            flj = (r2inv * r6) * fma(c.lj1, r6, -c.lj2);
+            elj = fma(r6, fma(c.lj3, r6, -c.lj4), -c.shift);
+        }
         fpair = in_lj ? flj : T(0);
         a.elj += in_lj ? sg * elj : T(0);
     }
@@ -98,7 +106,13 @@ ATVB_DEV void pair_term(const RowConst<T>& c, T dx, T dy, T dz, T qj,
         else
             p = erfcx_of_t(t);
         const T pref = qq * rinv * e;
-        fpair += in_c ? pref * (p + (T)kEwaldF * x) * r2inv : T(0);
+        const T fc = pref * (p + (T)kEwaldF * x) * r2inv;
+        // a plain rounded add: never fused with the product above, so every
+        // instantiation (lane count) rounds each pair force the same way
+        if constexpr (F)
+            fpair = __fadd_rn(fpair, in_c ? fc : T(0));
+        else
+            fpair = __dadd_rn(fpair, in_c ? fc : T(0));
         a.ec += in_c ? sg * (pref * p) : T(0);
     }
     const T fxp = fpair * dx, fyp = fpair * dy, fzp = fpair * dz;

@@ -113,7 +113,11 @@ ATVB_DEV float erfcx_of_t(float t) {
 // Per-row constants of one system, hoisted out of the pair loop.
 template <typename T>
 struct RowConst {
-    T lj_rc2, sig6, eps4, eps24, shift;
+    // shifted LJ with folded constants (r6 = 1/r^6): F/r = r6 (lj1 r6 - lj2) / r^2,
+    // E = r6 (lj3 r6 - lj4) - shift; lj1 = 48 eps sigma^12, lj2 = 24 eps sigma^6,
+    // lj3 = 4 eps sigma^12, lj4 = 4 eps sigma^6
+    T lj_rc2, lj1, lj2, lj3, lj4, shift;
+    T sig6, eps4, eps24; // the unfolded form (FP32 build)
     T c_rc2, alpha, alpha2; // alpha2: alpha^2 (FP64) or alpha^2 log2(e) (FP32)
     T kqi;
     T band_lj, band_c; // FP32 only: error band of r^2 around each cutoff
@@ -155,10 +159,14 @@ template <typename T>
 ATVB_DEV RowConst<T> row_const(const SysParams& P, double qi) {
     RowConst<T> c;
     c.lj_rc2 = (T)P.lj_rc2;
+    c.lj1 = (T)(2.0 * P.lj_eps24 * P.lj_sig6 * P.lj_sig6);
+    c.lj2 = (T)(P.lj_eps24 * P.lj_sig6);
+    c.lj3 = (T)(P.lj_eps4 * P.lj_sig6 * P.lj_sig6);
+    c.lj4 = (T)(P.lj_eps4 * P.lj_sig6);
+    c.shift = (T)P.lj_shift;
     c.sig6 = (T)P.lj_sig6;
     c.eps4 = (T)P.lj_eps4;
     c.eps24 = (T)P.lj_eps24;
-    c.shift = (T)P.lj_shift;
     c.c_rc2 = (T)P.coul_rc2;
     c.alpha = (T)P.coul_alpha;
     c.alpha2 = sizeof(T) == 4 ? (T)(P.coul_alpha2 * 1.4426950408889634) : (T)P.coul_alpha2;
