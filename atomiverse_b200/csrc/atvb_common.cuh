@@ -192,6 +192,7 @@ struct SysParams {
     double4* posd4;  // FP64 sorted positions used by the pair-set test
     int4* lpos;      // fixed-point sorted positions at the last build (prefilter)
     double4* f4;     // forces in sorted order
+    double4* fp4;    // PME reciprocal forces of this step (sorted; PME systems)
     int *perm, *rank, *cell_of, *slot, *cell_count, *cell_start, *cellS;
     int *nbr, *nnbr;
     // PME buffers

@@ -159,7 +159,7 @@ class Engine {
     void release_plans(Slot& s);
     FftPlans& shape_plans(const Slot& s);
     void ensure_lane_plan(const Slot& s, int lane);
-    void exec_fft(const std::vector<int>& pme, bool forward);
+    void exec_fft(const std::vector<int>& pme, bool forward, cudaStream_t base);
     void ensure_table();
     void push_params(int id);
     void build_lists();
@@ -170,7 +170,7 @@ class Engine {
     LaunchCfg restricted_cfg(int id);
     void enqueue_step(bool profile);
     void enqueue_forces(const LaunchCfg& lc, const std::vector<int>& pme,
-                        bool profile);
+                        bool profile, bool overlap);
     void prof_mark(bool profile, const char* next);
     void collect_profile();
     void release_graph();
@@ -185,6 +185,7 @@ class Engine {
     uint64_t plan_clock_ = 0;
     cudaStream_t fft_streams_[kFftLanes] = {};
     cudaEvent_t fft_fork_ = nullptr, fft_join_[kFftLanes] = {};
+    cudaEvent_t pme_fork_ = nullptr, pme_join_ = nullptr; // PME beside the pair kernel
     int num_sms_ = 148;
     std::vector<std::unique_ptr<Slot>> slots_;
     SysParams* d_sp_ = nullptr;

@@ -68,6 +68,7 @@ void launch_state_out(const LaunchCfg& lc, int what, cudaStream_t s);
 void launch_npt_prep(const LaunchCfg& lc, cudaStream_t s);
 void launch_repack(const LaunchCfg& lc, cudaStream_t s);
 void launch_snapshots(const LaunchCfg& lc, cudaStream_t s);
+void launch_force_combine(const LaunchCfg& lc, cudaStream_t s);
 void launch_kinetic(const LaunchCfg& lc, cudaStream_t s);
 
 } // namespace atvb

@@ -480,6 +480,7 @@ Slot::Slot(const atvb_system_desc& d, const DevMem& mem) : desc(d), mem_(mem) {
         const size_t K0 = hp.K[0], K1 = hp.K[1], K2 = hp.K[2], Kh = hp.Kh;
         const size_t nt = K0 * K1 * K2, nh = K0 * K1 * Kh;
         const size_t rs = hp.prec == kMixed ? 4 : 8;
+        hp.fp4 = (double4*)dalloc((size_t)n * sizeof(double4));
         hp.grid_fix = (unsigned long long*)dalloc(nt * 8);
         CK(cudaMemsetAsync(hp.grid_fix, 0, nt * 8, stream));
         hp.grid_real = dalloc(nt * rs);
@@ -521,6 +522,8 @@ Engine::Engine(int device) : device_(device) {
         CK(cudaEventCreateWithFlags(&fft_join_[l], cudaEventDisableTiming));
     }
     CK(cudaEventCreateWithFlags(&fft_fork_, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&pme_fork_, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&pme_join_, cudaEventDisableTiming));
 }
 
 constexpr int kPlanCacheIdle = 16;
@@ -598,7 +601,7 @@ void Engine::release_plans(Slot& s) {
 // back, so small transforms run side by side; inside a captured step the
 // fork and join become parallel branches of the graph.  Every system keeps
 // its own single-grid plan, so its numbers do not depend on the others.
-void Engine::exec_fft(const std::vector<int>& pme, bool forward) {
+void Engine::exec_fft(const std::vector<int>& pme, bool forward, cudaStream_t base) {
     auto run = [&](const Slot& sl, int lane) {
         const FftPlans& p = plans_.at(shape_key(sl));
         const bool mixed = sl.hp.prec == kMixed;
@@ -618,19 +621,24 @@ void Engine::exec_fft(const std::vector<int>& pme, bool forward) {
                                  (cufftDoubleReal*)sl.hp.grid_real));
         }
     };
+    // base: the engine stream, or lane 0 when the PME chain runs beside the
+    // pair kernel (its plans are bound to that lane)
     if (pme.size() == 1) {
-        run(*slots_[pme[0]], kFftLanes);
+        run(*slots_[pme[0]], base == stream_ ? kFftLanes : 0);
         return;
     }
     const int used = (int)std::min<size_t>(pme.size(), kFftLanes);
-    CK(cudaEventRecord(fft_fork_, stream_));
+    CK(cudaEventRecord(fft_fork_, base));
     for (int l = 0; l < used; ++l)
-        CK(cudaStreamWaitEvent(fft_streams_[l], fft_fork_, 0));
+        if (fft_streams_[l] != base)
+            CK(cudaStreamWaitEvent(fft_streams_[l], fft_fork_, 0));
     for (size_t q = 0; q < pme.size(); ++q)
         run(*slots_[pme[q]], (int)(q % kFftLanes));
     for (int l = 0; l < used; ++l) {
+        if (fft_streams_[l] == base)
+            continue;
         CK(cudaEventRecord(fft_join_[l], fft_streams_[l]));
-        CK(cudaStreamWaitEvent(stream_, fft_join_[l], 0));
+        CK(cudaStreamWaitEvent(base, fft_join_[l], 0));
     }
 }
 
@@ -657,6 +665,10 @@ Engine::~Engine() {
     }
     if (fft_fork_)
         cudaEventDestroy(fft_fork_);
+    if (pme_fork_)
+        cudaEventDestroy(pme_fork_);
+    if (pme_join_)
+        cudaEventDestroy(pme_join_);
     if (mem_.pool)
         cudaMemPoolDestroy(mem_.pool);
     for (auto& e : prof_events_)
@@ -875,8 +887,7 @@ void Engine::build_lists() {
     for (size_t q = 0; q < pme_slots_.size(); ++q) {
         const Slot& sl = *slots_[pme_slots_[q]];
         ensure_lane_plan(sl, kFftLanes);
-        if (pme_slots_.size() > 1)
-            ensure_lane_plan(sl, (int)(q % kFftLanes));
+        ensure_lane_plan(sl, (int)(q % kFftLanes));
     }
     lc_.pme_mixed = pme_prec == kMixed ? 1 : 0;
     lc_.pme_order = pme_order > 0 ? pme_order : 4;
@@ -904,27 +915,42 @@ int64_t Engine::kernels_per_step() const {
     return k;
 }
 
+// Pair forces and the PME chain.  `overlap`: the PME chain (spread, FFTs,
+// influence, gather into fp4) runs on lane 0 beside the pair kernel -- the
+// pair kernel is arithmetic-bound, the PME kernels memory- and
+// atomic-bound -- and joins before the next atom pass; otherwise (profiling,
+// force passes) everything runs in order on the engine stream.
 void Engine::enqueue_forces(const LaunchCfg& lc, const std::vector<int>& pme,
-                            bool profile) {
+                            bool profile, bool overlap) {
+    const bool side = overlap && !profile && !pme.empty();
+    cudaStream_t ps = side ? fft_streams_[0] : stream_;
+    if (side) {
+        CK(cudaEventRecord(pme_fork_, stream_));
+        CK(cudaStreamWaitEvent(ps, pme_fork_, 0));
+    }
+    if (!pme.empty()) {
+        prof_mark(profile, "pme_spread");
+        launch_pme_spread(lc, ps);
+        prof_mark(profile, "pme_convert");
+        launch_pme_convert(lc, ps);
+        prof_mark(profile, "pme_fft_fwd");
+        exec_fft(pme, true, ps);
+        prof_mark(profile, "pme_influence");
+        launch_pme_influence(lc, ps);
+        prof_mark(profile, "pme_fft_inv");
+        exec_fft(pme, false, ps);
+        prof_mark(profile, "pme_gather");
+        launch_pme_gather(lc, ps);
+    }
     prof_mark(profile, "pair");
     launch_pair(lc, stream_);
     if (lc.any_near) {
         prof_mark(profile, "pair_fix");
         launch_pair_fix(lc, stream_);
     }
-    if (!pme.empty()) {
-        prof_mark(profile, "pme_spread");
-        launch_pme_spread(lc, stream_);
-        prof_mark(profile, "pme_convert");
-        launch_pme_convert(lc, stream_);
-        prof_mark(profile, "pme_fft_fwd");
-        exec_fft(pme, true);
-        prof_mark(profile, "pme_influence");
-        launch_pme_influence(lc, stream_);
-        prof_mark(profile, "pme_fft_inv");
-        exec_fft(pme, false);
-        prof_mark(profile, "pme_gather");
-        launch_pme_gather(lc, stream_);
+    if (side) {
+        CK(cudaEventRecord(pme_join_, ps));
+        CK(cudaStreamWaitEvent(stream_, pme_join_, 0));
     }
 }
 
@@ -934,7 +960,7 @@ void Engine::enqueue_step(bool profile) {
     launch_sys_a(lc_, stream_);
     prof_mark(profile, "neighbor");
     launch_rebuild(lc_, stream_);
-    enqueue_forces(lc_, pme_slots_, profile);
+    enqueue_forces(lc_, pme_slots_, profile, true);
     prof_mark(profile, "integrate_b");
     launch_integrate_b(lc_, stream_);
     launch_sys_b(lc_, stream_);
@@ -1054,7 +1080,8 @@ void Engine::compute_forces() {
     CK(cudaSetDevice(device_));
     ensure_ready();
     sized_rebuild(lc_);
-    enqueue_forces(lc_, pme_slots_, false);
+    enqueue_forces(lc_, pme_slots_, false, false);
+    launch_force_combine(lc_, stream_);
     launch_sys_energy(lc_, stream_);
     launch_npt_prep(lc_, stream_);
     CK(cudaGetLastError());
@@ -1071,7 +1098,8 @@ void Engine::compute_forces_one(int id) {
     std::vector<int> pme;
     if (slot(id)->hp.has_pme)
         pme.push_back(id);
-    enqueue_forces(one, pme, false);
+    enqueue_forces(one, pme, false, false);
+    launch_force_combine(one, stream_);
     launch_sys_energy(one, stream_);
     launch_npt_prep(one, stream_);
     CK(cudaGetLastError());

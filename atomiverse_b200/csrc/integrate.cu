@@ -226,6 +226,15 @@ __global__ void __launch_bounds__(kChunk)
             const double m = P.mass[i];
             double v[3] = {__dmul_rn(P.vx[i], sc), __dmul_rn(P.vy[i], sc),
                            __dmul_rn(P.vz[i], sc)};
+            if (P.has_pme) {
+                // pair + reciprocal forces; the sum is the step's force
+                const double4 g = P.fp4[r];
+                f.x = __dadd_rn(f.x, g.x);
+                f.y = __dadd_rn(f.y, g.y);
+                f.z = __dadd_rn(f.z, g.z);
+                if (P.thermostat != kLangevin)
+                    P.f4[r] = f;
+            }
             if (P.thermostat == kLangevin) {
                 const unsigned long long base =
                     (unsigned long long)P.seed * 0x9E3779B97F4A7C15ull +
@@ -618,7 +627,29 @@ __global__ void k_snap_close(const int* sys_list, int nsys, const SysParams* sp)
     st->snap_slot = -1;
 }
 
+// After a force pass outside the step: pair + reciprocal forces into f4.
+__global__ void k_force_combine(const Item* items, int nitems, const SysParams* sp) {
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const Item item = items[it];
+        const SysParams& P = sp[item.sys];
+        const int i = item.begin + threadIdx.x;
+        if (!P.has_pme || i >= P.n)
+            continue;
+        const int r = P.rank[i];
+        double4 f = P.f4[r];
+        const double4 g = P.fp4[r];
+        f.x = __dadd_rn(f.x, g.x);
+        f.y = __dadd_rn(f.y, g.y);
+        f.z = __dadd_rn(f.z, g.z);
+        P.f4[r] = f;
+    }
+}
+
 static int sys_blocks(int nsys) { return (nsys + 127) / 128; }
+
+void launch_force_combine(const LaunchCfg& lc, cudaStream_t s) {
+    k_force_combine<<<lc.atoms.grid, kChunk, 0, s>>>(lc.atoms.d, lc.atoms.n, lc.sp);
+}
 
 void launch_snapshots(const LaunchCfg& lc, cudaStream_t s) {
     k_snap_open<<<sys_blocks(lc.nsys), 128, 0, s>>>(lc.sys_list, lc.nsys, lc.sp);

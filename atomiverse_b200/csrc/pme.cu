@@ -290,12 +290,9 @@ __global__ void __launch_bounds__(256)
             fy = pref * ((double)g1s * P.K[1] * P.invL[1]);
             fz = pref * ((double)g2s * P.K[2] * P.invL[2]);
         }
-        // the pair kernel has written f4 for every system this step
-        double4 f = P.f4[s];
-        f.x += fx;
-        f.y += fy;
-        f.z += fz;
-        P.f4[s] = f;
+        // reciprocal-space forces go to their own buffer, so this chain can
+        // run beside the pair kernel; the next atom pass adds them
+        P.fp4[s] = make_double4(fx, fy, fz, 0.0);
     }
 }
 
