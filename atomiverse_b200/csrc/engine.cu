@@ -146,11 +146,17 @@ Geometry make_geometry(const atvb_system_desc& d, double shrink) {
         Lp[k] = g.L[k] * (1.0 - shrink);
         g.Lmin[k] = Lp[k];
     }
-    // Bins of at least a third of the list radius (reach 3), finer than the
-    // reference's half-reach bins (cell_list.cpp:112-121, reach :186-191):
-    // fewer candidates per atom.  The pair set does not depend on the bins.
+    // Bins of at least rlist / reach.  Reach 3 (finer than the reference's
+    // half-reach bins, cell_list.cpp:112-121, reach :186-191) gives the
+    // fewest candidates per atom; the list kernel spends a warp per bin, so
+    // sparse systems (few atoms per bin, e.g. reduced-unit LJ with a short
+    // list radius) take coarser bins that amortise the per-bin stencil work.
+    // The pair set does not depend on the bins.
+    const double density = d.n_atoms / (Lp[0] * Lp[1] * Lp[2]);
+    auto per_bin = [&](double reach) { return density * std::pow(g.rlist / reach, 3.0); };
+    const double reach_t = per_bin(3.0) >= 2.5 ? 3.0 : (per_bin(2.0) >= 1.5 ? 2.0 : 1.0);
     for (int k = 0; k < 3; ++k) {
-        int c = (int)std::floor(Lp[k] / (g.rlist / 3.0));
+        int c = (int)std::floor(Lp[k] / (g.rlist / reach_t));
         g.nc[k] = c < 1 ? 1 : c;
         g.cs[k] = Lp[k] / g.nc[k];
         int r = (int)std::ceil(g.rlist / g.cs[k] - 1e-12);

@@ -339,16 +339,18 @@ __global__ void __launch_bounds__(256)
                         const float rz = (float)(int)((unsigned)qj.z - (unsigned)org.z) * sz;
                         // two atoms of the cell per pass: their screens,
                         // votes and appends are independent, so their
-                        // latencies overlap
-                        for (int ii = 0; ii < ni; ii += 2) {
-                            const int i1 = ii + 1 < ni ? ii + 1 : ii;
+                        // latencies overlap; an odd last atom takes the
+                        // one-atom pass (sparse cells hold one atom or two)
+                        int ii = 0;
+                        for (; ii + 1 < ni; ii += 2) {
+                            const int i1 = ii + 1;
                             const float4 ra = sr[warp][ii], rb = sr[warp][i1];
                             const float ax = ra.x - rx, ay = ra.y - ry, az = ra.z - rz;
                             const float bx = rb.x - rx, by = rb.y - ry, bz = rb.z - rz;
                             const float r2a = ax * ax + ay * ay + az * az;
                             const float r2b = bx * bx + by * by + bz * bz;
                             const bool va = live && j != i0 + ii;
-                            const bool vb = live && ii + 1 < ni && j != i0 + i1;
+                            const bool vb = live && j != i0 + i1;
                             bool ha = va && r2a < flo, hb = vb && r2b < flo;
                             const bool aa = va && !(r2a < flo) && r2a < fhi;
                             const bool ab = vb && !(r2b < flo) && r2b < fhi;
@@ -381,8 +383,34 @@ __global__ void __launch_bounds__(256)
                                 }
                                 if (lane == ii)
                                     cnt += __popc(ma);
-                                if (lane == i1 && ii + 1 < ni)
+                                if (lane == i1)
                                     cnt += __popc(mb);
+                            }
+                        }
+                        if (ii < ni) {
+                            const float4 ri = sr[warp][ii];
+                            const float dx = ri.x - rx, dy = ri.y - ry, dz = ri.z - rz;
+                            const float r2f = dx * dx + dy * dy + dz * dz;
+                            const bool valid = live && j != i0 + ii;
+                            bool hit = valid && r2f < flo;
+                            const bool amb = valid && !(r2f < flo) && r2f < fhi;
+                            if (__any_sync(full, amb)) {
+                                if (amb)
+                                    hit = exact_r2(pos[i0 + ii], pos[j], L, hL) < rl2;
+                            }
+                            const unsigned m = __ballot_sync(full, hit);
+                            if (m) {
+                                const int base = __shfl_sync(full, cnt, ii);
+                                if (hit) {
+                                    const int wpos = base + __popc(m & lt);
+                                    unsigned e = (unsigned)j;
+                                    if (P.has_special)
+                                        e |= special_class(P, i0 + ii, j) << 30;
+                                    if (wpos < cap)
+                                        P.nbr[(size_t)(i0 + ii) * cap + wpos] = (int)e;
+                                }
+                                if (lane == ii)
+                                    cnt += __popc(m);
                             }
                         }
                     } else {
