@@ -148,13 +148,15 @@ Geometry make_geometry(const atvb_system_desc& d, double shrink) {
     }
     // Bins of at least rlist / reach.  Reach 3 (finer than the reference's
     // half-reach bins, cell_list.cpp:112-121, reach :186-191) gives the
-    // fewest candidates per atom; the list kernel spends a warp per bin, so
-    // sparse systems (few atoms per bin, e.g. reduced-unit LJ with a short
-    // list radius) take coarser bins that amortise the per-bin stencil work.
+    // fewest candidates per atom, but the list kernel spends a warp per bin
+    // and resolves the stencil per bin, so bins must hold enough atoms to
+    // amortise that: reach 3 from 5 atoms per bin, else reach 2 from 1.5,
+    // else reach 1 (measured: the 262k-ion melt builds fastest at reach 2,
+    // 12 ions per bin; reduced-unit LJ at reach 2, 2.3 atoms per bin).
     // The pair set does not depend on the bins.
     const double density = d.n_atoms / (Lp[0] * Lp[1] * Lp[2]);
     auto per_bin = [&](double reach) { return density * std::pow(g.rlist / reach, 3.0); };
-    const double reach_t = per_bin(3.0) >= 2.5 ? 3.0 : (per_bin(2.0) >= 1.5 ? 2.0 : 1.0);
+    const double reach_t = per_bin(3.0) >= 5.0 ? 3.0 : (per_bin(2.0) >= 1.5 ? 2.0 : 1.0);
     for (int k = 0; k < 3; ++k) {
         int c = (int)std::floor(Lp[k] / (g.rlist / reach_t));
         g.nc[k] = c < 1 ? 1 : c;
