@@ -69,7 +69,7 @@ ATVB_DEV void pair_term(const RowConst<T>& c, T dx, T dy, T dz, T qj,
     if constexpr (F)
         rinv = rsqrt_approx(r2);
     else
-        rinv = rsqrt(r2);
+        rinv = rsqrt64(r2);
     const T r2inv = rinv * rinv;
     const T sg = neg ? T(-1) : T(1);
     T fpair = 0;

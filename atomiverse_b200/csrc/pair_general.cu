@@ -92,7 +92,7 @@ ATVB_DEV void row_general(const SysParams& P, int s, int g, PairAcc& acc) {
         if (MIXED)
             rinv = (T)rsqrt_approx((float)r2);
         else
-            rinv = (T)rsqrt((double)r2);
+            rinv = (T)rsqrt64((double)r2);
         const T r2inv = rinv * rinv;
         T fpair = 0;
         const T sl = cls ? (T)P.sp_lj[cls] : T(1); // 0: excluded from LJ

@@ -67,6 +67,16 @@ ATVB_DEV double rcp64(double v) {
     return fma(t, fma(-v, t, 1.0), t);
 }
 
+// 1 / sqrt(v) in FP64 for v in the FP32 normal range: FP32 estimate
+// (rsqrt.approx), then two Newton steps y <- y (3/2 - (v/2) y^2) (relative
+// error 2^-22 -> 2^-45 -> rounding level).
+ATVB_DEV double rsqrt64(double v) {
+    double y = (double)rsqrt_approx((float)v);
+    const double h = 0.5 * v;
+    y = y * fma(-h, y * y, 1.5);
+    return y * fma(-h, y * y, 1.5);
+}
+
 // erfcx(x) for 0 <= x <= 6 from the universal polynomial of erfcx_coef.h,
 // given t = 1 / (1 + kErfcxP x).  Coefficients are compile-time constants.
 // FP64: the even and odd coefficients as two Horner chains in u^2 (half
