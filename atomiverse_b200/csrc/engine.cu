@@ -399,6 +399,9 @@ Slot::Slot(const atvb_system_desc& d, const DevMem& mem) : desc(d), mem_(mem) {
             throw Error(ATVB_ERR_INVALID,
                         "CoulLong: alpha * cutoff must not exceed 6 "
                         "(erfc(6) = 2e-17 is below double precision)");
+        if (d.coul_alpha * geo.rlist > 26.0)
+            throw Error(ATVB_ERR_INVALID,
+                        "CoulLong: alpha * (cutoff + skin) must not exceed 26");
     }
     // integrator / thermostat
     if (!(d.dt > 0.0))
@@ -525,8 +528,13 @@ Engine::Engine(int device) : device_(device) {
     uint64_t keep = UINT64_MAX;
     CK(cudaMemPoolSetAttribute(mem_.pool, cudaMemPoolAttrReleaseThreshold, &keep));
     mem_.stream = stream_;
+    // the PME branch (lane 0 and the FFT lanes) at the highest priority: its
+    // short memory-bound kernels take SMs as pair blocks retire instead of
+    // waiting for the whole pair grid
+    int prio_lo = 0, prio_hi = 0;
+    CK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
     for (int l = 0; l < kFftLanes; ++l) {
-        CK(cudaStreamCreateWithFlags(&fft_streams_[l], cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithPriority(&fft_streams_[l], cudaStreamNonBlocking, prio_hi));
         CK(cudaEventCreateWithFlags(&fft_join_[l], cudaEventDisableTiming));
     }
     CK(cudaEventCreateWithFlags(&fft_fork_, cudaEventDisableTiming));

@@ -98,7 +98,7 @@ ATVB_DEV void pair_term(const RowConst<T>& c, T dx, T dy, T dz, T qj,
             e = ex2_approx(-c.alpha2 * r2);
         } else {
             t = rcp64(fma(SHORT ? kErfcxSP : kErfcxP, x, 1.0));
-            e = exp_neg64(c.alpha2 * r2);
+            e = exp_neg64_small(-(c.alpha2 * r2)); // alpha rlist <= 26 (checked at setup)
         }
         T p;
         if constexpr (!F && SHORT)

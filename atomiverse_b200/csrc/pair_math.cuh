@@ -42,8 +42,9 @@ ATVB_DEV float rsqrt_approx(float x) {
 // exp(r) with 2^(j/64) from a 64-entry table and exp(r) by its Taylor
 // series to degree 5 (truncation < 4e-17).  z is clamped at 708 (the result
 // is then ~1e-308, far below anything the callers keep).
-ATVB_DEV double exp_neg64(double z) {
-    const double w = -fmin(z, 708.0);
+// exp(w) for -708 <= w <= 0, no clamp (the pair kernels' arguments
+// -alpha^2 r^2 stay above -(alpha rlist)^2 >= -676, checked at setup)
+ATVB_DEV double exp_neg64_small(double w) {
     const double n = rint(w * kExp64ByLn2);
     double r = fma(-n, kExpLn2By64Hi, w);
     r = fma(-n, kExpLn2By64Lo, r);
@@ -58,6 +59,8 @@ ATVB_DEV double exp_neg64(double z) {
     const long long e = (long long)((ni >> 6) + 1023) << 52; // ni >> 6 >= -1022
     return (t * p) * __longlong_as_double(e);
 }
+
+ATVB_DEV double exp_neg64(double z) { return exp_neg64_small(-fmin(z, 708.0)); }
 
 // 1 / v for 1 <= v <= 4 in FP64: FP32 estimate, two Newton steps
 // (relative error 2^-22 -> 2^-44 -> below one FP64 ulp).
