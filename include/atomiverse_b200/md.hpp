@@ -292,7 +292,84 @@ class MD {
         if (have_pair_ && !have_nl_)
             throw std::invalid_argument(
                 "cuda::md::MD: Add `sim.set_neighbor(cuda::NeighborList{cutoff})`.");
-        if (!sys_) {
+        ensure_system(frame);
+        atvb_soa_view v = frame.view();
+        atvb_scalars s{};
+        check(atvb_system_run(sys_, &v, n_steps, &s));
+        for (int k = 0; k < 3; ++k) // the cell moves under NPT
+            frame.box[k] = s.box[k];
+        return s;
+    }
+
+    /// Checkpoint of the whole resumable state (atvb_system_save).
+    std::vector<char> checkpoint() {
+        if (!sys_)
+            throw std::logic_error("MD::checkpoint: nothing has run yet");
+        int64_t nb = 0;
+        check(atvb_system_checkpoint_size(sys_, &nb));
+        std::vector<char> blob((size_t)nb);
+        check(atvb_system_save(sys_, blob.data(), nb));
+        return blob;
+    }
+
+    /// Resume from checkpoint() bytes in place of the first run's upload;
+    /// `frame` supplies the atom count and box (same as the saved system).
+    /// The next run(frame, n) continues the saved trajectory bit for bit.
+    void restore(Frame& frame, const std::vector<char>& blob) {
+        if (sys_)
+            throw std::logic_error("MD::restore: the system already exists");
+        create_system(frame);
+        check(atvb_system_restore(sys_, blob.data(), (int64_t)blob.size()));
+    }
+
+    /// Trajectory snapshots every `every` steps into a host ring of `depth`
+    /// frames (atvb_system_set_snapshots); read them with poll_snapshots.
+    MD& set_snapshots(int every, int depth) {
+        snap_every_ = every;
+        snap_depth_ = depth;
+        if (sys_)
+            check(atvb_system_set_snapshots(sys_, every, depth));
+        return *this;
+    }
+
+    /// Frames published since the last poll, no device synchronisation:
+    /// steps[f], and x, y, z of frame f at xyz[3 n f + {0, n, 2n} + i].
+    int poll_snapshots(std::vector<int64_t>& steps, std::vector<double>& xyz, int max_frames = 16) {
+        if (!sys_)
+            return 0;
+        const int n = d_.n_atoms;
+        steps.assign(max_frames, 0);
+        xyz.assign((size_t)3 * n * max_frames, 0.0);
+        std::vector<double> x((size_t)n * max_frames), y(x.size()), z(x.size());
+        int32_t cnt = 0;
+        int64_t dropped = 0;
+        check(atvb_system_snapshot_poll(sys_, max_frames, steps.data(), nullptr, x.data(),
+                                        y.data(), z.data(), nullptr, nullptr, nullptr, &cnt,
+                                        &dropped));
+        for (int f = 0; f < cnt; ++f)
+            for (int i = 0; i < n; ++i) {
+                xyz[(size_t)3 * n * f + i] = x[(size_t)n * f + i];
+                xyz[(size_t)3 * n * f + n + i] = y[(size_t)n * f + i];
+                xyz[(size_t)3 * n * f + 2 * n + i] = z[(size_t)n * f + i];
+            }
+        steps.resize(cnt);
+        xyz.resize((size_t)3 * n * cnt);
+        return cnt;
+    }
+
+  private:
+    void ensure_system(Frame& frame) {
+        if (!sys_)
+            create_system(frame);
+    }
+
+    void create_system(Frame& frame) {
+        if (!have_integrator_)
+            throw std::invalid_argument("MD: set_integrator is required");
+        if (have_pair_ && !have_nl_)
+            throw std::invalid_argument(
+                "cuda::md::MD: Add `sim.set_neighbor(cuda::NeighborList{cutoff})`.");
+        {
             d_.n_atoms = frame.n();
             d_.precision = precision_;
             for (int k = 0; k < 9; ++k)
@@ -326,16 +403,11 @@ class MD {
                 check(atvb_system_set_special_bonds(sys_, lj, co, (int64_t)a.size(), a.data(),
                                                     b.data()));
             }
+            if (snap_every_ > 0)
+                check(atvb_system_set_snapshots(sys_, snap_every_, snap_depth_));
         }
-        atvb_soa_view v = frame.view();
-        atvb_scalars s{};
-        check(atvb_system_run(sys_, &v, n_steps, &s));
-        for (int k = 0; k < 3; ++k) // the cell moves under NPT
-            frame.box[k] = s.box[k];
-        return s;
     }
 
-  private:
     atvb_ctx* ctx_ = nullptr;
     atvb_system* sys_ = nullptr;
     atvb_system_desc d_;
@@ -344,6 +416,7 @@ class MD {
     std::vector<LJTypeCoeff> lj_coeffs_;
     atvb_npt_desc npt_{};
     bool have_npt_ = false;
+    int snap_every_ = 0, snap_depth_ = 0;
     SpecialScales lj_special_, coul_special_;
 };
 } // namespace md

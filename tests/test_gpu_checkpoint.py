@@ -147,3 +147,20 @@ def test_server_resumable_segments(atvb, ctx):
         assert np.array_equal(out[k], ref["lj"][k]), k
     srv.close()
     srv2.close()
+
+
+@pytest.mark.gpu
+def test_cpp_checkpoint_resume(atvb, tmp_path):
+    """md::MD::checkpoint / restore continue an NPT run bit for bit; the
+    snapshot ring delivered the frames of steps 20, 40, 60, 80."""
+    import os
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    exe = str(tmp_path / "md_resume")
+    lib_dir = os.path.join(root, "atomiverse_b200")
+    subprocess.run(["g++", "-std=c++17", "-O2", "-I", os.path.join(root, "include"),
+                    os.path.join(root, "tests", "cpp", "md_resume.cpp"), "-o", exe,
+                    "-L", lib_dir, "-latvb", "-Wl,-rpath," + lib_dir], check=True)
+    r = subprocess.run([exe], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert r.stdout.split() == ["OK", "4"]
