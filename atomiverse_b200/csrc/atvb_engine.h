@@ -85,6 +85,7 @@ class Slot {
     void free_alloc(void* p);
     void replan_cells(double shrink);
     bool npt = false; // MTK NPT configured (atvb_system_set_npt)
+    atvb_npt_desc npt_desc{};
     char* snap_host = nullptr; // trajectory snapshot ring (host-mapped)
     long long snap_read = 0;   // snapshots consumed by the host
 
@@ -121,7 +122,8 @@ class Engine {
                        double* const out[6], int64_t* dropped);
     size_t checkpoint_bytes(int id);
     void save(int id, void* buf, size_t cap);
-    void restore(int id, const void* buf, size_t size);
+    void restore(int id, const void* buf, size_t size, bool fresh_list = false);
+    void replan_npt();
     void compute_forces();
     void compute_forces_one(int id);
     void step(int n);
@@ -186,6 +188,7 @@ class Engine {
     cudaStream_t fft_streams_[kFftLanes] = {};
     cudaEvent_t fft_fork_ = nullptr, fft_join_[kFftLanes] = {};
     cudaEvent_t pme_fork_ = nullptr, pme_join_ = nullptr; // PME beside the pair kernel
+    bool any_npt_ = false; // an MTK NPT system exists (re-plan check per step call)
     int num_sms_ = 148;
     std::vector<std::unique_ptr<Slot>> slots_;
     SysParams* d_sp_ = nullptr;

@@ -1016,6 +1016,8 @@ void Engine::step(int n) {
     CK(cudaSetDevice(device_));
     if (n < 0)
         throw Error(ATVB_ERR_INVALID, "n_steps must be >= 0");
+    if (any_npt_)
+        replan_npt();
     ensure_ready();
     if (profiling_) {
         for (int k = 0; k < n; ++k) {
@@ -1282,6 +1284,8 @@ void Engine::set_npt(int id, const atvb_npt_desc& p) {
         cut = std::max(cut, sl->desc.coul_cutoff);
     h.npt_cut = cut;
     sl->npt = true;
+    sl->npt_desc = p;
+    any_npt_ = true;
     push_params(id);
     dirty_ = true;
 }
@@ -1850,7 +1854,7 @@ void Engine::save(int id, void* buf, size_t cap) {
     CK(cudaStreamSynchronize(stream_));
 }
 
-void Engine::restore(int id, const void* buf, size_t size) {
+void Engine::restore(int id, const void* buf, size_t size, bool fresh_list) {
     CK(cudaSetDevice(device_));
     Slot* s = slot(id);
     if (s->uploaded)
@@ -1875,7 +1879,8 @@ void Engine::restore(int id, const void* buf, size_t size) {
     SysState st;
     std::memcpy(&st, p, sizeof(st));
     p += sizeof(SysState);
-    st.snap_count = 0; // snapshot rings belong to the running process
+    if (!fresh_list)
+        st.snap_count = 0; // snapshot rings belong to the running process
     st.snap_slot = -1;
     const double* a[kCkptArrays];
     for (int k = 0; k < kCkptArrays; ++k) {
@@ -1890,14 +1895,16 @@ void Engine::restore(int id, const void* buf, size_t size) {
         std::memcpy(type.data(), p, n * 4);
     }
     // 1. the positions and cell of the last neighbour build: the upload's
-    //    list build then reproduces the saved run's list
+    //    list build then reproduces the saved run's list (fresh_list: a new
+    //    list from the current positions in the current cell instead)
     if (s->npt)
-        apply_box(P, st.Lb, true);
+        apply_box(P, fresh_list ? st.box : st.Lb, true);
+    const int bx = fresh_list ? 0 : 9;
     atvb_soa_view v;
     std::memset(&v, 0, sizeof(v));
-    v.x = const_cast<double*>(a[9]);
-    v.y = const_cast<double*>(a[10]);
-    v.z = const_cast<double*>(a[11]);
+    v.x = const_cast<double*>(a[bx]);
+    v.y = const_cast<double*>(a[bx + 1]);
+    v.z = const_cast<double*>(a[bx + 2]);
     v.vx = const_cast<double*>(a[3]);
     v.vy = const_cast<double*>(a[4]);
     v.vz = const_cast<double*>(a[5]);
@@ -1919,16 +1926,109 @@ void Engine::restore(int id, const void* buf, size_t size) {
     CK(cudaMemcpyAsync(P.x, a[0], b, cudaMemcpyHostToDevice, stream_));
     CK(cudaMemcpyAsync(P.y, a[1], b, cudaMemcpyHostToDevice, stream_));
     CK(cudaMemcpyAsync(P.z, a[2], b, cudaMemcpyHostToDevice, stream_));
-    CK(cudaMemcpyAsync(P.xr, a[9], b, cudaMemcpyHostToDevice, stream_));
-    CK(cudaMemcpyAsync(P.yr, a[10], b, cudaMemcpyHostToDevice, stream_));
-    CK(cudaMemcpyAsync(P.zr, a[11], b, cudaMemcpyHostToDevice, stream_));
+    if (fresh_list) {
+        // the list was built now, from the current positions and cell
+        for (int d = 0; d < 3; ++d) {
+            st.Lb[d] = st.box[d];
+            st.Lb_inv[d] = 1.0 / st.box[d];
+        }
+        double lam = 1e300;
+        for (int d = 0; d < 3; ++d) {
+            st.ub[d] = st.Lb[d] / st.Lnext[d];
+            lam = std::min(lam, st.Lnext[d] / st.Lb[d]);
+        }
+        const double thr = 0.5 * (P.rlist - P.npt_cut / lam);
+        st.disp_thr2 = thr > 0.0 ? thr * thr : -1.0;
+        st.need_rebuild = thr > 0.0 ? 0 : 1;
+        st.ago = 0;
+        st.status &= ~kStatusBoxRange;
+    } else {
+        CK(cudaMemcpyAsync(P.xr, a[9], b, cudaMemcpyHostToDevice, stream_));
+        CK(cudaMemcpyAsync(P.yr, a[10], b, cudaMemcpyHostToDevice, stream_));
+        CK(cudaMemcpyAsync(P.zr, a[11], b, cudaMemcpyHostToDevice, stream_));
+    }
     const LaunchCfg one = restricted_cfg(id);
     launch_repack(one, stream_);
+    if (fresh_list) {
+        // keep the list statistics of the build just made
+        SysState cur;
+        CK(cudaMemcpy(&cur, P.st, sizeof(cur), cudaMemcpyDeviceToHost));
+        st.max_nnbr = cur.max_nnbr;
+        st.list_entries = cur.list_entries;
+        st.overflow = cur.overflow;
+        st.rebuilds += 1;
+    }
     CK(cudaMemcpyAsync(P.st, &st, sizeof(st), cudaMemcpyHostToDevice, stream_));
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(stream_));
-    s->mean_row = h.mean_row;
+    if (!fresh_list)
+        s->mean_row = h.mean_row;
     dirty_ = true;
+}
+
+// MTK NPT systems whose cell has moved close to the edge of the range their
+// bins were planned for (or far beyond it, where the bins grow coarse) are
+// re-planned between step calls, as the reference re-derives its grid and
+// PME mesh when the cell changes (pme.cpp:64-131): checkpoint, a new slot
+// for the current cell with the same configuration, restore with a new
+// list.  The trajectory continues (not bit for bit: the new bins order the
+// list differently).
+void Engine::replan_npt() {
+    for (auto& up : slots_) {
+        if (!up || !up->npt || !up->uploaded)
+            continue;
+        Slot* old = up.get();
+        SysState st;
+        CK(cudaMemcpy(&st, old->hp.st, sizeof(st), cudaMemcpyDeviceToHost));
+        bool need = (st.status & kStatusBoxRange) != 0;
+        for (int k = 0; k < 3; ++k) {
+            const double lo = old->hp.npt_Lmin[k], plan = old->geo.L[k];
+            if (st.Lnext[k] < lo * 1.02 || st.Lnext[k] > plan * 1.25)
+                need = true;
+        }
+        if (!need)
+            continue;
+        const int id = old->index;
+        std::vector<char> blob(checkpoint_bytes(id));
+        save(id, blob.data(), blob.size());
+        atvb_system_desc d = old->desc;
+        for (int k = 0; k < 9; ++k)
+            d.box[k] = 0.0;
+        for (int k = 0; k < 3; ++k)
+            d.box[4 * k] = st.box[k];
+        auto s = std::make_unique<Slot>(d, mem_);
+        s->index = id;
+        s->ntypes = old->ntypes;
+        s->lj_ti = old->lj_ti;
+        s->lj_tj = old->lj_tj;
+        s->lj_eps = old->lj_eps;
+        s->lj_sig = old->lj_sig;
+        s->special_set = old->special_set;
+        for (int k = 0; k < 3; ++k) {
+            s->sp_lj[k] = old->sp_lj[k];
+            s->sp_coul[k] = old->sp_coul[k];
+        }
+        s->bond_a = old->bond_a;
+        s->bond_b = old->bond_b;
+        s->hp.general = old->hp.general;
+        // the snapshot ring moves over with its read position
+        s->snap_host = old->snap_host;
+        s->snap_read = old->snap_read;
+        s->hp.snap_ring = old->hp.snap_ring;
+        s->hp.snap_every = old->hp.snap_every;
+        s->hp.snap_depth = old->hp.snap_depth;
+        s->hp.snap_slot_bytes = old->hp.snap_slot_bytes;
+        old->snap_host = nullptr;
+        const atvb_npt_desc npt = old->npt_desc;
+        CK(cudaStreamSynchronize(stream_));
+        release_graph();
+        release_plans(*old);
+        up = std::move(s);
+        acquire_plans(*up);
+        push_params(id);
+        set_npt(id, npt);
+        restore(id, blob.data(), blob.size(), true);
+    }
 }
 
 } // namespace atvb

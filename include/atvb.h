@@ -206,8 +206,10 @@ int atvb_system_set_special_bonds(atvb_system* sys, const double lj[3],
  * desc.thermostat must be ATVB_NVE; stress is then always computed.  Before
  * the first upload.  The neighbour bins are planned for cells down to 90 %
  * of the initial edge (less when the box is barely larger than 2 (cutoff +
- * skin)); a cell that shrinks further is held and flagged in
- * atvb_scalars.status (re-create the system from the current frame). */
+ * skin)); between step calls a system near that limit is re-planned for its
+ * current cell (checkpoint, new bins and PME mesh, restore); a cell that
+ * leaves the range within one call is held and flagged in
+ * atvb_scalars.status. */
 int atvb_system_set_npt(atvb_system* sys, const atvb_npt_desc* npt);
 /* Checkpoints (state I/O; the reference's resumable record is
  * cpu/record/mrec.h MrecWriter::flush, a molrs Zarr store, and

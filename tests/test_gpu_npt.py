@@ -171,3 +171,26 @@ def test_python_md_mirror_npt(atvb, ctx):
     sim.run(fr, 40)
     sim.run(fr, 40)
     assert float(np.prod(fr["box"])) == pytest.approx(269.425432, abs=1e-6)
+
+
+@pytest.mark.gpu
+def test_npt_cell_leaving_the_planned_range_is_replanned(atvb, ctx, orc):
+    """A dilute LJ system compressed at high pressure shrinks far beyond the
+    90 % its first bins were planned for; between step calls the library
+    re-plans bins (and the list) for the current cell, and the run matches
+    the oracle, which rebuilds every step, to rounding level."""
+    from atomiverse_b200 import workloads as W
+    desc, frame = W.lj_fcc(ncell=7, rho=0.5, t_star=1.0, seed=9)
+    L0 = desc["box"][0]
+    npt = dict(T_target=1.0 / KB, tau_T=1.0, P_target=5.0, tau_P=5.0, dt=desc["dt"])
+    s = atvb.System(ctx, desc, frame, npt=npt)
+    s.compute_forces()
+    for _ in range(200):
+        s.step(3)            # 3 steps shrink an edge by at most 1.5 %
+        sc = s.scalars()
+        assert sc["status"] == 0
+    out, sc = s.download()
+    s.close()
+    assert sc["box"][0] < 0.85 * L0              # beyond the first plan's range
+    o = _oracle_npt(orc, desc, frame, npt, 600, setup=True)
+    assert np.allclose(sc["box"], o.npt_state()["box"], rtol=1e-8, atol=0)
