@@ -5,8 +5,10 @@ domain decomposition, so a single system runs on one GPU and N GPUs run
 independent work.  The replica ladder and the request stream partition by
 system: each rank owns whole systems, its step has no collective, and the
 only exchange is a host gather of per-system scalars at the end of a
-segment (``gather_scalars``).  One process per GPU, ``torch.distributed``
-for the plumbing (NCCL on GPUs; gloo works the same for these host objects).
+segment (``gather_scalars``).  Served requests can move between ranks
+between ticks as checkpoints (``rebalance``, ``exchange_checkpoints``).  One
+process per GPU, ``torch.distributed`` for the plumbing (NCCL on GPUs; gloo
+works the same for these host objects).
 """
 from __future__ import annotations
 
@@ -45,6 +47,65 @@ def route_request(request_index: int, n_atoms: int, loads: list[int]) -> int:
     r = min(range(len(loads)), key=lambda q: (loads[q], q))
     loads[r] += int(n_atoms)
     return r
+
+
+def rebalance(held: list[list[tuple[int, int]]]) -> list[tuple[int, int, int]]:
+    """Moves that even out the resident atoms of the served form.
+
+    ``held[r]`` lists ``(request id, atoms)`` resident on rank r.  Returns
+    ``(request id, from rank, to rank)`` moves: repeatedly the largest request
+    of the heaviest rank that lowers the larger of the two loads goes to the
+    lightest rank.  Deterministic (ties by id, then rank), so every rank
+    computes the same plan from the same ``held``.  A request moves as its
+    checkpoint (``Server.checkpoint`` -> ``exchange_checkpoints`` ->
+    ``Server.submit_checkpoint``) and continues bit for bit on its new rank.
+    """
+    loads = [sum(a for _, a in h) for h in held]
+    where = {rid: r for r, h in enumerate(held) for rid, _ in h}
+    atoms = {rid: a for h in held for rid, a in h}
+    moves = []
+    for _ in range(sum(len(h) for h in held)):
+        hi = max(range(len(loads)), key=lambda q: (loads[q], -q))
+        lo = min(range(len(loads)), key=lambda q: (loads[q], q))
+        best = None
+        for rid in sorted((rid for rid, r in where.items() if r == hi), key=lambda x: (-atoms[x], x)):
+            if max(loads[hi] - atoms[rid], loads[lo] + atoms[rid]) < loads[hi]:
+                best = rid
+                break
+        if best is None:
+            break
+        loads[hi] -= atoms[best]
+        loads[lo] += atoms[best]
+        where[best] = lo
+        moves.append((best, hi, lo))
+    return moves
+
+
+def exchange_checkpoints(moves: list[tuple[int, int, int]], blobs: dict, group=None) -> dict:
+    """Carry the checkpoints of ``moves`` to their new ranks.
+
+    ``blobs`` maps this rank's outgoing request ids to their checkpoint
+    bytes; returns ``{request id: bytes}`` for the requests that move to this
+    rank.  Every rank must call it (collective; any backend, the blobs travel
+    as byte tensors of a size agreed first)."""
+    import torch
+    import torch.distributed as dist
+    rank = dist.get_rank(group)
+    incoming = {}
+    for rid, src, dst in moves:
+        if src == dst:
+            continue
+        if rank == src:
+            data = torch.frombuffer(bytearray(blobs[rid]), dtype=torch.uint8)
+            dist.send(torch.tensor([data.numel()], dtype=torch.int64), dst=dst, group=group)
+            dist.send(data, dst=dst, group=group)
+        elif rank == dst:
+            n = torch.zeros(1, dtype=torch.int64)
+            dist.recv(n, src=src, group=group)
+            data = torch.empty(int(n.item()), dtype=torch.uint8)
+            dist.recv(data, src=src, group=group)
+            incoming[rid] = data.numpy().tobytes()
+    return incoming
 
 
 def gather_scalars(local: dict, group=None, dst: int = 0) -> dict | None:

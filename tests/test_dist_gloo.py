@@ -77,3 +77,61 @@ def test_gather_scalars_two_gloo_ranks():
     for k, v in merged.items():
         assert v["energy"] == -float(sizes[k])
         assert k in owned[v["rank"]]
+
+
+def test_rebalance_plan():
+    held = [[(1, 5000), (2, 3000), (3, 2000)], [(4, 500)], []]
+    moves = shard.rebalance(held)
+    loads = [sum(a for _, a in h) for h in held]
+    atoms = {rid: a for h in held for rid, a in h}
+    for rid, src, dst in moves:
+        loads[src] -= atoms[rid]
+        loads[dst] += atoms[rid]
+    assert max(loads) - min(loads) <= 5000
+    assert max(loads) < 10000
+    assert moves == shard.rebalance(held)            # same plan on every rank
+    assert shard.rebalance([[(1, 100)], [(2, 100)]]) == []
+
+
+def _migrate_worker(rank, ws, port, q):
+    import datetime
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=ws,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        # rank 0 holds three requests, rank 1 none; blobs stand in for checkpoints
+        held = [[(10, 4000), (11, 3000), (12, 2500)], []]
+        rng = np.random.default_rng(rank + 7)
+        mine = {rid: bytes(rng.integers(0, 256, size=1000 + rid, dtype=np.uint8))
+                for rid, _ in held[rank]}
+        moves = shard.rebalance(held)
+        outgoing = {rid: mine[rid] for rid, src, _ in moves if src == rank}
+        got = shard.exchange_checkpoints(moves, outgoing)
+        q.put((rank, moves, {k: v.hex() for k, v in got.items()},
+               {k: v.hex() for k, v in mine.items()}))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_checkpoint_migration_two_gloo_ranks():
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_migrate_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = {}
+    for _ in range(2):
+        rank, moves, got, mine = q.get(timeout=120)
+        res[rank] = (moves, got, mine)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    moves = res[0][0]
+    assert moves and all(src == 0 and dst == 1 for _, src, dst in moves)
+    for rid, _, _ in moves:
+        assert res[1][1][rid] == res[0][2][rid]        # the bytes arrived intact
+    assert res[0][1] == {}
