@@ -22,7 +22,7 @@ __all__ = [
     "FP64", "MIXED", "NVE", "NOSE_HOOVER", "LANGEVIN", "AtvbError",
     "Context", "System", "Batch", "Server", "make_desc",
     "NeighborList", "PairLJCut", "CoulLong", "KSpacePME", "VelocityVerlet",
-    "NoseHoover", "FixLangevin", "NoseHooverNPT", "MD", "library_path",
+    "NoseHoover", "FixLangevin", "NoseHooverNPT", "Barostat", "MD", "library_path",
 ]
 
 FRAME_KEYS = ("x", "y", "z", "vx", "vy", "vz", "fx", "fy", "fz", "mass", "charge")
@@ -123,6 +123,13 @@ def scalars_dict(s: Scalars) -> dict:
     }
 
 
+def _baro_args(b) -> tuple:
+    """Barostat (or a dict of its fields) -> (P_target, tau_P, bulk_modulus)."""
+    if isinstance(b, dict):
+        b = Barostat(**b)
+    return float(b.P_target), float(b.tau_P), float(b.bulk_modulus)
+
+
 def _npt_desc(npt) -> "_abi.NptDesc":
     """NoseHooverNPT (or a dict of its fields) -> atvb_npt_desc."""
     if isinstance(npt, dict):
@@ -167,11 +174,12 @@ class System:
     """One MD system on the device (cuda::md::MD + its components)."""
 
     def __init__(self, ctx: Context, desc: SystemDesc | dict, frame: dict | None = None,
-                 lj_types=None, special_bonds=None, npt=None):
+                 lj_types=None, special_bonds=None, npt=None, barostat=None):
         """lj_types: [(type_i, type_j, epsilon, sigma), ...] (PairLJCut's
         per-type form; per-atom types in frame["type"]); special_bonds:
         dict(lj=(s12, s13, s14), coul=(s12, s13, s14), bonds=[(tag_a, tag_b), ...]);
-        npt: a NoseHooverNPT (MTK NPT in place of velocity Verlet, desc NVE).
+        npt: a NoseHooverNPT (MTK NPT in place of velocity Verlet, desc NVE);
+        barostat: a Barostat (Berendsen, beside the thermostat).
         All are applied before the frame is uploaded."""
         self.ctx = ctx
         self.lib = ctx.lib
@@ -190,6 +198,8 @@ class System:
             check(self.lib.atvb_system_set_special_bonds(self._h, *args))
         if npt is not None:
             check(self.lib.atvb_system_set_npt(self._h, C.byref(_npt_desc(npt))))
+        if barostat is not None:
+            check(self.lib.atvb_system_set_barostat(self._h, *_baro_args(barostat)))
         if frame is not None:
             self.upload(frame)
 
@@ -340,6 +350,8 @@ class Batch:
                 check(self.lib.atvb_batch_set_special_bonds(self._h, k, *args))
             if opts.get("npt") is not None:
                 check(self.lib.atvb_batch_set_npt(self._h, k, C.byref(_npt_desc(opts["npt"]))))
+            if opts.get("barostat") is not None:
+                check(self.lib.atvb_batch_set_barostat(self._h, k, *_baro_args(opts["barostat"])))
         for k, it in enumerate(items):
             if it[1] is not None:
                 self.upload(k, it[1])
@@ -585,6 +597,17 @@ class NoseHooverNPT:
 
 
 @dataclass
+class Barostat:
+    """Barostat(P_target, tau_P, dt, bulk_modulus=1.0) (Berendsen,
+    cpu/dynamics/barostat.h:86): end-of-step pressure coupling beside the
+    thermostat; P_target and bulk_modulus in eV/A^3."""
+    P_target: float
+    tau_P: float
+    dt: float
+    bulk_modulus: float = 1.0
+
+
+@dataclass
 class MD:
     """cuda::md::MD: categorical setters, build(), run(frame, n)
     (include/atomiverse/cuda/dynamics/md.cuh:118-385)."""
@@ -644,6 +667,8 @@ class MD:
             else:
                 raise TypeError(f"unsupported evaluator {type(ev).__name__}")
         for th in self._thermostats:
+            if isinstance(th, Barostat):
+                continue              # applied after create (System barostat=)
             if isinstance(th, NoseHoover):
                 kw.update(thermostat=NOSE_HOOVER, temperature=th.T, tau=th.tau)
             elif isinstance(th, FixLangevin):
@@ -661,8 +686,9 @@ class MD:
                 self.ctx = Context(0)
             n = len(frame["x"])
             npt = self._integrator if isinstance(self._integrator, NoseHooverNPT) else None
+            baro = next((t for t in self._thermostats if isinstance(t, Barostat)), None)
             self._system = System(self.ctx, self.desc(n, box if box is not None else frame["box"]),
-                                  npt=npt)
+                                  npt=npt, barostat=baro)
         sc = self._system.run(frame, n_steps)
         frame["box"] = tuple(sc["box"])   # the cell moves under NPT
         return sc

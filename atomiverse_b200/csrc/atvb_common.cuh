@@ -85,6 +85,7 @@ struct SysState {
     double Lb[3], Lb_inv[3]; // cell at the last neighbour build
     double ub[3];      // Lb / Lnext: next positions mapped into the build cell
     double disp_thr2;  // squared displacement that forces a rebuild
+    double mu;         // Berendsen dilation of this step's end
     // trajectory snapshots published so far, and the ring slot being
     // written this step (-1: none)
     long long snap_count;
@@ -178,6 +179,10 @@ struct SysParams {
     long long npt_nfirst, npt_nlast;
     double npt_Lmin[3]; // smallest cell the neighbour grid is valid for
     double npt_cut;     // largest interaction cutoff (rebuild rule)
+    // Berendsen barostat (beside velocity Verlet and the thermostat):
+    // mu^3 = 1 - baro_coef (baro_P - P), baro_coef = dt / (tau_P bulk_modulus)
+    int baro;
+    double baro_P, baro_coef;
     // trajectory snapshots: every `snap_every` steps positions and
     // velocities go to a ring of `snap_depth` slots in host-mapped memory
     char* snap_ring;    // device view of the ring (null: off)

@@ -86,6 +86,8 @@ class Slot {
     void replan_cells(double shrink);
     bool npt = false; // MTK NPT configured (atvb_system_set_npt)
     atvb_npt_desc npt_desc{};
+    bool baro = false; // Berendsen barostat configured (atvb_system_set_barostat)
+    double baro_args[3] = {0, 0, 0}; // P_target, tau_P, bulk_modulus
     char* snap_host = nullptr; // trajectory snapshot ring (host-mapped)
     long long snap_read = 0;   // snapshots consumed by the host
 
@@ -117,6 +119,7 @@ class Engine {
     void set_special_bonds(int id, const double lj[3], const double coul[3],
                            int64_t nbonds, const int64_t* a, const int64_t* b);
     void set_npt(int id, const atvb_npt_desc& p);
+    void set_barostat(int id, double P_target, double tau_P, double bulk_modulus);
     void set_snapshots(int id, int every, int depth);
     int poll_snapshots(int id, int max_frames, int64_t* steps, double* box,
                        double* const out[6], int64_t* dropped);

@@ -38,6 +38,7 @@ struct LaunchCfg {
     int pair_G = 4;     // lanes per atom of the largest system (reported)
     int any_mixed = 0, any_fp64 = 0;
     int any_snap = 0;   // a system publishes trajectory snapshots
+    int any_baro = 0;   // a system runs the Berendsen barostat (k_baro_scale)
     int any_near = 0;   // a mixed system settles near-cutoff LJ pairs (k_pair_fix)
     int pme_order = 4;  // common PME order (the PME kernels are templated)
     int pme_mixed = 0;

@@ -268,6 +268,24 @@ int atvb_batch_restore(atvb_batch* b, int32_t index, const void* buf, int64_t si
     });
 }
 
+int atvb_system_set_barostat(atvb_system* sys, double P_target, double tau_P,
+                             double bulk_modulus) {
+    return guard([&] {
+        need(sys, "sys");
+        sys->eng->set_barostat(sys->id, P_target, tau_P, bulk_modulus);
+    });
+}
+
+int atvb_batch_set_barostat(atvb_batch* b, int32_t index, double P_target, double tau_P,
+                            double bulk_modulus) {
+    return guard([&] {
+        need(b, "batch");
+        if (index < 0 || index >= (int)b->ids.size())
+            throw Error(ATVB_ERR_NOTFOUND, "no system " + std::to_string(index) + " in batch");
+        b->eng->set_barostat(b->ids[index], P_target, tau_P, bulk_modulus);
+    });
+}
+
 int atvb_system_set_npt(atvb_system* sys, const atvb_npt_desc* npt) {
     return guard([&] {
         need(sys, "sys");

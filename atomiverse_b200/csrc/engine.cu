@@ -758,7 +758,7 @@ void Engine::ensure_table() {
 
 void Engine::push_params(int id) {
     Slot* s = slot(id);
-    if (s->npt && s->uploaded) {
+    if ((s->npt || s->baro) && s->uploaded) {
         // the device owns an NPT system's cell: keep it
         SysParams dev;
         CK(cudaMemcpyAsync(&dev, d_sp_ + id, sizeof(SysParams), cudaMemcpyDeviceToHost,
@@ -861,6 +861,8 @@ void Engine::build_lists() {
             lc_.any_near = 1;
         if (P.snap_ring)
             lc_.any_snap = 1;
+        if (P.baro)
+            lc_.any_baro = 1;
         if (P.has_pme) {
             if (pme_prec >= 0 && (pme_prec != P.prec || pme_order != P.order))
                 throw Error(ATVB_ERR_INVALID,
@@ -931,6 +933,7 @@ int64_t Engine::kernels_per_step() const {
         k += 4;                               // spread, convert, influence, gather
     k += 2;                                   // integrate_b, sys_b
     k += lc_.any_snap ? 3 : 0;                // trajectory snapshots
+    k += lc_.any_baro ? 1 : 0;                // Berendsen position scaling
     return k;
 }
 
@@ -1218,6 +1221,7 @@ LaunchCfg Engine::restricted_cfg(int id) {
     c.any_mixed = P.prec == kMixed;
     c.any_fp64 = P.prec != kMixed;
     c.any_near = P.prec == kMixed && P.has_lj && !P.general && P.mix_band_lj > 0.0;
+    c.any_baro = P.baro;
     if (P.has_pme) {
         c.pme_mixed = P.prec == kMixed;
         c.pme_order = P.order;
@@ -1243,6 +1247,8 @@ void Engine::set_npt(int id, const atvb_npt_desc& p) {
     if (sl->desc.thermostat != ATVB_NVE)
         throw Error(ATVB_ERR_INVALID,
                     "NoseHooverNPT replaces the thermostat: the system must be NVE");
+    if (sl->baro)
+        throw Error(ATVB_ERR_INVALID, "Barostat and NoseHooverNPT cannot be combined");
     if (p.mtchain < 1 || p.mtchain > kMaxChain || p.mpchain < 1 || p.mpchain > kMaxChain)
         throw Error(ATVB_ERR_INVALID, "NoseHooverNPT: chain lengths must be in [1, 10]");
     if (!(p.tau_T > 0.0) || !(p.tau_P > 0.0) || !(p.T_start > 0.0))
@@ -1285,6 +1291,43 @@ void Engine::set_npt(int id, const atvb_npt_desc& p) {
     h.npt_cut = cut;
     sl->npt = true;
     sl->npt_desc = p;
+    any_npt_ = true;
+    push_params(id);
+    dirty_ = true;
+}
+
+// md::Barostat (Berendsen, src/cpu/dynamics/barostat.cpp:22-110): beside
+// velocity Verlet and any thermostat, at end_of_step; the bins are planned
+// for a breathing cell as for MTK NPT.
+void Engine::set_barostat(int id, double P_target, double tau_P, double bulk_modulus) {
+    Slot* sl = slot(id);
+    if (sl->uploaded)
+        throw Error(ATVB_ERR_STATE, "Barostat must be set before the first upload");
+    if (sl->npt)
+        throw Error(ATVB_ERR_INVALID, "Barostat and NoseHooverNPT cannot be combined");
+    if (!(tau_P > 0.0) || !(bulk_modulus > 0.0) || !std::isfinite(P_target))
+        throw Error(ATVB_ERR_INVALID, "Barostat: tau_P and bulk_modulus must be > 0");
+    SysParams& h = sl->hp;
+    double shrink = 0.1;
+    for (int k = 0; k < 3; ++k)
+        shrink = std::min(shrink, 1.0 - 2.0 * sl->geo.rlist * (1.0 + 1e-9) / sl->geo.L[k]);
+    if (shrink < 0.0)
+        shrink = 0.0;
+    sl->replan_cells(shrink);
+    h.baro = 1;
+    h.baro_P = P_target;
+    h.baro_coef = h.dt / (tau_P * bulk_modulus);
+    h.need_virial = 1;
+    double cut = sl->desc.nl_cutoff;
+    if (h.has_lj)
+        cut = std::max(cut, sl->desc.lj_cutoff);
+    if (h.has_coul)
+        cut = std::max(cut, sl->desc.coul_cutoff);
+    h.npt_cut = cut;
+    sl->baro = true;
+    sl->baro_args[0] = P_target;
+    sl->baro_args[1] = tau_P;
+    sl->baro_args[2] = bulk_modulus;
     any_npt_ = true;
     push_params(id);
     dirty_ = true;
@@ -1549,6 +1592,17 @@ void Engine::upload(int id, const atvb_soa_view& f) {
         st0.Lb[k] = st0.Lnext[k] = s->hp.L[k];
         st0.Lb_inv[k] = 1.0 / s->hp.L[k];
         st0.vs[k] = st0.vs_out[k] = 1.0;
+        // drift factors of a cell that does not move (the Berendsen
+        // barostat's first step; MTK NPT prepares its own)
+        st0.npt_a[k] = st0.npt_drift[k] = 1.0;
+        st0.fixn_scale[k] = s->hp.fix_scale[k];
+        st0.fixn64_scale[k] = s->hp.fix64_scale[k];
+        st0.ub[k] = 1.0;
+    }
+    st0.mu = 1.0;
+    {
+        const double thr = 0.5 * (s->hp.rlist - s->hp.npt_cut);
+        st0.disp_thr2 = thr > 0.0 ? thr * thr : -1.0;
     }
     CK(cudaMemcpyAsync(s->hp.st, &st0, sizeof(st0), cudaMemcpyHostToDevice,
                        stream_));
@@ -1897,7 +1951,7 @@ void Engine::restore(int id, const void* buf, size_t size, bool fresh_list) {
     // 1. the positions and cell of the last neighbour build: the upload's
     //    list build then reproduces the saved run's list (fresh_list: a new
     //    list from the current positions in the current cell instead)
-    if (s->npt)
+    if (s->npt || s->baro)
         apply_box(P, fresh_list ? st.box : st.Lb, true);
     const int bx = fresh_list ? 0 : 9;
     atvb_soa_view v;
@@ -1917,7 +1971,7 @@ void Engine::restore(int id, const void* buf, size_t size, bool fresh_list) {
     v.type = type.empty() ? nullptr : type.data();
     upload(id, v);
     // 2. the current cell, positions and state
-    if (s->npt) {
+    if (s->npt || s->baro) {
         apply_box(P, st.box, true);
         CK(cudaMemcpyAsync(d_sp_ + id, &P, sizeof(SysParams), cudaMemcpyHostToDevice,
                            stream_));
@@ -1975,7 +2029,7 @@ void Engine::restore(int id, const void* buf, size_t size, bool fresh_list) {
 // list differently).
 void Engine::replan_npt() {
     for (auto& up : slots_) {
-        if (!up || !up->npt || !up->uploaded)
+        if (!up || !(up->npt || up->baro) || !up->uploaded)
             continue;
         Slot* old = up.get();
         SysState st;
@@ -2020,13 +2074,18 @@ void Engine::replan_npt() {
         s->hp.snap_slot_bytes = old->hp.snap_slot_bytes;
         old->snap_host = nullptr;
         const atvb_npt_desc npt = old->npt_desc;
+        const bool was_npt = old->npt, was_baro = old->baro;
+        const double ba[3] = {old->baro_args[0], old->baro_args[1], old->baro_args[2]};
         CK(cudaStreamSynchronize(stream_));
         release_graph();
         release_plans(*old);
         up = std::move(s);
         acquire_plans(*up);
         push_params(id);
-        set_npt(id, npt);
+        if (was_npt)
+            set_npt(id, npt);
+        if (was_baro)
+            set_barostat(id, ba[0], ba[1], ba[2]);
         restore(id, blob.data(), blob.size(), true);
     }
 }

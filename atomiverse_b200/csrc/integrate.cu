@@ -61,7 +61,7 @@ ATVB_DEV double fix_to_d(unsigned long long v) {
 // closed-form drift x e^{eps dt} + v dt drift into the next cell, wrap,
 // sorted repack with the next cell's scales, displacement check in the
 // build cell.
-ATVB_DEV void npt_drift_atom(const SysParams& P, int i) {
+ATVB_DEV double npt_drift_atom(const SysParams& P, int i) {
     const SysState* st = P.st;
     const int r = P.rank[i];
     const double4 f = P.f4[r];
@@ -102,6 +102,7 @@ ATVB_DEV void npt_drift_atom(const SysParams& P, int i) {
     }
     if (d2 > st->disp_thr2)
         P.st->need_rebuild = 1;
+    return P.mass[i] * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
 }
 
 // Initial half: deferred scale, kick, drift, wrap, sorted repack,
@@ -114,8 +115,8 @@ __global__ void __launch_bounds__(kChunk)
         const SysParams& P = sp[item.sys];
         const int i = item.begin + threadIdx.x;
         double ke = 0.0;
-        if (i < P.n && P.thermostat == kNPT) {
-            npt_drift_atom(P, i);
+        if (i < P.n && (P.thermostat == kNPT || P.baro)) {
+            ke = npt_drift_atom(P, i);
         } else if (i < P.n) {
             const double sc = P.st->vscale;
             const int r = P.rank[i];
@@ -306,6 +307,65 @@ ATVB_DEV void record_history(const SysParams& P, SysState* st) {
     }
 }
 
+// Berendsen barostat at end_of_step (barostat.cpp:27-110): from the scalar
+// pressure of this step (st->pressure, virial + kinetic), the dilation
+// mu = cbrt(clamp(1 - dt/(tau_P beta) (P_target - P), 0.5, 2)); the cell is
+// committed here, k_baro_scale scales the positions, and the next initial
+// half drifts in the new cell with the build-cell displacement rule.
+ATVB_DEV void berendsen(const SysParams& P, SysState* st) {
+    double mu3 = 1.0 - P.baro_coef * (P.baro_P - st->pressure);
+    mu3 = mu3 < 0.5 ? 0.5 : (mu3 > 2.0 ? 2.0 : mu3);
+    double mu = cbrt(mu3);
+    double Ln[3];
+    bool ok = true;
+    for (int d = 0; d < 3; ++d) {
+        Ln[d] = P.L[d] * mu;
+        if (!(Ln[d] >= P.npt_Lmin[d]))
+            ok = false;
+    }
+    if (!ok) {
+        st->status |= kStatusBoxRange;
+        mu = 1.0;
+        for (int d = 0; d < 3; ++d)
+            Ln[d] = P.L[d];
+    }
+    st->mu = mu;
+    SysParams& W = const_cast<SysParams&>(P);
+    apply_box(W, Ln, true);
+    double lam = 1e300;
+    for (int d = 0; d < 3; ++d) {
+        st->box[d] = Ln[d];
+        st->vs[d] = st->vscale;
+        st->vs_out[d] = st->vscale;
+        st->npt_a[d] = 1.0;
+        st->npt_drift[d] = 1.0;
+        st->Lnext[d] = Ln[d];
+        st->fixn_scale[d] = W.fix_scale[d];
+        st->fixn64_scale[d] = W.fix64_scale[d];
+        st->ub[d] = st->Lb[d] / Ln[d];
+        lam = fmin(lam, Ln[d] / st->Lb[d]);
+    }
+    const double thr = 0.5 * (P.rlist - P.npt_cut / lam);
+    st->disp_thr2 = thr > 0.0 ? thr * thr : -1.0;
+    if (thr <= 0.0)
+        st->need_rebuild = 1;
+}
+
+// Positions scaled by this step's Berendsen dilation (original order).
+__global__ void k_baro_scale(const Item* items, int nitems, const SysParams* sp) {
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const Item item = items[it];
+        const SysParams& P = sp[item.sys];
+        const int i = item.begin + threadIdx.x;
+        if (!P.baro || i >= P.n)
+            continue;
+        const double mu = P.st->mu;
+        P.x[i] *= mu;
+        P.y[i] *= mu;
+        P.z[i] *= mu;
+    }
+}
+
 // MTK NPT end of step (nose_hoover_npt.cpp:855-885, P8-P11) from the
 // per-axis kinetic energies of the kicked velocities, then the scalars of
 // the next step's initial half (npt_prepare).
@@ -359,6 +419,8 @@ __global__ void k_sys_b(const int* sys_list, int nsys, const SysParams* sp) {
     finish_energy(P, st);
     st->conserved = st->energy + st->kinetic;
     cell_scalars(P, st);
+    if (P.baro)
+        berendsen(P, st);
     if (P.ehist_cap > 0) {
         const long long slot = st->step % P.ehist_cap;
         P.ehist[3 * slot + 0] = st->energy;
@@ -679,6 +741,8 @@ void launch_integrate_b(const LaunchCfg& lc, cudaStream_t s) {
 }
 void launch_sys_b(const LaunchCfg& lc, cudaStream_t s) {
     k_sys_b<<<sys_blocks(lc.nsys), 128, 0, s>>>(lc.sys_list, lc.nsys, lc.sp);
+    if (lc.any_baro)
+        k_baro_scale<<<lc.atoms.grid, kChunk, 0, s>>>(lc.atoms.d, lc.atoms.n, lc.sp);
 }
 void launch_sys_energy(const LaunchCfg& lc, cudaStream_t s) {
     k_sys_energy<<<sys_blocks(lc.nsys), 128, 0, s>>>(lc.sys_list, lc.nsys,

@@ -161,6 +161,17 @@ struct FixLangevin {
     FixLangevin(double t0, double t1, double damp_, double dt_, uint32_t seed_)
         : T_start(t0), T_stop(t1 < 0 ? t0 : t1), damp(damp_), dt(dt_), seed(seed_) {}
 };
+/// md::Barostat(P_target, tau_P, dt, bulk_modulus = 1) -- Berendsen pressure
+/// coupling at end_of_step beside the thermostat (cpu/dynamics/barostat.h:86;
+/// LAMMPS-standard pressure sign).  Bound with set_thermostat.
+struct Barostat {
+    double P_target, tau_P, dt, bulk_modulus;
+    Barostat(double P, double tau, double dt_, double bulk = 1.0)
+        : P_target(P), tau_P(tau), dt(dt_), bulk_modulus(bulk) {
+        if (!(tau > 0.0) || !(bulk > 0.0))
+            throw std::invalid_argument("Barostat: tau_P and bulk_modulus must be > 0");
+    }
+};
 /// cuda::md::NoseHooverNPT(T_target, tau_T, P_target, tau_P, dt, drag,
 /// mtchain, mpchain, couple_axis, T_stop) + set_run_span
 /// (cuda/dynamics/nose_hoover_npt.cuh:60-70).  An integrator: it replaces
@@ -262,6 +273,11 @@ class MD {
         npt_ = v.p;
         have_npt_ = true;
         have_integrator_ = true;
+        return *this;
+    }
+    MD& set_thermostat(const Barostat& b) {
+        baro_ = b;
+        have_baro_ = true;
         return *this;
     }
     MD& set_thermostat(const NoseHoover& t) {
@@ -380,6 +396,9 @@ class MD {
             check(atvb_system_create(ctx_, &d_, &sys_));
             if (have_npt_)
                 check(atvb_system_set_npt(sys_, &npt_));
+            if (have_baro_)
+                check(atvb_system_set_barostat(sys_, baro_.P_target, baro_.tau_P,
+                                               baro_.bulk_modulus));
             if (!lj_coeffs_.empty()) {
                 std::vector<int32_t> ti, tj;
                 std::vector<double> e, sg;
@@ -417,6 +436,8 @@ class MD {
     atvb_npt_desc npt_{};
     bool have_npt_ = false;
     int snap_every_ = 0, snap_depth_ = 0;
+    Barostat baro_{0.0, 1.0, 1.0};
+    bool have_baro_ = false;
     SpecialScales lj_special_, coul_special_;
 };
 } // namespace md

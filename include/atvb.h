@@ -211,6 +211,15 @@ int atvb_system_set_special_bonds(atvb_system* sys, const double lj[3],
  * leaves the range within one call is held and flagged in
  * atvb_scalars.status. */
 int atvb_system_set_npt(atvb_system* sys, const atvb_npt_desc* npt);
+/* md::Barostat(P_target, tau_P, dt, bulk_modulus) (cuda/dynamics/barostat.cuh,
+ * src/cpu/dynamics/barostat.cpp:22-110): Berendsen isotropic pressure
+ * coupling at end_of_step beside velocity Verlet and any thermostat, with
+ * the LAMMPS-standard scalar pressure (W_xx + W_yy + W_zz + 2 KE) / (3 V),
+ * mu = cbrt(clamp(1 - dt/(tau_P bulk_modulus) (P_target - P), 0.5, 2)), cell
+ * and positions scaled by mu.  P_target and bulk_modulus in eV/A^3; stress is
+ * then always computed.  Before the first upload; not with set_npt. */
+int atvb_system_set_barostat(atvb_system* sys, double P_target, double tau_P,
+                             double bulk_modulus);
 /* Checkpoints (state I/O; the reference's resumable record is
  * cpu/record/mrec.h MrecWriter::flush, a molrs Zarr store, and
  * cpu/io/frame_writer.h write_frame_zarr): the whole resumable state of a
@@ -269,6 +278,8 @@ int atvb_batch_checkpoint_size(atvb_batch* b, int32_t index, int64_t* bytes);
 int atvb_batch_save(atvb_batch* b, int32_t index, void* buf, int64_t capacity);
 int atvb_batch_restore(atvb_batch* b, int32_t index, const void* buf, int64_t size);
 int atvb_batch_set_npt(atvb_batch* b, int32_t index, const atvb_npt_desc* npt);
+int atvb_batch_set_barostat(atvb_batch* b, int32_t index, double P_target, double tau_P,
+                            double bulk_modulus);
 int atvb_batch_set_lj_types(atvb_batch* b, int32_t index, int32_t ncoef,
                             const int32_t* type_i, const int32_t* type_j,
                             const double* epsilon, const double* sigma);

@@ -117,6 +117,8 @@ def lib():
         L.orc_set_npt.restype = C.c_int
         L.orc_set_npt.argtypes = [C.c_void_p, C.POINTER(OrcNpt)]
         L.orc_npt_state.argtypes = [C.c_void_p, dp]
+        L.orc_set_barostat.restype = C.c_int
+        L.orc_set_barostat.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double]
         _lib = L
     return _lib
 
@@ -246,6 +248,11 @@ class OracleSystem:
                    int(span[1]))
         if lib().orc_set_npt(self._h, C.byref(p)) != 0:
             raise ValueError("bad NPT parameters")
+
+    def set_barostat(self, P, tau_P, bulk_modulus=1.0):
+        """Berendsen barostat at end_of_step (P in eV/A^3)."""
+        if lib().orc_set_barostat(self._h, float(P), float(tau_P), float(bulk_modulus)) != 0:
+            raise ValueError("bad barostat parameters")
 
     def npt_state(self) -> dict:
         o = np.zeros(NPT_NSTATE)

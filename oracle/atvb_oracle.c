@@ -122,6 +122,9 @@ struct orc_sys {
     double eta_t[ORC_MAXCHAIN], eta_t_dot[ORC_MAXCHAIN];
     double eta_b[ORC_MAXCHAIN], eta_b_dot[ORC_MAXCHAIN];
     double eps_dot[3];
+    /* Berendsen barostat (barostat.cpp) */
+    int baro_on;
+    double baro_P, baro_tau, baro_bulk;
 };
 
 orc_sys* orc_create(const orc_desc* d) {
@@ -1616,13 +1619,45 @@ static void npt_step(orc_sys* s) {
     s->conserved = npt_hamiltonian(s);
 }
 
+/* Berendsen barostat at end_of_step (barostat.cpp:27-110): scalar pressure
+ * P = (W_xx + W_yy + W_zz + 2 KE) / (3 V), dilation
+ * mu = cbrt(clamp(1 - dt / (tau_P beta) (P_target - P), 0.5, 2)), cell and
+ * positions scaled by mu. */
+static void berendsen(orc_sys* s) {
+    const double V = s->d.L[0] * s->d.L[1] * s->d.L[2];
+    if (V <= 0.0)
+        return;
+    const double P = (s->vir[0] + s->vir[1] + s->vir[2] + 2.0 * s->ke) / (3.0 * V);
+    double mu3 = 1.0 - (s->d.dt / (s->baro_tau * s->baro_bulk)) * (s->baro_P - P);
+    mu3 = mu3 < 0.5 ? 0.5 : (mu3 > 2.0 ? 2.0 : mu3);
+    const double mu = cbrt(mu3);
+    for (int d = 0; d < 3; ++d)
+        s->d.L[d] *= mu;
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < s->n; ++i) {
+        s->x[i] *= mu;
+        s->y[i] *= mu;
+        s->z[i] *= mu;
+    }
+}
+
+int orc_set_barostat(orc_sys* s, double P_target, double tau_P, double bulk_modulus) {
+    if (!(tau_P > 0.0) || !(bulk_modulus > 0.0) || s->npt_on)
+        return -1;
+    s->baro_on = 1;
+    s->baro_P = P_target;
+    s->baro_tau = tau_P;
+    s->baro_bulk = bulk_modulus;
+    s->d.need_virial = 1;
+    return 0;
+}
+
 /* runtime.cpp:452-501 step order with VelocityVerlet (velocity_verlet.cpp)
  * at order 0 and the thermostat at +100 in both integrate phases. */
 int orc_run(orc_sys* s, int n_steps, double* hist) {
     const int n = s->n;
     const double dt = s->d.dt;
     const double dtf = 0.5 * dt * ORC_FTM2V;
-    const double L0 = s->d.L[0], L1 = s->d.L[1], L2 = s->d.L[2];
     int rebuilds = 0;
     if (s->npairs == 0 && s->nbr == NULL)
         orc_build_list(s);
@@ -1640,6 +1675,7 @@ int orc_run(orc_sys* s, int n_steps, double* hist) {
     }
     for (int st = 0; st < n_steps; ++st) {
         /* initial_integrate */
+        const double L0 = s->d.L[0], L1 = s->d.L[1], L2 = s->d.L[2];
 #pragma omp parallel for schedule(static)
         for (int i = 0; i < n; ++i) {
             const double dtfm = dtf / s->m[i];
@@ -1659,8 +1695,9 @@ int orc_run(orc_sys* s, int n_steps, double* hist) {
         s->ago++;
         const int every = s->d.nl_every < 1 ? 1 : s->d.nl_every;
         const int delay = s->d.nl_delay < 0 ? 0 : s->d.nl_delay;
-        if (s->ago >= delay && (s->ago % every) == 0 &&
-            (!s->d.nl_check || needs_rebuild(s))) {
+        /* the cell changes every step under the barostat: rebuild every step */
+        if (s->baro_on || (s->ago >= delay && (s->ago % every) == 0 &&
+                           (!s->d.nl_check || needs_rebuild(s)))) {
             orc_build_list(s);
             ++rebuilds;
             ++s->rebuilds;
@@ -1682,6 +1719,8 @@ int orc_run(orc_sys* s, int n_steps, double* hist) {
             nose_hoover(s);
         /* end_of_step */
         s->ke = kinetic(s);
+        if (s->baro_on)
+            berendsen(s);
         if (hist) {
             hist[2 * st] = s->e_lj + s->e_coul + s->e_recip + s->e_const;
             hist[2 * st + 1] = s->ke;

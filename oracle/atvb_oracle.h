@@ -122,6 +122,10 @@ void orc_set_special(orc_sys* s, int npairs, const int32_t* pi, const int32_t* p
  * the thermostat; nose_hoover_npt.cpp:87-172 build).  Returns 0, or -1 on a
  * bad parameter (chain length outside [1, ORC_MAXCHAIN], tau <= 0). */
 int orc_set_npt(orc_sys* s, const orc_npt* p);
+/* Berendsen barostat (cpu::md::Barostat(P_target, tau_P, dt, bulk_modulus),
+ * src/cpu/dynamics/barostat.cpp:22-110) at end_of_step, beside velocity
+ * Verlet and the thermostat; P_target in eV/A^3.  Returns 0 or -1. */
+int orc_set_barostat(orc_sys* s, double P_target, double tau_P, double bulk_modulus);
 /* NPT state: [0..2] box edges, [3] conserved extended Hamiltonian,
  * [4..6] eps_dot, [7] eta_t[0], [8] eta_t_dot[0], [9] eta_b[0],
  * [10] eta_b_dot[0], [11] live temperature setpoint, [12] KE_global. */

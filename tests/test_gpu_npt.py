@@ -194,3 +194,61 @@ def test_npt_cell_leaving_the_planned_range_is_replanned(atvb, ctx, orc):
     assert sc["box"][0] < 0.85 * L0              # beyond the first plan's range
     o = _oracle_npt(orc, desc, frame, npt, 600, setup=True)
     assert np.allclose(sc["box"], o.npt_state()["box"], rtol=1e-8, atol=0)
+
+
+def _baro_case(thermostat=1, precision=0):
+    from atomiverse_b200 import workloads as W
+    desc, frame = W.lj_fcc(ncell=6, t_star=1.0, seed=3, thermostat=thermostat, precision=precision)
+    return dict(desc, tau=50.0), frame, dict(P_target=0.5, tau_P=20.0, dt=desc["dt"],
+                                             bulk_modulus=10.0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("thermostat,precision,tol", [(1, 0, 1e-10), (2, 0, 1e-10), (1, 1, 1e-6)])
+def test_berendsen_barostat_matches_oracle(atvb, ctx, orc, thermostat, precision, tol):
+    """md::Barostat (Berendsen) beside Nose-Hoover or Langevin: cell and
+    positions follow the oracle over 200 steps."""
+    desc, frame, baro = _baro_case(thermostat, precision)
+    s = atvb.System(ctx, desc, frame, barostat=baro)
+    s.compute_forces()
+    s.step(200)
+    out, sc = s.download()
+    s.close()
+    o = oracle_system(orc, desc, frame)
+    o.set_barostat(baro["P_target"], baro["tau_P"], baro["bulk_modulus"])
+    o.build_list()
+    o.compute_forces()
+    o.run(200)
+    box = o.npt_state()["box"]
+    assert sc["box"][0] != desc["box"][0]
+    assert np.allclose(sc["box"], box, rtol=tol, atol=0)
+    d = _pos(out) - _pos(o.state())
+    d -= np.rint(d / sc["box"]) * sc["box"]
+    assert np.abs(d).max() < 1e4 * tol * box[0]
+    assert sc["status"] == 0
+
+
+@pytest.mark.gpu
+def test_berendsen_batch_equals_alone_and_resumes(atvb, ctx):
+    desc, frame, baro = _baro_case(1, 1)
+    from atomiverse_b200 import workloads as W
+    d2, f2 = W.lj_fcc(ncell=5, seed=4)
+    items = [(desc, frame, dict(barostat=baro)), (d2, f2)]
+    b = atvb.Batch(ctx, items)
+    b.compute_forces()
+    b.step(30)
+    ob, sb = b.download(0)
+    b.close()
+    s = atvb.System(ctx, desc, frame, barostat=baro)
+    s.compute_forces()
+    s.step(12)
+    blob = s.save()
+    s.close()
+    r = atvb.System(ctx, desc, None, barostat=baro)
+    r.restore(blob)
+    r.step(18)
+    oa, sa = r.download()
+    r.close()
+    for k in ("x", "y", "z", "vx", "vy", "vz"):
+        assert np.array_equal(ob[k], oa[k]), k
+    assert np.array_equal(sb["box"], sa["box"])

@@ -131,3 +131,39 @@ def test_pme_tables_follow_the_cell(orc):
         assert np.array_equal(st[k], f1[k])
     # energies: OpenMP reduction order may differ in the last bit
     assert fresh.scalars()["e_recip"] == pytest.approx(s.scalars()["e_recip"], rel=1e-14)
+
+
+def _lj_baro(orc, P, thermostat=1):
+    from atomiverse_b200 import workloads as W
+    import sys, os
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    from conftest import oracle_system
+    desc, frame = W.lj_fcc(ncell=5, t_star=1.0, seed=3, thermostat=thermostat)
+    o = oracle_system(orc, dict(desc, tau=50.0), frame)
+    o.set_barostat(P, 20.0, 10.0)
+    o.build_list()
+    o.compute_forces()
+    return o, desc
+
+
+def test_berendsen_one_step_dilation(orc):
+    """barostat.cpp:27-110: after one step the cell is the old one times
+    cbrt(1 - dt/(tau_P beta) (P_target - P)), P = (trace W + 2 KE)/(3 V) of
+    that step's end."""
+    o, desc = _lj_baro(orc, 0.5)
+    L0 = desc["box"][0]
+    o.run(1)
+    sc = o.scalars()
+    P = (sc["virial"][:3].sum() + 2.0 * sc["kinetic"]) / (3.0 * L0 ** 3)
+    mu = np.cbrt(1.0 - desc["dt"] / (20.0 * 10.0) * (0.5 - P))
+    assert o.npt_state()["box"][0] == pytest.approx(L0 * mu, rel=1e-15)
+
+
+def test_berendsen_moves_the_cell_toward_the_target(orc):
+    for P, sign in ((20.0, -1), (-20.0, 1)):
+        o, desc = _lj_baro(orc, P)
+        o.run(50)
+        dL = o.npt_state()["box"][0] - desc["box"][0]
+        assert np.sign(dL) == sign
+    with pytest.raises(ValueError):
+        o.set_barostat(0.0, 0.0, 1.0)
