@@ -22,7 +22,8 @@ __all__ = [
     "FP64", "MIXED", "NVE", "NOSE_HOOVER", "LANGEVIN", "AtvbError",
     "Context", "System", "Batch", "Server", "make_desc",
     "NeighborList", "PairLJCut", "CoulLong", "KSpacePME", "VelocityVerlet",
-    "NoseHoover", "FixLangevin", "NoseHooverNPT", "Barostat", "MD", "library_path",
+    "NoseHoover", "FixLangevin", "NoseHooverNPT", "Barostat", "NVELimit", "Deform", "MD",
+    "library_path",
 ]
 
 FRAME_KEYS = ("x", "y", "z", "vx", "vy", "vz", "fx", "fy", "fz", "mass", "charge")
@@ -174,12 +175,14 @@ class System:
     """One MD system on the device (cuda::md::MD + its components)."""
 
     def __init__(self, ctx: Context, desc: SystemDesc | dict, frame: dict | None = None,
-                 lj_types=None, special_bonds=None, npt=None, barostat=None):
+                 lj_types=None, special_bonds=None, npt=None, barostat=None,
+                 nve_limit=None, deform=None):
         """lj_types: [(type_i, type_j, epsilon, sigma), ...] (PairLJCut's
         per-type form; per-atom types in frame["type"]); special_bonds:
         dict(lj=(s12, s13, s14), coul=(s12, s13, s14), bonds=[(tag_a, tag_b), ...]);
         npt: a NoseHooverNPT (MTK NPT in place of velocity Verlet, desc NVE);
-        barostat: a Barostat (Berendsen, beside the thermostat).
+        barostat: a Barostat (Berendsen, beside the thermostat); nve_limit:
+        xmax [A] (NVELimit); deform: (axis, strain_rate) (Deform).
         All are applied before the frame is uploaded."""
         self.ctx = ctx
         self.lib = ctx.lib
@@ -200,6 +203,10 @@ class System:
             check(self.lib.atvb_system_set_npt(self._h, C.byref(_npt_desc(npt))))
         if barostat is not None:
             check(self.lib.atvb_system_set_barostat(self._h, *_baro_args(barostat)))
+        if nve_limit is not None:
+            check(self.lib.atvb_system_set_nve_limit(self._h, float(nve_limit)))
+        if deform is not None:
+            check(self.lib.atvb_system_set_deform(self._h, int(deform[0]), float(deform[1])))
         if frame is not None:
             self.upload(frame)
 
@@ -352,6 +359,11 @@ class Batch:
                 check(self.lib.atvb_batch_set_npt(self._h, k, C.byref(_npt_desc(opts["npt"]))))
             if opts.get("barostat") is not None:
                 check(self.lib.atvb_batch_set_barostat(self._h, k, *_baro_args(opts["barostat"])))
+            if opts.get("nve_limit") is not None:
+                check(self.lib.atvb_batch_set_nve_limit(self._h, k, float(opts["nve_limit"])))
+            if opts.get("deform") is not None:
+                a, r = opts["deform"]
+                check(self.lib.atvb_batch_set_deform(self._h, k, int(a), float(r)))
         for k, it in enumerate(items):
             if it[1] is not None:
                 self.upload(k, it[1])
@@ -597,6 +609,23 @@ class NoseHooverNPT:
 
 
 @dataclass
+class NVELimit:
+    """NVELimit(dt, xmax) (cuda/dynamics/nve_limit.cuh): velocity Verlet with
+    each half kick's speed capped at xmax / dt.  An integrator."""
+    dt: float
+    xmax: float
+
+
+@dataclass
+class Deform:
+    """Deform(axis, strain_rate, dt) (cuda/dynamics/deform.cuh): constant
+    engineering strain along one axis; bound with set_thermostat."""
+    axis: int
+    strain_rate: float
+    dt: float
+
+
+@dataclass
 class Barostat:
     """Barostat(P_target, tau_P, dt, bulk_modulus=1.0) (Berendsen,
     cpu/dynamics/barostat.h:86): end-of-step pressure coupling beside the
@@ -667,8 +696,8 @@ class MD:
             else:
                 raise TypeError(f"unsupported evaluator {type(ev).__name__}")
         for th in self._thermostats:
-            if isinstance(th, Barostat):
-                continue              # applied after create (System barostat=)
+            if isinstance(th, (Barostat, Deform)):
+                continue              # applied after create (System barostat= / deform=)
             if isinstance(th, NoseHoover):
                 kw.update(thermostat=NOSE_HOOVER, temperature=th.T, tau=th.tau)
             elif isinstance(th, FixLangevin):
@@ -687,8 +716,11 @@ class MD:
             n = len(frame["x"])
             npt = self._integrator if isinstance(self._integrator, NoseHooverNPT) else None
             baro = next((t for t in self._thermostats if isinstance(t, Barostat)), None)
+            dfm = next((t for t in self._thermostats if isinstance(t, Deform)), None)
+            lim = self._integrator.xmax if isinstance(self._integrator, NVELimit) else None
             self._system = System(self.ctx, self.desc(n, box if box is not None else frame["box"]),
-                                  npt=npt, barostat=baro)
+                                  npt=npt, barostat=baro, nve_limit=lim,
+                                  deform=(dfm.axis, dfm.strain_rate) if dfm else None)
         sc = self._system.run(frame, n_steps)
         frame["box"] = tuple(sc["box"])   # the cell moves under NPT
         return sc

@@ -166,6 +166,10 @@ SIGNATURES = {
                                                C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "atvb_system_set_npt": (C.c_int, [_vp, C.POINTER(NptDesc)]),
     "atvb_system_set_barostat": (C.c_int, [_vp, C.c_double, C.c_double, C.c_double]),
+    "atvb_system_set_nve_limit": (C.c_int, [_vp, C.c_double]),
+    "atvb_system_set_deform": (C.c_int, [_vp, C.c_int32, C.c_double]),
+    "atvb_batch_set_nve_limit": (C.c_int, [_vp, C.c_int32, C.c_double]),
+    "atvb_batch_set_deform": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_double]),
     "atvb_batch_set_barostat": (C.c_int, [_vp, C.c_int32, C.c_double, C.c_double, C.c_double]),
     "atvb_server_keep_checkpoints": (C.c_int, [_vp, C.c_int32]),
     "atvb_server_suspend": (C.c_int, [_vp, C.c_int64]),

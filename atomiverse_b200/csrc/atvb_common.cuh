@@ -183,6 +183,15 @@ struct SysParams {
     // mu^3 = 1 - baro_coef (baro_P - P), baro_coef = dt / (tau_P bulk_modulus)
     int baro;
     double baro_P, baro_coef;
+    // md::NVELimit: speed cap vlimit = xmax / dt after each half kick (0: off)
+    double vlimit, vlimit2;
+    // the initial half through npt_drift_atom's per-axis factors (barostat,
+    // speed cap, deformation) instead of the plain kick-drift
+    int generic_drift;
+    // md::Deform: engineering strain along deform_axis (-1: off), the edge of
+    // step k being deform_L0 (1 + deform_rate dt k)
+    int deform_axis;
+    double deform_rate, deform_L0;
     // trajectory snapshots: every `snap_every` steps positions and
     // velocities go to a ring of `snap_depth` slots in host-mapped memory
     char* snap_ring;    // device view of the ring (null: off)

@@ -88,6 +88,8 @@ class Slot {
     atvb_npt_desc npt_desc{};
     bool baro = false; // Berendsen barostat configured (atvb_system_set_barostat)
     double baro_args[3] = {0, 0, 0}; // P_target, tau_P, bulk_modulus
+    double vlimit_xmax = 0.0;        // NVELimit xmax (0: plain velocity Verlet)
+    double deform_args[3] = {0, 0, 0}; // Deform axis, strain rate, L0
     char* snap_host = nullptr; // trajectory snapshot ring (host-mapped)
     long long snap_read = 0;   // snapshots consumed by the host
 
@@ -120,6 +122,8 @@ class Engine {
                            int64_t nbonds, const int64_t* a, const int64_t* b);
     void set_npt(int id, const atvb_npt_desc& p);
     void set_barostat(int id, double P_target, double tau_P, double bulk_modulus);
+    void set_nve_limit(int id, double xmax);
+    void set_deform(int id, int axis, double rate, double L0 = 0.0);
     void set_snapshots(int id, int every, int depth);
     int poll_snapshots(int id, int max_frames, int64_t* steps, double* box,
                        double* const out[6], int64_t* dropped);

@@ -286,6 +286,38 @@ int atvb_batch_set_barostat(atvb_batch* b, int32_t index, double P_target, doubl
     });
 }
 
+int atvb_system_set_nve_limit(atvb_system* sys, double xmax) {
+    return guard([&] {
+        need(sys, "sys");
+        sys->eng->set_nve_limit(sys->id, xmax);
+    });
+}
+
+int atvb_system_set_deform(atvb_system* sys, int32_t axis, double strain_rate) {
+    return guard([&] {
+        need(sys, "sys");
+        sys->eng->set_deform(sys->id, axis, strain_rate);
+    });
+}
+
+int atvb_batch_set_nve_limit(atvb_batch* b, int32_t index, double xmax) {
+    return guard([&] {
+        need(b, "batch");
+        if (index < 0 || index >= (int)b->ids.size())
+            throw Error(ATVB_ERR_NOTFOUND, "no system " + std::to_string(index) + " in batch");
+        b->eng->set_nve_limit(b->ids[index], xmax);
+    });
+}
+
+int atvb_batch_set_deform(atvb_batch* b, int32_t index, int32_t axis, double strain_rate) {
+    return guard([&] {
+        need(b, "batch");
+        if (index < 0 || index >= (int)b->ids.size())
+            throw Error(ATVB_ERR_NOTFOUND, "no system " + std::to_string(index) + " in batch");
+        b->eng->set_deform(b->ids[index], axis, strain_rate);
+    });
+}
+
 int atvb_system_set_npt(atvb_system* sys, const atvb_npt_desc* npt) {
     return guard([&] {
         need(sys, "sys");

@@ -335,6 +335,7 @@ Slot::Slot(const atvb_system_desc& d, const DevMem& mem) : desc(d), mem_(mem) {
     if (n > kMaxAtoms)
         throw Error(ATVB_ERR_INVALID, "at most 2^30 - 1 atoms per system");
     hp.n = n;
+    hp.deform_axis = -1;
     hp.prec = d.precision == ATVB_MIXED ? kMixed : kFP64;
     if (d.precision != ATVB_FP64 && d.precision != ATVB_MIXED)
         throw Error(ATVB_ERR_INVALID, "unknown precision");
@@ -403,6 +404,13 @@ Slot::Slot(const atvb_system_desc& d, const DevMem& mem) : desc(d), mem_(mem) {
             throw Error(ATVB_ERR_INVALID,
                         "CoulLong: alpha * (cutoff + skin) must not exceed 26");
     }
+    // the largest interaction cutoff: the build-cell displacement rule of the
+    // per-axis drift path (barostats, speed cap, deformation)
+    hp.npt_cut = d.nl_cutoff;
+    if (hp.has_lj)
+        hp.npt_cut = std::max(hp.npt_cut, d.lj_cutoff);
+    if (hp.has_coul)
+        hp.npt_cut = std::max(hp.npt_cut, d.coul_cutoff);
     // integrator / thermostat
     if (!(d.dt > 0.0))
         throw Error(ATVB_ERR_INVALID, "VelocityVerlet: dt must be > 0");
@@ -758,7 +766,7 @@ void Engine::ensure_table() {
 
 void Engine::push_params(int id) {
     Slot* s = slot(id);
-    if ((s->npt || s->baro) && s->uploaded) {
+    if ((s->npt || s->baro || s->hp.deform_axis >= 0) && s->uploaded) {
         // the device owns an NPT system's cell: keep it
         SysParams dev;
         CK(cudaMemcpyAsync(&dev, d_sp_ + id, sizeof(SysParams), cudaMemcpyDeviceToHost,
@@ -1249,6 +1257,10 @@ void Engine::set_npt(int id, const atvb_npt_desc& p) {
                     "NoseHooverNPT replaces the thermostat: the system must be NVE");
     if (sl->baro)
         throw Error(ATVB_ERR_INVALID, "Barostat and NoseHooverNPT cannot be combined");
+    if (sl->vlimit_xmax > 0.0)
+        throw Error(ATVB_ERR_INVALID, "NoseHooverNPT replaces velocity Verlet, as NVELimit does");
+    if (sl->hp.deform_axis >= 0)
+        throw Error(ATVB_ERR_INVALID, "Deform cannot be combined with a barostat here");
     if (p.mtchain < 1 || p.mtchain > kMaxChain || p.mpchain < 1 || p.mpchain > kMaxChain)
         throw Error(ATVB_ERR_INVALID, "NoseHooverNPT: chain lengths must be in [1, 10]");
     if (!(p.tau_T > 0.0) || !(p.tau_P > 0.0) || !(p.T_start > 0.0))
@@ -1305,6 +1317,8 @@ void Engine::set_barostat(int id, double P_target, double tau_P, double bulk_mod
         throw Error(ATVB_ERR_STATE, "Barostat must be set before the first upload");
     if (sl->npt)
         throw Error(ATVB_ERR_INVALID, "Barostat and NoseHooverNPT cannot be combined");
+    if (sl->hp.deform_axis >= 0)
+        throw Error(ATVB_ERR_INVALID, "Deform cannot be combined with a barostat here");
     if (!(tau_P > 0.0) || !(bulk_modulus > 0.0) || !std::isfinite(P_target))
         throw Error(ATVB_ERR_INVALID, "Barostat: tau_P and bulk_modulus must be > 0");
     SysParams& h = sl->hp;
@@ -1315,6 +1329,7 @@ void Engine::set_barostat(int id, double P_target, double tau_P, double bulk_mod
         shrink = 0.0;
     sl->replan_cells(shrink);
     h.baro = 1;
+    h.generic_drift = 1;
     h.baro_P = P_target;
     h.baro_coef = h.dt / (tau_P * bulk_modulus);
     h.need_virial = 1;
@@ -1329,6 +1344,57 @@ void Engine::set_barostat(int id, double P_target, double tau_P, double bulk_mod
     sl->baro_args[1] = tau_P;
     sl->baro_args[2] = bulk_modulus;
     any_npt_ = true;
+    push_params(id);
+    dirty_ = true;
+}
+
+// md::Deform(axis, strain_rate, dt) (cuda/dynamics/deform.cuh): constant
+// engineering strain rate along one axis, from the cell at the first upload
+// (L0 > 0: from that edge, as a re-planned system keeps its original L0).
+void Engine::set_deform(int id, int axis, double rate, double L0) {
+    Slot* sl = slot(id);
+    if (sl->uploaded)
+        throw Error(ATVB_ERR_STATE, "Deform must be set before the first upload");
+    if (axis < 0 || axis > 2)
+        throw Error(ATVB_ERR_INVALID, "Deform: axis must be 0, 1 or 2");
+    if (!std::isfinite(rate))
+        throw Error(ATVB_ERR_INVALID, "Deform: bad strain rate");
+    if (sl->npt || sl->baro)
+        throw Error(ATVB_ERR_INVALID, "Deform cannot be combined with a barostat here");
+    SysParams& h = sl->hp;
+    double shrink = 0.1;
+    for (int k = 0; k < 3; ++k)
+        shrink = std::min(shrink, 1.0 - 2.0 * sl->geo.rlist * (1.0 + 1e-9) / sl->geo.L[k]);
+    if (shrink < 0.0)
+        shrink = 0.0;
+    sl->replan_cells(shrink);
+    h.deform_axis = axis;
+    h.deform_rate = rate;
+    h.deform_L0 = L0 > 0.0 ? L0 : sl->geo.L[axis];
+    h.generic_drift = 1;
+    sl->deform_args[0] = axis;
+    sl->deform_args[1] = rate;
+    sl->deform_args[2] = h.deform_L0;
+    any_npt_ = true;
+    push_params(id);
+    dirty_ = true;
+}
+
+// md::NVELimit(dt, xmax) (cuda/dynamics/nve_limit.cuh): velocity Verlet
+// with each half kick's speed capped at xmax / dt.
+void Engine::set_nve_limit(int id, double xmax) {
+    Slot* sl = slot(id);
+    if (sl->uploaded)
+        throw Error(ATVB_ERR_STATE, "NVELimit must be set before the first upload");
+    if (sl->npt)
+        throw Error(ATVB_ERR_INVALID, "NVELimit replaces velocity Verlet, as NoseHooverNPT does");
+    if (!(xmax > 0.0))
+        throw Error(ATVB_ERR_INVALID, "NVELimit: xmax must be > 0");
+    SysParams& h = sl->hp;
+    h.vlimit = xmax / h.dt;
+    h.vlimit2 = h.vlimit * h.vlimit;
+    h.generic_drift = 1;
+    sl->vlimit_xmax = xmax;
     push_params(id);
     dirty_ = true;
 }
@@ -1951,7 +2017,7 @@ void Engine::restore(int id, const void* buf, size_t size, bool fresh_list) {
     // 1. the positions and cell of the last neighbour build: the upload's
     //    list build then reproduces the saved run's list (fresh_list: a new
     //    list from the current positions in the current cell instead)
-    if (s->npt || s->baro)
+    if (s->npt || s->baro || P.deform_axis >= 0)
         apply_box(P, fresh_list ? st.box : st.Lb, true);
     const int bx = fresh_list ? 0 : 9;
     atvb_soa_view v;
@@ -1971,7 +2037,7 @@ void Engine::restore(int id, const void* buf, size_t size, bool fresh_list) {
     v.type = type.empty() ? nullptr : type.data();
     upload(id, v);
     // 2. the current cell, positions and state
-    if (s->npt || s->baro) {
+    if (s->npt || s->baro || P.deform_axis >= 0) {
         apply_box(P, st.box, true);
         CK(cudaMemcpyAsync(d_sp_ + id, &P, sizeof(SysParams), cudaMemcpyHostToDevice,
                            stream_));
@@ -2029,7 +2095,7 @@ void Engine::restore(int id, const void* buf, size_t size, bool fresh_list) {
 // list differently).
 void Engine::replan_npt() {
     for (auto& up : slots_) {
-        if (!up || !(up->npt || up->baro) || !up->uploaded)
+        if (!up || !(up->npt || up->baro || up->hp.deform_axis >= 0) || !up->uploaded)
             continue;
         Slot* old = up.get();
         SysState st;
@@ -2075,6 +2141,9 @@ void Engine::replan_npt() {
         old->snap_host = nullptr;
         const atvb_npt_desc npt = old->npt_desc;
         const bool was_npt = old->npt, was_baro = old->baro;
+        const double vx = old->vlimit_xmax;
+        const bool was_def = old->hp.deform_axis >= 0;
+        const double da[3] = {old->deform_args[0], old->deform_args[1], old->deform_args[2]};
         const double ba[3] = {old->baro_args[0], old->baro_args[1], old->baro_args[2]};
         CK(cudaStreamSynchronize(stream_));
         release_graph();
@@ -2086,6 +2155,10 @@ void Engine::replan_npt() {
             set_npt(id, npt);
         if (was_baro)
             set_barostat(id, ba[0], ba[1], ba[2]);
+        if (vx > 0.0)
+            set_nve_limit(id, vx);
+        if (was_def)
+            set_deform(id, (int)da[0], da[1], da[2]);
         restore(id, blob.data(), blob.size(), true);
     }
 }

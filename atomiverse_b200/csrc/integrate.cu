@@ -55,6 +55,20 @@ ATVB_DEV double fix_to_d(unsigned long long v) {
     return (double)(long long)v * kEFixInv;
 }
 
+// md::NVELimit (nve_limit.cu:20-30, LAMMPS fix nve/limit): after a half
+// kick, a speed above vmax = xmax / dt is scaled back to vmax.
+ATVB_DEV void speed_cap(const SysParams& P, double v[3]) {
+    if (!(P.vlimit2 > 0.0))
+        return;
+    const double vsq = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+    if (vsq > P.vlimit2) {
+        const double s = P.vlimit / sqrt(vsq);
+        v[0] *= s;
+        v[1] *= s;
+        v[2] *= s;
+    }
+}
+
 // MTK NPT initial half for atom i (nose_hoover_npt.cpp:812-850 P2-P6): the
 // pending per-axis velocity scale (end-of-step chain and barostat factors of
 // the previous step, initial-half ones of this step), the force kick, the
@@ -72,8 +86,11 @@ ATVB_DEV double npt_drift_atom(const SysParams& P, int i) {
     double x[3];
     double d2 = 0.0;
 #pragma unroll
-    for (int d = 0; d < 3; ++d) {
+    for (int d = 0; d < 3; ++d)
         v[d] = __dadd_rn(__dmul_rn(v[d], st->vs[d]), __dmul_rn(dtfm, fa[d]));
+    speed_cap(P, v);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
         const double Ln = st->Lnext[d];
         double xd = __dadd_rn(__dmul_rn(xs[d][i], st->npt_a[d]),
                               __dmul_rn(__dmul_rn(v[d], P.dt), st->npt_drift[d]));
@@ -115,7 +132,7 @@ __global__ void __launch_bounds__(kChunk)
         const SysParams& P = sp[item.sys];
         const int i = item.begin + threadIdx.x;
         double ke = 0.0;
-        if (i < P.n && (P.thermostat == kNPT || P.baro)) {
+        if (i < P.n && (P.thermostat == kNPT || P.generic_drift)) {
             ke = npt_drift_atom(P, i);
         } else if (i < P.n) {
             const double sc = P.st->vscale;
@@ -174,7 +191,7 @@ __global__ void k_sys_a(const int* sys_list, int nsys, const SysParams* sp) {
         return;
     const SysParams& P = sp[sys_list[k]];
     SysState* st = P.st;
-    if (P.thermostat == kNPT) {
+    if (P.thermostat == kNPT || P.deform_axis >= 0) {
         // commit the cell of this step's drift: every later kernel of the
         // step (neighbour build, forces, PME) reads it from SysParams
         apply_box(const_cast<SysParams&>(sp[sys_list[k]]), st->Lnext, true);
@@ -255,6 +272,7 @@ __global__ void __launch_bounds__(kChunk)
             v[0] = __dadd_rn(v[0], __dmul_rn(dtfm, f.x));
             v[1] = __dadd_rn(v[1], __dmul_rn(dtfm, f.y));
             v[2] = __dadd_rn(v[2], __dmul_rn(dtfm, f.z));
+            speed_cap(P, v);
             P.vx[i] = v[0];
             P.vy[i] = v[1];
             P.vz[i] = v[2];
@@ -351,6 +369,43 @@ ATVB_DEV void berendsen(const SysParams& P, SysState* st) {
         st->need_rebuild = 1;
 }
 
+// md::Deform (deform.cu:55-95, initial_integrate +200: after the drift):
+// the k-th deformation step takes the axis edge from L0 (1 + r dt (k-1)) to
+// L0 (1 + r dt k) (engineering strain, linear in time) and scales positions
+// along it by the same ratio.  Folded into the next initial half's drift
+// (x s + v dt s along the axis, in the new cell); k_sys_a commits the cell.
+ATVB_DEV void deform_prepare(const SysParams& P, SysState* st, long long k) {
+    const int ax = P.deform_axis;
+    const double rdt = P.deform_rate * P.dt;
+    const double Lp = P.deform_L0 * (1.0 + rdt * (double)(k - 1));
+    const double Lc = P.deform_L0 * (1.0 + rdt * (double)k);
+    const double sc = Lc / Lp;
+    double lam = 1e300;
+    bool ok = true;
+    for (int d = 0; d < 3; ++d) {
+        const double f = d == ax ? sc : 1.0;
+        st->vs[d] = st->vscale;
+        st->vs_out[d] = st->vscale;
+        st->npt_a[d] = f;
+        st->npt_drift[d] = f;
+        st->Lnext[d] = P.L[d] * f;
+        if (!(st->Lnext[d] >= P.npt_Lmin[d]))
+            ok = false;
+    }
+    if (!ok)
+        st->status |= kStatusBoxRange;
+    for (int d = 0; d < 3; ++d) {
+        st->fixn_scale[d] = 4294967296.0 / st->Lnext[d];
+        st->fixn64_scale[d] = 18446744073709551616.0 / st->Lnext[d];
+        st->ub[d] = st->Lb[d] / st->Lnext[d];
+        lam = fmin(lam, st->Lnext[d] / st->Lb[d]);
+    }
+    const double thr = 0.5 * (P.rlist - P.npt_cut / lam);
+    st->disp_thr2 = thr > 0.0 ? thr * thr : -1.0;
+    if (thr <= 0.0)
+        st->need_rebuild = 1;
+}
+
 // Positions scaled by this step's Berendsen dilation (original order).
 __global__ void k_baro_scale(const Item* items, int nitems, const SysParams* sp) {
     for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
@@ -421,6 +476,11 @@ __global__ void k_sys_b(const int* sys_list, int nsys, const SysParams* sp) {
     cell_scalars(P, st);
     if (P.baro)
         berendsen(P, st);
+    else if (P.deform_axis >= 0)
+        deform_prepare(P, st, st->step + 2); // st->step counts this step only below
+    else if (P.generic_drift)
+        for (int d = 0; d < 3; ++d)
+            st->vs[d] = st->vscale; // fixed cell: the identity drift factors stay
     if (P.ehist_cap > 0) {
         const long long slot = st->step % P.ehist_cap;
         P.ehist[3 * slot + 0] = st->energy;
@@ -578,6 +638,10 @@ __global__ void k_npt_prep(const int* sys_list, int nsys, const SysParams* sp) {
         return;
     const SysParams& P = sp[sys_list[k]];
     SysState* st = P.st;
+    if (P.deform_axis >= 0 && st->step == 0) {
+        deform_prepare(P, st, 1);
+        return;
+    }
     if (P.thermostat != kNPT || st->step != 0)
         return;
     double ke[3];

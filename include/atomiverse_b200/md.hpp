@@ -161,6 +161,25 @@ struct FixLangevin {
     FixLangevin(double t0, double t1, double damp_, double dt_, uint32_t seed_)
         : T_start(t0), T_stop(t1 < 0 ? t0 : t1), damp(damp_), dt(dt_), seed(seed_) {}
 };
+/// md::NVELimit(dt, xmax) (cuda/dynamics/nve_limit.cuh): velocity Verlet
+/// with each half kick's speed capped at xmax / dt.  An integrator.
+struct NVELimit {
+    double dt, xmax;
+    NVELimit(double dt_, double xmax_) : dt(dt_), xmax(xmax_) {
+        if (!(xmax_ > 0.0))
+            throw std::invalid_argument("NVELimit: xmax must be > 0");
+    }
+};
+/// md::Deform(axis, strain_rate, dt) (cuda/dynamics/deform.cuh): constant
+/// engineering strain rate along one axis after each drift.
+struct Deform {
+    int axis;
+    double strain_rate, dt;
+    Deform(int axis_, double rate, double dt_) : axis(axis_), strain_rate(rate), dt(dt_) {
+        if (axis_ < 0 || axis_ > 2)
+            throw std::invalid_argument("Deform: axis must be 0, 1 or 2");
+    }
+};
 /// md::Barostat(P_target, tau_P, dt, bulk_modulus = 1) -- Berendsen pressure
 /// coupling at end_of_step beside the thermostat (cpu/dynamics/barostat.h:86;
 /// LAMMPS-standard pressure sign).  Bound with set_thermostat.
@@ -273,6 +292,20 @@ class MD {
         npt_ = v.p;
         have_npt_ = true;
         have_integrator_ = true;
+        return *this;
+    }
+    MD& set_integrator(const NVELimit& v) {
+        if (have_integrator_)
+            throw std::invalid_argument("set_integrator already configured");
+        d_.dt = v.dt;
+        vlimit_ = v.xmax;
+        have_integrator_ = true;
+        return *this;
+    }
+    /// Deform binds at initial_integrate +200 (deform.cu:40-46).
+    MD& set_deform(const Deform& d) {
+        deform_axis_ = d.axis;
+        deform_rate_ = d.strain_rate;
         return *this;
     }
     MD& set_thermostat(const Barostat& b) {
@@ -399,6 +432,10 @@ class MD {
             if (have_baro_)
                 check(atvb_system_set_barostat(sys_, baro_.P_target, baro_.tau_P,
                                                baro_.bulk_modulus));
+            if (vlimit_ > 0.0)
+                check(atvb_system_set_nve_limit(sys_, vlimit_));
+            if (deform_axis_ >= 0)
+                check(atvb_system_set_deform(sys_, deform_axis_, deform_rate_));
             if (!lj_coeffs_.empty()) {
                 std::vector<int32_t> ti, tj;
                 std::vector<double> e, sg;
@@ -438,6 +475,9 @@ class MD {
     int snap_every_ = 0, snap_depth_ = 0;
     Barostat baro_{0.0, 1.0, 1.0};
     bool have_baro_ = false;
+    double vlimit_ = 0.0;
+    int deform_axis_ = -1;
+    double deform_rate_ = 0.0;
     SpecialScales lj_special_, coul_special_;
 };
 } // namespace md

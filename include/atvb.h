@@ -220,6 +220,14 @@ int atvb_system_set_npt(atvb_system* sys, const atvb_npt_desc* npt);
  * then always computed.  Before the first upload; not with set_npt. */
 int atvb_system_set_barostat(atvb_system* sys, double P_target, double tau_P,
                              double bulk_modulus);
+/* md::NVELimit(dt, xmax) (cuda/dynamics/nve_limit.cuh, nve_limit.cu:20-130):
+ * velocity Verlet whose half kicks cap the speed at xmax / dt [A]. */
+int atvb_system_set_nve_limit(atvb_system* sys, double xmax);
+/* md::Deform(axis, strain_rate, dt) (cuda/dynamics/deform.cuh,
+ * deform.cu:55-95): after the drift of step k the edge along `axis` is
+ * L0 (1 + strain_rate dt k) (engineering strain, L0 the edge at upload) and
+ * positions along it are scaled by the same ratio.  Not with a barostat. */
+int atvb_system_set_deform(atvb_system* sys, int32_t axis, double strain_rate);
 /* Checkpoints (state I/O; the reference's resumable record is
  * cpu/record/mrec.h MrecWriter::flush, a molrs Zarr store, and
  * cpu/io/frame_writer.h write_frame_zarr): the whole resumable state of a
@@ -280,6 +288,8 @@ int atvb_batch_restore(atvb_batch* b, int32_t index, const void* buf, int64_t si
 int atvb_batch_set_npt(atvb_batch* b, int32_t index, const atvb_npt_desc* npt);
 int atvb_batch_set_barostat(atvb_batch* b, int32_t index, double P_target, double tau_P,
                             double bulk_modulus);
+int atvb_batch_set_nve_limit(atvb_batch* b, int32_t index, double xmax);
+int atvb_batch_set_deform(atvb_batch* b, int32_t index, int32_t axis, double strain_rate);
 int atvb_batch_set_lj_types(atvb_batch* b, int32_t index, int32_t ncoef,
                             const int32_t* type_i, const int32_t* type_j,
                             const double* epsilon, const double* sigma);

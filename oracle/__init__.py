@@ -119,6 +119,10 @@ def lib():
         L.orc_npt_state.argtypes = [C.c_void_p, dp]
         L.orc_set_barostat.restype = C.c_int
         L.orc_set_barostat.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double]
+        L.orc_set_nve_limit.restype = C.c_int
+        L.orc_set_nve_limit.argtypes = [C.c_void_p, C.c_double]
+        L.orc_set_deform.restype = C.c_int
+        L.orc_set_deform.argtypes = [C.c_void_p, C.c_int, C.c_double]
         _lib = L
     return _lib
 
@@ -253,6 +257,14 @@ class OracleSystem:
         """Berendsen barostat at end_of_step (P in eV/A^3)."""
         if lib().orc_set_barostat(self._h, float(P), float(tau_P), float(bulk_modulus)) != 0:
             raise ValueError("bad barostat parameters")
+
+    def set_nve_limit(self, xmax):
+        if lib().orc_set_nve_limit(self._h, float(xmax)) != 0:
+            raise ValueError("bad xmax")
+
+    def set_deform(self, axis, rate):
+        if lib().orc_set_deform(self._h, int(axis), float(rate)) != 0:
+            raise ValueError("bad deform axis")
 
     def npt_state(self) -> dict:
         o = np.zeros(NPT_NSTATE)

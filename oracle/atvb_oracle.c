@@ -125,6 +125,11 @@ struct orc_sys {
     /* Berendsen barostat (barostat.cpp) */
     int baro_on;
     double baro_P, baro_tau, baro_bulk;
+    /* NVELimit speed cap (0: off) and Deform (axis -1: off) */
+    double vmax;
+    int def_axis;
+    double def_rate, def_L0;
+    int64_t def_count;
 };
 
 orc_sys* orc_create(const orc_desc* d) {
@@ -141,6 +146,7 @@ orc_sys* orc_create(const orc_desc* d) {
     s->num = (int32_t*)calloc(n, sizeof(int32_t));
     s->nbr = NULL;
     s->nbr_cap = 0;
+    s->def_axis = -1;
     s->n_dof = 3 * d->n - 3;
     if (s->n_dof < 0)
         s->n_dof = 0;
@@ -1641,6 +1647,53 @@ static void berendsen(orc_sys* s) {
     }
 }
 
+/* NVELimit (nve_limit.cu:20-30, LAMMPS fix nve/limit): after a half kick a
+ * speed above xmax / dt is scaled back to it. */
+static inline void speed_cap(const orc_sys* s, int i) {
+    if (!(s->vmax > 0.0))
+        return;
+    const double vsq = s->vx[i] * s->vx[i] + s->vy[i] * s->vy[i] + s->vz[i] * s->vz[i];
+    if (vsq > s->vmax * s->vmax) {
+        const double f = s->vmax / sqrt(vsq);
+        s->vx[i] *= f;
+        s->vy[i] *= f;
+        s->vz[i] *= f;
+    }
+}
+
+/* Deform (deform.cu:55-95, initial_integrate +200): the k-th step takes the
+ * axis edge from L0 (1 + r dt (k-1)) to L0 (1 + r dt k) and scales positions
+ * along the axis by the ratio. */
+static void deform(orc_sys* s) {
+    s->def_count += 1;
+    const double rdt = s->def_rate * s->d.dt;
+    const double Lp = s->def_L0 * (1.0 + rdt * (double)(s->def_count - 1));
+    const double Lc = s->def_L0 * (1.0 + rdt * (double)s->def_count);
+    const double f = Lc / Lp;
+    double* p = s->def_axis == 0 ? s->x : (s->def_axis == 1 ? s->y : s->z);
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < s->n; ++i)
+        p[i] *= f;
+    s->d.L[s->def_axis] *= f;
+}
+
+int orc_set_nve_limit(orc_sys* s, double xmax) {
+    if (!(xmax > 0.0))
+        return -1;
+    s->vmax = xmax / s->d.dt;
+    return 0;
+}
+
+int orc_set_deform(orc_sys* s, int axis, double rate) {
+    if (axis < 0 || axis > 2)
+        return -1;
+    s->def_axis = axis;
+    s->def_rate = rate;
+    s->def_L0 = s->d.L[axis];
+    s->def_count = 0;
+    return 0;
+}
+
 int orc_set_barostat(orc_sys* s, double P_target, double tau_P, double bulk_modulus) {
     if (!(tau_P > 0.0) || !(bulk_modulus > 0.0) || s->npt_on)
         return -1;
@@ -1682,6 +1735,7 @@ int orc_run(orc_sys* s, int n_steps, double* hist) {
             s->vx[i] += dtfm * s->fx[i];
             s->vy[i] += dtfm * s->fy[i];
             s->vz[i] += dtfm * s->fz[i];
+            speed_cap(s, i);
             s->x[i] += dt * s->vx[i];
             s->y[i] += dt * s->vy[i];
             s->z[i] += dt * s->vz[i];
@@ -1691,12 +1745,14 @@ int orc_run(orc_sys* s, int n_steps, double* hist) {
         }
         if (s->d.thermostat == ORC_THERMO_NH)
             nose_hoover(s);
+        if (s->def_axis >= 0)
+            deform(s);
         /* neighbor decide (neighbor_list.h:128-141) */
         s->ago++;
         const int every = s->d.nl_every < 1 ? 1 : s->d.nl_every;
         const int delay = s->d.nl_delay < 0 ? 0 : s->d.nl_delay;
         /* the cell changes every step under the barostat: rebuild every step */
-        if (s->baro_on || (s->ago >= delay && (s->ago % every) == 0 &&
+        if (s->baro_on || s->def_axis >= 0 || (s->ago >= delay && (s->ago % every) == 0 &&
                            (!s->d.nl_check || needs_rebuild(s)))) {
             orc_build_list(s);
             ++rebuilds;
@@ -1714,6 +1770,7 @@ int orc_run(orc_sys* s, int n_steps, double* hist) {
             s->vx[i] += dtfm * s->fx[i];
             s->vy[i] += dtfm * s->fy[i];
             s->vz[i] += dtfm * s->fz[i];
+            speed_cap(s, i);
         }
         if (s->d.thermostat == ORC_THERMO_NH)
             nose_hoover(s);

@@ -126,6 +126,12 @@ int orc_set_npt(orc_sys* s, const orc_npt* p);
  * src/cpu/dynamics/barostat.cpp:22-110) at end_of_step, beside velocity
  * Verlet and the thermostat; P_target in eV/A^3.  Returns 0 or -1. */
 int orc_set_barostat(orc_sys* s, double P_target, double tau_P, double bulk_modulus);
+/* NVELimit(dt, xmax) (cuda/dynamics/nve_limit.cu:20-130): speed cap xmax/dt
+ * after each half kick.  Deform(axis, strain_rate, dt) (cuda/dynamics/
+ * deform.cu:55-95): engineering strain along one axis after the drift.
+ * Return 0 or -1 on a bad argument. */
+int orc_set_nve_limit(orc_sys* s, double xmax);
+int orc_set_deform(orc_sys* s, int axis, double rate);
 /* NPT state: [0..2] box edges, [3] conserved extended Hamiltonian,
  * [4..6] eps_dot, [7] eta_t[0], [8] eta_t_dot[0], [9] eta_b[0],
  * [10] eta_b_dot[0], [11] live temperature setpoint, [12] KE_global. */

@@ -252,3 +252,39 @@ def test_berendsen_batch_equals_alone_and_resumes(atvb, ctx):
     for k in ("x", "y", "z", "vx", "vy", "vz"):
         assert np.array_equal(ob[k], oa[k]), k
     assert np.array_equal(sb["box"], sa["box"])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["nve_limit", "deform"])
+def test_nve_limit_and_deform_match_oracle(atvb, ctx, orc, kind):
+    """md::NVELimit (speed cap) and md::Deform (engineering strain) against
+    the oracle over 150 steps (FP64)."""
+    from atomiverse_b200 import workloads as W
+    desc, frame = W.lj_fcc(ncell=6, t_star=3.0 if kind == "nve_limit" else 1.0, seed=3)
+    if kind == "nve_limit":
+        opts, xmax = dict(nve_limit=0.002), 0.002
+    else:
+        opts = dict(deform=(2, 2e-3))
+    s = atvb.System(ctx, desc, frame, **opts)
+    s.compute_forces()
+    s.step(150)
+    out, sc = s.download()
+    s.close()
+    o = oracle_system(orc, desc, frame)
+    if kind == "nve_limit":
+        o.set_nve_limit(xmax)
+    else:
+        o.set_deform(2, 2e-3)
+    o.build_list()
+    o.compute_forces()
+    o.run(150)
+    box = o.npt_state()["box"]
+    assert np.allclose(sc["box"], box, rtol=1e-12, atol=0)
+    d = _pos(out) - _pos(o.state())
+    d -= np.rint(d / sc["box"]) * sc["box"]
+    assert np.abs(d).max() < 1e-8
+    if kind == "deform":
+        assert sc["box"][2] > desc["box"][2] * 1.01
+    else:
+        v = np.sqrt(out["vx"] ** 2 + out["vy"] ** 2 + out["vz"] ** 2)
+        assert v.max() <= xmax / desc["dt"] * (1 + 1e-12)

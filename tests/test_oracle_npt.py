@@ -167,3 +167,44 @@ def test_berendsen_moves_the_cell_toward_the_target(orc):
         assert np.sign(dL) == sign
     with pytest.raises(ValueError):
         o.set_barostat(0.0, 0.0, 1.0)
+
+
+def test_deform_follows_engineering_strain(orc):
+    """deform.cu:55-95: after k steps the edge is L0 (1 + rate dt k)."""
+    from atomiverse_b200 import workloads as W
+    import sys, os
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    from conftest import oracle_system
+    desc, frame = W.lj_fcc(ncell=5, t_star=1.0, seed=3)
+    o = oracle_system(orc, desc, frame)
+    rate = 2e-3
+    o.set_deform(2, rate)
+    o.build_list()
+    o.compute_forces()
+    o.run(40)
+    L = o.npt_state()["box"]
+    L0 = desc["box"][0]
+    assert L[2] == pytest.approx(L0 * (1.0 + rate * desc["dt"] * 40), rel=1e-13)
+    assert L[0] == L0 and L[1] == L0
+    with pytest.raises(ValueError):
+        o.set_deform(3, rate)
+
+
+def test_nve_limit_caps_speeds(orc):
+    """nve_limit.cu:20-30: no atom moves faster than xmax / dt."""
+    from atomiverse_b200 import workloads as W
+    import sys, os
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    from conftest import oracle_system
+    desc, frame = W.lj_fcc(ncell=5, t_star=3.0, seed=3)
+    o = oracle_system(orc, desc, frame)
+    xmax = 0.002
+    o.set_nve_limit(xmax)
+    o.build_list()
+    o.compute_forces()
+    o.run(5)
+    st = o.state()
+    v = np.sqrt(st["vx"] ** 2 + st["vy"] ** 2 + st["vz"] ** 2)
+    vmax = xmax / desc["dt"]
+    assert v.max() <= vmax * (1 + 1e-12)
+    assert v.max() > 0.99 * vmax                  # the cap was active
