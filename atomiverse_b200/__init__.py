@@ -664,8 +664,14 @@ class MD:
         return self
 
     def set_thermostat(self, th):
+        """Plural (md.cuh:229-233): Nose-Hoover / Langevin, or any component
+        bound at its default slot (Deform, Barostat)."""
         self._thermostats.append(th)
         return self
+
+    def set_barostat(self, b: "Barostat"):
+        """LAMMPS `fix press/berendsen` (md.cuh:239-243)."""
+        return self.set_thermostat(b)
 
     def set_stress_required(self, on: bool = True):
         self._stress = on

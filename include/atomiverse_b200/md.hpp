@@ -302,17 +302,22 @@ class MD {
         have_integrator_ = true;
         return *this;
     }
-    /// Deform binds at initial_integrate +200 (deform.cu:40-46).
-    MD& set_deform(const Deform& d) {
+    /// Deform is a plain component: set_thermostat binds it at its default
+    /// slot, initial_integrate +200 (md.cuh:229-233, deform.cu:40-46).
+    MD& set_thermostat(const Deform& d) {
         deform_axis_ = d.axis;
         deform_rate_ = d.strain_rate;
         return *this;
     }
-    MD& set_thermostat(const Barostat& b) {
+    MD& set_deform(const Deform& d) { return set_thermostat(d); }
+    /// LAMMPS `fix press/berendsen` (md.cuh:239-243); set_thermostat takes
+    /// it too, as the reference's bind_defaults does.
+    MD& set_barostat(const Barostat& b) {
         baro_ = b;
         have_baro_ = true;
         return *this;
     }
+    MD& set_thermostat(const Barostat& b) { return set_barostat(b); }
     MD& set_thermostat(const NoseHoover& t) {
         d_.thermostat = ATVB_NOSE_HOOVER;
         d_.temperature = t.T;

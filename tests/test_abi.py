@@ -70,3 +70,34 @@ def test_cpp_header_compiles():
                             "-"], input='#include "atvb.h"\nint main(void){return 0;}\n',
                            capture_output=True, text=True)
         assert r.returncode == 0, r.stderr
+
+
+def test_cpp_mirror_compiles():
+    """The header-only C++ mirror compiles with every component bound, and
+    so does each C++ driver program under tests/cpp."""
+    snippet = r'''
+#include <atomiverse_b200/md.hpp>
+int main() {
+    using namespace atvb_cpp;
+    md::MD a(0, ATVB_FP64);
+    a.set_neighbor(NeighborList(2.5, 0.3)).set_evaluator(PairLJCut(1.0, 1.0, 2.5))
+     .set_integrator(md::NVELimit(0.005, 0.01));
+    a.set_thermostat(md::Deform(2, 1e-3, 0.005));
+    a.set_barostat(md::Barostat(0.0, 1.0, 0.005));
+    md::MD b(0, ATVB_MIXED);
+    b.set_neighbor(NeighborList(2.5, 0.3)).set_evaluator(PairLJCut(1.0, 1.0, 2.5))
+     .set_integrator(md::NoseHooverNPT(100.0, 0.1, 0.0, 1.0, 0.005));
+    return 0;
+}
+'''
+    r = subprocess.run(["g++", "-std=c++17", "-x", "c++", "-fsyntax-only", "-I",
+                        os.path.join(ROOT, "include"), "-"], input=snippet,
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    cpp = os.path.join(ROOT, "tests", "cpp")
+    for name in sorted(os.listdir(cpp)):
+        if name.endswith(".cpp"):
+            r = subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-I",
+                                os.path.join(ROOT, "include"), os.path.join(cpp, name)],
+                               capture_output=True, text=True)
+            assert r.returncode == 0, (name, r.stderr)

@@ -288,3 +288,31 @@ def test_nve_limit_and_deform_match_oracle(atvb, ctx, orc, kind):
     else:
         v = np.sqrt(out["vx"] ** 2 + out["vy"] ** 2 + out["vz"] ** 2)
         assert v.max() <= xmax / desc["dt"] * (1 + 1e-12)
+
+
+@pytest.mark.gpu
+def test_python_md_mirror_nve_limit_deform(atvb, ctx):
+    """md.MD with NVELimit as its integrator and Deform bound beside it runs
+    the same steps as System(nve_limit=, deform=) on the same description,
+    bit for bit."""
+    from atomiverse_b200 import workloads as W
+    desc, frame = W.lj_fcc(ncell=6, t_star=3.0, seed=5)
+    sim = atvb.MD(ctx=ctx)
+    sim.set_neighbor(atvb.NeighborList(desc["nl_cutoff"], desc["nl_skin"]))
+    sim.set_evaluator(atvb.PairLJCut(desc["lj_epsilon"], desc["lj_sigma"], desc["lj_cutoff"]))
+    sim.set_integrator(atvb.NVELimit(desc["dt"], 0.002))
+    sim.set_thermostat(atvb.Deform(1, 1e-3, desc["dt"]))
+    n = len(frame["x"])
+    ref = atvb.System(ctx, sim.desc(n, desc["box"]), None, nve_limit=0.002, deform=(1, 1e-3))
+    fa = {k: np.array(v) for k, v in frame.items()}
+    s = ref.run(fa, 60)
+    ref.close()
+    fb = dict({k: np.array(v) for k, v in frame.items()}, box=desc["box"])
+    sm = sim.run(fb, 60)
+    assert sm["box"][1] > desc["box"][1] * 1.002
+    assert np.array_equal(np.asarray(sm["box"]), np.asarray(s["box"]))
+    assert sm["energy"] == s["energy"] and sm["kinetic"] == s["kinetic"]
+    for k in ("x", "y", "z", "vx", "vy", "vz"):
+        assert np.array_equal(fa[k], fb[k]), k
+    v = np.sqrt(fb["vx"] ** 2 + fb["vy"] ** 2 + fb["vz"] ** 2)
+    assert v.max() <= 0.002 / desc["dt"] * (1 + 1e-12)
