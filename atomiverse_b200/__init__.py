@@ -27,6 +27,8 @@ __all__ = [
 ]
 
 FRAME_KEYS = ("x", "y", "z", "vx", "vy", "vz", "fx", "fy", "fz", "mass", "charge")
+KB_EV_PER_K = 8.617333262e-5   # units.h:138
+HISTORY_DEFAULT = 4096         # per-step energy ring of a system (history_capacity 0)
 
 
 def library_path() -> str:
@@ -648,6 +650,7 @@ class MD:
     _thermostats: list = field(default_factory=list)
     _stress: bool = False
     _system: System | None = None
+    _thermo: tuple | None = None          # (every, file or None, header printed)
 
     def set_neighbor(self, nl: NeighborList):
         self._neighbor = nl
@@ -672,6 +675,45 @@ class MD:
     def set_barostat(self, b: "Barostat"):
         """LAMMPS `fix press/berendsen` (md.cuh:239-243)."""
         return self.set_thermostat(b)
+
+    def set_thermo(self, every: int, filename: str | None = None):
+        """Thermo output every `every` steps (md.cuh:249-262, cuda::Thermo in
+        record/thermo.cuh): Step, Temp (2 KE / (Ndof k_B), Ndof = 3N - 3),
+        PotEng, KinEng, TotEng in the columns of cpu::thermo_print
+        (record/thermo.cpp:56-81), read from the device's per-step energy
+        ring after each run.  Step is the driver's zero-based iteration
+        index, continued across run() calls (md.cuh:170); a row is printed
+        where it is a multiple of `every` (driver.cu:128).  Singular: a
+        different cadence throws."""
+        every = int(every) if int(every) > 0 else 1      # 0 is every step
+        if self._thermo is not None:
+            if self._thermo[0] == every:
+                return self
+            raise ValueError(f"set_thermo already configured with {self._thermo[0]}, "
+                             f"rejected re-call with {every}")
+        fh = None
+        if filename:
+            fh = open(filename, "w")
+            fh.write("# Step Temp PotEng KinEng TotEng\n")
+        self._thermo = [every, fh, False]
+        return self
+
+    def _thermo_rows(self, hist: np.ndarray, n_atoms: int):
+        every, fh, header = self._thermo
+        ndof = 3 * n_atoms - 3
+        for pe, ke, step in hist:
+            step = int(step)
+            if step % every:
+                continue
+            temp = 2.0 * ke / (ndof * KB_EV_PER_K) if ndof > 0 else 0.0
+            if not header:
+                print(f"{'Step':>8s} {'Temp':>12s} {'PotEng':>14s} {'KinEng':>14s} {'TotEng':>14s}")
+                header = self._thermo[2] = True
+            print(f"{step:8d} {temp:12.4f} {pe:14.6f} {ke:14.6f} {pe + ke:14.6f}")
+            if fh is not None:
+                fh.write(f"{step} {temp:.6f} {pe:.6f} {ke:.6f} {pe + ke:.6f}\n")
+        if fh is not None:
+            fh.flush()
 
     def set_stress_required(self, on: bool = True):
         self._stress = on
@@ -727,6 +769,19 @@ class MD:
             self._system = System(self.ctx, self.desc(n, box if box is not None else frame["box"]),
                                   npt=npt, barostat=baro, nve_limit=lim,
                                   deform=(dfm.axis, dfm.strain_rate) if dfm else None)
-        sc = self._system.run(frame, n_steps)
+        if self._thermo is None:
+            sc = self._system.run(frame, n_steps)
+        else:
+            # in pieces no longer than the energy ring, printing each piece
+            cap = HISTORY_DEFAULT
+            left = int(n_steps)
+            while True:
+                k = min(left, cap)
+                sc = self._system.run(frame, k)
+                if k > 0:
+                    self._thermo_rows(self._system.history(k), len(frame["x"]))
+                left -= k
+                if left <= 0:
+                    break
         frame["box"] = tuple(sc["box"])   # the cell moves under NPT
         return sc

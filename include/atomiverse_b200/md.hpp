@@ -23,7 +23,9 @@
 
 #include <array>
 #include <cstdint>
+#include <cstdio>
 #include <cstring>
+#include <fstream>
 #include <stdexcept>
 #include <string>
 #include <utility>
@@ -338,6 +340,34 @@ class MD {
         return *this;
     }
 
+    /// Thermo output every `every` steps (MD::set_thermo, md.cuh:249-262;
+    /// cuda::Thermo, record/thermo.cuh): Step, Temp (2 KE / (Ndof k_B),
+    /// Ndof = 3N - 3), PotEng, KinEng, TotEng in the columns of
+    /// cpu::thermo_print (record/thermo.cpp:56-81), read from the device's
+    /// per-step energy ring after each run.  Step is the driver's zero-based
+    /// iteration index, continued across run() calls (md.cuh:170), and a row
+    /// is printed where it is a multiple of `every` (driver.cu:128).
+    /// Singular: a different cadence on a second call throws.  `filename`
+    /// also writes the rows there.
+    MD& set_thermo(int every, const std::string& filename = "") {
+        if (every <= 0)
+            every = 1; // "0 is every step"
+        if (thermo_every_ > 0) {
+            if (thermo_every_ == every)
+                return *this;
+            throw std::invalid_argument("set_thermo already configured with " +
+                                        std::to_string(thermo_every_) +
+                                        ", rejected re-call with " + std::to_string(every));
+        }
+        thermo_every_ = every;
+        if (!filename.empty()) {
+            thermo_file_.open(filename);
+            if (thermo_file_.is_open())
+                thermo_file_ << "# Step Temp PotEng KinEng TotEng\n";
+        }
+        return *this;
+    }
+
     /// Advance n_steps; the first call uploads `frame`, every call leaves the
     /// device state in `frame` (MD::run, md.cuh:155-178).
     atvb_scalars run(Frame& frame, int n_steps) {
@@ -349,7 +379,24 @@ class MD {
         ensure_system(frame);
         atvb_soa_view v = frame.view();
         atvb_scalars s{};
-        check(atvb_system_run(sys_, &v, n_steps, &s));
+        if (thermo_every_ <= 0) {
+            check(atvb_system_run(sys_, &v, n_steps, &s));
+        } else {
+            // in pieces no longer than the energy ring, printing each piece
+            const int cap = d_.history_capacity > 0 ? d_.history_capacity : 4096;
+            std::vector<double> h((size_t)3 * cap);
+            int left = n_steps;
+            do {
+                const int k = left < cap ? left : cap;
+                check(atvb_system_run(sys_, &v, k, &s));
+                int32_t cnt = 0;
+                if (k > 0)
+                    check(atvb_system_energy_history(sys_, h.data(), k, &cnt));
+                for (int r = 0; r < cnt; ++r)
+                    thermo_row((long long)h[3 * r + 2], h[3 * r], h[3 * r + 1]);
+                left -= k;
+            } while (left > 0);
+        }
         for (int k = 0; k < 3; ++k) // the cell moves under NPT
             frame.box[k] = s.box[k];
         return s;
@@ -412,6 +459,26 @@ class MD {
     }
 
   private:
+    void thermo_row(long long step, double pe, double ke) {
+        if (step % thermo_every_ != 0)
+            return;
+        const int ndof = 3 * d_.n_atoms - 3;
+        const double kB = 8.617333262e-5; // eV/K (units.h:138)
+        const double temp = ndof > 0 ? 2.0 * ke / ((double)ndof * kB) : 0.0;
+        if (!thermo_header_) {
+            std::printf("%8s %12s %14s %14s %14s\n", "Step", "Temp", "PotEng", "KinEng",
+                        "TotEng");
+            thermo_header_ = true;
+        }
+        std::printf("%8lld %12.4f %14.6f %14.6f %14.6f\n", step, temp, pe, ke, pe + ke);
+        if (thermo_file_.is_open()) {
+            char line[160];
+            std::snprintf(line, sizeof line, "%lld %.6f %.6f %.6f %.6f\n", step, temp, pe, ke,
+                          pe + ke);
+            thermo_file_ << line;
+        }
+    }
+
     void ensure_system(Frame& frame) {
         if (!sys_)
             create_system(frame);
@@ -480,6 +547,9 @@ class MD {
     int snap_every_ = 0, snap_depth_ = 0;
     Barostat baro_{0.0, 1.0, 1.0};
     bool have_baro_ = false;
+    int thermo_every_ = 0;
+    bool thermo_header_ = false;
+    std::ofstream thermo_file_;
     double vlimit_ = 0.0;
     int deform_axis_ = -1;
     double deform_rate_ = 0.0;

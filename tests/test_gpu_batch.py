@@ -185,6 +185,60 @@ def test_cpp_md_example(atvb):
 
 
 @pytest.mark.gpu
+def test_cpp_thermo_output(atvb, tmp_path):
+    """md::MD::set_thermo(25, file): cpu::thermo_print's columns on stdout and
+    in the file; steps carry the driver's zero-based iteration index, which
+    runs on across run() calls (md.cuh:170), so 2 x 50 steps print 0, 25,
+    50, 75."""
+    exe = str(tmp_path / "md_example")
+    lib_dir = os.path.join(ROOT, "atomiverse_b200")
+    subprocess.run(["g++", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "cpp", "md_example.cpp"), "-o", exe,
+                    "-L", lib_dir, "-latvb", "-Wl,-rpath," + lib_dir], check=True)
+    dat = tmp_path / "thermo.dat"
+    lines = subprocess.run([exe, "25", str(dat)], capture_output=True, text=True,
+                           check=True).stdout.splitlines()
+    assert lines[0].split() == ["Step", "Temp", "PotEng", "KinEng", "TotEng"]
+    rows = [[float(v) for v in ln.split()] for ln in lines[1:5]]
+    assert [int(r[0]) for r in rows] == [0, 25, 50, 75]
+    final = [float(v) for v in lines[5].split()]
+    n = 4 * 6 ** 3
+    for r in rows:
+        assert r[4] == pytest.approx(r[2] + r[3], abs=2e-6)         # TotEng = Pot + Kin
+        assert r[1] == pytest.approx(2 * r[3] / ((3 * n - 3) * 8.617333262e-5), rel=1e-4)
+        assert r[4] == pytest.approx(final[2], rel=1e-3)             # NVE
+    body = dat.read_text().splitlines()
+    assert body[0] == "# Step Temp PotEng KinEng TotEng"
+    assert [int(b.split()[0]) for b in body[1:]] == [0, 25, 50, 75]
+
+
+@pytest.mark.gpu
+def test_python_md_thermo(atvb, ctx, capsys):
+    """md.MD.set_thermo(5): rows for steps 0, 5, .., 25 across two run()
+    calls of 23 and 7 steps, the header once, values from the energy ring."""
+    from atomiverse_b200 import workloads as W
+    desc, frame = W.lj_fcc(ncell=5, seed=4)
+    sim = atvb.MD(ctx=ctx)
+    sim.set_neighbor(atvb.NeighborList(desc["nl_cutoff"], desc["nl_skin"]))
+    sim.set_evaluator(atvb.PairLJCut(desc["lj_epsilon"], desc["lj_sigma"], desc["lj_cutoff"]))
+    sim.set_integrator(atvb.VelocityVerlet(desc["dt"]))
+    sim.set_thermo(5)
+    fr = dict(frame, box=desc["box"])
+    sim.run(fr, 23)
+    sim.run(fr, 7)
+    out = capsys.readouterr().out.splitlines()
+    assert out[0].split() == ["Step", "Temp", "PotEng", "KinEng", "TotEng"]
+    rows = [ln.split() for ln in out[1:]]
+    assert [int(r[0]) for r in rows] == [0, 5, 10, 15, 20, 25]
+    hist = sim._system.history(30)
+    for r in rows:
+        pe, ke, st = hist[int(r[0])]
+        assert int(st) == int(r[0])
+        assert float(r[2]) == pytest.approx(pe, abs=1e-6)
+        assert float(r[3]) == pytest.approx(ke, abs=1e-6)
+
+
+@pytest.mark.gpu
 def test_server_resident_atom_limit(atvb, ctx):
     from atomiverse_b200 import workloads as W
     reqs = [W.lj_fcc(ncell=c, seed=30 + c, precision=1) for c in (5, 6, 4)]  # 500, 864, 256 atoms
