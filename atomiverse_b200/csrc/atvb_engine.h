@@ -179,7 +179,7 @@ class Engine {
     LaunchCfg restricted_cfg(int id);
     void enqueue_step(bool profile);
     void enqueue_forces(const LaunchCfg& lc, const std::vector<int>& pme,
-                        bool profile, bool overlap);
+                        bool profile, bool overlap, bool build_list = false);
     void prof_mark(bool profile, const char* next);
     void collect_profile();
     void release_graph();

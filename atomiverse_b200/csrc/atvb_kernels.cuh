@@ -46,6 +46,8 @@ struct LaunchCfg {
 
 // neighbor.cu
 void launch_rebuild(const LaunchCfg& lc, cudaStream_t s);
+void launch_sort_cells(const LaunchCfg& lc, cudaStream_t s);
+void launch_build_list(const LaunchCfg& lc, cudaStream_t s);
 // pair.cu
 void launch_pair(const LaunchCfg& lc, cudaStream_t s);
 void launch_pair_fix(const LaunchCfg& lc, cudaStream_t s);

@@ -951,13 +951,19 @@ int64_t Engine::kernels_per_step() const {
 // atomic-bound -- and joins before the next atom pass; otherwise (profiling,
 // force passes) everything runs in order on the engine stream.
 void Engine::enqueue_forces(const LaunchCfg& lc, const std::vector<int>& pme,
-                            bool profile, bool overlap) {
+                            bool profile, bool overlap, bool build_list) {
     const bool side = overlap && !profile && !pme.empty();
     cudaStream_t ps = side ? fft_streams_[0] : stream_;
     if (side) {
         CK(cudaEventRecord(pme_fork_, stream_));
         CK(cudaStreamWaitEvent(ps, pme_fork_, 0));
     }
+    // The PME chain reads only the sorted positions and charges, final once
+    // the cells are sorted, so on a rebuild step it also runs beside the
+    // list build (issue-bound at low occupancy), not only beside the pair
+    // kernel.
+    if (build_list)
+        launch_build_list(lc, stream_);
     if (!pme.empty()) {
         prof_mark(profile, "pme_spread");
         launch_pme_spread(lc, ps);
@@ -989,8 +995,8 @@ void Engine::enqueue_step(bool profile) {
     launch_integrate_a(lc_, stream_);
     launch_sys_a(lc_, stream_);
     prof_mark(profile, "neighbor");
-    launch_rebuild(lc_, stream_);
-    enqueue_forces(lc_, pme_slots_, profile, true);
+    launch_sort_cells(lc_, stream_);
+    enqueue_forces(lc_, pme_slots_, profile, true, true);
     prof_mark(profile, "integrate_b");
     launch_integrate_b(lc_, stream_);
     launch_sys_b(lc_, stream_);

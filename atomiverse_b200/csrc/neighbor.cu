@@ -458,7 +458,10 @@ __global__ void __launch_bounds__(256)
     }
 }
 
-void launch_rebuild(const LaunchCfg& lc, cudaStream_t s) {
+// Binning and the sorted repack: after these the sorted positions (pos4)
+// that the PME chain reads are final, so that chain may start beside the
+// list build.
+void launch_sort_cells(const LaunchCfg& lc, cudaStream_t s) {
     k_cell_count<<<lc.atoms.grid, kChunk, 0, s>>>(lc.atoms.d, lc.atoms.n,
                                                    lc.sp);
     k_cell_scan<<<lc.nsys, 1024, 0, s>>>(lc.sys_list, lc.sp);
@@ -467,8 +470,16 @@ void launch_rebuild(const LaunchCfg& lc, cudaStream_t s) {
     k_cell_sort<<<lc.cells.grid, kChunk, 0, s>>>(lc.cells.d, lc.cells.n,
                                                   lc.sp);
     k_permute<<<lc.atoms.grid, kChunk, 0, s>>>(lc.atoms.d, lc.atoms.n, lc.sp);
+}
+
+void launch_build_list(const LaunchCfg& lc, cudaStream_t s) {
     k_build_list<<<lc.list.grid, 32 * kListChunk, 0, s>>>(lc.list.d,
                                                            lc.list.n, lc.sp);
+}
+
+void launch_rebuild(const LaunchCfg& lc, cudaStream_t s) {
+    launch_sort_cells(lc, s);
+    launch_build_list(lc, s);
 }
 
 } // namespace atvb
