@@ -197,6 +197,10 @@ struct SysParams {
     char* snap_ring;    // device view of the ring (null: off)
     int snap_every, snap_depth;
     long long snap_slot_bytes;
+    // host-mapped: the longest row of the last neighbour build, written at
+    // the end of every step so the host can widen the rows between step
+    // calls, before a build overflows them (null: off)
+    int* row_hint;
     // per-atom master state (original order)
     double *x, *y, *z, *vx, *vy, *vz, *mass, *q;
     long long* tag;

@@ -61,6 +61,7 @@ class Slot {
     Slot(const Slot&) = delete;
     Slot& operator=(const Slot&) = delete;
     void alloc_list(int cap);
+    void widen_list(int cap); // wider rows, the current list copied in
 
     atvb_system_desc desc;
     Geometry geo;
@@ -178,6 +179,9 @@ class Engine {
     void sized_rebuild(const LaunchCfg& lc);
     LaunchCfg restricted_cfg(int id);
     void enqueue_step(bool profile);
+    void widen_rows();
+    int deform_budget(int n);
+    void run_steps(int n);
     void enqueue_forces(const LaunchCfg& lc, const std::vector<int>& pme,
                         bool profile, bool overlap, bool build_list = false);
     void prof_mark(bool profile, const char* next);
@@ -200,6 +204,9 @@ class Engine {
     std::vector<std::unique_ptr<Slot>> slots_;
     SysParams* d_sp_ = nullptr;
     int sp_cap_ = 0;
+    // host-mapped longest-row hints, one per table entry (SysParams::row_hint)
+    int* row_hint_host_ = nullptr;
+    int* row_hint_dev_ = nullptr;
     std::vector<void*> list_allocs_;
     LaunchCfg lc_;
     std::vector<int> pme_slots_;

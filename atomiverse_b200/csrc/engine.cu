@@ -327,6 +327,20 @@ void Slot::alloc_list(int new_cap) {
     hp.cap = new_cap;
 }
 
+void Slot::widen_list(int new_cap) {
+    const int oc = hp.cap;
+    if (new_cap <= oc)
+        return;
+    const size_t n = (size_t)hp.n;
+    void* p = mem_.alloc(n * (size_t)new_cap * sizeof(int));
+    CK(cudaMemcpy2DAsync(p, (size_t)new_cap * sizeof(int), hp.nbr, (size_t)oc * sizeof(int),
+                         (size_t)oc * sizeof(int), n, cudaMemcpyDeviceToDevice, mem_.stream));
+    mem_.free(nbr_alloc);
+    nbr_alloc = p;
+    hp.nbr = (int*)p;
+    hp.cap = new_cap;
+}
+
 Slot::Slot(const atvb_system_desc& d, const DevMem& mem) : desc(d), mem_(mem) {
     cudaStream_t stream = mem.stream;
     geo = make_geometry(d);
@@ -674,6 +688,8 @@ Engine::~Engine() {
         mem_.free(p);
     mem_.free(d_sp_);
     cudaStreamSynchronize(stream_);
+    if (row_hint_host_)
+        cudaFreeHost(row_hint_host_);
     for (auto& kv : plans_)
         for (int l = 0; l <= kFftLanes; ++l) {
             if (kv.second.f[l])
@@ -727,6 +743,7 @@ int Engine::add(const atvb_system_desc& d) {
     s->index = id;
     slots_[id] = std::move(s);
     ensure_table();
+    row_hint_host_[id] = 0; // a reused entry may hold its last owner's hint
     push_params(id);
     dirty_ = true;
     return id;
@@ -759,13 +776,52 @@ void Engine::ensure_table() {
         mem_.free(d_sp_);
     }
     release_graph(); // captured launches point at the old table
+    // the row hints move with the table: nothing in flight may still write
+    // the old array when it is freed, and every entry is re-pointed
+    void* h = nullptr;
+    CK(cudaHostAlloc(&h, sizeof(int) * cap, cudaHostAllocMapped));
+    std::memset(h, 0, sizeof(int) * cap);
+    if (row_hint_host_) {
+        CK(cudaDeviceSynchronize());
+        std::memcpy(h, row_hint_host_, sizeof(int) * sp_cap_);
+        CK(cudaFreeHost(row_hint_host_));
+    }
+    row_hint_host_ = (int*)h;
+    void* hd = nullptr;
+    CK(cudaHostGetDevicePointer(&hd, h, 0));
+    row_hint_dev_ = (int*)hd;
     d_sp_ = nd;
     sp_cap_ = cap;
+    for (int id = 0; id < (int)slots_.size(); ++id)
+        if (slots_[id])
+            push_params(id); // re-points row_hint at the new array
     dirty_ = true;
+}
+
+// Between step calls: a system whose last build filled more than 80 % of
+// its row capacity gets rows 1.5 x that long.  The old rows are copied into
+// the wider ones, stream-ordered behind the steps in flight, so the list
+// and every later result stay exactly what they would have been; no build
+// overflows unless a row grows by more than a quarter within one call.
+void Engine::widen_rows() {
+    if (!row_hint_host_)
+        return;
+    for (int id = 0; id < (int)slots_.size(); ++id) {
+        Slot* s = slots_[id].get();
+        if (!s || !s->uploaded || !s->hp.nbr)
+            continue;
+        const int m = ((volatile int*)row_hint_host_)[id];
+        const int oc = s->hp.cap;
+        if ((long long)m * 5 <= (long long)oc * 4)
+            continue;
+        s->widen_list(round_up((long long)(m * 1.5) + 32, 32));
+        push_params(id);
+    }
 }
 
 void Engine::push_params(int id) {
     Slot* s = slot(id);
+    s->hp.row_hint = (row_hint_dev_ && id < sp_cap_) ? row_hint_dev_ + id : nullptr;
     if ((s->npt || s->baro || s->hp.deform_axis >= 0) && s->uploaded) {
         // the device owns an NPT system's cell: keep it
         SysParams dev;
@@ -1029,13 +1085,53 @@ void Engine::ensure_ready() {
         throw Error(ATVB_ERR_STATE, "no uploaded system to advance");
 }
 
+// Steps every Deform system can take before its cell passes the smallest
+// edge its bins were planned for (with the 2 % margin of the re-plan test):
+// the edge of step k is L0 (1 + rate dt k), known in advance.  Reads the
+// state after the stream has drained.
+int Engine::deform_budget(int n) {
+    long long k = n;
+    for (auto& up : slots_) {
+        if (!up || !up->uploaded || up->hp.deform_axis < 0)
+            continue;
+        const SysParams& P = up->hp;
+        const double rdt = P.deform_rate * P.dt;
+        if (!(rdt < 0.0))
+            continue;
+        long long step = 0;
+        CK(cudaMemcpy(&step, &P.st->step, sizeof(step), cudaMemcpyDeviceToHost));
+        const double lo = P.npt_Lmin[P.deform_axis] * 1.02;
+        const double last = std::floor((lo / P.deform_L0 - 1.0) / rdt) - (double)step - 1.0;
+        k = std::min<long long>(k, last < 1.0 ? 1 : (long long)std::min(last, 1e9));
+    }
+    return (int)k;
+}
+
 void Engine::step(int n) {
     CK(cudaSetDevice(device_));
     if (n < 0)
         throw Error(ATVB_ERR_INVALID, "n_steps must be >= 0");
-    if (any_npt_)
-        replan_npt();
-    ensure_ready();
+    int left = n;
+    do {
+        // The cell re-plan and the row check read what the previous call
+        // left (the engine stream is non-blocking, so a plain copy would not
+        // wait for it): a step call starts once the one before has finished.
+        CK(cudaStreamSynchronize(stream_));
+        if (any_npt_)
+            replan_npt();
+        widen_rows();
+        ensure_ready();
+        // a Deform cell is re-planned between pieces, before it shrinks out
+        // of its bins
+        const int k = any_npt_ ? deform_budget(left) : left;
+        run_steps(k);
+        left -= k;
+    } while (left > 0);
+    last_launches_ = kernels_per_step() * n;
+    steps_since_check_ += n;
+}
+
+void Engine::run_steps(int n) {
     if (profiling_) {
         for (int k = 0; k < n; ++k) {
             enqueue_step(true);
@@ -1060,8 +1156,6 @@ void Engine::step(int n) {
         for (int k = 0; k < n; ++k)
             CK(cudaGraphLaunch(gexec_, stream_));
     }
-    last_launches_ = kernels_per_step() * n;
-    steps_since_check_ += n;
 }
 
 void Engine::step_timed(int n, double* step_ms, double* total_ms) {

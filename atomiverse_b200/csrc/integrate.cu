@@ -323,6 +323,8 @@ ATVB_DEV void record_history(const SysParams& P, SysState* st) {
         P.ehist[3 * slot + 1] = st->kinetic;
         P.ehist[3 * slot + 2] = (double)st->step;
     }
+    if (P.row_hint)
+        *(volatile int*)P.row_hint = st->max_nnbr;
 }
 
 // Berendsen barostat at end_of_step (barostat.cpp:27-110): from the scalar
@@ -487,6 +489,8 @@ __global__ void k_sys_b(const int* sys_list, int nsys, const SysParams* sp) {
         P.ehist[3 * slot + 1] = st->kinetic;
         P.ehist[3 * slot + 2] = (double)st->step;
     }
+    if (P.row_hint)
+        *(volatile int*)P.row_hint = st->max_nnbr;
     st->step += 1;
 }
 

@@ -316,3 +316,39 @@ def test_python_md_mirror_nve_limit_deform(atvb, ctx):
         assert np.array_equal(fa[k], fb[k]), k
     v = np.sqrt(fb["vx"] ** 2 + fb["vy"] ** 2 + fb["vz"] ** 2)
     assert v.max() <= 0.002 / desc["dt"] * (1 + 1e-12)
+
+
+@pytest.mark.gpu
+def test_rows_widen_between_calls_under_compression(atvb, ctx, orc):
+    """A Langevin gas (rho* = 0.2, T* = 1) squeezed along z to a fifth of its
+    edge by Deform in calls of 40 steps, with no synchronisation between
+    them: the longest neighbour row goes from 18 to ~104 entries, past the 96
+    the rows were sized for.  Between calls (and between the pieces a call is
+    cut into so that the shrinking cell never leaves its bins) the rows are
+    widened once a build fills 80 % of them, so no build overflows (status 0)
+    and the run matches the oracle."""
+    from atomiverse_b200 import workloads as W
+    desc, frame = W.lj_fcc(ncell=11, rho=0.2, t_star=1.0, seed=12, thermostat=2,
+                           damp_tau=0.5)
+    steps, chunk = 1000, 40
+    rate = -0.8 / (steps * desc["dt"])
+    s = atvb.System(ctx, desc, frame, deform=(2, rate))
+    s.compute_forces()
+    first = s.scalars()["max_neighbors"]
+    for _ in range(steps // chunk):
+        s.step(chunk)
+    out, sc = s.download()
+    s.close()
+    o = oracle_system(orc, desc, frame)
+    o.set_deform(2, rate)
+    o.build_list()
+    o.compute_forces()
+    o.run(steps)
+    d = _pos(out) - _pos(o.state())
+    d -= np.rint(d / sc["box"]) * sc["box"]
+    err = np.abs(d).max()
+    e_rel = abs(sc["energy"] / o.scalars()["energy"] - 1.0)
+    assert first < 40 and sc["max_neighbors"] > 96, (first, sc["max_neighbors"])
+    assert sc["status"] == 0
+    assert np.allclose(sc["box"], o.npt_state()["box"], rtol=1e-12, atol=0)
+    assert err < 1e-6 and e_rel < 1e-8, (err, e_rel)
