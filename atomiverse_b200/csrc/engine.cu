@@ -2172,6 +2172,7 @@ void Engine::restore(int id, const void* buf, size_t size, bool fresh_list) {
     if (fresh_list) {
         // keep the list statistics of the build just made
         SysState cur;
+        CK(cudaStreamSynchronize(stream_)); // the stream does not block a plain copy
         CK(cudaMemcpy(&cur, P.st, sizeof(cur), cudaMemcpyDeviceToHost));
         st.max_nnbr = cur.max_nnbr;
         st.list_entries = cur.list_entries;
