@@ -198,8 +198,8 @@ struct SysParams {
     int snap_every, snap_depth;
     long long snap_slot_bytes;
     // host-mapped: the longest row of the last neighbour build, written at
-    // the end of every step so the host can widen the rows between step
-    // calls, before a build overflows them (null: off)
+    // the end of each step that built the list, so the host can widen the
+    // rows between step calls before a build overflows them (null: off)
     int* row_hint;
     // per-atom master state (original order)
     double *x, *y, *z, *vx, *vy, *vz, *mass, *q;

@@ -323,7 +323,7 @@ ATVB_DEV void record_history(const SysParams& P, SysState* st) {
         P.ehist[3 * slot + 1] = st->kinetic;
         P.ehist[3 * slot + 2] = (double)st->step;
     }
-    if (P.row_hint)
+    if (P.row_hint && st->rebuild) // the longest row changes only at a build
         *(volatile int*)P.row_hint = st->max_nnbr;
 }
 
@@ -489,7 +489,7 @@ __global__ void k_sys_b(const int* sys_list, int nsys, const SysParams* sp) {
         P.ehist[3 * slot + 1] = st->kinetic;
         P.ehist[3 * slot + 2] = (double)st->step;
     }
-    if (P.row_hint)
+    if (P.row_hint && st->rebuild) // the longest row changes only at a build
         *(volatile int*)P.row_hint = st->max_nnbr;
     st->step += 1;
 }
