@@ -1089,6 +1089,8 @@ void Engine::ensure_ready() {
 // edge its bins were planned for (with the 2 % margin of the re-plan test):
 // the edge of step k is L0 (1 + rate dt k), known in advance.  Reads the
 // state after the stream has drained.
+constexpr int kMaxPiece = 1000; // steps between host checks within one call
+
 int Engine::deform_budget(int n) {
     long long k = n;
     for (auto& up : slots_) {
@@ -1121,9 +1123,11 @@ void Engine::step(int n) {
             replan_npt();
         widen_rows();
         ensure_ready();
-        // a Deform cell is re-planned between pieces, before it shrinks out
-        // of its bins
-        const int k = any_npt_ ? deform_budget(left) : left;
+        // Long calls run in pieces of at most kMaxPiece steps, so the row
+        // check and the cell re-plan above also happen inside them; a Deform
+        // cell is re-planned between pieces before it shrinks out of its bins
+        const int piece = std::min(left, kMaxPiece);
+        const int k = any_npt_ ? deform_budget(piece) : piece;
         run_steps(k);
         left -= k;
     } while (left > 0);
