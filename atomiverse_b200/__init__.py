@@ -15,14 +15,15 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _abi
-from ._abi import (FP64, LANGEVIN, MIXED, NOSE_HOOVER, NVE, AtvbError,
-                   Scalars, SoaView, SystemDesc, check, load)
+from ._abi import (FP64, LANGEVIN, MIXED, NOSE_HOOVER, NVE, AtvbError, PhysicsError,
+                   Scalars, SoaView, SystemDesc, check, check_status, load)
 
 __all__ = [
-    "FP64", "MIXED", "NVE", "NOSE_HOOVER", "LANGEVIN", "AtvbError",
+    "FP64", "MIXED", "NVE", "NOSE_HOOVER", "LANGEVIN", "AtvbError", "PhysicsError",
     "Context", "System", "Batch", "Server", "make_desc",
     "NeighborList", "PairLJCut", "CoulLong", "KSpacePME", "VelocityVerlet",
     "NoseHoover", "FixLangevin", "NoseHooverNPT", "Barostat", "NVELimit", "Deform", "MD",
+    "StopOnNaN",
     "library_path",
 ]
 
@@ -122,6 +123,7 @@ def scalars_dict(s: Scalars) -> dict:
         "energy_const": s.energy_const, "kinetic": s.kinetic, "conserved": s.conserved,
         "stress": np.array(list(s.stress)), "nh_xi": s.nh_xi, "step": s.step,
         "rebuilds": s.rebuilds, "max_neighbors": s.max_neighbors, "status": s.status,
+        "status_bits": s.status_bits, "halted": bool(s.halted),
         "list_pairs": s.list_pairs, "box": np.array(list(s.box)), "pressure": s.pressure,
     }
 
@@ -274,19 +276,37 @@ class System:
             self._h, int(n), per.ctypes.data_as(C.POINTER(C.c_double)), C.byref(tot)))
         return tot.value, per
 
-    def download(self, keys=FRAME_KEYS) -> tuple[dict, dict]:
+    def download(self, keys=FRAME_KEYS, check: bool = True) -> tuple[dict, dict]:
+        """Frame and scalars.  A sticky status bit (wrong or non-finite
+        physics in some step) raises PhysicsError unless check=False; its
+        `result` carries the (frame, scalars) anyway."""
         out = {k: np.zeros(self.n) for k in keys}
         v, keep = _soa(out, self.n, writable=True)
         s = Scalars()
-        check(self.lib.atvb_system_download(self._h, C.byref(v), C.byref(s)))
-        return out, scalars_dict(s)
+        rc = self.lib.atvb_system_download(self._h, C.byref(v), C.byref(s))
+        return check_status(rc, (out, scalars_dict(s)), check)
 
-    def scalars(self) -> dict:
+    def scalars(self, check: bool = True) -> dict:
+        """SystemScalars; raises PhysicsError on a sticky status bit unless
+        check=False (the dict's status_bits then tells which)."""
         s = Scalars()
-        check(self.lib.atvb_system_scalars(self._h, C.byref(s)))
-        return scalars_dict(s)
+        rc = self.lib.atvb_system_scalars(self._h, C.byref(s))
+        return check_status(rc, scalars_dict(s), check)
 
-    def run(self, frame: dict, n_steps: int) -> dict:
+    def clear_status(self):
+        """Reset the sticky status bits (and a StopOnNaN halt)."""
+        _abi.check(self.lib.atvb_system_clear_status(self._h))
+
+    def set_stop_on_nan(self, on: bool = True):
+        """cuda::StopOnNaN: stop integrating at a non-finite state."""
+        _abi.check(self.lib.atvb_system_set_stop_on_nan(self._h, 1 if on else 0))
+
+    def set_capacity(self, row_capacity: int = 0, nearq_capacity: int = 0):
+        """Pin the neighbour row length / size the near-cutoff queue (0: auto)."""
+        _abi.check(self.lib.atvb_system_set_capacity(self._h, int(row_capacity),
+                                                     int(nearq_capacity)))
+
+    def run(self, frame: dict, n_steps: int, check: bool = True) -> dict:
         """MD::run(frame, n): upload on first use, step, download into frame."""
         for k in FRAME_KEYS:
             if k not in frame:
@@ -294,8 +314,8 @@ class System:
             frame[k] = np.ascontiguousarray(frame[k], dtype=np.float64)
         v, keep = _soa(frame, self.n, writable=True)
         s = Scalars()
-        check(self.lib.atvb_system_run(self._h, C.byref(v), int(n_steps), C.byref(s)))
-        return scalars_dict(s)
+        rc = self.lib.atvb_system_run(self._h, C.byref(v), int(n_steps), C.byref(s))
+        return check_status(rc, scalars_dict(s), check)
 
     def history(self, max_steps: int = 4096) -> np.ndarray:
         buf = np.zeros(3 * max_steps)
@@ -398,12 +418,18 @@ class Batch:
     def step(self, n: int):
         check(self.lib.atvb_batch_step(self._h, int(n)))
 
-    def download(self, k: int, keys=FRAME_KEYS) -> tuple[dict, dict]:
+    def download(self, k: int, keys=FRAME_KEYS, check: bool = True) -> tuple[dict, dict]:
         out = {key: np.zeros(self.sizes[k]) for key in keys}
         v, keep = _soa(out, self.sizes[k], writable=True)
         s = Scalars()
-        check(self.lib.atvb_batch_download(self._h, int(k), C.byref(v), C.byref(s)))
-        return out, scalars_dict(s)
+        rc = self.lib.atvb_batch_download(self._h, int(k), C.byref(v), C.byref(s))
+        return check_status(rc, (out, scalars_dict(s)), check)
+
+    def clear_status(self, k: int):
+        _abi.check(self.lib.atvb_batch_clear_status(self._h, int(k)))
+
+    def set_stop_on_nan(self, k: int, on: bool = True):
+        _abi.check(self.lib.atvb_batch_set_stop_on_nan(self._h, int(k), 1 if on else 0))
 
     def autotune(self) -> int:
         g = C.c_int32()
@@ -639,6 +665,15 @@ class Barostat:
 
 
 @dataclass
+class StopOnNaN:
+    """cuda::StopOnNaN (include/atomiverse/cuda/driver/criterion.cuh:166-178):
+    abandon the run once the state is no longer finite.  Attached with
+    MD.add_criterion; the device halts the system at the step where a
+    position or velocity turned non-finite and run() raises PhysicsError."""
+    name: str = "stop_on_nan"
+
+
+@dataclass
 class MD:
     """cuda::md::MD: categorical setters, build(), run(frame, n)
     (include/atomiverse/cuda/dynamics/md.cuh:118-385)."""
@@ -651,6 +686,17 @@ class MD:
     _stress: bool = False
     _system: System | None = None
     _thermo: tuple | None = None          # (every, file or None, header printed)
+    _criteria: list = field(default_factory=list)
+
+    def add_criterion(self, c):
+        """Driver::add_criterion (driver.cuh:151); StopOnNaN is the one the
+        device path evaluates."""
+        if not isinstance(c, StopOnNaN):
+            raise TypeError(f"unsupported criterion {type(c).__name__}")
+        self._criteria.append(c)
+        if self._system is not None:
+            self._system.set_stop_on_nan(True)
+        return self
 
     def set_neighbor(self, nl: NeighborList):
         self._neighbor = nl
@@ -769,6 +815,8 @@ class MD:
             self._system = System(self.ctx, self.desc(n, box if box is not None else frame["box"]),
                                   npt=npt, barostat=baro, nve_limit=lim,
                                   deform=(dfm.axis, dfm.strain_rate) if dfm else None)
+            if self._criteria:
+                self._system.set_stop_on_nan(True)
         if self._thermo is None:
             sc = self._system.run(frame, n_steps)
         else:

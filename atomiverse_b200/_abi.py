@@ -14,6 +14,14 @@ ATVB_ERR_OVERFLOW = 3
 ATVB_ERR_STATE = 4
 ATVB_ERR_NOMEM = 5
 ATVB_ERR_NOTFOUND = 6
+ATVB_ERR_PHYSICS = 7
+
+# atvb_scalars.status_bits (sticky until clear_status)
+STATUS_ROW_OVERFLOW = 1
+STATUS_BOX_RANGE = 2
+STATUS_NEARQ_LOST = 4
+STATUS_NONFINITE = 8
+STATUS_FORCE_RANGE = 16
 
 FP64, MIXED = 0, 1
 NVE, NOSE_HOOVER, LANGEVIN = 0, 1, 2
@@ -89,6 +97,8 @@ class Scalars(C.Structure):
         ("list_pairs", C.c_int64),
         ("box", C.c_double * 3),
         ("pressure", C.c_double),
+        ("status_bits", C.c_uint32),
+        ("halted", C.c_int32),
     ]
 
 
@@ -144,6 +154,11 @@ SIGNATURES = {
     "atvb_system_energy_history": (C.c_int, [_vp, _dp, C.c_int32, C.POINTER(C.c_int32)]),
     "atvb_system_pairs": (C.c_int, [_vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                     C.c_int64, C.POINTER(C.c_int64)]),
+    "atvb_system_clear_status": (C.c_int, [_vp]),
+    "atvb_system_set_stop_on_nan": (C.c_int, [_vp, C.c_int32]),
+    "atvb_system_set_capacity": (C.c_int, [_vp, C.c_int32, C.c_int32]),
+    "atvb_batch_clear_status": (C.c_int, [_vp, C.c_int32]),
+    "atvb_batch_set_stop_on_nan": (C.c_int, [_vp, C.c_int32, C.c_int32]),
     "atvb_system_profile": (C.c_int, [_vp, C.c_int32]),
     "atvb_system_profile_read": (C.c_int, [_vp, C.POINTER(KernelTime), C.c_int32,
                                            C.POINTER(C.c_int32)]),
@@ -223,6 +238,15 @@ class AtvbError(RuntimeError):
         self.code = code
 
 
+class PhysicsError(AtvbError):
+    """A sticky status bit is set (ATVB_ERR_PHYSICS): some step ran on wrong
+    or non-finite physics.  `result` holds what the call returned anyway."""
+
+    def __init__(self, code: int, msg: str, result=None):
+        super().__init__(code, msg)
+        self.result = result
+
+
 def load(path: str | None = None):
     """Load libatvb.so; raises if it is missing (no fallback exists)."""
     global _lib
@@ -245,4 +269,20 @@ def load(path: str | None = None):
 def check(rc: int) -> None:
     if rc != ATVB_OK:
         msg = load().atvb_last_error()
-        raise AtvbError(rc, msg.decode() if msg else "")
+        text = msg.decode() if msg else ""
+        if rc == ATVB_ERR_PHYSICS:
+            raise PhysicsError(rc, text)
+        raise AtvbError(rc, text)
+
+
+def check_status(rc: int, result, strict: bool):
+    """check() for calls that fill their outputs before reporting a sticky
+    status bit: with strict=False that code is not an error."""
+    if rc == ATVB_ERR_PHYSICS and not strict:
+        return result
+    try:
+        check(rc)
+    except PhysicsError as e:
+        e.result = result
+        raise
+    return result

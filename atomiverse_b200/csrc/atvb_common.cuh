@@ -12,6 +12,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "atvb.h"
+
 namespace atvb {
 
 // units.h:138,165,166,173 of the reference (metal units)
@@ -28,8 +30,12 @@ enum Thermostat : int { kNVE = 0, kNoseHoover = 1, kLangevin = 2, kNPT = 3 };
 // longest Nose-Hoover chain of the MTK NPT integrator
 constexpr int kMaxChain = 10;
 
-// SysState::status bits
-constexpr int kStatusBoxRange = 1; // NPT cell left the range its grid was planned for
+// SysState::status bits (sticky; the ATVB_STATUS_* values of atvb.h)
+constexpr int kStatusRowOverflow = ATVB_STATUS_ROW_OVERFLOW; // a step ran on cut rows
+constexpr int kStatusBoxRange = ATVB_STATUS_BOX_RANGE; // cell left its planned range
+constexpr int kStatusNearqLost = ATVB_STATUS_NEARQ_LOST; // settle queue overflowed
+constexpr int kStatusNonFinite = ATVB_STATUS_NONFINITE;  // NaN / inf position or velocity
+constexpr int kStatusForceRange = ATVB_STATUS_FORCE_RANGE; // pair force beyond fixed point
 
 // Fixed-point scales.  Energies/virials/KE are accumulated per system as
 // 64-bit integers in units of 2^-32 eV (range +-2.1e9 eV), so their sums are
@@ -64,7 +70,10 @@ struct SysState {
     int rebuild;       // decision for this step
     int overflow;      // neighbour row overflowed its capacity
     int max_nnbr;      // largest row seen at the last build
-    int status;        // sticky error bits
+    int status;        // sticky error bits (kStatus*)
+    int force_build;   // host request: build the list at the next step
+    int halted;        // StopOnNaN: the system no longer integrates
+    int held;          // the cell is held at the edge of its planned range
     unsigned long long list_entries; // row entries of the last build (2 x pairs)
     int nearq_n;       // mixed build: pairs queued this step for an exact LJ cutoff test
     int nearq_lost;    // pairs that did not fit the queue (decided in FP32)
@@ -201,6 +210,10 @@ struct SysParams {
     // the end of each step that built the list, so the host can widen the
     // rows between step calls before a build overflows them (null: off)
     int* row_hint;
+    // host-mapped copy of SysState::status, written when a step ends with a
+    // bit set (null: off), so the host sees errors without a device read
+    int* status_hint;
+    int stop_on_nan; // cuda::StopOnNaN attached: halt at a non-finite state
     // per-atom master state (original order)
     double *x, *y, *z, *vx, *vy, *vz, *mass, *q;
     long long* tag;

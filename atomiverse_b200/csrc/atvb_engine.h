@@ -91,6 +91,7 @@ class Slot {
     double baro_args[3] = {0, 0, 0}; // P_target, tau_P, bulk_modulus
     double vlimit_xmax = 0.0;        // NVELimit xmax (0: plain velocity Verlet)
     double deform_args[3] = {0, 0, 0}; // Deform axis, strain rate, L0
+    int row_cap_fixed = 0;     // atvb_system_set_capacity: pinned row length
     char* snap_host = nullptr; // trajectory snapshot ring (host-mapped)
     long long snap_read = 0;   // snapshots consumed by the host
 
@@ -136,6 +137,10 @@ class Engine {
     void compute_forces_one(int id);
     void step(int n);
     void step_timed(int n, double* step_ms, double* total_ms);
+    void check_halted(int id); // throws ATVB_ERR_PHYSICS if StopOnNaN stopped it
+    void clear_status(int id);
+    void set_stop_on_nan(int id, bool on);
+    void set_capacity(int id, int row_cap, int nearq_cap);
     void download(int id, atvb_soa_view* f, atvb_scalars* sc);
     void scalars(int id, atvb_scalars* out);
     int64_t pairs(int id, int32_t* pi, int32_t* pj, int64_t capacity);
@@ -182,6 +187,9 @@ class Engine {
     void widen_rows();
     int deform_budget(int n);
     void run_steps(int n);
+    void run_pieces(int n, double* step_ms, double* total_ms);
+    void ensure_graph();
+    bool all_halted() const;
     void enqueue_forces(const LaunchCfg& lc, const std::vector<int>& pme,
                         bool profile, bool overlap, bool build_list = false);
     void prof_mark(bool profile, const char* next);
@@ -204,7 +212,9 @@ class Engine {
     std::vector<std::unique_ptr<Slot>> slots_;
     SysParams* d_sp_ = nullptr;
     int sp_cap_ = 0;
-    // host-mapped longest-row hints, one per table entry (SysParams::row_hint)
+    // host-mapped words, 2 per table entry: the longest-row hints
+    // (SysParams::row_hint) in [0, sp_cap_), the status words
+    // (SysParams::status_hint) in [sp_cap_, 2 sp_cap_)
     int* row_hint_host_ = nullptr;
     int* row_hint_dev_ = nullptr;
     std::vector<void*> list_allocs_;

@@ -54,6 +54,34 @@ void need(const void* p, const char* what) {
         throw Error(ATVB_ERR_INVALID, std::string(what) + " is NULL");
 }
 
+// After a call has filled its outputs: any sticky status bit of the system
+// makes it return ATVB_ERR_PHYSICS, so wrong physics is never silent.
+void raise_status(Engine& e, int id, const atvb_scalars* sc) {
+    atvb_scalars local;
+    if (!sc) {
+        e.scalars(id, &local);
+        sc = &local;
+    }
+    const uint32_t b = sc->status_bits;
+    if (!b)
+        return;
+    std::string m = "system status:";
+    if (b & ATVB_STATUS_ROW_OVERFLOW)
+        m += " neighbour rows were cut at capacity (pairs lost);";
+    if (b & ATVB_STATUS_BOX_RANGE)
+        m += " the cell was held at the edge of its planned range;";
+    if (b & ATVB_STATUS_NEARQ_LOST)
+        m += " near-cutoff pairs overflowed the settle queue;";
+    if (b & ATVB_STATUS_NONFINITE)
+        m += " a position or velocity is not finite;";
+    if (b & ATVB_STATUS_FORCE_RANGE)
+        m += " a pair force exceeded the fixed-point range;";
+    if (sc->halted)
+        m += " stopped by StopOnNaN at step " + std::to_string(sc->step) + ";";
+    m += " (atvb_system_clear_status resets the bits)";
+    throw Error(ATVB_ERR_PHYSICS, m);
+}
+
 } // namespace
 
 extern "C" {
@@ -125,6 +153,7 @@ int atvb_system_step(atvb_system* sys, int32_t n_steps) {
         need(sys, "sys");
         if (!sys->uploaded)
             throw Error(ATVB_ERR_STATE, "step before upload");
+        sys->eng->check_halted(sys->id);
         sys->eng->step(n_steps);
     });
 }
@@ -137,6 +166,7 @@ int atvb_system_step_timed(atvb_system* sys, int32_t n_steps, double* step_ms,
             throw Error(ATVB_ERR_STATE, "step before upload");
         if (n_steps < 1)
             throw Error(ATVB_ERR_INVALID, "n_steps must be >= 1");
+        sys->eng->check_halted(sys->id);
         sys->eng->step_timed(n_steps, step_ms, total_ms);
     });
 }
@@ -146,6 +176,7 @@ int atvb_system_download(atvb_system* sys, atvb_soa_view* frame,
     return guard([&] {
         need(sys, "sys");
         sys->eng->download(sys->id, frame, scalars);
+        raise_status(*sys->eng, sys->id, scalars);
     });
 }
 
@@ -154,6 +185,29 @@ int atvb_system_scalars(atvb_system* sys, atvb_scalars* scalars) {
         need(sys, "sys");
         need(scalars, "scalars");
         sys->eng->scalars(sys->id, scalars);
+        raise_status(*sys->eng, sys->id, scalars);
+    });
+}
+
+int atvb_system_clear_status(atvb_system* sys) {
+    return guard([&] {
+        need(sys, "sys");
+        sys->eng->clear_status(sys->id);
+    });
+}
+
+int atvb_system_set_stop_on_nan(atvb_system* sys, int32_t on) {
+    return guard([&] {
+        need(sys, "sys");
+        sys->eng->set_stop_on_nan(sys->id, on != 0);
+    });
+}
+
+int atvb_system_set_capacity(atvb_system* sys, int32_t row_capacity,
+                             int32_t nearq_capacity) {
+    return guard([&] {
+        need(sys, "sys");
+        sys->eng->set_capacity(sys->id, row_capacity, nearq_capacity);
     });
 }
 
@@ -166,8 +220,10 @@ int atvb_system_run(atvb_system* sys, atvb_soa_view* frame, int32_t n_steps,
             sys->eng->upload(sys->id, *frame);
             sys->uploaded = true;
         }
+        sys->eng->check_halted(sys->id);
         sys->eng->step(n_steps);
         sys->eng->download(sys->id, frame, scalars);
+        raise_status(*sys->eng, sys->id, scalars);
     });
 }
 
@@ -451,6 +507,21 @@ int atvb_batch_download(atvb_batch* b, int32_t index, atvb_soa_view* frame,
     return guard([&] {
         need(b, "batch");
         b->eng->download(batch_id(b, index), frame, scalars);
+        raise_status(*b->eng, batch_id(b, index), scalars);
+    });
+}
+
+int atvb_batch_clear_status(atvb_batch* b, int32_t index) {
+    return guard([&] {
+        need(b, "batch");
+        b->eng->clear_status(batch_id(b, index));
+    });
+}
+
+int atvb_batch_set_stop_on_nan(atvb_batch* b, int32_t index, int32_t on) {
+    return guard([&] {
+        need(b, "batch");
+        b->eng->set_stop_on_nan(batch_id(b, index), on != 0);
     });
 }
 

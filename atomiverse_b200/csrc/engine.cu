@@ -744,6 +744,7 @@ int Engine::add(const atvb_system_desc& d) {
     slots_[id] = std::move(s);
     ensure_table();
     row_hint_host_[id] = 0; // a reused entry may hold its last owner's hint
+    row_hint_host_[sp_cap_ + id] = 0;
     push_params(id);
     dirty_ = true;
     return id;
@@ -778,12 +779,15 @@ void Engine::ensure_table() {
     release_graph(); // captured launches point at the old table
     // the row hints move with the table: nothing in flight may still write
     // the old array when it is freed, and every entry is re-pointed
+    // one host-mapped array: row hints in [0, cap), status words in
+    // [cap, 2 cap)
     void* h = nullptr;
-    CK(cudaHostAlloc(&h, sizeof(int) * cap, cudaHostAllocMapped));
-    std::memset(h, 0, sizeof(int) * cap);
+    CK(cudaHostAlloc(&h, sizeof(int) * 2 * cap, cudaHostAllocMapped));
+    std::memset(h, 0, sizeof(int) * 2 * cap);
     if (row_hint_host_) {
         CK(cudaDeviceSynchronize());
         std::memcpy(h, row_hint_host_, sizeof(int) * sp_cap_);
+        std::memcpy((int*)h + cap, row_hint_host_ + sp_cap_, sizeof(int) * sp_cap_);
         CK(cudaFreeHost(row_hint_host_));
     }
     row_hint_host_ = (int*)h;
@@ -814,14 +818,27 @@ void Engine::widen_rows() {
         const int oc = s->hp.cap;
         if ((long long)m * 5 <= (long long)oc * 4)
             continue;
+        if (s->row_cap_fixed > 0)
+            continue; // pinned by atvb_system_set_capacity: reported, not grown
         s->widen_list(round_up((long long)(m * 1.5) + 32, 32));
         push_params(id);
+        if (m > oc) {
+            // a build within the last call cut a row (its forces missed
+            // pairs, flagged in the status bits): build again at the next
+            // step, into the wider rows, instead of waiting for the skin
+            const int one = 1;
+            CK(cudaMemcpyAsync(&s->hp.st->force_build, &one, sizeof(int),
+                               cudaMemcpyHostToDevice, stream_));
+            CK(cudaStreamSynchronize(stream_)); // `one` lives on this frame
+        }
     }
 }
 
 void Engine::push_params(int id) {
     Slot* s = slot(id);
     s->hp.row_hint = (row_hint_dev_ && id < sp_cap_) ? row_hint_dev_ + id : nullptr;
+    s->hp.status_hint =
+        (row_hint_dev_ && id < sp_cap_) ? row_hint_dev_ + sp_cap_ + id : nullptr;
     if ((s->npt || s->baro || s->hp.deform_axis >= 0) && s->uploaded) {
         // the device owns an NPT system's cell: keep it
         SysParams dev;
@@ -1109,30 +1126,118 @@ int Engine::deform_budget(int n) {
     return (int)k;
 }
 
-void Engine::step(int n) {
+void Engine::step(int n) { run_pieces(n, nullptr, nullptr); }
+
+// Systems stopped by StopOnNaN: every slot's host-mapped status word
+// (bit 30), read after the stream has drained.
+bool Engine::all_halted() const {
+    bool any = false;
+    for (const auto& up : slots_) {
+        if (!up || !up->uploaded)
+            continue;
+        any = true;
+        if (!(((volatile int*)row_hint_host_)[sp_cap_ + up->index] & (1 << 30)))
+            return false;
+    }
+    return any;
+}
+
+void Engine::check_halted(int id) {
+    CK(cudaSetDevice(device_));
+    CK(cudaStreamSynchronize(stream_));
+    Slot* s = slot(id);
+    if (!row_hint_host_ || id >= sp_cap_)
+        return;
+    if (((volatile int*)row_hint_host_)[sp_cap_ + id] & (1 << 30)) {
+        SysState st;
+        CK(cudaMemcpy(&st, s->hp.st, sizeof(st), cudaMemcpyDeviceToHost));
+        throw Error(ATVB_ERR_PHYSICS, "stopped by StopOnNaN at step " +
+                                          std::to_string(st.step) +
+                                          ": a position or velocity is not finite");
+    }
+}
+
+// Steps in pieces of at most kMaxPiece, with the host checks between them
+// (row widening, cell re-plan, Deform budget), outside any timed span.
+// Timed (total_ms != null): a CUDA event before each piece and after every
+// step on the engine stream; step_ms (may be null) gets each step's time,
+// *total_ms the sum of the pieces' spans.
+void Engine::run_pieces(int n, double* step_ms, double* total_ms) {
     CK(cudaSetDevice(device_));
     if (n < 0)
         throw Error(ATVB_ERR_INVALID, "n_steps must be >= 0");
-    int left = n;
+    const bool timed = total_ms != nullptr;
+    if (timed && profiling_)
+        throw Error(ATVB_ERR_STATE, "step_timed is not available in profiling mode");
+    std::vector<cudaEvent_t> ev;
+    double tot = 0.0;
+    int left = n, done = 0;
     do {
         // The cell re-plan and the row check read what the previous call
         // left (the engine stream is non-blocking, so a plain copy would not
-        // wait for it): a step call starts once the one before has finished.
+        // wait for it): a piece starts once the one before has finished.
         CK(cudaStreamSynchronize(stream_));
         if (any_npt_)
             replan_npt();
         widen_rows();
         ensure_ready();
+        if (done > 0 && all_halted())
+            break; // every system stopped by StopOnNaN: nothing moves
         // Long calls run in pieces of at most kMaxPiece steps, so the row
         // check and the cell re-plan above also happen inside them; a Deform
         // cell is re-planned between pieces before it shrinks out of its bins
         const int piece = std::min(left, kMaxPiece);
         const int k = any_npt_ ? deform_budget(piece) : piece;
-        run_steps(k);
+        if (!timed) {
+            run_steps(k);
+        } else {
+            ensure_graph();
+            while ((int)ev.size() < k + 1) {
+                cudaEvent_t e;
+                CK(cudaEventCreate(&e));
+                ev.push_back(e);
+            }
+            CK(cudaEventRecord(ev[0], stream_));
+            for (int j = 0; j < k; ++j) {
+                CK(cudaGraphLaunch(gexec_, stream_));
+                CK(cudaEventRecord(ev[j + 1], stream_));
+            }
+            CK(cudaEventSynchronize(ev[k]));
+            float ms = 0.f;
+            if (step_ms)
+                for (int j = 0; j < k; ++j) {
+                    CK(cudaEventElapsedTime(&ms, ev[j], ev[j + 1]));
+                    step_ms[done + j] = ms;
+                }
+            CK(cudaEventElapsedTime(&ms, ev[0], ev[k]));
+            tot += ms;
+        }
         left -= k;
+        done += k;
     } while (left > 0);
-    last_launches_ = kernels_per_step() * n;
-    steps_since_check_ += n;
+    for (auto& e : ev)
+        cudaEventDestroy(e);
+    if (timed)
+        *total_ms = tot;
+    last_launches_ = kernels_per_step() * done;
+    steps_since_check_ += done;
+}
+
+void Engine::ensure_graph() {
+    if (gexec_)
+        return;
+    CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+    try {
+        enqueue_step(false);
+    } catch (...) {
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(stream_, &g);
+        if (g)
+            cudaGraphDestroy(g);
+        throw;
+    }
+    CK(cudaStreamEndCapture(stream_, &graph_));
+    CK(cudaGraphInstantiate(&gexec_, graph_, 0));
 }
 
 void Engine::run_steps(int n) {
@@ -1143,52 +1248,17 @@ void Engine::run_steps(int n) {
         }
         collect_profile();
     } else {
-        if (!gexec_) {
-            CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
-            try {
-                enqueue_step(false);
-            } catch (...) {
-                cudaGraph_t g = nullptr;
-                cudaStreamEndCapture(stream_, &g);
-                if (g)
-                    cudaGraphDestroy(g);
-                throw;
-            }
-            CK(cudaStreamEndCapture(stream_, &graph_));
-            CK(cudaGraphInstantiate(&gexec_, graph_, 0));
-        }
+        ensure_graph();
         for (int k = 0; k < n; ++k)
             CK(cudaGraphLaunch(gexec_, stream_));
     }
 }
 
 void Engine::step_timed(int n, double* step_ms, double* total_ms) {
-    CK(cudaSetDevice(device_));
-    ensure_ready();
-    if (profiling_)
-        throw Error(ATVB_ERR_STATE, "step_timed is not available in profiling mode");
-    step(0); // capture the graph outside the timed span
-    std::vector<cudaEvent_t> ev(n + 1);
-    for (auto& e : ev)
-        CK(cudaEventCreate(&e));
-    CK(cudaEventRecord(ev[0], stream_));
-    for (int k = 0; k < n; ++k) {
-        CK(cudaGraphLaunch(gexec_, stream_));
-        CK(cudaEventRecord(ev[k + 1], stream_));
-    }
-    CK(cudaEventSynchronize(ev[n]));
-    float ms = 0.f;
-    if (step_ms)
-        for (int k = 0; k < n; ++k) {
-            CK(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
-            step_ms[k] = ms;
-        }
-    CK(cudaEventElapsedTime(&ms, ev[0], ev[n]));
+    double tot = 0.0;
+    run_pieces(n, step_ms, &tot);
     if (total_ms)
-        *total_ms = ms;
-    for (auto& e : ev)
-        cudaEventDestroy(e);
-    last_launches_ = kernels_per_step() * n;
+        *total_ms = tot;
 }
 
 void Engine::collect_profile() {
@@ -1245,13 +1315,32 @@ void Engine::compute_forces_one(int id) {
 // Forced neighbour build of the systems in `lc`, repeated with larger rows
 // until no row overflows.  Outside the step loop only (upload, force pass).
 void Engine::sized_rebuild(const LaunchCfg& lc) {
+    // row-overflow bits raised by earlier steps stay; those of the attempts
+    // below are dropped with the cut lists they describe
+    std::vector<int> ids(lc.nsys);
+    CK(cudaMemcpy(ids.data(), lc.sys_list, sizeof(int) * lc.nsys, cudaMemcpyDeviceToHost));
+    std::vector<int> before(lc.nsys);
+    for (int k = 0; k < lc.nsys; ++k) {
+        SysState st;
+        CK(cudaMemcpy(&st, slot(ids[k])->hp.st, sizeof(st), cudaMemcpyDeviceToHost));
+        before[k] = st.status & kStatusRowOverflow;
+    }
     for (int attempt = 0; attempt < 4; ++attempt) {
         launch_force_rebuild(lc, stream_);
         launch_rebuild(lc, stream_);
         CK(cudaGetLastError());
         CK(cudaStreamSynchronize(stream_));
-        if (!check_lists(lc))
+        if (!check_lists(lc)) {
+            for (int k = 0; k < lc.nsys; ++k)
+                if (before[k]) {
+                    SysState* d = slot(ids[k])->hp.st;
+                    int st = 0;
+                    CK(cudaMemcpy(&st, &d->status, sizeof(int), cudaMemcpyDeviceToHost));
+                    st |= kStatusRowOverflow;
+                    CK(cudaMemcpy(&d->status, &st, sizeof(int), cudaMemcpyHostToDevice));
+                }
             return;
+        }
     }
     throw Error(ATVB_ERR_OVERFLOW, "neighbour rows kept overflowing");
 }
@@ -1268,10 +1357,21 @@ bool Engine::check_lists(const LaunchCfg& lc) {
         SysState st;
         CK(cudaMemcpy(&st, sp->hp.st, sizeof(st), cudaMemcpyDeviceToHost));
         if (st.overflow || st.max_nnbr > sp->hp.cap) {
+            if (sp->row_cap_fixed > 0)
+                throw Error(ATVB_ERR_OVERFLOW,
+                            "neighbour rows need " + std::to_string(st.max_nnbr) +
+                                " entries, above the pinned capacity " +
+                                std::to_string(sp->row_cap_fixed));
             const int cap = round_up((long long)(st.max_nnbr * 1.25) + 32, 32);
             sp->alloc_list(cap);
+            // the cut list is rebuilt before any force kernel reads it: the
+            // row-overflow bit this build raised does not stand (one that
+            // an earlier step raised is put back by sized_rebuild)
             int zero = 0;
             CK(cudaMemcpy(&sp->hp.st->overflow, &zero, sizeof(int),
+                          cudaMemcpyHostToDevice));
+            const int status = st.status & ~kStatusRowOverflow;
+            CK(cudaMemcpy(&sp->hp.st->status, &status, sizeof(int),
                           cudaMemcpyHostToDevice));
             push_params(sp->index);
             regrow = true;
@@ -1481,6 +1581,62 @@ void Engine::set_deform(int id, int axis, double rate, double L0) {
     sl->deform_args[2] = h.deform_L0;
     any_npt_ = true;
     push_params(id);
+    dirty_ = true;
+}
+
+// Sticky status bits and the StopOnNaN halt of one system, cleared (the
+// caller has dealt with the cause, e.g. restored a checkpoint).
+void Engine::clear_status(int id) {
+    CK(cudaSetDevice(device_));
+    Slot* s = slot(id);
+    CK(cudaStreamSynchronize(stream_));
+    if (s->uploaded) {
+        SysState st;
+        CK(cudaMemcpy(&st, s->hp.st, sizeof(st), cudaMemcpyDeviceToHost));
+        st.status = 0;
+        st.halted = 0;
+        st.nearq_lost = 0;
+        CK(cudaMemcpy(s->hp.st, &st, sizeof(st), cudaMemcpyHostToDevice));
+    }
+    if (row_hint_host_ && id < sp_cap_)
+        ((volatile int*)row_hint_host_)[sp_cap_ + id] = 0;
+}
+
+// cuda::StopOnNaN attached to (or detached from) one system.
+void Engine::set_stop_on_nan(int id, bool on) {
+    Slot* s = slot(id);
+    s->hp.stop_on_nan = on ? 1 : 0;
+    push_params(id);
+    CK(cudaStreamSynchronize(stream_));
+}
+
+// Capacity overrides: a pinned row length (0: automatic) and the size of
+// the mixed build's near-cutoff queue (0: automatic).
+void Engine::set_capacity(int id, int row_cap, int nearq_cap) {
+    CK(cudaSetDevice(device_));
+    if (row_cap < 0 || nearq_cap < 0)
+        throw Error(ATVB_ERR_INVALID, "capacities must be >= 0");
+    Slot* s = slot(id);
+    CK(cudaStreamSynchronize(stream_));
+    release_graph();
+    s->row_cap_fixed = row_cap;
+    if (row_cap > 0 && row_cap != s->hp.cap)
+        s->alloc_list(row_cap); // rows are rebuilt by the next upload or build
+    if (nearq_cap > 0 && s->hp.nearq) {
+        s->free_alloc(s->hp.nearq);
+        s->hp.nearq = (int2*)s->dalloc((size_t)nearq_cap * sizeof(int2));
+        s->hp.nearq_cap = nearq_cap;
+    }
+    push_params(id);
+    CK(cudaStreamSynchronize(stream_));
+    if (s->uploaded && row_cap > 0) {
+        // the old rows are gone: build into the pinned ones now
+        const LaunchCfg one = restricted_cfg(id);
+        launch_force_rebuild(one, stream_);
+        launch_rebuild(one, stream_);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(stream_));
+    }
     dirty_ = true;
 }
 
@@ -1778,6 +1934,8 @@ void Engine::upload(int id, const atvb_soa_view& f) {
                        stream_));
     push_params(id);
     CK(cudaStreamSynchronize(stream_));
+    if (row_hint_host_ && id < sp_cap_)
+        ((volatile int*)row_hint_host_)[sp_cap_ + id] = 0; // a fresh state: no status
     s->uploaded = true;
     s->snap_read = 0; // the published snapshot count restarts with the state
     dirty_ = true;
@@ -1823,8 +1981,12 @@ void Engine::scalars(int id, atvb_scalars* out) {
     out->step = st.step;
     out->rebuilds = st.rebuilds;
     out->max_neighbors = st.max_nnbr;
-    out->status = st.overflow ? ATVB_ERR_OVERFLOW
-                              : ((st.status & kStatusBoxRange) ? ATVB_ERR_STATE : 0);
+    out->status_bits = (uint32_t)st.status;
+    out->halted = st.halted;
+    out->status = (st.status & kStatusRowOverflow)
+                      ? ATVB_ERR_OVERFLOW
+                      : ((st.status & kStatusBoxRange) ? ATVB_ERR_STATE
+                                                        : (st.status ? ATVB_ERR_PHYSICS : 0));
     out->list_pairs = (int64_t)(st.list_entries / 2);
     for (int k = 0; k < 3; ++k)
         out->box[k] = st.box[k];
@@ -2002,7 +2164,7 @@ namespace atvb {
 
 namespace {
 constexpr char kCkptMagic[8] = {'A', 'T', 'V', 'B', 'C', 'K', 'P', '1'};
-constexpr uint32_t kCkptVersion = 1;
+constexpr uint32_t kCkptVersion = 2;
 
 struct CkptHeader {
     char magic[8];
@@ -2165,7 +2327,7 @@ void Engine::restore(int id, const void* buf, size_t size, bool fresh_list) {
         st.disp_thr2 = thr > 0.0 ? thr * thr : -1.0;
         st.need_rebuild = thr > 0.0 ? 0 : 1;
         st.ago = 0;
-        st.status &= ~kStatusBoxRange;
+        st.held = 0; // the new bins cover the current cell (the sticky bit stays)
     } else {
         CK(cudaMemcpyAsync(P.xr, a[9], b, cudaMemcpyHostToDevice, stream_));
         CK(cudaMemcpyAsync(P.yr, a[10], b, cudaMemcpyHostToDevice, stream_));
@@ -2205,7 +2367,7 @@ void Engine::replan_npt() {
         Slot* old = up.get();
         SysState st;
         CK(cudaMemcpy(&st, old->hp.st, sizeof(st), cudaMemcpyDeviceToHost));
-        bool need = (st.status & kStatusBoxRange) != 0;
+        bool need = st.held != 0;
         for (int k = 0; k < 3; ++k) {
             const double lo = old->hp.npt_Lmin[k], plan = old->geo.L[k];
             if (st.Lnext[k] < lo * 1.02 || st.Lnext[k] > plan * 1.25)

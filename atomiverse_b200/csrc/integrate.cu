@@ -69,6 +69,17 @@ ATVB_DEV void speed_cap(const SysParams& P, double v[3]) {
     }
 }
 
+// cuda::StopOnNaN's condition (criterion.cuh:166-178), per atom: a NaN or
+// infinite position or velocity raises the sticky status bit.  Positions
+// enter the force kernels as fixed point, where a NaN would become an
+// ordinary coordinate, so the check sits here, on the FP64 master state of
+// every drift (a non-finite force shows in the kicked velocity).
+ATVB_DEV void check_finite(const SysParams& P, const double x[3], const double v[3]) {
+    const double t = (x[0] + x[1]) + (x[2] + v[0]) + (v[1] + v[2]);
+    if (!isfinite(t))
+        atomicOr(&P.st->status, kStatusNonFinite);
+}
+
 // MTK NPT initial half for atom i (nose_hoover_npt.cpp:812-850 P2-P6): the
 // pending per-axis velocity scale (end-of-step chain and barostat factors of
 // the previous step, initial-half ones of this step), the force kick, the
@@ -106,6 +117,7 @@ ATVB_DEV double npt_drift_atom(const SysParams& P, int i) {
     P.x[i] = x[0];
     P.y[i] = x[1];
     P.z[i] = x[2];
+    check_finite(P, x, v);
     const double q = P.q[i];
     if (P.prec == kMixed) {
         int4 p;
@@ -130,6 +142,8 @@ __global__ void __launch_bounds__(kChunk)
     for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
         const Item item = items[it];
         const SysParams& P = sp[item.sys];
+        if (P.st->halted)
+            continue; // block-uniform: the item belongs to one system
         const int i = item.begin + threadIdx.x;
         double ke = 0.0;
         if (i < P.n && (P.thermostat == kNPT || P.generic_drift)) {
@@ -156,6 +170,7 @@ __global__ void __launch_bounds__(kChunk)
             P.x[i] = x[0];
             P.y[i] = x[1];
             P.z[i] = x[2];
+            check_finite(P, x, v);
             const double q = P.q[i];
             if (P.prec == kMixed) {
                 int4 p;
@@ -191,6 +206,10 @@ __global__ void k_sys_a(const int* sys_list, int nsys, const SysParams* sp) {
         return;
     const SysParams& P = sp[sys_list[k]];
     SysState* st = P.st;
+    if (st->halted) {
+        st->rebuild = 0; // nothing of this system moves: no list build either
+        return;
+    }
     if (P.thermostat == kNPT || P.deform_axis >= 0) {
         // commit the cell of this step's drift: every later kernel of the
         // step (neighbour build, forces, PME) reads it from SysParams
@@ -211,10 +230,15 @@ __global__ void k_sys_a(const int* sys_list, int nsys, const SysParams* sp) {
     st->ago += 1;
     const bool disp = st->need_rebuild != 0;
     st->need_rebuild = 0;
-    const bool rebuild = st->ago >= P.nl_delay && (st->ago % P.nl_every) == 0 &&
-                         (!P.nl_check || disp);
+    // a build the host asked for (rows widened after one was cut) comes
+    // first, whatever every/delay/check would say
+    const bool forced = st->force_build != 0;
+    st->force_build = 0;
+    const bool rebuild = forced || (st->ago >= P.nl_delay && (st->ago % P.nl_every) == 0 &&
+                                    (!P.nl_check || disp));
     st->rebuild = rebuild ? 1 : 0;
     if (rebuild) {
+        st->overflow = 0; // set again by the build if a row is cut
         for (int d = 0; d < 3; ++d) {
             st->Lb[d] = P.L[d];
             st->Lb_inv[d] = 1.0 / P.L[d];
@@ -234,6 +258,8 @@ __global__ void __launch_bounds__(kChunk)
     for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
         const Item item = items[it];
         const SysParams& P = sp[item.sys];
+        if (P.st->halted)
+            continue;
         const int i = item.begin + threadIdx.x;
         double ke = 0.0;
         double kax[3] = {0.0, 0.0, 0.0};
@@ -316,6 +342,15 @@ ATVB_DEV void cell_scalars(const SysParams& P, SysState* st) {
         (2.0 * st->kinetic + st->virial[0] + st->virial[1] + st->virial[2]) / (3.0 * V);
 }
 
+// End of a step: StopOnNaN halts a system whose state went non-finite, and
+// any sticky bit is published to the host-mapped status word.
+ATVB_DEV void end_status(const SysParams& P, SysState* st) {
+    if (P.stop_on_nan && (st->status & kStatusNonFinite))
+        st->halted = 1;
+    if (P.status_hint && st->status)
+        *(volatile int*)P.status_hint = st->status | (st->halted ? (1 << 30) : 0);
+}
+
 ATVB_DEV void record_history(const SysParams& P, SysState* st) {
     if (P.ehist_cap > 0) {
         const long long slot = st->step % P.ehist_cap;
@@ -325,6 +360,7 @@ ATVB_DEV void record_history(const SysParams& P, SysState* st) {
     }
     if (P.row_hint && st->rebuild) // the longest row changes only at a build
         *(volatile int*)P.row_hint = st->max_nnbr;
+    end_status(P, st);
 }
 
 // Berendsen barostat at end_of_step (barostat.cpp:27-110): from the scalar
@@ -345,6 +381,7 @@ ATVB_DEV void berendsen(const SysParams& P, SysState* st) {
     }
     if (!ok) {
         st->status |= kStatusBoxRange;
+        st->held = 1;
         mu = 1.0;
         for (int d = 0; d < 3; ++d)
             Ln[d] = P.L[d];
@@ -394,8 +431,10 @@ ATVB_DEV void deform_prepare(const SysParams& P, SysState* st, long long k) {
         if (!(st->Lnext[d] >= P.npt_Lmin[d]))
             ok = false;
     }
-    if (!ok)
+    if (!ok) {
         st->status |= kStatusBoxRange;
+        st->held = 1;
+    }
     for (int d = 0; d < 3; ++d) {
         st->fixn_scale[d] = 4294967296.0 / st->Lnext[d];
         st->fixn64_scale[d] = 18446744073709551616.0 / st->Lnext[d];
@@ -458,6 +497,8 @@ __global__ void k_sys_b(const int* sys_list, int nsys, const SysParams* sp) {
         return;
     const SysParams& P = sp[sys_list[k]];
     SysState* st = P.st;
+    if (st->halted)
+        return;
     if (P.thermostat == kNPT) {
         npt_end_of_step(P, st);
         return;
@@ -491,6 +532,7 @@ __global__ void k_sys_b(const int* sys_list, int nsys, const SysParams* sp) {
     }
     if (P.row_hint && st->rebuild) // the longest row changes only at a build
         *(volatile int*)P.row_hint = st->max_nnbr;
+    end_status(P, st);
     st->step += 1;
 }
 

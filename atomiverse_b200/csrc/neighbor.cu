@@ -451,8 +451,11 @@ __global__ void __launch_bounds__(256)
                 P.nnbr[i] = cnt < cap ? cnt : cap;
                 atomicMax(&P.st->max_nnbr, cnt);
                 atomicAdd(&P.st->list_entries, (unsigned long long)cnt);
-                if (cnt > cap)
+                if (cnt > cap) {
+                    // the row is cut: pairs are missing until rows are widened
                     atomicOr(&P.st->overflow, 1);
+                    atomicOr(&P.st->status, kStatusRowOverflow);
+                }
             }
         }
     }

@@ -211,6 +211,7 @@ ATVB_DEV void npt_prepare(const SysParams& P, SysState* st, double ke[3], const 
     }
     if (!ok) {
         st->status |= kStatusBoxRange;
+        st->held = 1;
         for (int d = 0; d < 3; ++d) {
             a[d] = 1.0;
             dr[d] = 1.0;

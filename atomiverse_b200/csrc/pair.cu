@@ -219,8 +219,11 @@ ATVB_DEV void queue_near(const SysParams& P, int s, int code) {
     const int q = atomicAdd(&P.st->nearq_n, 1);
     if (q < P.nearq_cap)
         P.nearq[q] = make_int2(s, code);
-    else
+    else {
+        // the share keeps its FP32 cutoff decisions: flagged, never silent
         atomicAdd(&P.st->nearq_lost, 1);
+        atomicOr(&P.st->status, kStatusNearqLost);
+    }
 }
 
 template <bool LJ, bool CO, bool VIR, bool NEAR>

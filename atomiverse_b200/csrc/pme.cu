@@ -11,9 +11,10 @@
 //  * the transforms are real-to-complex / complex-to-real on the half grid
 //    (K0 x K1 x (K2/2+1)); the half-grid energy and virial weight every
 //    mode with 0 < m2 < K2/2 twice;
-//  * H(m) is tabulated once per box (the CPU-style tables of
-//    pme_influence.h:104-155), and the virial that the reference CUDA PME
-//    omits is produced from the same pass.
+//  * H(m) is evaluated on the fly from the per-axis B-spline moduli and the
+//    current cell (no 3D table: a changing NPT cell needs no rebuild), and
+//    the virial that the reference CUDA PME omits is produced from the same
+//    pass.
 #include "atvb_common.cuh"
 #include "atvb_kernels.cuh"
 #include "pair_math.cuh"

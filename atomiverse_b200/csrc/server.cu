@@ -179,7 +179,10 @@ struct atvb_server {
         for (int64_t id : done) {
             Request& r = get(id);
             retire(r, true, keep_ckpt);
-            r.state = 2;
+            // a segment that ran on wrong or non-finite physics (a sticky
+            // status bit, atvb_scalars.status_bits) ends as failed; its frame
+            // can still be collected
+            r.state = r.sc.status_bits ? 4 : 2;
             r.t_done = now();
         }
     }

@@ -10,16 +10,22 @@
 // order their streams); two calls in flight at once corrupt each other's
 // scratch.  The first call on a device looks the array's address up with
 // cudaGetSymbolAddress; make that first call outside any stream capture.
+// The address is kept per device together with the id of the context it
+// belongs to, and looked up again when that context changes (after a
+// cudaDeviceReset the array lives at a new address).
 //
-// Method: cells of edge >= the larger cutoff, count / scan / scatter into a
-// cell-sorted copy, each cell's atoms put in index order (so sums run in a
-// fixed order and repeat bit for bit), then one thread per atom walks the
+// Method: cells of edge >= the larger cutoff, count / scan / scatter of
+// atom indices, then each atom's place in its cell from the number of
+// smaller indices in that cell (so every cell is in index order, sums run
+// in a fixed order and repeat bit for bit; one thread per atom, no serial
+// per-cell sort), then one thread per atom walks the
 // 27 neighbouring cells (every cell along an axis with fewer than 3 cells).
 // Physics as the library's main pair kernel: shifted LJ
 // (src/cpu/potentials/pair_lj_cut.cpp:723-800, shift
 // cuda/potentials/lj_kernel.cuh:59-65) and Coulomb
 // k_e q_i q_j erfc(alpha r)/r (src/cpu/potentials/coul_long.cpp:146-222),
 // minimum image in an orthorhombic box, energy halved per visit.
+#include <cuda.h> // CUcontext / CUresult types only: no libcuda link
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -44,9 +50,11 @@ constexpr size_t kOffSlot = kOffCell + 4 * (size_t)kStaticMaxAtoms;  // int[atom
 constexpr size_t kOffIdx = kOffSlot + 4 * (size_t)kStaticMaxAtoms;   // int[atoms]
 constexpr size_t kOffPos = kOffIdx + 4 * (size_t)kStaticMaxAtoms;    // double4[atoms]
 constexpr size_t kOffEnergy = kOffPos + 32 * (size_t)kStaticMaxAtoms; // u64[2]
-constexpr size_t kStaticBytes = kOffEnergy + 256;
+constexpr size_t kOffTmp = kOffEnergy + 256;                        // int[atoms]
+constexpr size_t kStaticBytes = kOffTmp + 4 * (size_t)kStaticMaxAtoms;
 static_assert(kOffStart % 256 == 0 && kOffCell % 256 == 0 && kOffSlot % 256 == 0 &&
-                  kOffIdx % 256 == 0 && kOffPos % 256 == 0 && kOffEnergy % 256 == 0,
+                  kOffIdx % 256 == 0 && kOffPos % 256 == 0 && kOffEnergy % 256 == 0 &&
+                  kOffTmp % 256 == 0,
               "scratch regions must stay 256-byte aligned");
 
 __device__ __align__(256) unsigned char g_static_scratch[kStaticBytes];
@@ -66,6 +74,7 @@ struct StaticArgs {
     int* cell;
     int* slot;
     int* sidx;
+    int* tmp; // atom indices of each cell in arrival order
     double4* pos;
     unsigned long long* esum;
 };
@@ -143,36 +152,32 @@ __global__ void __launch_bounds__(1024) k_static_scan(StaticArgs a) {
         a.start[a.ncell] = run;
 }
 
+// Atom indices into their cells, in arrival order (which varies from call
+// to call with the atomic slots).
 __global__ void k_static_scatter(StaticArgs a) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.n)
         return;
-    const int s = a.start[a.cell[i]] + a.slot[i];
+    a.tmp[a.start[a.cell[i]] + a.slot[i]] = i;
+}
+
+// Each atom's place in its cell = the number of smaller indices in that cell,
+// so every cell ends up in original-index order whatever the arrival order.
+// One thread per atom, O(atoms in the cell) each: a cell holding many atoms
+// costs a longer scan per thread, never a serial sort.
+__global__ void k_static_rank(StaticArgs a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n)
+        return;
+    const int c = a.cell[i];
+    const int b = a.start[c], e = a.start[c + 1];
+    int r = 0;
+    for (int k = b; k < e; ++k)
+        r += a.tmp[k] < i ? 1 : 0;
+    const int s = b + r;
     a.pos[s] = make_double4(wrap_static(a.x[i], a.L[0]), wrap_static(a.y[i], a.L[1]),
                             wrap_static(a.z[i], a.L[2]), a.has_coul ? a.q[i] : 0.0);
     a.sidx[s] = i;
-}
-
-// Put each cell's atoms in original-index order (insertion sort, one thread
-// per cell): the atomic slot order above varies from call to call, this
-// order does not.
-__global__ void k_static_order(StaticArgs a) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= a.ncell)
-        return;
-    const int b = a.start[c], e = a.start[c + 1];
-    for (int k = b + 1; k < e; ++k) {
-        const int key = a.sidx[k];
-        const double4 p = a.pos[k];
-        int m = k - 1;
-        while (m >= b && a.sidx[m] > key) {
-            a.sidx[m + 1] = a.sidx[m];
-            a.pos[m + 1] = a.pos[m];
-            --m;
-        }
-        a.sidx[m + 1] = key;
-        a.pos[m + 1] = p;
-    }
 }
 
 ATVB_DEV double img(double d, double L, double halfL) {
@@ -276,18 +281,50 @@ __global__ void k_static_energy(StaticArgs a) {
 
 std::mutex g_scratch_mu;
 void* g_scratch_addr[kStaticMaxDevices] = {};
+unsigned long long g_scratch_ctx[kStaticMaxDevices] = {};
+
+// Unique id of the calling thread's current context (cuCtxGetId), 0 if there
+// is none yet.  The driver calls come through the runtime's entry-point
+// lookup, so the library does not link libcuda itself.
+unsigned long long current_ctx_id() {
+    using GetCur = CUresult (*)(CUcontext*);
+    using GetId = CUresult (*)(CUcontext, unsigned long long*);
+    static GetCur get_cur = nullptr;
+    static GetId get_id = nullptr;
+    if (!get_cur || !get_id) {
+        void* p = nullptr;
+        void* q = nullptr;
+        cudaDriverEntryPointQueryResult r1, r2;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &p, 12000, cudaEnableDefault,
+                                             &r1) != cudaSuccess ||
+            cudaGetDriverEntryPointByVersion("cuCtxGetId", &q, 12000, cudaEnableDefault,
+                                             &r2) != cudaSuccess ||
+            !p || !q)
+            return 0;
+        get_cur = reinterpret_cast<GetCur>(p);
+        get_id = reinterpret_cast<GetId>(q);
+    }
+    CUcontext c = nullptr;
+    unsigned long long id = 0;
+    if (get_cur(&c) != CUDA_SUCCESS || c == nullptr || get_id(c, &id) != CUDA_SUCCESS)
+        return 0;
+    return id;
+}
 
 unsigned char* static_scratch(int dev) {
     if (dev < 0 || dev >= kStaticMaxDevices)
         throw Error(ATVB_ERR_INVALID, "device ordinal out of range for the static scratch");
     std::lock_guard<std::mutex> lk(g_scratch_mu);
-    if (g_scratch_addr[dev] == nullptr) {
+    const unsigned long long ctx = current_ctx_id();
+    if (g_scratch_addr[dev] == nullptr || ctx == 0 || ctx != g_scratch_ctx[dev]) {
+        // first call on this device, or a new context (a device reset)
         void* p = nullptr;
         const cudaError_t rc = cudaGetSymbolAddress(&p, g_static_scratch);
         if (rc != cudaSuccess || p == nullptr)
             throw Error(ATVB_ERR_CUDA, std::string("cudaGetSymbolAddress(static scratch): ") +
                                            cudaGetErrorString(rc));
         g_scratch_addr[dev] = p;
+        g_scratch_ctx[dev] = current_ctx_id(); // the context now exists
     }
     return static_cast<unsigned char*>(g_scratch_addr[dev]);
 }
@@ -365,6 +402,7 @@ void run_static(const atvb_system_desc& d, const double* x, const double* y,
     a.sidx = reinterpret_cast<int*>(base + kOffIdx);
     a.pos = reinterpret_cast<double4*>(base + kOffPos);
     a.esum = reinterpret_cast<unsigned long long*>(base + kOffEnergy);
+    a.tmp = reinterpret_cast<int*>(base + kOffTmp);
     a.x = x;
     a.y = y;
     a.z = z;
@@ -379,7 +417,7 @@ void run_static(const atvb_system_desc& d, const double* x, const double* y,
     k_static_bin<<<ab, 256, 0, stream>>>(a);
     k_static_scan<<<1, 1024, 0, stream>>>(a);
     k_static_scatter<<<ab, 256, 0, stream>>>(a);
-    k_static_order<<<cb, 256, 0, stream>>>(a);
+    k_static_rank<<<ab, 256, 0, stream>>>(a);
     k_static_forces<<<ab, 256, 0, stream>>>(a);
     if (energy)
         k_static_energy<<<1, 32, 0, stream>>>(a);

@@ -27,6 +27,26 @@ extern "C" {
 #define ATVB_ERR_STATE 4    /* call out of order (e.g. step before upload) */
 #define ATVB_ERR_NOMEM 5    /* device memory budget exceeded */
 #define ATVB_ERR_NOTFOUND 6 /* unknown request / slot id */
+#define ATVB_ERR_PHYSICS 7  /* a sticky status bit is set: some step ran on
+                               wrong or non-finite physics (status_bits) */
+
+/* atvb_scalars.status_bits: sticky until atvb_system_clear_status.  When any
+ * is set, atvb_system_scalars / _download / _run and atvb_batch_download
+ * still fill their outputs and then return ATVB_ERR_PHYSICS. */
+#define ATVB_STATUS_ROW_OVERFLOW 1u  /* a step used a neighbour list whose row
+                                        was cut at its capacity (pairs lost);
+                                        the next step call widens the rows and
+                                        rebuilds before stepping on */
+#define ATVB_STATUS_BOX_RANGE 2u     /* an NPT / barostat / Deform cell left the
+                                        range its bins were planned for within
+                                        one call and was held */
+#define ATVB_STATUS_NEARQ_LOST 4u    /* mixed: near-cutoff LJ pairs overflowed the
+                                        settle queue and kept their FP32 cutoff
+                                        decision */
+#define ATVB_STATUS_NONFINITE 8u     /* a position or velocity became NaN or
+                                        infinite (cuda::StopOnNaN's condition) */
+#define ATVB_STATUS_FORCE_RANGE 16u  /* a pair force beyond the range of the
+                                        fixed-point force accumulators */
 
 enum atvb_precision {
     ATVB_FP64 = 0,  /* FP64 pair, PME and integrator (reference ATV_CUDA_PREC_MODE=double) */
@@ -124,11 +144,14 @@ typedef struct atvb_scalars {
     int64_t step;
     int64_t rebuilds;
     int32_t max_neighbors;
-    int32_t status;       /* 0, ATVB_ERR_OVERFLOW, or ATVB_ERR_STATE (an NPT cell
-                             left the range its neighbour grid was planned for) */
+    int32_t status;       /* 0, or the ATVB_ERR_* code of the lowest status bit:
+                             ATVB_ERR_OVERFLOW (row overflow), ATVB_ERR_STATE
+                             (cell held), ATVB_ERR_PHYSICS (the others) */
     int64_t list_pairs;   /* unordered pairs in the current list (cutoff + skin) */
     double box[3];        /* current cell edges [A] (change under NPT) */
     double pressure;      /* (2 KE + W_xx + W_yy + W_zz) / (3 V) [eV/A^3] */
+    uint32_t status_bits; /* ATVB_STATUS_* (sticky) */
+    int32_t halted;       /* 1: stopped by StopOnNaN at step `step` */
 } atvb_scalars;
 
 /* Per-kernel-group device time from CUDA events (profiling mode). */
@@ -258,6 +281,24 @@ int atvb_system_set_snapshots(atvb_system* sys, int32_t every, int32_t depth);
 int atvb_system_snapshot_poll(atvb_system* sys, int32_t max_frames, int64_t* steps,
                               double* box, double* x, double* y, double* z, double* vx,
                               double* vy, double* vz, int32_t* count, int64_t* dropped);
+/* Sticky status bits (atvb_scalars.status_bits): clear them (and un-halt a
+ * system stopped by StopOnNaN) once the caller has dealt with the cause. */
+int atvb_system_clear_status(atvb_system* sys);
+/* cuda::StopOnNaN (include/atomiverse/cuda/driver/criterion.cuh:166-178):
+ * with on != 0, the step at which a position or velocity of the system
+ * turns non-finite is its last: the device stops integrating it (positions,
+ * velocities and the step counter stay as they were), later step calls
+ * return ATVB_ERR_PHYSICS at once, and scalars report halted = 1.  Off by
+ * default (the reference stops only with the criterion attached); the
+ * ATVB_STATUS_NONFINITE bit is raised either way. */
+int atvb_system_set_stop_on_nan(atvb_system* sys, int32_t on);
+/* Capacity overrides (0 = automatic sizing).  row_capacity pins the
+ * neighbour row length (no automatic growth: a build that needs longer rows
+ * fails with ATVB_ERR_OVERFLOW outside a step call, and raises
+ * ATVB_STATUS_ROW_OVERFLOW within one); nearq_capacity sizes the mixed
+ * build's near-cutoff settle queue.  For tuning and for tests. */
+int atvb_system_set_capacity(atvb_system* sys, int32_t row_capacity,
+                             int32_t nearq_capacity);
 /* Profiling: enable per-kernel-group CUDA events on subsequent steps. */
 int atvb_system_profile(atvb_system* sys, int32_t enable);
 int atvb_system_profile_read(atvb_system* sys, atvb_kernel_time* out,
@@ -278,6 +319,9 @@ int atvb_batch_compute_forces(atvb_batch* b);
 int atvb_batch_step(atvb_batch* b, int32_t n_steps);
 int atvb_batch_download(atvb_batch* b, int32_t index, atvb_soa_view* frame,
                         atvb_scalars* scalars);
+/* atvb_system_clear_status / _set_stop_on_nan for system `index`. */
+int atvb_batch_clear_status(atvb_batch* b, int32_t index);
+int atvb_batch_set_stop_on_nan(atvb_batch* b, int32_t index, int32_t on);
 /* atvb_system_set_lj_types / _set_special_bonds for system `index` of a
  * batch, before that system's first upload. */
 /* atvb_system_set_npt for system `index` of a batch, before its first upload. */
@@ -309,7 +353,9 @@ int atvb_batch_profile_read(atvb_batch* b, atvb_kernel_time* out,
 /* ---- server: continuous batching of MD segments ------------------------ */
 typedef struct atvb_request_result {
     int64_t id;
-    int32_t state;        /* 0 queued, 1 running, 2 done, 3 cancelled, 4 failed,
+    int32_t state;        /* 0 queued, 1 running, 2 done, 3 cancelled, 4 failed
+                             (not admitted, or finished with a sticky status
+                             bit: the frame can still be collected),
                              5 suspended */
     int32_t steps_done;
     double t_submit, t_start, t_done; /* seconds on the server clock */

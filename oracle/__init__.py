@@ -71,11 +71,16 @@ class OrcDesc(C.Structure):
 _lib = None
 
 
+# where the reference source tree sits in the build container (it is absent
+# on GPU machines, which use the prebuilt oracle/_ref)
+REFERENCE_ROOT = os.environ.get("ATVB_REFERENCE_ROOT", "/root/reference")
+
+
 def build() -> str:
     """Compile liboracle.so (and the reference PME wrapper when the
     reference tree is present)."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
-    subprocess.run([os.path.join(HERE, "ref_build.sh")], check=True)
+    subprocess.run([os.path.join(HERE, "ref_build.sh"), REFERENCE_ROOT], check=True)
     return LIB_PATH
 
 

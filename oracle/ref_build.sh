@@ -2,10 +2,14 @@
 # Compile the reference's own header-only PME math from the reference tree
 # (never copied into this repository) into oracle/_ref/libref_pme.so.
 # Test infrastructure: the oracle's restatement is checked against it.
-# Usage: oracle/ref_build.sh [REFERENCE_ROOT]   (default /root/reference)
+# Usage: oracle/ref_build.sh REFERENCE_ROOT
 set -e
 here=$(cd "$(dirname "$0")" && pwd)
-ref=${1:-/root/reference}
+if [ $# -lt 1 ]; then
+    echo "usage: $0 REFERENCE_ROOT (the Atomiverse source tree)" >&2
+    exit 2
+fi
+ref=$1
 if [ ! -f "$ref/include/atomiverse/cpu/longrange/pme_spline.h" ]; then
     echo "reference tree not found at $ref; skipping" >&2
     exit 0

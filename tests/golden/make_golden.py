@@ -6,7 +6,7 @@ The reference leaves the 3D FFT to FFTW (src/cpu/longrange/pme.cpp:203-210:
 FFTW_FORWARD then unnormalised FFTW_BACKWARD); numpy's fftn / ifftn*N are
 the same transforms.  Run from the repository root:
 
-    oracle/ref_build.sh && python tests/golden/make_golden.py
+    oracle/ref_build.sh <reference tree> && python tests/golden/make_golden.py
 
 Writes tests/golden/pme_reference.npz (small: a few KB).
 """
@@ -60,7 +60,7 @@ def ref_pme(lib, pos, q, L, alpha, K, order):
 def main():
     lib = oracle.ref_pme_lib()
     if lib is None:
-        raise SystemExit("build oracle/_ref first: oracle/ref_build.sh")
+        raise SystemExit("build oracle/_ref first: oracle/ref_build.sh <reference tree>")
     out = {}
     # bspline / moduli / FFT sizes (pme_spline.h)
     for n in (4, 5, 6, 8):

@@ -2,16 +2,17 @@
 
 Compared with the library's main path (atvb_system_compute_forces on a
 system without PME, whose pair forces and LJ / real-space Coulomb energies
-are the same physics) on two calls in a row with different inputs, plus
-the up-front rejections.  This file sorts last so it also runs after every
-other GPU test in the same process.
+are the same physics) on two calls in a row with different inputs, with
+the CPU FP64 oracle directly, in its LJ-only (no charge array),
+Coulomb-only and no-energy forms, plus the up-front rejections.  This file
+sorts last so it also runs after every other GPU test in the same process.
 """
 import ctypes as C
 
 import numpy as np
 import pytest
 
-from conftest import rms_rel
+from conftest import oracle_system, rms_rel
 
 
 def _case(atvb, ncell, seed, rc=10.0):
@@ -22,7 +23,7 @@ def _case(atvb, ncell, seed, rc=10.0):
     return desc, frame
 
 
-def _static(atvb, torch, desc, frame, stream=None):
+def _static(atvb, torch, desc, frame, stream=None, charges=True, energy=True):
     dev = torch.device("cuda:0")
     t = {k: torch.as_tensor(np.ascontiguousarray(frame[k]), dtype=torch.float64, device=dev)
          for k in ("x", "y", "z", "charge")}
@@ -33,11 +34,20 @@ def _static(atvb, torch, desc, frame, stream=None):
     lib = atvb.load()
     rc = lib.atvb_pair_forces_static(
         C.byref(d), t["x"].data_ptr(), t["y"].data_ptr(), t["z"].data_ptr(),
-        t["charge"].data_ptr(), f[0].data_ptr(), f[1].data_ptr(), f[2].data_ptr(),
-        e.data_ptr(), stream)
+        t["charge"].data_ptr() if charges else None, f[0].data_ptr(), f[1].data_ptr(),
+        f[2].data_ptr(), e.data_ptr() if energy else None, stream)
     atvb.check(rc)
     torch.cuda.synchronize()
     return np.stack([a.cpu().numpy() for a in f], axis=1), e.cpu().numpy()
+
+
+def _oracle(orc, desc, frame):
+    o = oracle_system(orc, dict(desc, pme_enabled=0), frame)
+    o.build_list()
+    o.compute_forces()
+    st, sc = o.state(), o.scalars()
+    o.close()
+    return np.stack([st["fx"], st["fy"], st["fz"]], axis=1), sc
 
 
 @pytest.mark.gpu
@@ -89,3 +99,45 @@ def test_static_rejects_oversize_and_bad_boxes(atvb):
     assert call() == 1                        # valid description, NULL arrays
     assert "NULL" in lib.atvb_last_error().decode()
     assert lib.atvb_pair_forces_static(None, *null) == 1
+
+
+@pytest.mark.gpu
+def test_static_matches_oracle(atvb, ctx, orc):
+    """Against the CPU FP64 oracle directly (LJ + real-space Coulomb)."""
+    torch = pytest.importorskip("torch")
+    desc, frame = _case(atvb, 12, 6)
+    fref, sc = _oracle(orc, desc, frame)
+    f, e = _static(atvb, torch, desc, frame)
+    assert rms_rel(f, fref) <= 1e-6
+    assert e[0] == pytest.approx(sc["e_lj"], rel=1e-9, abs=1e-6)
+    assert e[1] == pytest.approx(sc["e_coul"], rel=1e-9, abs=1e-6)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("form", ["lj_only", "coul_only", "no_energy"])
+def test_static_partial_forms(atvb, ctx, orc, form):
+    """LJ only with no charge array, Coulomb only, and no energy output:
+    forces against the main path and the oracle, twice in a row."""
+    torch = pytest.importorskip("torch")
+    for seed in (7, 8):
+        desc, frame = _case(atvb, 12, seed)
+        if form == "lj_only":
+            desc["coul_enabled"] = 0
+        elif form == "coul_only":
+            desc["lj_enabled"] = 0
+        sys_ = atvb.System(ctx, desc, frame)
+        sys_.compute_forces()
+        out, sc = sys_.download()
+        sys_.close()
+        ref = np.stack([out["fx"], out["fy"], out["fz"]], axis=1)
+        fref, osc = _oracle(orc, desc, frame)
+        f, e = _static(atvb, torch, desc, frame, charges=(form != "lj_only"),
+                       energy=(form != "no_energy"))
+        assert np.all(np.isfinite(f))
+        assert rms_rel(f, ref) <= 1e-6
+        assert rms_rel(f, fref) <= 1e-6
+        if form == "no_energy":
+            assert np.all(np.isnan(e))         # the energy buffer is not touched
+        else:
+            assert e[0] == pytest.approx(sc["energy_lj"], rel=1e-9, abs=1e-6)
+            assert e[1] == pytest.approx(sc["energy_coul"], rel=1e-9, abs=1e-6)
