@@ -113,6 +113,8 @@ static std::vector<double> spline_moduli(int K, int n) {
 
 // ------------------------------------------------------------ geometry
 
+constexpr double kTileAtoms = 128.0; // target atoms per tile
+
 // `shrink` > 0 (MTK NPT): plan the bins and stencil for every cell down to
 // L (1 - shrink) per axis, so that the grid stays valid while the cell
 // breathes; the bins then grow with the cell (bin count fixed).
@@ -157,9 +159,28 @@ Geometry make_geometry(const atvb_system_desc& d, double shrink) {
     const double density = d.n_atoms / (Lp[0] * Lp[1] * Lp[2]);
     auto per_bin = [&](double reach) { return density * std::pow(g.rlist / reach, 3.0); };
     const double reach_t = per_bin(3.0) >= 5.0 ? 3.0 : (per_bin(2.0) >= 1.5 ? 2.0 : 1.0);
+    // Tiles (the half-row pair kernel's unit of work and shared-memory
+    // window): whole bins, an edge of at least rlist so that a listed pair
+    // lies in one tile or two neighbouring ones, sized for ~kTileAtoms atoms;
+    // an axis with fewer than 3 such tiles is a single tile.
+    const double per_rl3 = density * g.rlist * g.rlist * g.rlist;
+    const double tscale = per_rl3 >= kTileAtoms ? 1.0 : std::cbrt(kTileAtoms / per_rl3);
     for (int k = 0; k < 3; ++k) {
-        int c = (int)std::floor(Lp[k] / (g.rlist / reach_t));
-        g.nc[k] = c < 1 ? 1 : c;
+        int t = (int)std::floor(Lp[k] / (tscale * g.rlist));
+        if (t < 3)
+            t = 1;
+        int c;
+        if (t >= 3) {
+            const int b = (int)std::floor((Lp[k] / t) / (g.rlist / reach_t));
+            g.bt[k] = b < 1 ? 1 : b;
+            c = t * g.bt[k];
+        } else {
+            c = (int)std::floor(Lp[k] / (g.rlist / reach_t));
+            c = c < 1 ? 1 : c;
+            g.bt[k] = c;
+        }
+        g.nt[k] = t;
+        g.nc[k] = c;
         g.cs[k] = Lp[k] / g.nc[k];
         int r = (int)std::ceil(g.rlist / g.cs[k] - 1e-12);
         g.reach[k] = r < 1 ? 1 : r;
@@ -283,6 +304,20 @@ void Slot::free_alloc(void* p) {
     }
 }
 
+// Bin and tile counts of the geometry into the device parameters.
+static void set_bins(SysParams& hp, const Geometry& g) {
+    for (int k = 0; k < 3; ++k) {
+        hp.nc[k] = g.nc[k];
+        hp.alias[k] = g.alias[k];
+        hp.npt_Lmin[k] = g.Lmin[k];
+        hp.nt[k] = g.nt[k];
+        hp.bt[k] = g.bt[k];
+    }
+    hp.ncell = g.nc[0] * g.nc[1] * g.nc[2];
+    hp.bpt = g.bt[0] * g.bt[1] * g.bt[2];
+    hp.ntile = g.nt[0] * g.nt[1] * g.nt[2];
+}
+
 // Re-plan the bins and stencil for cells down to L (1 - shrink) per axis
 // (MTK NPT): new bin arrays and columns, box-dependent fields recomputed.
 void Slot::replan_cells(double shrink) {
@@ -291,12 +326,7 @@ void Slot::replan_cells(double shrink) {
     free_alloc(hp.cell_count);
     free_alloc(hp.cell_start);
     free_alloc(hp.cols);
-    for (int k = 0; k < 3; ++k) {
-        hp.nc[k] = geo.nc[k];
-        hp.alias[k] = geo.alias[k];
-        hp.npt_Lmin[k] = geo.Lmin[k];
-    }
-    hp.ncell = geo.nc[0] * geo.nc[1] * geo.nc[2];
+    set_bins(hp, geo);
     hp.ncol = (int)geo.cols.size();
     hp.cell_count = (int*)dalloc(sizeof(int) * hp.ncell);
     hp.cell_start = (int*)dalloc(sizeof(int) * (hp.ncell + 1));
@@ -347,18 +377,14 @@ Slot::Slot(const atvb_system_desc& d, const DevMem& mem) : desc(d), mem_(mem) {
     std::memset(&hp, 0, sizeof(hp));
     const int n = d.n_atoms;
     if (n > kMaxAtoms)
-        throw Error(ATVB_ERR_INVALID, "at most 2^30 - 1 atoms per system");
+        throw Error(ATVB_ERR_INVALID, "at most 2^27 - 1 atoms per system");
     hp.n = n;
     hp.deform_axis = -1;
     hp.prec = d.precision == ATVB_MIXED ? kMixed : kFP64;
     if (d.precision != ATVB_FP64 && d.precision != ATVB_MIXED)
         throw Error(ATVB_ERR_INVALID, "unknown precision");
-    for (int k = 0; k < 3; ++k) {
-        hp.nc[k] = geo.nc[k];
-        hp.alias[k] = geo.alias[k];
-        hp.npt_Lmin[k] = geo.Lmin[k];
-    }
-    hp.ncell = geo.nc[0] * geo.nc[1] * geo.nc[2];
+    set_bins(hp, geo);
+    hp.half = 1; // until per-type LJ or special bonds make it general
     hp.rlist = geo.rlist;
     hp.rlist2 = geo.rlist * geo.rlist;
     hp.nl_cut = d.nl_cutoff;
@@ -478,6 +504,16 @@ Slot::Slot(const atvb_system_desc& d, const DevMem& mem) : desc(d), mem_(mem) {
     hp.pos4 = hp.prec == kMixed ? dalloc((size_t)n * sizeof(int4))
                                 : dalloc((size_t)n * sizeof(double4));
     hp.f4 = (double4*)dalloc((size_t)n * sizeof(double4));
+    // fixed-point pair forces of half-row systems: 2^32 per eV/A in the
+    // mixed build (range +-2^31 eV/A), 2^40 in FP64 (range +-2^23 eV/A, a
+    // quantum of 9e-13 eV/A); a pair force above 2^22 (mixed) or 2^14 eV/A
+    // (FP64) is flagged, so that no sum of up to 512 such pairs wraps
+    hp.ffix = (unsigned long long*)dalloc((size_t)n * 3 * sizeof(unsigned long long));
+    CK(cudaMemsetAsync(hp.ffix, 0, (size_t)n * 3 * sizeof(unsigned long long), stream));
+    hp.force_scale = hp.prec == kMixed ? 4294967296.0 : 1099511627776.0;
+    hp.force_scale_inv = 1.0 / hp.force_scale;
+    hp.force_lim2 = hp.prec == kMixed ? 17592186044416.0 /* (2^22)^2 */
+                                      : 268435456.0 /* (2^14)^2 */;
     auto di = [&](size_t cnt) { return (int*)dalloc(cnt * sizeof(int)); };
     hp.perm = di(n);
     hp.rank = di(n);
@@ -1688,6 +1724,7 @@ void Engine::set_lj_types(int id, int ncoef, const int32_t* ti, const int32_t* t
     sl->lj_sig.assign(sigma, sigma + ncoef);
     sl->ntypes = nt;
     sl->hp.general = 1;
+    sl->hp.half = 0; // full rows: the general pair kernel
     push_params(id);
     dirty_ = true;
 }
@@ -1776,6 +1813,7 @@ void Engine::set_special_bonds(int id, const double lj[3], const double coul[3],
     sl->bond_b.assign(b, b + nbonds);
     sl->special_set = true;
     sl->hp.general = 1;
+    sl->hp.half = 0; // full rows: the general pair kernel
     push_params(id);
     dirty_ = true;
 }
@@ -2398,6 +2436,7 @@ void Engine::replan_npt() {
         s->bond_a = old->bond_a;
         s->bond_b = old->bond_b;
         s->hp.general = old->hp.general;
+        s->hp.half = old->hp.half;
         // the snapshot ring moves over with its read position
         s->snap_host = old->snap_host;
         s->snap_read = old->snap_read;

@@ -129,16 +129,17 @@ def test_stop_on_nan_halts_the_system(atvb, ctx):
     md.set_evaluator(atvb.PairLJCut(1.0, 1.0, desc["lj_cutoff"]))
     md.set_integrator(atvb.VelocityVerlet(desc["dt"]))
     md.add_criterion(atvb.StopOnNaN())
-    fr = dict(frame, box=desc["box"])
+    fr = {k: (v.copy() if hasattr(v, "copy") else v) for k, v in frame.items()}
+    fr["box"] = desc["box"]
     with pytest.raises(atvb.PhysicsError):
-        md.run(fr, 4)
+        md.run(fr, 4)                     # (run() downloads into fr's arrays)
     # clearing the status resumes a system whose state was repaired
     s2 = atvb.System(ctx, desc, frame)
     s2.set_stop_on_nan(True)
     s2.step(2)
     assert s2.scalars(check=False)["halted"]
-    good = dict(frame)
-    good["vy"] = np.zeros_like(frame["vy"])
+    _, good = _hot_lj(ncell=6)            # a finite state, freshly made
+    good["vy"] = np.zeros_like(good["vy"])
     s2.upload(good)
     s2.clear_status()
     s2.step(3)
