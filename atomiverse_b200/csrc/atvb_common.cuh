@@ -136,16 +136,6 @@ struct SysParams {
     int nl_every, nl_delay, nl_check;
     int nc[3], ncell;
     double cs_inv[3];
-    // tiles: blocks of bt[k] bins per axis (edge >= cutoff + skin, so a pair
-    // lies in one tile or in two neighbouring ones), nt[k] tiles per axis
-    // (1: the tile spans the axis); atoms are sorted tile by tile, bins in
-    // a tile in (x, y, z) order, so every tile is one contiguous range
-    int nt[3], bt[3], bpt, ntile;
-    // half rows (k_pair_half): each pair once, in the row of the atom whose
-    // tile sees the other's as its own or one of 13 forward tiles; entries
-    // carry the window segment (0: own tile, 1..13: forward tile) in the top
-    // bits.  0: full rows (per-type / special-bond systems, k_pair_general)
-    int half;
     int alias[3]; // axis has fewer than 2*reach+1 cells: visit every cell
     int ncol;     // stencil columns
     int4* cols;   // {dx, dy, zreach(-1 = whole column), 0}
@@ -233,12 +223,10 @@ struct SysParams {
     double4* posd4;  // FP64 sorted positions used by the pair-set test
     int4* lpos;      // fixed-point sorted positions at the last build (prefilter)
     double4* f4;     // forces in sorted order
-    // half-row systems: pair forces in 64-bit fixed point, 3 per atom in
-    // sorted order (force_scale units per eV/A), summed by the pair kernel,
-    // turned into f4 and cleared by the next atom pass
-    unsigned long long* ffix;
-    double force_scale, force_scale_inv;
-    double force_lim2; // a pair force^2 above this raises kStatusForceRange
+    // mixed build: pairs closer than this may carry a force beyond the range
+    // of the 64-bit fixed-point sums (2^-32 eV/A units); set at upload from
+    // the LJ parameters and the largest charge product (0 in FP64)
+    double force_r2_safe;
     double4* fp4;    // PME reciprocal forces of this step (sorted; PME systems)
     int *perm, *rank, *cell_of, *slot, *cell_count, *cell_start, *cellS;
     int *nbr, *nnbr;
@@ -254,15 +242,10 @@ struct SysParams {
     int ehist_cap;
 };
 
-// Row entries of the neighbour list.  Full rows: sorted index in the low 30
-// bits, the special class (0: none, 1: 1-2, 2: 1-3, 3: 1-4) in the top 2
-// bits.  Half rows: sorted index in the low 27 bits, the window segment of
-// its tile (0..13) in bits 27-30.
+// Row entries of the neighbour list: sorted index in the low 30 bits, the
+// special class (0: none, 1: 1-2, 2: 1-3, 3: 1-4) in the top 2 bits.
 constexpr unsigned kRowIdxMask = 0x3fffffffu;
-constexpr unsigned kHalfIdxMask = (1u << 27) - 1u;
-constexpr int kHalfSegShift = 27;
-constexpr int kMaxAtoms = (1 << 27) - 1;
-constexpr int kWinSegs = 14; // own tile + 13 forward tiles
+constexpr int kMaxAtoms = (1 << 30) - 1;
 
 // A unit of work: a chunk of atoms (or grid points) of one system.
 struct Item {
@@ -273,37 +256,6 @@ struct Item {
 #define ATVB_DEV __device__ __forceinline__
 
 ATVB_DEV long long to_fix(double v) { return __double2ll_rn(v * kEFix); }
-
-// The 13 forward tile offsets (lexicographically positive), segment k + 1.
-ATVB_DEV int3 fwd_offset(int k) {
-    if (k < 9)
-        return make_int3(1, k / 3 - 1, k % 3 - 1);
-    if (k < 12)
-        return make_int3(0, 1, k - 10);
-    return make_int3(0, 0, 1);
-}
-
-// Segment of tile offset (dx, dy, dz) in {-1, 0, 1}^3: 0 for the own tile,
-// 1..13 for a forward tile, -1 for a backward one.
-ATVB_DEV int offset_segment(int dx, int dy, int dz) {
-    if (dx == 1)
-        return 1 + (dy + 1) * 3 + (dz + 1);
-    if (dx == 0 && dy == 1)
-        return 10 + (dz + 1);
-    if (dx == 0 && dy == 0 && dz == 1)
-        return 13;
-    if (dx == 0 && dy == 0 && dz == 0)
-        return 0;
-    return -1;
-}
-
-// Bin key of bin (cx, cy, cz): tile-major, bins of a tile in (x, y, z) order.
-ATVB_DEV int bin_key(const int nt[3], const int bt[3], int bpt, int cx, int cy, int cz) {
-    const int tx = cx / bt[0], ty = cy / bt[1], tz = cz / bt[2];
-    const int bx = cx - tx * bt[0], by = cy - ty * bt[1], bz = cz - tz * bt[2];
-    return ((tx * nt[1] + ty) * nt[2] + tz) * bpt + (bx * bt[1] + by) * bt[2] + bz;
-}
-
 
 // Fire-and-forget 64-bit integer reduction (no value returned, so the
 // issuing thread never waits for the L2 round trip).

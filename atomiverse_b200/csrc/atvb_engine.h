@@ -39,7 +39,6 @@ struct Geometry {
     double cs[3];
     int reach[3];
     int alias[3];
-    int nt[3], bt[3]; // tiles per axis, bins per tile per axis
     std::vector<int4> cols;
 };
 Geometry make_geometry(const atvb_system_desc& d, double shrink = 0.0);

@@ -113,8 +113,6 @@ static std::vector<double> spline_moduli(int K, int n) {
 
 // ------------------------------------------------------------ geometry
 
-constexpr double kTileAtoms = 128.0; // target atoms per tile
-
 // `shrink` > 0 (MTK NPT): plan the bins and stencil for every cell down to
 // L (1 - shrink) per axis, so that the grid stays valid while the cell
 // breathes; the bins then grow with the cell (bin count fixed).
@@ -159,28 +157,9 @@ Geometry make_geometry(const atvb_system_desc& d, double shrink) {
     const double density = d.n_atoms / (Lp[0] * Lp[1] * Lp[2]);
     auto per_bin = [&](double reach) { return density * std::pow(g.rlist / reach, 3.0); };
     const double reach_t = per_bin(3.0) >= 5.0 ? 3.0 : (per_bin(2.0) >= 1.5 ? 2.0 : 1.0);
-    // Tiles (the half-row pair kernel's unit of work and shared-memory
-    // window): whole bins, an edge of at least rlist so that a listed pair
-    // lies in one tile or two neighbouring ones, sized for ~kTileAtoms atoms;
-    // an axis with fewer than 3 such tiles is a single tile.
-    const double per_rl3 = density * g.rlist * g.rlist * g.rlist;
-    const double tscale = per_rl3 >= kTileAtoms ? 1.0 : std::cbrt(kTileAtoms / per_rl3);
     for (int k = 0; k < 3; ++k) {
-        int t = (int)std::floor(Lp[k] / (tscale * g.rlist));
-        if (t < 3)
-            t = 1;
-        int c;
-        if (t >= 3) {
-            const int b = (int)std::floor((Lp[k] / t) / (g.rlist / reach_t));
-            g.bt[k] = b < 1 ? 1 : b;
-            c = t * g.bt[k];
-        } else {
-            c = (int)std::floor(Lp[k] / (g.rlist / reach_t));
-            c = c < 1 ? 1 : c;
-            g.bt[k] = c;
-        }
-        g.nt[k] = t;
-        g.nc[k] = c;
+        int c = (int)std::floor(Lp[k] / (g.rlist / reach_t));
+        g.nc[k] = c < 1 ? 1 : c;
         g.cs[k] = Lp[k] / g.nc[k];
         int r = (int)std::ceil(g.rlist / g.cs[k] - 1e-12);
         g.reach[k] = r < 1 ? 1 : r;
@@ -271,6 +250,42 @@ size_t estimate_bytes(const atvb_system_desc& d) {
 
 // --------------------------------------------------------------- Slot
 
+// The smallest separation at which no pair force of a mixed-precision
+// system can reach 2^21 eV/A (its row sums are 64-bit fixed point in units
+// of 2^-32 eV/A, range 2^31 eV/A; 2^21 keeps any row of up to 1,024 such
+// pairs in range), from the LJ parameters and the largest charge product
+// (an upper bound of the real-space Coulomb force).  Bisection on the
+// repulsive branch.  A closer pair raises kStatusForceRange.
+static double force_safe_r2(const SysParams& hp, double qq_max) {
+    if (hp.prec != kMixed)
+        return 0.0;
+    const double lim = 2097152.0;
+    auto fmax = [&](double r) {
+        double f = 0.0;
+        if (hp.has_lj) {
+            const double r2inv = 1.0 / (r * r);
+            const double r6 = hp.lj_sig6 * r2inv * r2inv * r2inv;
+            f += std::fabs(hp.lj_eps24 * r2inv * r6 * (2.0 * r6 - 1.0)) * r;
+        }
+        if (hp.has_coul)
+            f += kQqr2e * qq_max * (1.0 / (r * r) + kEwaldF * hp.coul_alpha / r);
+        return f;
+    };
+    double lo = 1e-9, hi = hp.rlist;
+    if (!(fmax(hi) < lim))
+        return hi * hi; // every listed pair may exceed it: all are flagged
+    if (fmax(lo) < lim)
+        return 0.0;
+    for (int it = 0; it < 200; ++it) {
+        const double mid = 0.5 * (lo + hi);
+        if (fmax(mid) >= lim)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return hi * hi;
+}
+
 void* DevMem::alloc(size_t b) const {
     void* p = nullptr;
     if (b == 0)
@@ -304,20 +319,6 @@ void Slot::free_alloc(void* p) {
     }
 }
 
-// Bin and tile counts of the geometry into the device parameters.
-static void set_bins(SysParams& hp, const Geometry& g) {
-    for (int k = 0; k < 3; ++k) {
-        hp.nc[k] = g.nc[k];
-        hp.alias[k] = g.alias[k];
-        hp.npt_Lmin[k] = g.Lmin[k];
-        hp.nt[k] = g.nt[k];
-        hp.bt[k] = g.bt[k];
-    }
-    hp.ncell = g.nc[0] * g.nc[1] * g.nc[2];
-    hp.bpt = g.bt[0] * g.bt[1] * g.bt[2];
-    hp.ntile = g.nt[0] * g.nt[1] * g.nt[2];
-}
-
 // Re-plan the bins and stencil for cells down to L (1 - shrink) per axis
 // (MTK NPT): new bin arrays and columns, box-dependent fields recomputed.
 void Slot::replan_cells(double shrink) {
@@ -326,7 +327,12 @@ void Slot::replan_cells(double shrink) {
     free_alloc(hp.cell_count);
     free_alloc(hp.cell_start);
     free_alloc(hp.cols);
-    set_bins(hp, geo);
+    for (int k = 0; k < 3; ++k) {
+        hp.nc[k] = geo.nc[k];
+        hp.alias[k] = geo.alias[k];
+        hp.npt_Lmin[k] = geo.Lmin[k];
+    }
+    hp.ncell = geo.nc[0] * geo.nc[1] * geo.nc[2];
     hp.ncol = (int)geo.cols.size();
     hp.cell_count = (int*)dalloc(sizeof(int) * hp.ncell);
     hp.cell_start = (int*)dalloc(sizeof(int) * (hp.ncell + 1));
@@ -377,14 +383,18 @@ Slot::Slot(const atvb_system_desc& d, const DevMem& mem) : desc(d), mem_(mem) {
     std::memset(&hp, 0, sizeof(hp));
     const int n = d.n_atoms;
     if (n > kMaxAtoms)
-        throw Error(ATVB_ERR_INVALID, "at most 2^27 - 1 atoms per system");
+        throw Error(ATVB_ERR_INVALID, "at most 2^30 - 1 atoms per system");
     hp.n = n;
     hp.deform_axis = -1;
     hp.prec = d.precision == ATVB_MIXED ? kMixed : kFP64;
     if (d.precision != ATVB_FP64 && d.precision != ATVB_MIXED)
         throw Error(ATVB_ERR_INVALID, "unknown precision");
-    set_bins(hp, geo);
-    hp.half = 1; // until per-type LJ or special bonds make it general
+    for (int k = 0; k < 3; ++k) {
+        hp.nc[k] = geo.nc[k];
+        hp.alias[k] = geo.alias[k];
+        hp.npt_Lmin[k] = geo.Lmin[k];
+    }
+    hp.ncell = geo.nc[0] * geo.nc[1] * geo.nc[2];
     hp.rlist = geo.rlist;
     hp.rlist2 = geo.rlist * geo.rlist;
     hp.nl_cut = d.nl_cutoff;
@@ -504,16 +514,6 @@ Slot::Slot(const atvb_system_desc& d, const DevMem& mem) : desc(d), mem_(mem) {
     hp.pos4 = hp.prec == kMixed ? dalloc((size_t)n * sizeof(int4))
                                 : dalloc((size_t)n * sizeof(double4));
     hp.f4 = (double4*)dalloc((size_t)n * sizeof(double4));
-    // fixed-point pair forces of half-row systems: 2^32 per eV/A in the
-    // mixed build (range +-2^31 eV/A), 2^40 in FP64 (range +-2^23 eV/A, a
-    // quantum of 9e-13 eV/A); a pair force above 2^22 (mixed) or 2^14 eV/A
-    // (FP64) is flagged, so that no sum of up to 512 such pairs wraps
-    hp.ffix = (unsigned long long*)dalloc((size_t)n * 3 * sizeof(unsigned long long));
-    CK(cudaMemsetAsync(hp.ffix, 0, (size_t)n * 3 * sizeof(unsigned long long), stream));
-    hp.force_scale = hp.prec == kMixed ? 4294967296.0 : 1099511627776.0;
-    hp.force_scale_inv = 1.0 / hp.force_scale;
-    hp.force_lim2 = hp.prec == kMixed ? 17592186044416.0 /* (2^22)^2 */
-                                      : 268435456.0 /* (2^14)^2 */;
     auto di = [&](size_t cnt) { return (int*)dalloc(cnt * sizeof(int)); };
     hp.perm = di(n);
     hp.rank = di(n);
@@ -1724,7 +1724,6 @@ void Engine::set_lj_types(int id, int ncoef, const int32_t* ti, const int32_t* t
     sl->lj_sig.assign(sigma, sigma + ncoef);
     sl->ntypes = nt;
     sl->hp.general = 1;
-    sl->hp.half = 0; // full rows: the general pair kernel
     push_params(id);
     dirty_ = true;
 }
@@ -1813,7 +1812,6 @@ void Engine::set_special_bonds(int id, const double lj[3], const double coul[3],
     sl->bond_b.assign(b, b + nbonds);
     sl->special_set = true;
     sl->hp.general = 1;
-    sl->hp.half = 0; // full rows: the general pair kernel
     push_params(id);
     dirty_ = true;
 }
@@ -1939,6 +1937,13 @@ void Engine::upload(int id, const atvb_soa_view& f) {
             qs += f.charge[i];
             q2 += f.charge[i] * f.charge[i];
         }
+    {
+        double qm = 0.0;
+        if (f.charge)
+            for (int i = 0; i < n; ++i)
+                qm = std::max(qm, std::fabs(f.charge[i]));
+        s->hp.force_r2_safe = force_safe_r2(s->hp, qm * qm);
+    }
     if (s->hp.has_pme) {
         const double vol = s->hp.L[0] * s->hp.L[1] * s->hp.L[2];
         const double a = s->desc.pme_alpha;
@@ -2436,7 +2441,6 @@ void Engine::replan_npt() {
         s->bond_a = old->bond_a;
         s->bond_b = old->bond_b;
         s->hp.general = old->hp.general;
-        s->hp.half = old->hp.half;
         // the snapshot ring moves over with its read position
         s->snap_host = old->snap_host;
         s->snap_read = old->snap_read;

@@ -6,15 +6,10 @@
 // in FP64 on the rebuild-time coordinates, satisfies r^2 < (cutoff+skin)^2.
 // Every product and sum of that test is rounded separately (__dmul_rn /
 // __dadd_rn), which is exactly the arithmetic of the FP64 oracle, so the
-// pair set equals the oracle's bit for bit.  Rows are in ELL form with a
-// fixed capacity.  Atoms are sorted tile by tile (tiles of whole bins with
-// an edge >= cutoff + skin).  Half rows (single-type systems): every pair
-// once, in the row of the atom whose tile sees the other's as its own (then
-// the larger sorted index is the partner) or as one of its 13 forward
-// neighbours; each entry names that tile's window segment for the pair
-// kernel's shared-memory accumulation.  Full rows (per-type and
-// special-bond systems): each pair in both rows, so k_pair_general writes
-// only its own atom and sums every row in a fixed order.
+// pair set equals the oracle's bit for bit.  The list itself is a FULL list
+// (each pair stored in both rows) in row-major ELL form with a fixed row
+// capacity, so the force kernel needs no atomics and sums every row in a
+// fixed order.
 #include "atvb_common.cuh"
 #include "atvb_kernels.cuh"
 
@@ -39,7 +34,7 @@ __global__ void k_cell_count(const Item* items, int nitems,
             cd = cd < 0 ? 0 : (cd > P.nc[d] - 1 ? P.nc[d] - 1 : cd);
             c[d] = cd;
         }
-        const int cell = bin_key(P.nt, P.bt, P.bpt, c[0], c[1], c[2]);
+        const int cell = (c[0] * P.nc[1] + c[1]) * P.nc[2] + c[2];
         P.cell_of[i] = cell;
         P.slot[i] = atomicAdd(&P.cell_count[cell], 1);
     }
@@ -191,68 +186,48 @@ ATVB_DEV double exact_r2(const double4& a, const double4& b, const double* L,
                      __dmul_rn(d[2], d[2]));
 }
 
-// Tile offset along one axis (-1, 0, 1) of tile t seen from tile h: tiles
-// of a pair are neighbours, so with nt >= 3 the difference is 0, +-1 or
-// +-(nt - 1) across the periodic seam; one tile spans an axis with nt = 1.
-ATVB_DEV int tile_off(int t, int h, int nt) {
-    if (nt == 1)
-        return 0;
-    const int d = t - h;
-    return d == nt - 1 ? -1 : (d == 1 - nt ? 1 : d);
-}
-
-// The sorted atoms of stencil column `col` around bin (cx, cy, cz) of home
-// tile (hx, hy, hz): up to three contiguous runs, each inside one tile (a z
-// range of bins splits where it enters the next tile or wraps; it spans at
-// most three tiles, as a tile is at least `reach` bins deep), with the
-// window segment of the run's tile.  Half rows drop the runs of backward
-// tiles: those pairs belong to the other atom's row.  Offsets along an axis
-// stay within one period of the bin index, so one conditional add or
-// subtract wraps them (also on an aliased axis, whose offsets are absolute
-// bin indices).
-struct ColRuns {
-    int a[3], l[3], seg[3];
-};
-
+// The sorted atoms of stencil column `col` around cell (cx, cy, cz): at most
+// two contiguous runs [a0, a0 + l0) and [a1, a1 + l1) (two when the z range
+// wraps).  Offsets along an axis stay within one period of the cell index,
+// so one conditional add or subtract wraps them (also on an aliased axis,
+// whose offsets are absolute cell indices).
 ATVB_DEV void column_runs(const SysParams& P, const int* __restrict__ cstart, int4 col,
-                          int cx, int cy, int cz, int hx, int hy, int hz, ColRuns& r) {
+                          int cx, int cy, int cz, int& a0, int& l0, int& a1, int& l1) {
     const int nc0 = P.nc[0], nc1 = P.nc[1], nc2 = P.nc[2];
     int xx = cx + col.x;
     xx += xx < 0 ? nc0 : (xx >= nc0 ? -nc0 : 0);
     int yy = cy + col.y;
     yy += yy < 0 ? nc1 : (yy >= nc1 ? -nc1 : 0);
-    const int dtx = tile_off(xx / P.bt[0], hx, P.nt[0]);
-    const int dty = tile_off(yy / P.bt[1], hy, P.nt[1]);
-#pragma unroll
-    for (int q = 0; q < 3; ++q) {
-        r.a[q] = 0;
-        r.l[q] = 0;
-        r.seg[q] = 0;
-    }
-    auto put = [&](int q, int z0, int z1) {
-        const int k0 = bin_key(P.nt, P.bt, P.bpt, xx, yy, z0);
-        const int k1 = bin_key(P.nt, P.bt, P.bpt, xx, yy, z1);
-        const int seg = P.half ? offset_segment(dtx, dty, tile_off(z0 / P.bt[2], hz, P.nt[2]))
-                               : 0;
-        if (seg < 0)
-            return;
-        r.a[q] = cstart[k0];
-        r.l[q] = cstart[k1 + 1] - r.a[q];
-        r.seg[q] = seg;
-    };
+    const int base = (xx * nc1 + yy) * nc2;
+    int lo0, hi0, lo1 = 0, hi1 = -1;
     if (col.z < 0) {
-        put(0, 0, nc2 - 1); // aliased z: one tile spans the axis, bins contiguous
-        return;
+        lo0 = base;
+        hi0 = base + nc2 - 1;
+    } else {
+        const int z0 = cz - col.z, z1 = cz + col.z;
+        if (z0 < 0) {
+            lo0 = base + z0 + nc2;
+            hi0 = base + nc2 - 1;
+            lo1 = base;
+            hi1 = base + z1;
+        } else if (z1 >= nc2) {
+            lo0 = base + z0;
+            hi0 = base + nc2 - 1;
+            lo1 = base;
+            hi1 = base + z1 - nc2;
+        } else {
+            lo0 = base + z0;
+            hi0 = base + z1;
+        }
     }
-    int z = cz - col.z;
-    const int zend = cz + col.z;
-    const int b2 = P.bt[2];
-    for (int q = 0; q < 3 && z <= zend; ++q) {
-        const int zw = z < 0 ? z + nc2 : (z >= nc2 ? z - nc2 : z);
-        const int tile_last = (zw / b2 + 1) * b2 - 1; // last bin of this z tile
-        const int len = min(tile_last - zw, zend - z) + 1;
-        put(q, zw, zw + len - 1);
-        z += len;
+    a0 = cstart[lo0];
+    l0 = cstart[hi0 + 1] - a0;
+    if (hi1 >= lo1) {
+        a1 = cstart[lo1];
+        l1 = cstart[hi1 + 1] - a1;
+    } else {
+        a1 = 0;
+        l1 = 0;
     }
 }
 
@@ -294,6 +269,7 @@ __global__ void __launch_bounds__(256)
         const int c = item.begin + warp;
         if (c >= P.ncell)
             continue; // warp-uniform
+        const int nc1 = P.nc[1], nc2 = P.nc[2];
         const double L[3] = {P.L[0], P.L[1], P.L[2]};
         const double hL[3] = {P.halfL[0], P.halfL[1], P.halfL[2]};
         const double rl2 = P.rlist2;
@@ -306,13 +282,7 @@ __global__ void __launch_bounds__(256)
         const float blo = P.lband_lo, bhi = P.lband_hi;
         const float flo = P.fband_lo, fhi = P.fband_hi;
         const bool local = P.lframe_ok != 0;
-        const bool half = P.half != 0;
-        // home bin (cx, cy, cz) and its tile (hx, hy, hz) from the bin key
-        const int T = c / P.bpt, lb = c - T * P.bpt;
-        const int hz = T % P.nt[2], hy = (T / P.nt[2]) % P.nt[1], hx = T / (P.nt[1] * P.nt[2]);
-        const int cz = hz * P.bt[2] + lb % P.bt[2];
-        const int cy = hy * P.bt[1] + (lb / P.bt[2]) % P.bt[1];
-        const int cx = hx * P.bt[0] + lb / (P.bt[1] * P.bt[2]);
+        const int cz = c % nc2, cy = (c / nc2) % nc1, cx = c / (nc1 * nc2);
         const int cs = cstart[c], ce = cstart[c + 1];
         for (int i0 = cs; i0 < ce; i0 += kCellAtomsWarp) {
             const int ni = min(kCellAtomsWarp, ce - i0);
@@ -329,17 +299,10 @@ __global__ void __launch_bounds__(256)
             __syncwarp();
             int cnt = 0; // row length of atom i0 + lane
             for (int c0 = 0; c0 < ncol; c0 += 32) {
-                ColRuns cr;
-                if (c0 + lane < ncol) {
-                    column_runs(P, cstart, cols[c0 + lane], cx, cy, cz, hx, hy, hz, cr);
-                } else {
-#pragma unroll
-                    for (int q = 0; q < 3; ++q)
-                        cr.a[q] = cr.l[q] = cr.seg[q] = 0;
-                }
-                const int l01 = cr.l[0] + cr.l[1];
-                const int tot = l01 + cr.l[2];
-                const int segs = cr.seg[0] | (cr.seg[1] << 4) | (cr.seg[2] << 8);
+                int a0 = 0, l0 = 0, a1 = 0, l1 = 0;
+                if (c0 + lane < ncol)
+                    column_runs(P, cstart, cols[c0 + lane], cx, cy, cz, a0, l0, a1, l1);
+                const int tot = l0 + l1;
                 int incl = tot;
 #pragma unroll
                 for (int o = 1; o < 32; o <<= 1) {
@@ -361,21 +324,11 @@ __global__ void __launch_bounds__(256)
                     }
                     own &= 31;
                     const int o = t - __shfl_sync(full, excl, own);
-                    const int oa0 = __shfl_sync(full, cr.a[0], own);
-                    const int ol0 = __shfl_sync(full, cr.l[0], own);
-                    const int oa1 = __shfl_sync(full, cr.a[1], own);
-                    const int ol01 = __shfl_sync(full, l01, own);
-                    const int oa2 = __shfl_sync(full, cr.a[2], own);
-                    const int osg = __shfl_sync(full, segs, own);
+                    const int oa0 = __shfl_sync(full, a0, own);
+                    const int ol0 = __shfl_sync(full, l0, own);
+                    const int oa1 = __shfl_sync(full, a1, own);
                     const bool live = t < total;
-                    const int run = o < ol0 ? 0 : (o < ol01 ? 1 : 2);
-                    const int j = !live ? -1
-                                        : (run == 0 ? oa0 + o
-                                                    : (run == 1 ? oa1 + (o - ol0) : oa2 + (o - ol01)));
-                    // half rows: the tile's window segment; its own tile
-                    // (segment 0) holds a pair in the smaller index's row
-                    const int seg = (osg >> (4 * run)) & 15;
-                    const unsigned eseg = (unsigned)seg << kHalfSegShift;
+                    const int j = live ? (o < ol0 ? oa0 + o : oa1 + (o - ol0)) : -1;
                     int4 qj = make_int4(0, 0, 0, 0);
                     if (live)
                         qj = lp[j];
@@ -396,10 +349,8 @@ __global__ void __launch_bounds__(256)
                             const float bx = rb.x - rx, by = rb.y - ry, bz = rb.z - rz;
                             const float r2a = ax * ax + ay * ay + az * az;
                             const float r2b = bx * bx + by * by + bz * bz;
-                            const bool va = live && (half ? (seg != 0 || j > i0 + ii)
-                                                          : j != i0 + ii);
-                            const bool vb = live && (half ? (seg != 0 || j > i0 + i1)
-                                                          : j != i0 + i1);
+                            const bool va = live && j != i0 + ii;
+                            const bool vb = live && j != i0 + i1;
                             bool ha = va && r2a < flo, hb = vb && r2b < flo;
                             const bool aa = va && !(r2a < flo) && r2a < fhi;
                             const bool ab = vb && !(r2b < flo) && r2b < fhi;
@@ -416,7 +367,7 @@ __global__ void __launch_bounds__(256)
                                 const int baseb = __shfl_sync(full, cnt, i1);
                                 if (ha) {
                                     const int wpos = basea + __popc(ma & lt);
-                                    unsigned e = half ? ((unsigned)j | eseg) : (unsigned)j;
+                                    unsigned e = (unsigned)j;
                                     if (P.has_special)
                                         e |= special_class(P, i0 + ii, j) << 30;
                                     if (wpos < cap)
@@ -424,7 +375,7 @@ __global__ void __launch_bounds__(256)
                                 }
                                 if (hb) {
                                     const int wpos = baseb + __popc(mb & lt);
-                                    unsigned e = half ? ((unsigned)j | eseg) : (unsigned)j;
+                                    unsigned e = (unsigned)j;
                                     if (P.has_special)
                                         e |= special_class(P, i0 + i1, j) << 30;
                                     if (wpos < cap)
@@ -440,8 +391,7 @@ __global__ void __launch_bounds__(256)
                             const float4 ri = sr[warp][ii];
                             const float dx = ri.x - rx, dy = ri.y - ry, dz = ri.z - rz;
                             const float r2f = dx * dx + dy * dy + dz * dz;
-                            const bool valid =
-                                live && (half ? (seg != 0 || j > i0 + ii) : j != i0 + ii);
+                            const bool valid = live && j != i0 + ii;
                             bool hit = valid && r2f < flo;
                             const bool amb = valid && !(r2f < flo) && r2f < fhi;
                             if (__any_sync(full, amb)) {
@@ -453,7 +403,7 @@ __global__ void __launch_bounds__(256)
                                 const int base = __shfl_sync(full, cnt, ii);
                                 if (hit) {
                                     const int wpos = base + __popc(m & lt);
-                                    unsigned e = half ? ((unsigned)j | eseg) : (unsigned)j;
+                                    unsigned e = (unsigned)j;
                                     if (P.has_special)
                                         e |= special_class(P, i0 + ii, j) << 30;
                                     if (wpos < cap)
@@ -471,8 +421,7 @@ __global__ void __launch_bounds__(256)
                             const float dy = (float)(int)((unsigned)qi.y - (unsigned)qj.y) * sy;
                             const float dz = (float)(int)((unsigned)qi.z - (unsigned)qj.z) * sz;
                             const float r2f = dx * dx + dy * dy + dz * dz;
-                            const bool valid =
-                                live && (half ? (seg != 0 || j > i0 + ii) : j != i0 + ii);
+                            const bool valid = live && j != i0 + ii;
                             bool hit = valid && r2f < blo;
                             const bool amb = valid && !(r2f < blo) && r2f < bhi;
                             if (__any_sync(full, amb)) {
@@ -484,7 +433,7 @@ __global__ void __launch_bounds__(256)
                                 const int base = __shfl_sync(full, cnt, ii);
                                 if (hit) {
                                     const int wpos = base + __popc(m & lt);
-                                    unsigned e = half ? ((unsigned)j | eseg) : (unsigned)j;
+                                    unsigned e = (unsigned)j;
                                     if (P.has_special)
                                         e |= special_class(P, i0 + ii, j) << 30;
                                     if (wpos < cap)

@@ -60,6 +60,7 @@ ATVB_DEV void pair_term(const RowConst<T>& c, T dx, T dy, T dz, T qj,
         // damped by erfc(alpha rc) (~3e-5 eV/A per pair at alpha rc = 3),
         // so a flipped Coulomb pair moves the forces by ~1e-7 relative
         near = LJ && fabsf(r2 - c.lj_rc2) < c.band_lj;
+        a.rmin = fminf(a.rmin, r2);
         if (force >= 0) {
             in_lj = force & 1;
             in_c = (force >> 1) & 1;
@@ -272,6 +273,8 @@ ATVB_DEV void row_mixed(const SysParams& P, int s, int g, int G, PairAcc& acc) {
     }
     if (NEAR && n_near)
         queue_near(P, s, g | (G << 6));
+    if (a.rmin < (float)P.force_r2_safe) // rare: a pair force may exceed the fixed point
+        atomicOr(&P.st->status, kStatusForceRange);
     finish_row(a, acc, VIR);
 }
 

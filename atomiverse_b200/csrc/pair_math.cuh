@@ -144,6 +144,9 @@ struct RowSums {
     // kForceFix^-1 eV/A (range +-2e9 eV/A), so the row sum is exact and
     // independent of summation order
     long long fq[3] = {0, 0, 0};
+    // mixed build: the row's smallest r^2 (a pair closer than
+    // SysParams::force_r2_safe may carry a force beyond the fixed point)
+    T rmin = T(1e30);
 };
 constexpr float kForceFix = 4294967296.0f;  // 2^32
 constexpr double kForceFixInv = 1.0 / 4294967296.0;

@@ -163,3 +163,23 @@ def test_step_timed_runs_in_pieces_like_step(atvb, ctx):
     for k in ("x", "y", "z", "vx", "vy", "vz"):
         assert np.array_equal(oa[k], ob[k])
     assert sa["step"] == sb["step"] == 1200
+
+
+def test_force_beyond_fixed_point_is_flagged(atvb, ctx):
+    # mixed LJ: two atoms 0.05 sigma apart carry a pair force far beyond the
+    # range of the 64-bit fixed-point row sums (2^31 eV/A)
+    desc, frame = W.lj_fcc(ncell=6, seed=4, precision=1)
+    frame = {k: (v.copy() if hasattr(v, "copy") else v) for k, v in frame.items()}
+    frame["x"][1], frame["y"][1], frame["z"][1] = frame["x"][0] + 0.05, frame["y"][0], frame["z"][0]
+    s = atvb.System(ctx, desc, frame)
+    s.compute_forces()
+    sc = s.scalars(check=False)
+    assert sc["status_bits"] & 16
+    with pytest.raises(atvb.PhysicsError):
+        s.scalars()
+    # the same system without the overlap raises nothing
+    desc2, frame2 = W.lj_fcc(ncell=6, seed=4, precision=1)
+    s2 = atvb.System(ctx, desc2, frame2)
+    s2.compute_forces()
+    s2.step(5)
+    assert s2.scalars()["status_bits"] == 0
