@@ -1,0 +1,486 @@
+// fft.cu -- the PME grid transforms, hand-written: a 3D real-to-complex
+// FFT, the influence function, and the complex-to-real inverse, in five
+// passes over the grid.
+//
+// The reference transforms with FFTW (src/cpu/longrange/pme.cpp:105-108,
+// 203-210) or cuFFT (src/cuda/longrange/pme.cu:293,330,334), unnormalised
+// in both directions, between its spread and its gather.  The same
+// transform here, on the half-complex grid K0 x K1 x (K2/2 + 1) (index
+// m2 + Kh (m1 + K1 m0)), with the stages of the PME step folded in:
+//   1. z forward (one block per line group): the 64-bit fixed-point charge
+//      grid read, converted and cleared, real-to-complex along z;
+//   2. y forward: complex FFT along y (tiles of a few m2 columns, loaded
+//      coalesced and transposed into shared memory);
+//   3. x forward, the influence function H(m) with the reciprocal energy
+//      and virial (pme_influence.h:159-199), x inverse: one kernel;
+//   4. y inverse;
+//   5. z inverse, complex-to-real into the real grid the gather reads.
+// Each line is transformed in shared memory by a mixed-radix Stockham
+// (self-sorting) FFT with radices 4, 2, 3, 5, 7 -- every PME mesh size is
+// 2,3,5,7-smooth (good_fft_size, pme_spline.h:99-111) -- and twiddles from
+// a per-axis table of the K-th roots of unity computed on the host.  Real
+// lines of even length go through the half-length complex FFT with the
+// standard even/odd split; odd lengths through the full complex one.
+#include "atvb_common.cuh"
+#include "atvb_kernels.cuh"
+#include "pair_math.cuh"
+
+namespace atvb {
+
+template <typename T>
+struct Cplx;
+template <>
+struct Cplx<double> {
+    using type = double2;
+};
+template <>
+struct Cplx<float> {
+    using type = float2;
+};
+
+template <typename T2>
+ATVB_DEV T2 cmul(T2 a, T2 b) {
+    T2 r;
+    r.x = a.x * b.x - a.y * b.y;
+    r.y = a.x * b.y + a.y * b.x;
+    return r;
+}
+template <typename T2>
+ATVB_DEV T2 cadd(T2 a, T2 b) {
+    T2 r;
+    r.x = a.x + b.x;
+    r.y = a.y + b.y;
+    return r;
+}
+template <typename T2>
+ATVB_DEV T2 csub(T2 a, T2 b) {
+    T2 r;
+    r.x = a.x - b.x;
+    r.y = a.y - b.y;
+    return r;
+}
+template <typename T2>
+ATVB_DEV T2 cconj(T2 a) {
+    a.y = -a.y;
+    return a;
+}
+// a times -i (forward) or +i (inverse)
+template <typename T2>
+ATVB_DEV T2 cmul_mi(T2 a, bool inv) {
+    T2 r;
+    r.x = inv ? -a.y : a.y;
+    r.y = inv ? a.x : -a.x;
+    return r;
+}
+
+// cos and sin of 2 pi k / p for the generic radices (mathematical constants)
+__device__ const double kCos5[5] = {1.0, 0.30901699437494745, -0.8090169943749475,
+                                   -0.8090169943749475, 0.30901699437494745};
+__device__ const double kSin5[5] = {0.0, 0.9510565162951535, 0.5877852522924731,
+                                   -0.5877852522924731, -0.9510565162951535};
+__device__ const double kCos7[7] = {1.0, 0.6234898018587336, -0.22252093395631434,
+                                   -0.900968867902419, -0.900968867902419,
+                                   -0.22252093395631434, 0.6234898018587336};
+__device__ const double kSin7[7] = {0.0, 0.7818314824680298, 0.9749279121818236,
+                                   0.43388373911755823, -0.43388373911755823,
+                                   -0.9749279121818236, -0.7818314824680298};
+
+// In-place p-point DFT of x[0..p) (sign -1 forward, +1 inverse).
+template <typename T, typename T2>
+ATVB_DEV void small_dft(T2* x, int p, bool inv) {
+    if (p == 2) {
+        const T2 a = x[0], b = x[1];
+        x[0] = cadd(a, b);
+        x[1] = csub(a, b);
+    } else if (p == 4) {
+        const T2 a = cadd(x[0], x[2]), b = csub(x[0], x[2]);
+        const T2 c = cadd(x[1], x[3]), d = cmul_mi(csub(x[1], x[3]), inv);
+        x[0] = cadd(a, c);
+        x[2] = csub(a, c);
+        x[1] = cadd(b, d);
+        x[3] = csub(b, d);
+    } else if (p == 3) {
+        const T s3 = (T)0.8660254037844386; // sqrt(3) / 2
+        const T2 s = cadd(x[1], x[2]);
+        const T2 d = cmul_mi(csub(x[1], x[2]), inv);
+        T2 m;
+        m.x = x[0].x - (T)0.5 * s.x;
+        m.y = x[0].y - (T)0.5 * s.y;
+        x[0] = cadd(x[0], s);
+        T2 e;
+        e.x = s3 * d.x;
+        e.y = s3 * d.y;
+        x[1] = cadd(m, e);
+        x[2] = csub(m, e);
+    } else {
+        // 5 or 7: the direct sum with the constant roots
+        const double* cs = p == 5 ? kCos5 : kCos7;
+        const double* sn = p == 5 ? kSin5 : kSin7;
+        T2 y[7];
+        for (int u = 0; u < p; ++u) {
+            T2 acc = x[0];
+            for (int t = 1; t < p; ++t) {
+                const int k = (u * t) % p;
+                T2 w;
+                w.x = (T)cs[k];
+                w.y = inv ? (T)sn[k] : -(T)sn[k];
+                acc = cadd(acc, cmul(x[t], w));
+            }
+            y[u] = acc;
+        }
+        for (int u = 0; u < p; ++u)
+            x[u] = y[u];
+    }
+}
+
+// One transform of `nlines` lines of length n held in shared memory (line l
+// at a + l * ls), by the whole block: Stockham stages, ping-ponging between
+// a and b.  roots: the table of e^{-2 pi i j / (n rs)}, read with stride rs.
+// Returns the buffer that holds the result.
+template <typename T, typename T2>
+ATVB_DEV T2* fft_lines(T2* a, T2* b, int nlines, int n, int ls, const int* fac, int nf,
+                       const T2* __restrict__ roots, int rs, bool inv) {
+    int Tsz = 1;
+    for (int f = 0; f < nf; ++f) {
+        const int p = fac[f];
+        const int m = n / p;
+        const int step = n / (p * Tsz); // root index step per t * k
+        const int nb = nlines * m;
+        for (int bi = threadIdx.x; bi < nb; bi += blockDim.x) {
+            const int line = bi / m, i = bi - line * m;
+            const T2* src = a + line * ls;
+            T2* dst = b + line * ls;
+            const int k = i % Tsz;
+            T2 x[7];
+            x[0] = src[i];
+            for (int t = 1; t < p; ++t) {
+                T2 w = roots[rs * (t * k * step)];
+                if (inv)
+                    w = cconj(w);
+                x[t] = cmul(src[i + t * m], w);
+            }
+            small_dft<T, T2>(x, p, inv);
+            const int j = (i - k) * p + k;
+            for (int u = 0; u < p; ++u)
+                dst[j + u * Tsz] = x[u];
+        }
+        __syncthreads();
+        T2* t = a;
+        a = b;
+        b = t;
+        Tsz *= p;
+    }
+    return a;
+}
+
+// Line length (with padding against bank conflicts) of a transform of n.
+ATVB_DEV int line_stride(int n) { return n + 1; }
+
+// ---- pass 1: z forward, from the fixed-point charge grid -----------------
+template <bool MIXED>
+__global__ void __launch_bounds__(kFftBlock)
+    k_fft_zf(const Item* items, int nitems, const SysParams* sp, int C) {
+    using T = typename std::conditional<MIXED, float, double>::type;
+    using T2 = typename Cplx<T>::type;
+    extern __shared__ unsigned char fsh_raw[];
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const Item item = items[it];
+        const SysParams& P = sp[item.sys];
+        if (!P.has_pme || P.prec != (MIXED ? kMixed : kFP64))
+            continue;
+        const int K0 = P.K[0], K1 = P.K[1], K2 = P.K[2], Kh = P.Kh;
+        const bool even = (K2 & 1) == 0;
+        const int n = even ? K2 / 2 : K2, ls = line_stride(n);
+        const int l0 = item.begin, nl = min(C, K0 * K1 - l0);
+        T2* a = reinterpret_cast<T2*>(fsh_raw);
+        T2* b = a + C * ls;
+        const T gs = (T)P.grid_scale_inv;
+        for (int q = threadIdx.x; q < nl * K2; q += blockDim.x) {
+            const int c = q / K2, z = q - c * K2;
+            const size_t gi = (size_t)(l0 + c) * K2 + z;
+            const long long v = (long long)P.grid_fix[gi];
+            P.grid_fix[gi] = 0ull; // ready for the next spread
+            const T x = (T)((double)v * P.grid_scale_inv);
+            (void)gs;
+            if (even) {
+                T* re = reinterpret_cast<T*>(a + c * ls);
+                re[z] = x; // x[2n], x[2n+1] interleave as z[n] = x[2n] + i x[2n+1]
+            } else {
+                T2 v2;
+                v2.x = x;
+                v2.y = (T)0;
+                a[c * ls + z] = v2;
+            }
+        }
+        __syncthreads();
+        const T2* roots = reinterpret_cast<const T2*>(P.fft_root[2]);
+        T2* r = fft_lines<T, T2>(a, b, nl, n, ls, P.fft_fac[2], P.fft_nf[2], roots,
+                                 even ? 2 : 1, false);
+        T2* __restrict__ out = reinterpret_cast<T2*>(P.grid_cplx);
+        for (int q = threadIdx.x; q < nl * Kh; q += blockDim.x) {
+            const int c = q / Kh, k = q - c * Kh;
+            T2 X;
+            if (even) {
+                // X[k] = E + e^{-2 pi i k / K2} O, E/O the spectra of the
+                // even / odd samples, from Z[k] and conj(Z[n - k])
+                const T2 Zk = r[c * ls + (k % n)];
+                const T2 Zc = cconj(r[c * ls + ((n - k) % n)]);
+                T2 E, O;
+                E.x = (T)0.5 * (Zk.x + Zc.x);
+                E.y = (T)0.5 * (Zk.y + Zc.y);
+                O.x = (T)0.5 * (Zk.y - Zc.y);
+                O.y = -(T)0.5 * (Zk.x - Zc.x);
+                X = cadd(E, cmul(O, roots[k]));
+            } else {
+                X = r[c * ls + k];
+            }
+            out[(size_t)(l0 + c) * Kh + k] = X;
+        }
+        __syncthreads();
+    }
+}
+
+// ---- passes 2 and 4: y forward / inverse ---------------------------------
+template <bool MIXED, bool INV>
+__global__ void __launch_bounds__(kFftBlock)
+    k_fft_y(const Item* items, int nitems, const SysParams* sp, int C) {
+    using T = typename std::conditional<MIXED, float, double>::type;
+    using T2 = typename Cplx<T>::type;
+    extern __shared__ unsigned char fsh_raw[];
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const Item item = items[it];
+        const SysParams& P = sp[item.sys];
+        if (!P.has_pme || P.prec != (MIXED ? kMixed : kFP64))
+            continue;
+        const int K1 = P.K[1], Kh = P.Kh;
+        const int nb2 = (Kh + C - 1) / C;
+        const int k0 = item.begin / nb2, m2a = (item.begin - k0 * nb2) * C;
+        const int nc = min(C, Kh - m2a);
+        const int ls = line_stride(K1);
+        T2* a = reinterpret_cast<T2*>(fsh_raw);
+        T2* b = a + C * ls;
+        T2* __restrict__ g = reinterpret_cast<T2*>(P.grid_cplx) + (size_t)k0 * K1 * Kh + m2a;
+        for (int q = threadIdx.x; q < K1 * nc; q += blockDim.x) {
+            const int k1 = q / nc, c = q - k1 * nc;
+            a[c * ls + k1] = g[(size_t)k1 * Kh + c];
+        }
+        __syncthreads();
+        T2* r = fft_lines<T, T2>(a, b, nc, K1, ls, P.fft_fac[1], P.fft_nf[1],
+                                 reinterpret_cast<const T2*>(P.fft_root[1]), 1, INV);
+        for (int q = threadIdx.x; q < K1 * nc; q += blockDim.x) {
+            const int k1 = q / nc, c = q - k1 * nc;
+            g[(size_t)k1 * Kh + c] = r[c * ls + k1];
+        }
+        __syncthreads();
+    }
+}
+
+// ---- pass 3: x forward, influence with energy and virial, x inverse ------
+template <bool MIXED>
+__global__ void __launch_bounds__(kFftBlock)
+    k_fft_x_infl(const Item* items, int nitems, const SysParams* sp, int C) {
+    using T = typename std::conditional<MIXED, float, double>::type;
+    using T2 = typename Cplx<T>::type;
+    extern __shared__ unsigned char fsh_raw[];
+    __shared__ double sh[32 * 7];
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const Item item = items[it];
+        const SysParams& P = sp[item.sys];
+        if (!P.has_pme || P.prec != (MIXED ? kMixed : kFP64))
+            continue;
+        const int K0 = P.K[0], K1 = P.K[1], K2 = P.K[2], Kh = P.Kh;
+        const int nb2 = (Kh + C - 1) / C;
+        const int m1 = item.begin / nb2, m2a = (item.begin - m1 * nb2) * C;
+        const int nc = min(C, Kh - m2a);
+        const int ls = line_stride(K0);
+        const size_t sx = (size_t)K1 * Kh; // stride along x
+        T2* a = reinterpret_cast<T2*>(fsh_raw);
+        T2* b = a + C * ls;
+        T2* __restrict__ g = reinterpret_cast<T2*>(P.grid_cplx) + (size_t)m1 * Kh + m2a;
+        for (int q = threadIdx.x; q < K0 * nc; q += blockDim.x) {
+            const int k0 = q / nc, c = q - k0 * nc;
+            a[c * ls + k0] = g[(size_t)k0 * sx + c];
+        }
+        __syncthreads();
+        const T2* roots = reinterpret_cast<const T2*>(P.fft_root[0]);
+        T2* r = fft_lines<T, T2>(a, b, nc, K0, ls, P.fft_fac[0], P.fft_nf[0], roots, 1, false);
+        // H(m) = exp(-pi^2 m^2 / alpha^2) / m^2 * B(m) (zero mode cleared,
+        // pme_influence.h:112-155) from the current cell; energy and virial
+        // with the half-grid weights (modes 0 < m2 < K2/2 stand for two)
+        const bool vir = P.need_virial;
+        double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+        const int h1 = m1 <= K1 / 2 ? m1 : m1 - K1;
+        const double my = h1 * P.invL[1];
+        for (int q = threadIdx.x; q < K0 * nc; q += blockDim.x) {
+            const int c = q / K0, m0 = q - c * K0;
+            const int m2 = m2a + c;
+            const int h0 = m0 <= K0 / 2 ? m0 : m0 - K0;
+            const int h2 = m2 <= K2 / 2 ? m2 : m2 - K2;
+            const double mx = h0 * P.invL[0], mz = h2 * P.invL[2];
+            const double msq = mx * mx + my * my + mz * mz;
+            const bool zero = m0 == 0 && m1 == 0 && m2 == 0;
+            const double imsq = zero ? 0.0 : rcp64(msq);
+            const double H = zero ? 0.0
+                                  : exp_neg64(P.pme_alpha2_pi2 * msq) * imsq *
+                                        (P.bmod[m0] * P.bmod[K0 + m1]) * P.bmod[K0 + K1 + m2];
+            T2 Qm = r[c * ls + m0];
+            const double re = (double)Qm.x, im = (double)Qm.y;
+            const double w = (m2 == 0 || 2 * m2 == K2) ? 1.0 : 2.0;
+            const double ug = w * H * (re * re + im * im);
+            acc[0] += ug;
+            if (vir && H != 0.0) {
+                const double vt = -2.0 * (imsq + P.pme_alpha2_pi2);
+                acc[1] += ug * (1.0 + vt * mx * mx);
+                acc[2] += ug * (1.0 + vt * my * my);
+                acc[3] += ug * (1.0 + vt * mz * mz);
+                acc[4] += ug * (vt * mx * my);
+                acc[5] += ug * (vt * mx * mz);
+                acc[6] += ug * (vt * my * mz);
+            }
+            Qm.x = (T)(H * re);
+            Qm.y = (T)(H * im);
+            r[c * ls + m0] = Qm;
+        }
+        __syncthreads();
+        T2* o = r == a ? b : a;
+        T2* r2 = fft_lines<T, T2>(r, o, nc, K0, ls, P.fft_fac[0], P.fft_nf[0], roots, 1, true);
+        for (int q = threadIdx.x; q < K0 * nc; q += blockDim.x) {
+            const int k0 = q / nc, c = q - k0 * nc;
+            g[(size_t)k0 * sx + c] = r2[c * ls + k0];
+        }
+        // per-item fixed-point flush (independent of batch composition)
+        if (vir) {
+            block_sum_vec<7>(acc, sh);
+            if (threadIdx.x == 0) {
+                fix_add(&P.st->acc[kAccERecip], acc[0] * P.pme_escale);
+                for (int k = 0; k < 6; ++k)
+                    fix_add(&P.st->acc[kAccVir + k], acc[1 + k] * P.pme_escale);
+            }
+        } else {
+            double e1[1] = {acc[0]};
+            block_sum_vec<1>(e1, sh);
+            if (threadIdx.x == 0)
+                fix_add(&P.st->acc[kAccERecip], e1[0] * P.pme_escale);
+        }
+        __syncthreads();
+    }
+}
+
+// ---- pass 5: z inverse, complex-to-real into the real grid ---------------
+template <bool MIXED>
+__global__ void __launch_bounds__(kFftBlock)
+    k_fft_zi(const Item* items, int nitems, const SysParams* sp, int C) {
+    using T = typename std::conditional<MIXED, float, double>::type;
+    using T2 = typename Cplx<T>::type;
+    extern __shared__ unsigned char fsh_raw[];
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const Item item = items[it];
+        const SysParams& P = sp[item.sys];
+        if (!P.has_pme || P.prec != (MIXED ? kMixed : kFP64))
+            continue;
+        const int K0 = P.K[0], K1 = P.K[1], K2 = P.K[2], Kh = P.Kh;
+        const bool even = (K2 & 1) == 0;
+        const int n = even ? K2 / 2 : K2, ls = line_stride(n);
+        const int l0 = item.begin, nl = min(C, K0 * K1 - l0);
+        T2* a = reinterpret_cast<T2*>(fsh_raw);
+        T2* b = a + C * ls;
+        const T2* roots = reinterpret_cast<const T2*>(P.fft_root[2]);
+        const T2* __restrict__ in = reinterpret_cast<const T2*>(P.grid_cplx);
+        if (even) {
+            // Z'[k] = (X[k] + conj X[n-k]) + i (X[k] - conj X[n-k]) e^{2 pi i k / K2}
+            for (int q = threadIdx.x; q < nl * n; q += blockDim.x) {
+                const int c = q / n, k = q - c * n;
+                const size_t row = (size_t)(l0 + c) * Kh;
+                const T2 Xk = in[row + k];
+                const T2 Xc = cconj(in[row + (n - k)]);
+                const T2 E = cadd(Xk, Xc);
+                const T2 O = cmul(csub(Xk, Xc), cconj(roots[k]));
+                T2 Z;
+                Z.x = E.x - O.y;
+                Z.y = E.y + O.x;
+                a[c * ls + k] = Z;
+            }
+        } else {
+            // the full Hermitian spectrum
+            for (int q = threadIdx.x; q < nl * K2; q += blockDim.x) {
+                const int c = q / K2, k = q - c * K2;
+                const size_t row = (size_t)(l0 + c) * Kh;
+                a[c * ls + k] = k < Kh ? in[row + k] : cconj(in[row + (K2 - k)]);
+            }
+        }
+        __syncthreads();
+        T2* r = fft_lines<T, T2>(a, b, nl, n, ls, P.fft_fac[2], P.fft_nf[2], roots,
+                                 even ? 2 : 1, true);
+        T* __restrict__ out = reinterpret_cast<T*>(P.grid_real);
+        for (int q = threadIdx.x; q < nl * K2; q += blockDim.x) {
+            const int c = q / K2, z = q - c * K2;
+            T v;
+            if (even) {
+                const T2 zz = r[c * ls + (z >> 1)];
+                v = (z & 1) ? zz.y : zz.x;
+            } else {
+                v = r[c * ls + z].x;
+            }
+            out[(size_t)(l0 + c) * K2 + z] = v;
+        }
+        __syncthreads();
+    }
+}
+
+static size_t fft_smem(int C, int n, bool mixed) {
+    return (size_t)2 * C * (n + 1) * (mixed ? sizeof(float2) : sizeof(double2));
+}
+
+template <bool MIXED>
+static void fft_all(const LaunchCfg& lc, cudaStream_t s) {
+    const FftCfg& f = lc.fft;
+    if (f.z.n) {
+        k_fft_zf<MIXED><<<f.z.grid, kFftBlock, fft_smem(f.cz, f.nz, MIXED), s>>>(f.z.d, f.z.n,
+                                                                              lc.sp, f.cz);
+        k_fft_y<MIXED, false><<<f.y.grid, kFftBlock, fft_smem(f.cy, f.ny, MIXED), s>>>(
+            f.y.d, f.y.n, lc.sp, f.cy);
+        k_fft_x_infl<MIXED><<<f.x.grid, kFftBlock, fft_smem(f.cx, f.nx, MIXED), s>>>(
+            f.x.d, f.x.n, lc.sp, f.cx);
+        k_fft_y<MIXED, true><<<f.y.grid, kFftBlock, fft_smem(f.cy, f.ny, MIXED), s>>>(
+            f.y.d, f.y.n, lc.sp, f.cy);
+        k_fft_zi<MIXED><<<f.z.grid, kFftBlock, fft_smem(f.cz, f.nz, MIXED), s>>>(f.z.d, f.z.n,
+                                                                              lc.sp, f.cz);
+    }
+}
+
+void launch_pme_fft(const LaunchCfg& lc, cudaStream_t s) {
+    if (lc.pme_mixed)
+        fft_all<true>(lc, s);
+    else
+        fft_all<false>(lc, s);
+}
+
+// The most dynamic shared memory an FFT launch may ask for, opted in once
+// per device (outside any stream capture).
+void fft_smem_optin(int bytes) {
+    auto set = [&](const void* f) {
+        cuda_check(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
+                   "cudaFuncSetAttribute(fft)");
+    };
+    set((const void*)k_fft_zf<false>);
+    set((const void*)k_fft_zf<true>);
+    set((const void*)k_fft_y<false, false>);
+    set((const void*)k_fft_y<false, true>);
+    set((const void*)k_fft_y<true, false>);
+    set((const void*)k_fft_y<true, true>);
+    set((const void*)k_fft_x_infl<false>);
+    set((const void*)k_fft_x_infl<true>);
+    set((const void*)k_fft_zi<false>);
+    set((const void*)k_fft_zi<true>);
+}
+
+// Lines per block for a transform of length n: as many as fit kFftSmem
+// bytes of shared memory (two buffers), at most kFftMaxLines.
+int fft_lines_per_block(int n, bool mixed) {
+    const size_t per = fft_smem(1, n, mixed);
+    int C = (int)(kFftSmem / per);
+    C = C > kFftMaxLines ? kFftMaxLines : C;
+    return C < 1 ? 1 : C;
+}
+
+} // namespace atvb

@@ -60,7 +60,8 @@ ATVB_DEV void pair_term(const RowConst<T>& c, T dx, T dy, T dz, T qj,
         // damped by erfc(alpha rc) (~3e-5 eV/A per pair at alpha rc = 3),
         // so a flipped Coulomb pair moves the forces by ~1e-7 relative
         near = LJ && fabsf(r2 - c.lj_rc2) < c.band_lj;
-        a.rmin = fminf(a.rmin, r2);
+        // (entries past a row's end are the atom itself, r^2 = 0: not pairs)
+        a.rmin = ok ? fminf(a.rmin, r2) : a.rmin;
         if (force >= 0) {
             in_lj = force & 1;
             in_c = (force >> 1) & 1;
