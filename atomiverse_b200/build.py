@@ -1,7 +1,7 @@
 """Build libatvb.so (every CUDA source under csrc/) for sm_100a, in-tree.
 
-nvcc cross-compiles without a GPU.  The library links cuFFT from the CUDA
-toolkit and the static CUDA runtime.
+nvcc cross-compiles without a GPU.  The library links the static CUDA
+runtime and no other CUDA library (the PME transforms are its own).
 """
 from __future__ import annotations
 
@@ -55,7 +55,7 @@ def build(verbose: bool = False, extra: list[str] | None = None) -> str:
             if r.returncode != 0:
                 raise RuntimeError("nvcc failed: " + " ".join(cmd))
     if jobs or not os.path.exists(LIB) or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):
-        cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcufft",
+        cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs,
                "-Xlinker", "-rpath=" + os.path.join(CUDA_HOME, "lib64")]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:

@@ -29,6 +29,8 @@ enum Thermostat : int { kNVE = 0, kNoseHoover = 1, kLangevin = 2, kNPT = 3 };
 
 // longest Nose-Hoover chain of the MTK NPT integrator
 constexpr int kMaxChain = 10;
+// most radices of one PME mesh axis (4, 2, 3, 5, 7)
+constexpr int kFftMaxFac = 16;
 
 // SysState::status bits (sticky; the ATVB_STATUS_* values of atvb.h)
 constexpr int kStatusRowOverflow = ATVB_STATUS_ROW_OVERFLOW; // a step ran on cut rows
@@ -172,6 +174,13 @@ struct SysParams {
     double pme_alpha2_pi2; // pi^2 / alpha^2
     double grid_scale, grid_scale_inv; // fixed-point charge scale
     const double* bmod;    // B-spline moduli |b(m)|^2 per axis: K0 + K1 + K2
+    // the hand-written transforms (fft.cu): per axis the radices of the
+    // complex FFT (z: of K2 / 2 when K2 is even, the real-to-complex split)
+    // and the table of the K-th roots of unity e^{-2 pi i j / K}, j < K
+    // (double2, float2 in the mixed build)
+    int fft_nf[3];
+    int fft_fac[3][kFftMaxFac];
+    const void* fft_root[3];
     double pme_alpha, pme_eself, pme_qsum2; // e_const = eself - k_e pi qsum2 / (2 V alpha^2)
     // integrator / thermostat
     double dt, dtf; // dtf = dt/2 * ftm2v

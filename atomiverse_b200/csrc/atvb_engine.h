@@ -1,8 +1,6 @@
 // atvb_engine.h -- host-side engine: systems (slots), work lists, graph.
 #pragma once
 
-#include <cufft.h>
-
 #include <map>
 #include <memory>
 #include <stdexcept>
@@ -161,20 +159,7 @@ class Engine {
     }
 
   private:
-    // cuFFT plans of one grid shape: one pair per stream lane (the FFTs of
-    // several systems run concurrently on kFftLanes forked streams; lane
-    // kFftLanes is the engine's own stream, used when one system transforms)
-    static constexpr int kFftLanes = 8;
-    struct FftPlans {
-        cufftHandle f[kFftLanes + 1] = {}, i[kFftLanes + 1] = {};
-        int refs = 0;
-        uint64_t last_use = 0;
-    };
-    void acquire_plans(Slot& s);
-    void release_plans(Slot& s);
-    FftPlans& shape_plans(const Slot& s);
-    void ensure_lane_plan(const Slot& s, int lane);
-    void exec_fft(const std::vector<int>& pme, bool forward, cudaStream_t base);
+    FftCfg fft_items(const std::vector<int>& pme);
     void ensure_table();
     void push_params(int id);
     void build_lists();
@@ -199,14 +184,8 @@ class Engine {
     int device_ = 0;
     cudaStream_t stream_ = nullptr;
     DevMem mem_;
-    // cuFFT plans by {K0, K1, K2, precision}, shared by every system of that
-    // grid (their FFTs run one after another on the engine's stream) and kept
-    // after the last user leaves, up to kPlanCacheIdle idle shapes
-    std::map<std::vector<int>, FftPlans> plans_;
-    uint64_t plan_clock_ = 0;
-    cudaStream_t fft_streams_[kFftLanes] = {};
-    cudaEvent_t fft_fork_ = nullptr, fft_join_[kFftLanes] = {};
-    cudaEvent_t pme_fork_ = nullptr, pme_join_ = nullptr; // PME beside the pair kernel
+    cudaStream_t pme_stream_ = nullptr; // the PME chain beside the pair kernel
+    cudaEvent_t pme_fork_ = nullptr, pme_join_ = nullptr;
     bool any_npt_ = false; // an MTK NPT system exists (re-plan check per step call)
     int num_sms_ = 148;
     std::vector<std::unique_ptr<Slot>> slots_;

@@ -19,6 +19,19 @@ struct ItemList {
     int grid = 0;            // blocks to launch (persistent loop covers n)
 };
 
+// The PME transforms of a launch (fft.cu): items of the z passes (first
+// line of a group), the y passes (k0 x column block) and the x pass
+// (m1 x column block); lines per block and the longest line, for the
+// shared-memory size.
+constexpr int kFftBlock = 256;          // threads per FFT block
+constexpr int kFftSmem = 96 * 1024;     // shared memory an FFT block may use
+constexpr int kFftMaxLines = 16;        // lines per FFT block
+struct FftCfg {
+    ItemList z, y, x;
+    int cz = 1, cy = 1, cx = 1;
+    int nz = 0, ny = 0, nx = 0;
+};
+
 struct LaunchCfg {
     const SysParams* sp = nullptr; // device table of every system
     ItemList atoms;     // kChunk atoms per item (original or sorted order)
@@ -40,6 +53,7 @@ struct LaunchCfg {
     int any_snap = 0;   // a system publishes trajectory snapshots
     int any_baro = 0;   // a system runs the Berendsen barostat (k_baro_scale)
     int any_near = 0;   // a mixed system settles near-cutoff LJ pairs (k_pair_fix)
+    FftCfg fft;         // the PME grid transforms
     int pme_order = 4;  // common PME order (the PME kernels are templated)
     int pme_mixed = 0;
 };
@@ -53,11 +67,15 @@ void launch_pair(const LaunchCfg& lc, cudaStream_t s);
 void launch_pair_fix(const LaunchCfg& lc, cudaStream_t s);
 // pair_general.cu
 void launch_pair_general(const LaunchCfg& lc, cudaStream_t s);
+void cuda_check(cudaError_t e, const char* what); // engine.cu: throws on error
+
 // pme.cu
 void launch_pme_spread(const LaunchCfg& lc, cudaStream_t s);
-void launch_pme_convert(const LaunchCfg& lc, cudaStream_t s);
-void launch_pme_influence(const LaunchCfg& lc, cudaStream_t s);
 void launch_pme_gather(const LaunchCfg& lc, cudaStream_t s);
+// fft.cu
+void launch_pme_fft(const LaunchCfg& lc, cudaStream_t s);
+void fft_smem_optin(int bytes);
+int fft_lines_per_block(int n, bool mixed);
 // integrate.cu
 void launch_integrate_a(const LaunchCfg& lc, cudaStream_t s);
 void launch_sys_a(const LaunchCfg& lc, cudaStream_t s);

@@ -9,7 +9,6 @@
 // host synchronisation.  An Engine holds any number of systems; the
 // single-system API is an Engine with one slot, the batch API an Engine
 // with many, and the server an Engine whose slots come and go.
-#include <cufft.h>
 
 #include <algorithm>
 #include <atomic>
@@ -38,13 +37,6 @@ void cuda_check(cudaError_t e, const char* what) {
                                        cudaGetErrorString(e));
 }
 #define CK(x) cuda_check((x), #x)
-
-static void cufft_check(cufftResult r, const char* what) {
-    if (r != CUFFT_SUCCESS)
-        throw Error(ATVB_ERR_CUDA,
-                    std::string(what) + ": cuFFT error " + std::to_string(r));
-}
-#define CKF(x) cufft_check((x), #x)
 
 // ---------------------------------------------------------------- helpers
 
@@ -243,7 +235,7 @@ size_t estimate_bytes(const atvb_system_desc& d) {
         const size_t nt = K0 * K1 * K2, nh = K0 * K1 * (K2 / 2 + 1);
         const size_t rs = d.precision == ATVB_MIXED ? 4 : 8;
         b += nt * 8 + nt * rs + nh * 2 * rs + (K0 + K1 + K2) * 8;
-        b += 2 * nh * 2 * rs; // cuFFT work areas (upper estimate)
+        b += (K0 + K1 + K2) * 2 * rs; // roots of unity of the transforms
     }
     return b;
 }
@@ -564,6 +556,42 @@ Slot::Slot(const atvb_system_desc& d, const DevMem& mem) : desc(d), mem_(mem) {
         double* dbm = dd(bm.size());
         CK(cudaMemcpyAsync(dbm, bm.data(), bm.size() * 8, cudaMemcpyHostToDevice, stream));
         hp.bmod = dbm;
+        // the transforms (fft.cu): radices per axis (z: the complex FFT of
+        // K2 / 2 when K2 is even) and the K-th roots of unity per axis
+        for (int k = 0; k < 3; ++k) {
+            const int K = hp.K[k];
+            int m = (k == 2 && K % 2 == 0) ? K / 2 : K;
+            int nf = 0;
+            for (int p : {4, 2, 3, 5, 7})
+                while (m % p == 0 && nf < kFftMaxFac) {
+                    hp.fft_fac[k][nf++] = p;
+                    m /= p;
+                }
+            if (m != 1)
+                throw Error(ATVB_ERR_INVALID, "KSpacePME: a mesh size must be 2,3,5,7-smooth "
+                                              "(good_fft_size), got " + std::to_string(K));
+            hp.fft_nf[k] = nf;
+            std::vector<double> rt(2 * (size_t)K);
+            for (int j = 0; j < K; ++j) {
+                const long double a = -2.0L * 3.14159265358979323846264338327950288L * j / K;
+                rt[2 * j] = (double)cosl(a);
+                rt[2 * j + 1] = (double)sinl(a);
+            }
+            if (hp.prec == kMixed) {
+                std::vector<float> rf(rt.begin(), rt.end());
+                void* d = dalloc(rf.size() * sizeof(float));
+                CK(cudaMemcpyAsync(d, rf.data(), rf.size() * sizeof(float),
+                                   cudaMemcpyHostToDevice, stream));
+                hp.fft_root[k] = d;
+                CK(cudaStreamSynchronize(stream)); // rf is a local
+            } else {
+                void* d = dalloc(rt.size() * sizeof(double));
+                CK(cudaMemcpyAsync(d, rt.data(), rt.size() * sizeof(double),
+                                   cudaMemcpyHostToDevice, stream));
+                hp.fft_root[k] = d;
+                CK(cudaStreamSynchronize(stream));
+            }
+        }
         CK(cudaStreamSynchronize(stream));
     }
     apply_box(hp, geo.L, false);
@@ -591,129 +619,11 @@ Engine::Engine(int device) : device_(device) {
     // waiting for the whole pair grid
     int prio_lo = 0, prio_hi = 0;
     CK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
-    for (int l = 0; l < kFftLanes; ++l) {
-        CK(cudaStreamCreateWithPriority(&fft_streams_[l], cudaStreamNonBlocking, prio_hi));
-        CK(cudaEventCreateWithFlags(&fft_join_[l], cudaEventDisableTiming));
-    }
-    CK(cudaEventCreateWithFlags(&fft_fork_, cudaEventDisableTiming));
+    CK(cudaStreamCreateWithPriority(&pme_stream_, cudaStreamNonBlocking, prio_hi));
     CK(cudaEventCreateWithFlags(&pme_fork_, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&pme_join_, cudaEventDisableTiming));
-}
-
-constexpr int kPlanCacheIdle = 16;
-
-static std::vector<int> shape_key(const Slot& s) {
-    return {s.hp.K[0], s.hp.K[1], s.hp.K[2], s.hp.prec == kMixed ? 1 : 0};
-}
-
-void Engine::acquire_plans(Slot& s) {
-    if (!s.hp.has_pme)
-        return;
-    FftPlans& p = plans_[shape_key(s)];
-    ++p.refs;
-    p.last_use = ++plan_clock_;
-}
-
-Engine::FftPlans& Engine::shape_plans(const Slot& s) {
-    return plans_[shape_key(s)];
-}
-
-// Creates (outside any stream capture) the plan pair of a shape for a lane.
-void Engine::ensure_lane_plan(const Slot& s, int lane) {
-    FftPlans& p = shape_plans(s);
-    if (p.f[lane])
-        return;
-    const std::vector<int> key = shape_key(s);
-    const bool mixed = key[3] == 1;
-    cufftHandle f = 0, i = 0;
-    CKF(cufftPlan3d(&f, key[0], key[1], key[2], mixed ? CUFFT_R2C : CUFFT_D2Z));
-    if (cufftPlan3d(&i, key[0], key[1], key[2], mixed ? CUFFT_C2R : CUFFT_Z2D) !=
-        CUFFT_SUCCESS) {
-        cufftDestroy(f);
-        throw Error(ATVB_ERR_CUDA, "cufftPlan3d failed");
-    }
-    cudaStream_t st = lane == kFftLanes ? stream_ : fft_streams_[lane];
-    cufftSetStream(f, st);
-    cufftSetStream(i, st);
-    p.f[lane] = f;
-    p.i[lane] = i;
-}
-
-void Engine::release_plans(Slot& s) {
-    if (!s.hp.has_pme)
-        return;
-    auto it = plans_.find(shape_key(s));
-    if (it != plans_.end() && it->second.refs > 0)
-        --it->second.refs;
-    // evict the least recently used idle shapes beyond the cache size
-    for (;;) {
-        int idle = 0;
-        auto lru = plans_.end();
-        for (auto j = plans_.begin(); j != plans_.end(); ++j)
-            if (j->second.refs == 0) {
-                ++idle;
-                if (lru == plans_.end() || j->second.last_use < lru->second.last_use)
-                    lru = j;
-            }
-        if (idle <= kPlanCacheIdle || lru == plans_.end())
-            break;
-        release_graph();
-        cudaStreamSynchronize(stream_);
-        for (int l = 0; l <= kFftLanes; ++l) {
-            if (lru->second.f[l])
-                cufftDestroy(lru->second.f[l]);
-            if (lru->second.i[l])
-                cufftDestroy(lru->second.i[l]);
-        }
-        plans_.erase(lru);
-    }
-}
-
-// The forward or inverse FFT of every system in `pme`.  One system: on the
-// engine stream.  Several: forked over the kFftLanes streams (system k of
-// the list on lane k mod kFftLanes, each lane with its own plans) and joined
-// back, so small transforms run side by side; inside a captured step the
-// fork and join become parallel branches of the graph.  Every system keeps
-// its own single-grid plan, so its numbers do not depend on the others.
-void Engine::exec_fft(const std::vector<int>& pme, bool forward, cudaStream_t base) {
-    auto run = [&](const Slot& sl, int lane) {
-        const FftPlans& p = plans_.at(shape_key(sl));
-        const bool mixed = sl.hp.prec == kMixed;
-        if (forward) {
-            if (mixed)
-                CKF(cufftExecR2C(p.f[lane], (cufftReal*)sl.hp.grid_real,
-                                 (cufftComplex*)sl.hp.grid_cplx));
-            else
-                CKF(cufftExecD2Z(p.f[lane], (cufftDoubleReal*)sl.hp.grid_real,
-                                 (cufftDoubleComplex*)sl.hp.grid_cplx));
-        } else {
-            if (mixed)
-                CKF(cufftExecC2R(p.i[lane], (cufftComplex*)sl.hp.grid_cplx,
-                                 (cufftReal*)sl.hp.grid_real));
-            else
-                CKF(cufftExecZ2D(p.i[lane], (cufftDoubleComplex*)sl.hp.grid_cplx,
-                                 (cufftDoubleReal*)sl.hp.grid_real));
-        }
-    };
-    // base: the engine stream, or lane 0 when the PME chain runs beside the
-    // pair kernel (its plans are bound to that lane)
-    if (pme.size() == 1) {
-        run(*slots_[pme[0]], base == stream_ ? kFftLanes : 0);
-        return;
-    }
-    const int used = (int)std::min<size_t>(pme.size(), kFftLanes);
-    CK(cudaEventRecord(fft_fork_, base));
-    for (int l = 0; l < used; ++l)
-        if (fft_streams_[l] != base)
-            CK(cudaStreamWaitEvent(fft_streams_[l], fft_fork_, 0));
-    for (size_t q = 0; q < pme.size(); ++q)
-        run(*slots_[pme[q]], (int)(q % kFftLanes));
-    for (int l = 0; l < used; ++l) {
-        if (fft_streams_[l] == base)
-            continue;
-        CK(cudaEventRecord(fft_join_[l], fft_streams_[l]));
-        CK(cudaStreamWaitEvent(base, fft_join_[l], 0));
-    }
+    // the FFT blocks' line buffers live in dynamic shared memory above 48 KB
+    fft_smem_optin(kFftSmem);
 }
 
 Engine::~Engine() {
@@ -726,21 +636,8 @@ Engine::~Engine() {
     cudaStreamSynchronize(stream_);
     if (row_hint_host_)
         cudaFreeHost(row_hint_host_);
-    for (auto& kv : plans_)
-        for (int l = 0; l <= kFftLanes; ++l) {
-            if (kv.second.f[l])
-                cufftDestroy(kv.second.f[l]);
-            if (kv.second.i[l])
-                cufftDestroy(kv.second.i[l]);
-        }
-    for (int l = 0; l < kFftLanes; ++l) {
-        if (fft_streams_[l])
-            cudaStreamDestroy(fft_streams_[l]);
-        if (fft_join_[l])
-            cudaEventDestroy(fft_join_[l]);
-    }
-    if (fft_fork_)
-        cudaEventDestroy(fft_fork_);
+    if (pme_stream_)
+        cudaStreamDestroy(pme_stream_);
     if (pme_fork_)
         cudaEventDestroy(pme_fork_);
     if (pme_join_)
@@ -765,7 +662,6 @@ void Engine::release_graph() {
 int Engine::add(const atvb_system_desc& d) {
     CK(cudaSetDevice(device_));
     auto s = std::make_unique<Slot>(d, mem_);
-    acquire_plans(*s);
     int id = -1;
     for (size_t k = 0; k < slots_.size(); ++k)
         if (!slots_[k]) {
@@ -789,7 +685,6 @@ int Engine::add(const atvb_system_desc& d) {
 void Engine::remove(int id) {
     Slot* s = slot(id);
     release_graph(); // the captured step references this system's memory
-    release_plans(*s);
     slots_[id].reset(); // stream-ordered frees: no wait for the device
     dirty_ = true;
 }
@@ -936,7 +831,7 @@ void Engine::build_lists() {
     for (void* p : list_allocs_)
         mem_.free(p);
     list_allocs_.clear();
-    std::vector<Item> atoms, list, cells, patoms, pgrid, preal;
+    std::vector<Item> atoms, list, cells, patoms;
     std::vector<int> sys;
     std::vector<Item> pair_by[2][kLaneClasses];
     std::vector<Item> pair_gen[2];
@@ -990,12 +885,6 @@ void Engine::build_lists() {
             pme_slots_.push_back(k);
             for (int b = 0; b < P.n; b += kChunk)
                 patoms.push_back({k, b});
-            const long long nh = (long long)P.K[0] * P.K[1] * P.Kh;
-            const long long nt = (long long)P.K[0] * P.K[1] * P.K[2];
-            for (long long b = 0; b < nh; b += kGridChunk)
-                pgrid.push_back({k, (int)b});
-            for (long long b = 0; b < nt; b += kGridChunk)
-                preal.push_back({k, (int)b});
         }
     }
     const int g_light = num_sms_ * 16;
@@ -1009,8 +898,6 @@ void Engine::build_lists() {
         lc_.pair_gen[p] = make_list(list_allocs_, pair_gen[p], num_sms_ * 16, mem_);
     lc_.cells = make_list(list_allocs_, cells, g_light, mem_);
     lc_.pme_atoms = make_list(list_allocs_, patoms, g_light, mem_);
-    lc_.pme_grid = make_list(list_allocs_, pgrid, g_light, mem_);
-    lc_.pme_real = make_list(list_allocs_, preal, g_light, mem_);
     lc_.nsys = (int)sys.size();
     if (!sys.empty()) {
         void* p = mem_.alloc(sizeof(int) * sys.size());
@@ -1019,14 +906,7 @@ void Engine::build_lists() {
                            cudaMemcpyHostToDevice, stream_));
         lc_.sys_list = (const int*)p;
     }
-    // plans for this work list, made now (plan creation cannot be captured):
-    // lane q mod kFftLanes for the step, the engine-stream lane for passes
-    // over one system
-    for (size_t q = 0; q < pme_slots_.size(); ++q) {
-        const Slot& sl = *slots_[pme_slots_[q]];
-        ensure_lane_plan(sl, kFftLanes);
-        ensure_lane_plan(sl, (int)(q % kFftLanes));
-    }
+    lc_.fft = fft_items(pme_slots_);
     lc_.pme_mixed = pme_prec == kMixed ? 1 : 0;
     lc_.pme_order = pme_order > 0 ? pme_order : 4;
     CK(cudaStreamSynchronize(stream_));
@@ -1036,7 +916,43 @@ void Engine::build_lists() {
     single_.clear();
 }
 
-// Kernel launches of one step (cuFFT's own kernels not counted).
+// The PME transforms' work items over the systems in `pme` (fft.cu): lines
+// per block from the longest line of each pass, then the z items (groups of
+// x-y lines), the y items (k0 x a block of m2 columns) and the x items (m1 x
+// a block of columns).
+FftCfg Engine::fft_items(const std::vector<int>& pme) {
+    FftCfg f;
+    if (pme.empty())
+        return f;
+    const bool mixed = slots_[pme[0]]->hp.prec == kMixed;
+    for (int id : pme) {
+        const SysParams& P = slots_[id]->hp;
+        f.nz = std::max(f.nz, (P.K[2] % 2 == 0) ? P.K[2] / 2 : P.K[2]);
+        f.ny = std::max(f.ny, P.K[1]);
+        f.nx = std::max(f.nx, P.K[0]);
+    }
+    f.cz = fft_lines_per_block(f.nz, mixed);
+    f.cy = fft_lines_per_block(f.ny, mixed);
+    f.cx = fft_lines_per_block(f.nx, mixed);
+    std::vector<Item> z, y, x;
+    for (int id : pme) {
+        const SysParams& P = slots_[id]->hp;
+        for (int l = 0; l < P.K[0] * P.K[1]; l += f.cz)
+            z.push_back({id, l});
+        const int by = (P.Kh + f.cy - 1) / f.cy, bx = (P.Kh + f.cx - 1) / f.cx;
+        for (int q = 0; q < P.K[0] * by; ++q)
+            y.push_back({id, q});
+        for (int q = 0; q < P.K[1] * bx; ++q)
+            x.push_back({id, q});
+    }
+    const int g = num_sms_ * 8;
+    f.z = make_list(list_allocs_, z, g, mem_);
+    f.y = make_list(list_allocs_, y, g, mem_);
+    f.x = make_list(list_allocs_, x, g, mem_);
+    return f;
+}
+
+// Kernel launches of one step.
 int64_t Engine::kernels_per_step() const {
     int64_t k = 0;
     k += 2;                                   // integrate_a, sys_a
@@ -1047,7 +963,7 @@ int64_t Engine::kernels_per_step() const {
     k += lc_.any_near ? 1 : 0;                // near-cutoff fix-up (mixed LJ)
     k += (lc_.pair_gen[0].n ? 1 : 0) + (lc_.pair_gen[1].n ? 1 : 0); // general pair
     if (!pme_slots_.empty())
-        k += 4;                               // spread, convert, influence, gather
+        k += 7;                               // spread, 5 transform passes, gather
     k += 2;                                   // integrate_b, sys_b
     k += lc_.any_snap ? 3 : 0;                // trajectory snapshots
     k += lc_.any_baro ? 1 : 0;                // Berendsen position scaling
@@ -1062,7 +978,7 @@ int64_t Engine::kernels_per_step() const {
 void Engine::enqueue_forces(const LaunchCfg& lc, const std::vector<int>& pme,
                             bool profile, bool overlap, bool build_list) {
     const bool side = overlap && !profile && !pme.empty();
-    cudaStream_t ps = side ? fft_streams_[0] : stream_;
+    cudaStream_t ps = side ? pme_stream_ : stream_;
     if (side) {
         CK(cudaEventRecord(pme_fork_, stream_));
         CK(cudaStreamWaitEvent(ps, pme_fork_, 0));
@@ -1076,14 +992,8 @@ void Engine::enqueue_forces(const LaunchCfg& lc, const std::vector<int>& pme,
     if (!pme.empty()) {
         prof_mark(profile, "pme_spread");
         launch_pme_spread(lc, ps);
-        prof_mark(profile, "pme_convert");
-        launch_pme_convert(lc, ps);
-        prof_mark(profile, "pme_fft_fwd");
-        exec_fft(pme, true, ps);
-        prof_mark(profile, "pme_influence");
-        launch_pme_influence(lc, ps);
-        prof_mark(profile, "pme_fft_inv");
-        exec_fft(pme, false, ps);
+        prof_mark(profile, "pme_fft");
+        launch_pme_fft(lc, ps); // convert, transforms, influence, inverse
         prof_mark(profile, "pme_gather");
         launch_pme_gather(lc, ps);
     }
@@ -1428,7 +1338,7 @@ LaunchCfg Engine::restricted_cfg(int id) {
         return it->second.second;
     Slot* s = slot(id);
     const SysParams& P = s->hp;
-    std::vector<Item> atoms, list, cells, pair, patoms, pgrid, preal;
+    std::vector<Item> atoms, list, cells, pair, patoms;
     for (int b = 0; b < P.n; b += kChunk)
         atoms.push_back({id, b});
     for (int b = 0; b < P.ncell; b += kListChunk)
@@ -1438,16 +1348,9 @@ LaunchCfg Engine::restricted_cfg(int id) {
     const int pchunk = kPairBlock / (P.general ? kGenLanes : s->lanes);
     for (int b = 0; b < P.n; b += pchunk)
         pair.push_back({id, b});
-    if (P.has_pme) {
+    if (P.has_pme)
         for (int b = 0; b < P.n; b += kChunk)
             patoms.push_back({id, b});
-        const long long nh = (long long)P.K[0] * P.K[1] * P.Kh;
-        const long long nt = (long long)P.K[0] * P.K[1] * P.K[2];
-        for (long long b = 0; b < nh; b += kGridChunk)
-            pgrid.push_back({id, (int)b});
-        for (long long b = 0; b < nt; b += kGridChunk)
-            preal.push_back({id, (int)b});
-    }
     LaunchCfg c = lc_;
     c.sp = d_sp_;
     c.atoms = make_list(list_allocs_, atoms, num_sms_ * 16, mem_);
@@ -1464,8 +1367,7 @@ LaunchCfg Engine::restricted_cfg(int id) {
         c.pair[P.prec == kMixed ? 1 : 0][lane_class(s->lanes)] =
             make_list(list_allocs_, pair, num_sms_ * 16, mem_);
     c.pme_atoms = make_list(list_allocs_, patoms, num_sms_ * 16, mem_);
-    c.pme_grid = make_list(list_allocs_, pgrid, num_sms_ * 16, mem_);
-    c.pme_real = make_list(list_allocs_, preal, num_sms_ * 16, mem_);
+    c.fft = fft_items(P.has_pme ? std::vector<int>{id} : std::vector<int>{});
     c.any_mixed = P.prec == kMixed;
     c.any_fp64 = P.prec != kMixed;
     c.any_near = P.prec == kMixed && P.has_lj && !P.general && P.mix_band_lj > 0.0;
@@ -2457,9 +2359,7 @@ void Engine::replan_npt() {
         const double ba[3] = {old->baro_args[0], old->baro_args[1], old->baro_args[2]};
         CK(cudaStreamSynchronize(stream_));
         release_graph();
-        release_plans(*old);
         up = std::move(s);
-        acquire_plans(*up);
         push_params(id);
         if (was_npt)
             set_npt(id, npt);

@@ -85,21 +85,23 @@ __device__ const double kSin7[7] = {0.0, 0.7818314824680298, 0.9749279121818236,
                                    0.43388373911755823, -0.43388373911755823,
                                    -0.9749279121818236, -0.7818314824680298};
 
-// In-place p-point DFT of x[0..p) (sign -1 forward, +1 inverse).
-template <typename T, typename T2>
-ATVB_DEV void small_dft(T2* x, int p, bool inv) {
-    if (p == 2) {
+// In-place P-point DFT of x[0..P) (sign -1 forward, +1 inverse); P is a
+// compile-time constant, so x stays in registers.
+template <typename T, typename T2, int P>
+ATVB_DEV void small_dft(T2 (&x)[P], bool inv) {
+    constexpr int p = P;
+    if constexpr (P == 2) {
         const T2 a = x[0], b = x[1];
         x[0] = cadd(a, b);
         x[1] = csub(a, b);
-    } else if (p == 4) {
+    } else if constexpr (P == 4) {
         const T2 a = cadd(x[0], x[2]), b = csub(x[0], x[2]);
         const T2 c = cadd(x[1], x[3]), d = cmul_mi(csub(x[1], x[3]), inv);
         x[0] = cadd(a, c);
         x[2] = csub(a, c);
         x[1] = cadd(b, d);
         x[3] = csub(b, d);
-    } else if (p == 3) {
+    } else if constexpr (P == 3) {
         const T s3 = (T)0.8660254037844386; // sqrt(3) / 2
         const T2 s = cadd(x[1], x[2]);
         const T2 d = cmul_mi(csub(x[1], x[2]), inv);
@@ -116,9 +118,11 @@ ATVB_DEV void small_dft(T2* x, int p, bool inv) {
         // 5 or 7: the direct sum with the constant roots
         const double* cs = p == 5 ? kCos5 : kCos7;
         const double* sn = p == 5 ? kSin5 : kSin7;
-        T2 y[7];
+        T2 y[P];
+#pragma unroll
         for (int u = 0; u < p; ++u) {
             T2 acc = x[0];
+#pragma unroll
             for (int t = 1; t < p; ++t) {
                 const int k = (u * t) % p;
                 T2 w;
@@ -128,8 +132,40 @@ ATVB_DEV void small_dft(T2* x, int p, bool inv) {
             }
             y[u] = acc;
         }
+#pragma unroll
         for (int u = 0; u < p; ++u)
             x[u] = y[u];
+    }
+}
+
+// One radix-P Stockham stage of every line: butterfly i of a line reads
+// x_t = src[i + t m] (m = n / P), twiddles it by w^(t k) (k = i mod T, w
+// the (P T)-th root), transforms, and writes dst[(i - k) P + k + u T].
+template <typename T, typename T2, int P>
+ATVB_DEV void fft_stage(const T2* a, T2* b, int nlines, int n, int ls, int Tsz,
+                        const T2* __restrict__ roots, int rs, bool inv) {
+    const int m = n / P;
+    const int step = n / (P * Tsz); // root index step per t * k
+    const int nb = nlines * m;
+    for (int bi = threadIdx.x; bi < nb; bi += blockDim.x) {
+        const int line = bi / m, i = bi - line * m;
+        const T2* src = a + line * ls;
+        T2* dst = b + line * ls;
+        const int k = i % Tsz;
+        T2 x[P];
+        x[0] = src[i];
+#pragma unroll
+        for (int t = 1; t < P; ++t) {
+            T2 w = roots[rs * (t * k * step)];
+            if (inv)
+                w = cconj(w);
+            x[t] = cmul(src[i + t * m], w);
+        }
+        small_dft<T, T2, P>(x, inv);
+        const int j = (i - k) * P + k;
+#pragma unroll
+        for (int u = 0; u < P; ++u)
+            dst[j + u * Tsz] = x[u];
     }
 }
 
@@ -143,26 +179,12 @@ ATVB_DEV T2* fft_lines(T2* a, T2* b, int nlines, int n, int ls, const int* fac, 
     int Tsz = 1;
     for (int f = 0; f < nf; ++f) {
         const int p = fac[f];
-        const int m = n / p;
-        const int step = n / (p * Tsz); // root index step per t * k
-        const int nb = nlines * m;
-        for (int bi = threadIdx.x; bi < nb; bi += blockDim.x) {
-            const int line = bi / m, i = bi - line * m;
-            const T2* src = a + line * ls;
-            T2* dst = b + line * ls;
-            const int k = i % Tsz;
-            T2 x[7];
-            x[0] = src[i];
-            for (int t = 1; t < p; ++t) {
-                T2 w = roots[rs * (t * k * step)];
-                if (inv)
-                    w = cconj(w);
-                x[t] = cmul(src[i + t * m], w);
-            }
-            small_dft<T, T2>(x, p, inv);
-            const int j = (i - k) * p + k;
-            for (int u = 0; u < p; ++u)
-                dst[j + u * Tsz] = x[u];
+        switch (p) {
+        case 4: fft_stage<T, T2, 4>(a, b, nlines, n, ls, Tsz, roots, rs, inv); break;
+        case 2: fft_stage<T, T2, 2>(a, b, nlines, n, ls, Tsz, roots, rs, inv); break;
+        case 3: fft_stage<T, T2, 3>(a, b, nlines, n, ls, Tsz, roots, rs, inv); break;
+        case 5: fft_stage<T, T2, 5>(a, b, nlines, n, ls, Tsz, roots, rs, inv); break;
+        default: fft_stage<T, T2, 7>(a, b, nlines, n, ls, Tsz, roots, rs, inv); break;
         }
         __syncthreads();
         T2* t = a;
@@ -194,14 +216,12 @@ __global__ void __launch_bounds__(kFftBlock)
         const int l0 = item.begin, nl = min(C, K0 * K1 - l0);
         T2* a = reinterpret_cast<T2*>(fsh_raw);
         T2* b = a + C * ls;
-        const T gs = (T)P.grid_scale_inv;
         for (int q = threadIdx.x; q < nl * K2; q += blockDim.x) {
             const int c = q / K2, z = q - c * K2;
             const size_t gi = (size_t)(l0 + c) * K2 + z;
             const long long v = (long long)P.grid_fix[gi];
             P.grid_fix[gi] = 0ull; // ready for the next spread
             const T x = (T)((double)v * P.grid_scale_inv);
-            (void)gs;
             if (even) {
                 T* re = reinterpret_cast<T*>(a + c * ls);
                 re[z] = x; // x[2n], x[2n+1] interleave as z[n] = x[2n] + i x[2n+1]

@@ -1,4 +1,5 @@
-// pme.cu -- smooth-PME reciprocal sum: spread, influence, gather.
+// pme.cu -- smooth-PME reciprocal sum: B-spline spread and force gather
+// (the transforms and the influence function are in fft.cu).
 //
 // Math follows the reference's header-only PME
 // (include/atomiverse/cpu/longrange/pme_spline.h:32-58 B-spline recursion,
@@ -8,8 +9,11 @@
 // pme.cpp:152-253 driver).  Differences of layout, not of math:
 //  * the charge grid is accumulated in 64-bit fixed point, so the spread is
 //    order-independent and bit-reproducible;
-//  * the transforms are real-to-complex / complex-to-real on the half grid
-//    (K0 x K1 x (K2/2+1)); the half-grid energy and virial weight every
+//  * the transforms (fft.cu, hand-written) are real-to-complex /
+//    complex-to-real on the half grid (K0 x K1 x (K2/2+1)), with the
+//    conversion of the fixed-point grid folded into the first pass and the
+//    influence function (in fft.cu's x pass) between the forward
+//    and inverse x transforms; the half-grid energy and virial weight every
 //    mode with 0 < m2 < K2/2 twice;
 //  * H(m) is evaluated on the fly from the per-axis B-spline moduli and the
 //    current cell (no 3D table: a changing NPT cell needs no rebuild), and
@@ -149,99 +153,6 @@ __global__ void __launch_bounds__(256)
     }
 }
 
-// fixed-point grid -> real grid for the transform; clears the fixed grid
-template <bool MIXED>
-__global__ void k_pme_convert(const Item* items, int nitems,
-                              const SysParams* sp) {
-    using T = typename std::conditional<MIXED, float, double>::type;
-    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
-        const Item item = items[it];
-        const SysParams& P = sp[item.sys];
-        if (P.prec != (MIXED ? kMixed : kFP64))
-            continue;
-        const size_t ntot = (size_t)P.K[0] * P.K[1] * P.K[2];
-        T* __restrict__ out = reinterpret_cast<T*>(P.grid_real);
-        for (int k = threadIdx.x; k < kGridChunk; k += blockDim.x) {
-            const size_t i = (size_t)item.begin + k;
-            if (i >= ntot)
-                break;
-            const long long v = (long long)P.grid_fix[i];
-            out[i] = (T)((double)v * P.grid_scale_inv);
-            P.grid_fix[i] = 0ull;
-        }
-    }
-}
-
-// pme_influence.h:159-199 on the half-complex grid
-template <bool MIXED>
-__global__ void __launch_bounds__(256)
-    k_pme_influence(const Item* items, int nitems, const SysParams* sp) {
-    using T2 = typename std::conditional<MIXED, float2, double2>::type;
-    __shared__ double sh[32 * 7];
-    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
-        const Item item = items[it];
-        const SysParams& P = sp[item.sys];
-        if (P.prec != (MIXED ? kMixed : kFP64))
-            continue;
-        const int K0 = P.K[0], K1 = P.K[1], K2 = P.K[2], Kh = P.Kh;
-        const size_t nh = (size_t)K0 * K1 * Kh;
-        T2* __restrict__ grid = reinterpret_cast<T2*>(P.grid_cplx);
-        const bool vir = P.need_virial;
-        double acc[7] = {0, 0, 0, 0, 0, 0, 0};
-        for (int k = threadIdx.x; k < kGridChunk; k += blockDim.x) {
-            const size_t idx = (size_t)item.begin + k;
-            if (idx >= nh)
-                break;
-            T2 Qm = grid[idx];
-            const double re = (double)Qm.x, im = (double)Qm.y;
-            // half grids stay below 2^31 points: 32-bit index arithmetic
-            const unsigned ui = (unsigned)idx, ur = ui / (unsigned)Kh;
-            const int m2 = (int)(ui - ur * (unsigned)Kh);
-            const int m1 = (int)(ur % (unsigned)K1), m0 = (int)(ur / (unsigned)K1);
-            const int h0 = m0 <= K0 / 2 ? m0 : m0 - K0;
-            const int h1 = m1 <= K1 / 2 ? m1 : m1 - K1;
-            const int h2 = m2 <= K2 / 2 ? m2 : m2 - K2;
-            const double mx = h0 * P.invL[0], my = h1 * P.invL[1], mz = h2 * P.invL[2];
-            const double msq = mx * mx + my * my + mz * mz;
-            // H(m) = exp(-pi^2 m^2 / alpha^2) / m^2 * B(m), zero mode
-            // cleared (pme_influence.h:112-155), from the current cell
-            const double imsq = idx == 0 ? 0.0 : rcp64(msq);
-            const double H = idx == 0 ? 0.0
-                                      : exp_neg64(P.pme_alpha2_pi2 * msq) * imsq *
-                                            (P.bmod[m0] * P.bmod[K0 + m1]) * P.bmod[K0 + K1 + m2];
-            const double w = (m2 == 0 || 2 * m2 == K2) ? 1.0 : 2.0;
-            const double ug = w * H * (re * re + im * im);
-            acc[0] += ug;
-            if (vir && H != 0.0) {
-                const double vt = -2.0 * (imsq + P.pme_alpha2_pi2);
-                acc[1] += ug * (1.0 + vt * mx * mx);
-                acc[2] += ug * (1.0 + vt * my * my);
-                acc[3] += ug * (1.0 + vt * mz * mz);
-                acc[4] += ug * (vt * mx * my);
-                acc[5] += ug * (vt * mx * mz);
-                acc[6] += ug * (vt * my * mz);
-            }
-            Qm.x = (decltype(Qm.x))(H * re);
-            Qm.y = (decltype(Qm.y))(H * im);
-            grid[idx] = Qm;
-        }
-        // per-item fixed-point flush (independent of batch composition)
-        if (vir) {
-            block_sum_vec<7>(acc, sh);
-            if (threadIdx.x == 0) {
-                fix_add(&P.st->acc[kAccERecip], acc[0] * P.pme_escale);
-                for (int k = 0; k < 6; ++k)
-                    fix_add(&P.st->acc[kAccVir + k], acc[1 + k] * P.pme_escale);
-            }
-        } else {
-            double e1[1] = {acc[0]};
-            block_sum_vec<1>(e1, sh);
-            if (threadIdx.x == 0)
-                fix_add(&P.st->acc[kAccERecip], e1[0] * P.pme_escale);
-        }
-    }
-}
-
 // pme_influence.h:217-280 (orthorhombic: inv_cell is diagonal)
 template <bool MIXED, int N>
 __global__ void __launch_bounds__(256)
@@ -328,22 +239,6 @@ void launch_pme_spread(const LaunchCfg& lc, cudaStream_t s) {
         spread_order<true>(lc, s);
     else
         spread_order<false>(lc, s);
-}
-
-void launch_pme_convert(const LaunchCfg& lc, cudaStream_t s) {
-    const ItemList& il = lc.pme_real;
-    if (lc.pme_mixed)
-        k_pme_convert<true><<<il.grid, 256, 0, s>>>(il.d, il.n, lc.sp);
-    else
-        k_pme_convert<false><<<il.grid, 256, 0, s>>>(il.d, il.n, lc.sp);
-}
-
-void launch_pme_influence(const LaunchCfg& lc, cudaStream_t s) {
-    const ItemList& il = lc.pme_grid;
-    if (lc.pme_mixed)
-        k_pme_influence<true><<<il.grid, 256, 0, s>>>(il.d, il.n, lc.sp);
-    else
-        k_pme_influence<false><<<il.grid, 256, 0, s>>>(il.d, il.n, lc.sp);
 }
 
 void launch_pme_gather(const LaunchCfg& lc, cudaStream_t s) {
