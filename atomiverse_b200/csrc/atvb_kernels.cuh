@@ -24,12 +24,13 @@ struct ItemList {
 // (m1 x column block); lines per block and the longest line, for the
 // shared-memory size.
 constexpr int kFftBlock = 256;          // threads per FFT block
-constexpr int kFftSmem = 96 * 1024;     // shared memory an FFT block may use
+constexpr int kFftSmem = 56 * 1024;     // shared memory an FFT block may use
 constexpr int kFftMaxLines = 16;        // lines per FFT block
 struct FftCfg {
     ItemList z, y, x;
     int cz = 1, cy = 1, cx = 1;
     int nz = 0, ny = 0, nx = 0;
+    int kz = 0; // longest root table of the z passes (K2; the line is K2/2 when even)
 };
 
 struct LaunchCfg {
@@ -75,7 +76,7 @@ void launch_pme_gather(const LaunchCfg& lc, cudaStream_t s);
 // fft.cu
 void launch_pme_fft(const LaunchCfg& lc, cudaStream_t s);
 void fft_smem_optin(int bytes);
-int fft_lines_per_block(int n, bool mixed);
+int fft_lines_per_block(int n, int K, bool mixed);
 // integrate.cu
 void launch_integrate_a(const LaunchCfg& lc, cudaStream_t s);
 void launch_sys_a(const LaunchCfg& lc, cudaStream_t s);

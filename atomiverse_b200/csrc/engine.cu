@@ -570,6 +570,9 @@ Slot::Slot(const atvb_system_desc& d, const DevMem& mem) : desc(d), mem_(mem) {
             if (m != 1)
                 throw Error(ATVB_ERR_INVALID, "KSpacePME: a mesh size must be 2,3,5,7-smooth "
                                               "(good_fft_size), got " + std::to_string(K));
+            if (K > 2048) // a line and its roots must fit one block's shared memory
+                throw Error(ATVB_ERR_INVALID, "KSpacePME: at most 2048 mesh points per axis, got " +
+                                                  std::to_string(K));
             hp.fft_nf[k] = nf;
             std::vector<double> rt(2 * (size_t)K);
             for (int j = 0; j < K; ++j) {
@@ -623,7 +626,7 @@ Engine::Engine(int device) : device_(device) {
     CK(cudaEventCreateWithFlags(&pme_fork_, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&pme_join_, cudaEventDisableTiming));
     // the FFT blocks' line buffers live in dynamic shared memory above 48 KB
-    fft_smem_optin(kFftSmem);
+    fft_smem_optin(kFftSmem + 1024);
 }
 
 Engine::~Engine() {
@@ -928,12 +931,13 @@ FftCfg Engine::fft_items(const std::vector<int>& pme) {
     for (int id : pme) {
         const SysParams& P = slots_[id]->hp;
         f.nz = std::max(f.nz, (P.K[2] % 2 == 0) ? P.K[2] / 2 : P.K[2]);
+        f.kz = std::max(f.kz, P.K[2]);
         f.ny = std::max(f.ny, P.K[1]);
         f.nx = std::max(f.nx, P.K[0]);
     }
-    f.cz = fft_lines_per_block(f.nz, mixed);
-    f.cy = fft_lines_per_block(f.ny, mixed);
-    f.cx = fft_lines_per_block(f.nx, mixed);
+    f.cz = fft_lines_per_block(f.nz, f.kz, mixed);
+    f.cy = fft_lines_per_block(f.ny, f.ny, mixed);
+    f.cx = fft_lines_per_block(f.nx, f.nx, mixed);
     std::vector<Item> z, y, x;
     for (int id : pme) {
         const SysParams& P = slots_[id]->hp;

@@ -138,41 +138,67 @@ ATVB_DEV void small_dft(T2 (&x)[P], bool inv) {
     }
 }
 
+// A walk over the cells of a rows x cols grid by the threads of a block,
+// q = threadIdx.x, threadIdx.x + blockDim.x, ...: row and column kept up to
+// date by additions (one division at the start, none per step).
+struct Walk2 {
+    int r, c, dr, dc, cols;
+    ATVB_DEV Walk2(int q0, int cols_, int stride) : cols(cols_) {
+        r = q0 / cols;
+        c = q0 - r * cols;
+        dr = stride / cols;
+        dc = stride - dr * cols;
+    }
+    ATVB_DEV void next() {
+        c += dc;
+        r += dr;
+        if (c >= cols) {
+            c -= cols;
+            ++r;
+        }
+    }
+};
+
 // One radix-P Stockham stage of every line: butterfly i of a line reads
 // x_t = src[i + t m] (m = n / P), twiddles it by w^(t k) (k = i mod T, w
 // the (P T)-th root), transforms, and writes dst[(i - k) P + k + u T].
+// T divides m, so k follows i by additions as the walk wraps.
 template <typename T, typename T2, int P>
-ATVB_DEV void fft_stage(const T2* a, T2* b, int nlines, int n, int ls, int Tsz,
-                        const T2* __restrict__ roots, int rs, bool inv) {
+ATVB_DEV void fft_stage(const T2* __restrict__ a, T2* __restrict__ b, int nlines, int n, int ls,
+                        int Tsz, const T2* __restrict__ roots, int rs, bool inv) {
     const int m = n / P;
-    const int step = n / (P * Tsz); // root index step per t * k
-    const int nb = nlines * m;
-    for (int bi = threadIdx.x; bi < nb; bi += blockDim.x) {
-        const int line = bi / m, i = bi - line * m;
-        const T2* src = a + line * ls;
-        T2* dst = b + line * ls;
-        const int k = i % Tsz;
+    const int step = rs * (n / (P * Tsz)); // root index per t * k
+    Walk2 w(threadIdx.x, m, blockDim.x);
+    int k = w.c % Tsz;
+    const int dk = w.dc % Tsz;
+    for (; w.r < nlines; w.next()) {
+        const int i = w.c;
+        const T2* src = a + w.r * ls;
+        T2* dst = b + w.r * ls;
         T2 x[P];
         x[0] = src[i];
 #pragma unroll
         for (int t = 1; t < P; ++t) {
-            T2 w = roots[rs * (t * k * step)];
+            T2 tw = roots[t * k * step];
             if (inv)
-                w = cconj(w);
-            x[t] = cmul(src[i + t * m], w);
+                tw = cconj(tw);
+            x[t] = cmul(src[i + t * m], tw);
         }
         small_dft<T, T2, P>(x, inv);
         const int j = (i - k) * P + k;
 #pragma unroll
         for (int u = 0; u < P; ++u)
             dst[j + u * Tsz] = x[u];
+        k += dk;
+        k -= k >= Tsz ? Tsz : 0;
     }
 }
 
 // One transform of `nlines` lines of length n held in shared memory (line l
 // at a + l * ls), by the whole block: Stockham stages, ping-ponging between
-// a and b.  roots: the table of e^{-2 pi i j / (n rs)}, read with stride rs.
-// Returns the buffer that holds the result.
+// a and b.  fac: the radices (shared memory); roots: the table of
+// e^{-2 pi i j / (n rs)}, read with stride rs.  Returns the buffer that
+// holds the result.
 template <typename T, typename T2>
 ATVB_DEV T2* fft_lines(T2* a, T2* b, int nlines, int n, int ls, const int* fac, int nf,
                        const T2* __restrict__ roots, int rs, bool inv) {
@@ -198,13 +224,33 @@ ATVB_DEV T2* fft_lines(T2* a, T2* b, int nlines, int n, int ls, const int* fac, 
 // Line length (with padding against bank conflicts) of a transform of n.
 ATVB_DEV int line_stride(int n) { return n + 1; }
 
+// The roots of unity of one axis (K entries) into shared memory after the
+// two line buffers; visible after the block's next barrier.
+template <typename T2>
+ATVB_DEV T2* stage_roots(T2* base, const T2* __restrict__ roots, int K) {
+    for (int j = threadIdx.x; j < K; j += blockDim.x)
+        base[j] = roots[j];
+    return base;
+}
+
+// The radices of one axis into shared memory (read by every stage).
+ATVB_DEV void load_fac(const SysParams& P, int axis, int* s_fac, int& nf) {
+    nf = P.fft_nf[axis];
+    if (threadIdx.x < kFftMaxFac)
+        s_fac[threadIdx.x] = P.fft_fac[axis][threadIdx.x];
+}
+
 // ---- pass 1: z forward, from the fixed-point charge grid -----------------
+// Every SysParams field a loop needs is read into a register first: the
+// loops write through pointers the compiler cannot prove apart from the
+// parameter table.
 template <bool MIXED>
-__global__ void __launch_bounds__(kFftBlock)
+__global__ void __launch_bounds__(kFftBlock, 3)
     k_fft_zf(const Item* items, int nitems, const SysParams* sp, int C) {
     using T = typename std::conditional<MIXED, float, double>::type;
     using T2 = typename Cplx<T>::type;
     extern __shared__ unsigned char fsh_raw[];
+    __shared__ int s_fac[kFftMaxFac];
     for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
         const Item item = items[it];
         const SysParams& P = sp[item.sys];
@@ -214,17 +260,24 @@ __global__ void __launch_bounds__(kFftBlock)
         const bool even = (K2 & 1) == 0;
         const int n = even ? K2 / 2 : K2, ls = line_stride(n);
         const int l0 = item.begin, nl = min(C, K0 * K1 - l0);
+        const double gsi = P.grid_scale_inv;
+        unsigned long long* __restrict__ gf = P.grid_fix + (size_t)l0 * K2;
+        T2* __restrict__ out = reinterpret_cast<T2*>(P.grid_cplx) + (size_t)l0 * Kh;
+        int nf;
+        load_fac(P, 2, s_fac, nf);
         T2* a = reinterpret_cast<T2*>(fsh_raw);
         T2* b = a + C * ls;
-        for (int q = threadIdx.x; q < nl * K2; q += blockDim.x) {
-            const int c = q / K2, z = q - c * K2;
-            const size_t gi = (size_t)(l0 + c) * K2 + z;
-            const long long v = (long long)P.grid_fix[gi];
-            P.grid_fix[gi] = 0ull; // ready for the next spread
-            const T x = (T)((double)v * P.grid_scale_inv);
+        const T2* roots = stage_roots(b + C * ls, reinterpret_cast<const T2*>(P.fft_root[2]), K2);
+        // the group's lines are contiguous in the grid: one flat walk
+        // (streaming loads, and the clear as a separate loop below: storing
+        // into each element right after loading it measured 4x slower)
+        for (Walk2 w(threadIdx.x, K2, blockDim.x); w.r < nl; w.next()) {
+            const int c = w.r, z = w.c, q = c * K2 + z;
+            const long long v = (long long)__ldcs(gf + q);
+            const T x = (T)((double)v * gsi);
             if (even) {
-                T* re = reinterpret_cast<T*>(a + c * ls);
-                re[z] = x; // x[2n], x[2n+1] interleave as z[n] = x[2n] + i x[2n+1]
+                // x[2n], x[2n+1] interleave as z[n] = x[2n] + i x[2n+1]
+                reinterpret_cast<T*>(a + c * ls)[z] = x;
             } else {
                 T2 v2;
                 v2.x = x;
@@ -233,18 +286,17 @@ __global__ void __launch_bounds__(kFftBlock)
             }
         }
         __syncthreads();
-        const T2* roots = reinterpret_cast<const T2*>(P.fft_root[2]);
-        T2* r = fft_lines<T, T2>(a, b, nl, n, ls, P.fft_fac[2], P.fft_nf[2], roots,
-                                 even ? 2 : 1, false);
-        T2* __restrict__ out = reinterpret_cast<T2*>(P.grid_cplx);
-        for (int q = threadIdx.x; q < nl * Kh; q += blockDim.x) {
-            const int c = q / Kh, k = q - c * Kh;
+        for (int q = threadIdx.x; q < nl * K2; q += blockDim.x)
+            __stcs(gf + q, 0ull); // ready for the next spread
+        T2* r = fft_lines<T, T2>(a, b, nl, n, ls, s_fac, nf, roots, even ? 2 : 1, false);
+        for (Walk2 w(threadIdx.x, Kh, blockDim.x); w.r < nl; w.next()) {
+            const int c = w.r, k = w.c;
             T2 X;
             if (even) {
                 // X[k] = E + e^{-2 pi i k / K2} O, E/O the spectra of the
                 // even / odd samples, from Z[k] and conj(Z[n - k])
-                const T2 Zk = r[c * ls + (k % n)];
-                const T2 Zc = cconj(r[c * ls + ((n - k) % n)]);
+                const T2 Zk = r[c * ls + (k == n ? 0 : k)];
+                const T2 Zc = cconj(r[c * ls + (k == 0 ? 0 : n - k)]);
                 T2 E, O;
                 E.x = (T)0.5 * (Zk.x + Zc.x);
                 E.y = (T)0.5 * (Zk.y + Zc.y);
@@ -254,7 +306,7 @@ __global__ void __launch_bounds__(kFftBlock)
             } else {
                 X = r[c * ls + k];
             }
-            out[(size_t)(l0 + c) * Kh + k] = X;
+            out[(size_t)c * Kh + k] = X;
         }
         __syncthreads();
     }
@@ -262,11 +314,12 @@ __global__ void __launch_bounds__(kFftBlock)
 
 // ---- passes 2 and 4: y forward / inverse ---------------------------------
 template <bool MIXED, bool INV>
-__global__ void __launch_bounds__(kFftBlock)
+__global__ void __launch_bounds__(kFftBlock, 3)
     k_fft_y(const Item* items, int nitems, const SysParams* sp, int C) {
     using T = typename std::conditional<MIXED, float, double>::type;
     using T2 = typename Cplx<T>::type;
     extern __shared__ unsigned char fsh_raw[];
+    __shared__ int s_fac[kFftMaxFac];
     for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
         const Item item = items[it];
         const SysParams& P = sp[item.sys];
@@ -277,31 +330,30 @@ __global__ void __launch_bounds__(kFftBlock)
         const int k0 = item.begin / nb2, m2a = (item.begin - k0 * nb2) * C;
         const int nc = min(C, Kh - m2a);
         const int ls = line_stride(K1);
+        T2* __restrict__ g = reinterpret_cast<T2*>(P.grid_cplx) + (size_t)k0 * K1 * Kh + m2a;
+        int nf;
+        load_fac(P, 1, s_fac, nf);
         T2* a = reinterpret_cast<T2*>(fsh_raw);
         T2* b = a + C * ls;
-        T2* __restrict__ g = reinterpret_cast<T2*>(P.grid_cplx) + (size_t)k0 * K1 * Kh + m2a;
-        for (int q = threadIdx.x; q < K1 * nc; q += blockDim.x) {
-            const int k1 = q / nc, c = q - k1 * nc;
-            a[c * ls + k1] = g[(size_t)k1 * Kh + c];
-        }
+        const T2* roots = stage_roots(b + C * ls, reinterpret_cast<const T2*>(P.fft_root[1]), K1);
+        for (Walk2 w(threadIdx.x, nc, blockDim.x); w.r < K1; w.next())
+            a[w.c * ls + w.r] = g[(size_t)w.r * Kh + w.c];
         __syncthreads();
-        T2* r = fft_lines<T, T2>(a, b, nc, K1, ls, P.fft_fac[1], P.fft_nf[1],
-                                 reinterpret_cast<const T2*>(P.fft_root[1]), 1, INV);
-        for (int q = threadIdx.x; q < K1 * nc; q += blockDim.x) {
-            const int k1 = q / nc, c = q - k1 * nc;
-            g[(size_t)k1 * Kh + c] = r[c * ls + k1];
-        }
+        T2* r = fft_lines<T, T2>(a, b, nc, K1, ls, s_fac, nf, roots, 1, INV);
+        for (Walk2 w(threadIdx.x, nc, blockDim.x); w.r < K1; w.next())
+            g[(size_t)w.r * Kh + w.c] = r[w.c * ls + w.r];
         __syncthreads();
     }
 }
 
 // ---- pass 3: x forward, influence with energy and virial, x inverse ------
 template <bool MIXED>
-__global__ void __launch_bounds__(kFftBlock)
+__global__ void __launch_bounds__(kFftBlock, 3)
     k_fft_x_infl(const Item* items, int nitems, const SysParams* sp, int C) {
     using T = typename std::conditional<MIXED, float, double>::type;
     using T2 = typename Cplx<T>::type;
     extern __shared__ unsigned char fsh_raw[];
+    __shared__ int s_fac[kFftMaxFac];
     __shared__ double sh[32 * 7];
     for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
         const Item item = items[it];
@@ -314,42 +366,47 @@ __global__ void __launch_bounds__(kFftBlock)
         const int nc = min(C, Kh - m2a);
         const int ls = line_stride(K0);
         const size_t sx = (size_t)K1 * Kh; // stride along x
+        T2* __restrict__ g = reinterpret_cast<T2*>(P.grid_cplx) + (size_t)m1 * Kh + m2a;
+        const double* __restrict__ bm = P.bmod;
+        const double ilx = P.invL[0], ily = P.invL[1], ilz = P.invL[2];
+        const double a2pi2 = P.pme_alpha2_pi2, escale = P.pme_escale;
+        const bool vir = P.need_virial;
+        unsigned long long* acc_st = P.st->acc;
+        int nf;
+        load_fac(P, 0, s_fac, nf);
         T2* a = reinterpret_cast<T2*>(fsh_raw);
         T2* b = a + C * ls;
-        T2* __restrict__ g = reinterpret_cast<T2*>(P.grid_cplx) + (size_t)m1 * Kh + m2a;
-        for (int q = threadIdx.x; q < K0 * nc; q += blockDim.x) {
-            const int k0 = q / nc, c = q - k0 * nc;
-            a[c * ls + k0] = g[(size_t)k0 * sx + c];
-        }
+        const T2* roots = stage_roots(b + C * ls, reinterpret_cast<const T2*>(P.fft_root[0]), K0);
+        for (Walk2 w(threadIdx.x, nc, blockDim.x); w.r < K0; w.next())
+            a[w.c * ls + w.r] = g[(size_t)w.r * sx + w.c];
         __syncthreads();
-        const T2* roots = reinterpret_cast<const T2*>(P.fft_root[0]);
-        T2* r = fft_lines<T, T2>(a, b, nc, K0, ls, P.fft_fac[0], P.fft_nf[0], roots, 1, false);
+        T2* r = fft_lines<T, T2>(a, b, nc, K0, ls, s_fac, nf, roots, 1, false);
         // H(m) = exp(-pi^2 m^2 / alpha^2) / m^2 * B(m) (zero mode cleared,
         // pme_influence.h:112-155) from the current cell; energy and virial
         // with the half-grid weights (modes 0 < m2 < K2/2 stand for two)
-        const bool vir = P.need_virial;
         double acc[7] = {0, 0, 0, 0, 0, 0, 0};
         const int h1 = m1 <= K1 / 2 ? m1 : m1 - K1;
-        const double my = h1 * P.invL[1];
-        for (int q = threadIdx.x; q < K0 * nc; q += blockDim.x) {
-            const int c = q / K0, m0 = q - c * K0;
+        const double my = h1 * ily;
+        const double bmy = bm[K0 + m1];
+        for (Walk2 w(threadIdx.x, K0, blockDim.x); w.r < nc; w.next()) {
+            const int c = w.r, m0 = w.c;
             const int m2 = m2a + c;
             const int h0 = m0 <= K0 / 2 ? m0 : m0 - K0;
             const int h2 = m2 <= K2 / 2 ? m2 : m2 - K2;
-            const double mx = h0 * P.invL[0], mz = h2 * P.invL[2];
+            const double mx = h0 * ilx, mz = h2 * ilz;
             const double msq = mx * mx + my * my + mz * mz;
             const bool zero = m0 == 0 && m1 == 0 && m2 == 0;
             const double imsq = zero ? 0.0 : rcp64(msq);
             const double H = zero ? 0.0
-                                  : exp_neg64(P.pme_alpha2_pi2 * msq) * imsq *
-                                        (P.bmod[m0] * P.bmod[K0 + m1]) * P.bmod[K0 + K1 + m2];
+                                  : exp_neg64(a2pi2 * msq) * imsq * (bm[m0] * bmy) *
+                                        bm[K0 + K1 + m2];
             T2 Qm = r[c * ls + m0];
             const double re = (double)Qm.x, im = (double)Qm.y;
-            const double w = (m2 == 0 || 2 * m2 == K2) ? 1.0 : 2.0;
-            const double ug = w * H * (re * re + im * im);
+            const double wt = (m2 == 0 || 2 * m2 == K2) ? 1.0 : 2.0;
+            const double ug = wt * H * (re * re + im * im);
             acc[0] += ug;
             if (vir && H != 0.0) {
-                const double vt = -2.0 * (imsq + P.pme_alpha2_pi2);
+                const double vt = -2.0 * (imsq + a2pi2);
                 acc[1] += ug * (1.0 + vt * mx * mx);
                 acc[2] += ug * (1.0 + vt * my * my);
                 acc[3] += ug * (1.0 + vt * mz * mz);
@@ -363,24 +420,22 @@ __global__ void __launch_bounds__(kFftBlock)
         }
         __syncthreads();
         T2* o = r == a ? b : a;
-        T2* r2 = fft_lines<T, T2>(r, o, nc, K0, ls, P.fft_fac[0], P.fft_nf[0], roots, 1, true);
-        for (int q = threadIdx.x; q < K0 * nc; q += blockDim.x) {
-            const int k0 = q / nc, c = q - k0 * nc;
-            g[(size_t)k0 * sx + c] = r2[c * ls + k0];
-        }
+        T2* r2 = fft_lines<T, T2>(r, o, nc, K0, ls, s_fac, nf, roots, 1, true);
+        for (Walk2 w(threadIdx.x, nc, blockDim.x); w.r < K0; w.next())
+            g[(size_t)w.r * sx + w.c] = r2[w.c * ls + w.r];
         // per-item fixed-point flush (independent of batch composition)
         if (vir) {
             block_sum_vec<7>(acc, sh);
             if (threadIdx.x == 0) {
-                fix_add(&P.st->acc[kAccERecip], acc[0] * P.pme_escale);
+                fix_add(&acc_st[kAccERecip], acc[0] * escale);
                 for (int k = 0; k < 6; ++k)
-                    fix_add(&P.st->acc[kAccVir + k], acc[1 + k] * P.pme_escale);
+                    fix_add(&acc_st[kAccVir + k], acc[1 + k] * escale);
             }
         } else {
             double e1[1] = {acc[0]};
             block_sum_vec<1>(e1, sh);
             if (threadIdx.x == 0)
-                fix_add(&P.st->acc[kAccERecip], e1[0] * P.pme_escale);
+                fix_add(&acc_st[kAccERecip], e1[0] * escale);
         }
         __syncthreads();
     }
@@ -388,11 +443,12 @@ __global__ void __launch_bounds__(kFftBlock)
 
 // ---- pass 5: z inverse, complex-to-real into the real grid ---------------
 template <bool MIXED>
-__global__ void __launch_bounds__(kFftBlock)
+__global__ void __launch_bounds__(kFftBlock, 3)
     k_fft_zi(const Item* items, int nitems, const SysParams* sp, int C) {
     using T = typename std::conditional<MIXED, float, double>::type;
     using T2 = typename Cplx<T>::type;
     extern __shared__ unsigned char fsh_raw[];
+    __shared__ int s_fac[kFftMaxFac];
     for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
         const Item item = items[it];
         const SysParams& P = sp[item.sys];
@@ -402,15 +458,19 @@ __global__ void __launch_bounds__(kFftBlock)
         const bool even = (K2 & 1) == 0;
         const int n = even ? K2 / 2 : K2, ls = line_stride(n);
         const int l0 = item.begin, nl = min(C, K0 * K1 - l0);
+        const T2* __restrict__ in = reinterpret_cast<const T2*>(P.grid_cplx) + (size_t)l0 * Kh;
+        T* __restrict__ out = reinterpret_cast<T*>(P.grid_real) + (size_t)l0 * K2;
+        int nf;
+        load_fac(P, 2, s_fac, nf);
         T2* a = reinterpret_cast<T2*>(fsh_raw);
         T2* b = a + C * ls;
-        const T2* roots = reinterpret_cast<const T2*>(P.fft_root[2]);
-        const T2* __restrict__ in = reinterpret_cast<const T2*>(P.grid_cplx);
+        const T2* roots = stage_roots(b + C * ls, reinterpret_cast<const T2*>(P.fft_root[2]), K2);
+        __syncthreads();
         if (even) {
             // Z'[k] = (X[k] + conj X[n-k]) + i (X[k] - conj X[n-k]) e^{2 pi i k / K2}
-            for (int q = threadIdx.x; q < nl * n; q += blockDim.x) {
-                const int c = q / n, k = q - c * n;
-                const size_t row = (size_t)(l0 + c) * Kh;
+            for (Walk2 w(threadIdx.x, n, blockDim.x); w.r < nl; w.next()) {
+                const int c = w.r, k = w.c;
+                const size_t row = (size_t)c * Kh;
                 const T2 Xk = in[row + k];
                 const T2 Xc = cconj(in[row + (n - k)]);
                 const T2 E = cadd(Xk, Xc);
@@ -422,18 +482,16 @@ __global__ void __launch_bounds__(kFftBlock)
             }
         } else {
             // the full Hermitian spectrum
-            for (int q = threadIdx.x; q < nl * K2; q += blockDim.x) {
-                const int c = q / K2, k = q - c * K2;
-                const size_t row = (size_t)(l0 + c) * Kh;
+            for (Walk2 w(threadIdx.x, K2, blockDim.x); w.r < nl; w.next()) {
+                const int c = w.r, k = w.c;
+                const size_t row = (size_t)c * Kh;
                 a[c * ls + k] = k < Kh ? in[row + k] : cconj(in[row + (K2 - k)]);
             }
         }
         __syncthreads();
-        T2* r = fft_lines<T, T2>(a, b, nl, n, ls, P.fft_fac[2], P.fft_nf[2], roots,
-                                 even ? 2 : 1, true);
-        T* __restrict__ out = reinterpret_cast<T*>(P.grid_real);
-        for (int q = threadIdx.x; q < nl * K2; q += blockDim.x) {
-            const int c = q / K2, z = q - c * K2;
+        T2* r = fft_lines<T, T2>(a, b, nl, n, ls, s_fac, nf, roots, even ? 2 : 1, true);
+        for (Walk2 w(threadIdx.x, K2, blockDim.x); w.r < nl; w.next()) {
+            const int c = w.r, z = w.c;
             T v;
             if (even) {
                 const T2 zz = r[c * ls + (z >> 1)];
@@ -441,30 +499,28 @@ __global__ void __launch_bounds__(kFftBlock)
             } else {
                 v = r[c * ls + z].x;
             }
-            out[(size_t)(l0 + c) * K2 + z] = v;
+            out[(size_t)c * K2 + z] = v;
         }
         __syncthreads();
     }
 }
 
-static size_t fft_smem(int C, int n, bool mixed) {
-    return (size_t)2 * C * (n + 1) * (mixed ? sizeof(float2) : sizeof(double2));
+// Two buffers of C lines (n + 1 each) and the K roots of unity.
+static size_t fft_smem(int C, int n, int K, bool mixed) {
+    return ((size_t)2 * C * (n + 1) + K) * (mixed ? sizeof(float2) : sizeof(double2));
 }
 
 template <bool MIXED>
 static void fft_all(const LaunchCfg& lc, cudaStream_t s) {
     const FftCfg& f = lc.fft;
     if (f.z.n) {
-        k_fft_zf<MIXED><<<f.z.grid, kFftBlock, fft_smem(f.cz, f.nz, MIXED), s>>>(f.z.d, f.z.n,
-                                                                              lc.sp, f.cz);
-        k_fft_y<MIXED, false><<<f.y.grid, kFftBlock, fft_smem(f.cy, f.ny, MIXED), s>>>(
-            f.y.d, f.y.n, lc.sp, f.cy);
-        k_fft_x_infl<MIXED><<<f.x.grid, kFftBlock, fft_smem(f.cx, f.nx, MIXED), s>>>(
-            f.x.d, f.x.n, lc.sp, f.cx);
-        k_fft_y<MIXED, true><<<f.y.grid, kFftBlock, fft_smem(f.cy, f.ny, MIXED), s>>>(
-            f.y.d, f.y.n, lc.sp, f.cy);
-        k_fft_zi<MIXED><<<f.z.grid, kFftBlock, fft_smem(f.cz, f.nz, MIXED), s>>>(f.z.d, f.z.n,
-                                                                              lc.sp, f.cz);
+        const size_t sz = fft_smem(f.cz, f.nz, f.kz, MIXED), sy = fft_smem(f.cy, f.ny, f.ny, MIXED),
+                     sx = fft_smem(f.cx, f.nx, f.nx, MIXED);
+        k_fft_zf<MIXED><<<f.z.grid, kFftBlock, sz, s>>>(f.z.d, f.z.n, lc.sp, f.cz);
+        k_fft_y<MIXED, false><<<f.y.grid, kFftBlock, sy, s>>>(f.y.d, f.y.n, lc.sp, f.cy);
+        k_fft_x_infl<MIXED><<<f.x.grid, kFftBlock, sx, s>>>(f.x.d, f.x.n, lc.sp, f.cx);
+        k_fft_y<MIXED, true><<<f.y.grid, kFftBlock, sy, s>>>(f.y.d, f.y.n, lc.sp, f.cy);
+        k_fft_zi<MIXED><<<f.z.grid, kFftBlock, sz, s>>>(f.z.d, f.z.n, lc.sp, f.cz);
     }
 }
 
@@ -494,11 +550,12 @@ void fft_smem_optin(int bytes) {
     set((const void*)k_fft_zi<true>);
 }
 
-// Lines per block for a transform of length n: as many as fit kFftSmem
-// bytes of shared memory (two buffers), at most kFftMaxLines.
-int fft_lines_per_block(int n, bool mixed) {
-    const size_t per = fft_smem(1, n, mixed);
-    int C = (int)(kFftSmem / per);
+// Lines per block for a transform of length n with K roots: as many as fit
+// kFftSmem bytes of shared memory, at most kFftMaxLines.
+int fft_lines_per_block(int n, int K, bool mixed) {
+    const size_t per = fft_smem(1, n, 0, mixed);
+    const size_t roots = fft_smem(0, 0, K, mixed);
+    int C = (int)((kFftSmem - roots) / per);
     C = C > kFftMaxLines ? kFftMaxLines : C;
     return C < 1 ? 1 : C;
 }
