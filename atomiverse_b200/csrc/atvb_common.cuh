@@ -169,6 +169,7 @@ struct SysParams {
     // PME
     int has_pme;
     int K[3], Kh, order;
+    int Khp; // row stride of the half-complex grid: Kh rounded up to 16
     double pme_fscale; // k_e / (pi V)
     double pme_escale; // k_e / (2 pi V)
     double pme_alpha2_pi2; // pi^2 / alpha^2

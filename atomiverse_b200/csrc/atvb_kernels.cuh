@@ -31,6 +31,9 @@ struct FftCfg {
     int cz = 1, cy = 1, cx = 1;
     int nz = 0, ny = 0, nx = 0;
     int kz = 0; // longest root table of the z passes (K2; the line is K2/2 when even)
+    // register forms (fft_reg.cu) per pass, -1 for the generic kernels: used
+    // when every system of the launch has the same line length on that axis
+    int rz = -1, ry = -1, rx = -1;
 };
 
 struct LaunchCfg {
@@ -77,6 +80,15 @@ void launch_pme_gather(const LaunchCfg& lc, cudaStream_t s);
 void launch_pme_fft(const LaunchCfg& lc, cudaStream_t s);
 void fft_smem_optin(int bytes);
 int fft_lines_per_block(int n, int K, bool mixed);
+// Register forms of the line transforms (fft_reg.cu): the form of a line
+// length (-1: none), z lines per item, y / x columns per item, and a launch
+// of one pass (0 z forward, 1 y forward, 2 x with the influence function,
+// 3 y inverse, 4 z inverse).
+int fft_reg_index(int n);
+int fft_reg_lines(int idx, bool mixed);
+int fft_reg_cols(bool mixed);
+void launch_fft_reg(int pass, int idx, bool mixed, const ItemList& il, const SysParams* sp,
+                    cudaStream_t s);
 // integrate.cu
 void launch_integrate_a(const LaunchCfg& lc, cudaStream_t s);
 void launch_sys_a(const LaunchCfg& lc, cudaStream_t s);

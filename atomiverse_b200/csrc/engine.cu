@@ -232,7 +232,7 @@ size_t estimate_bytes(const atvb_system_desc& d) {
     if (d.pme_enabled) {
         const size_t K0 = pme_K(d, g, 0), K1 = pme_K(d, g, 1),
                      K2 = pme_K(d, g, 2);
-        const size_t nt = K0 * K1 * K2, nh = K0 * K1 * (K2 / 2 + 1);
+        const size_t nt = K0 * K1 * K2, nh = K0 * K1 * ((K2 / 2 + 1 + 15) / 16 * 16);
         const size_t rs = d.precision == ATVB_MIXED ? 4 : 8;
         b += nt * 8 + nt * rs + nh * 2 * rs + (K0 + K1 + K2) * 8;
         b += (K0 + K1 + K2) * 2 * rs; // roots of unity of the transforms
@@ -534,12 +534,13 @@ Slot::Slot(const atvb_system_desc& d, const DevMem& mem) : desc(d), mem_(mem) {
         for (int k = 0; k < 3; ++k)
             hp.K[k] = pme_K(d, geo, k);
         hp.Kh = hp.K[2] / 2 + 1;
+        hp.Khp = (hp.Kh + 15) / 16 * 16;
         hp.pme_alpha = d.pme_alpha;
         hp.pme_alpha2_pi2 = kPi * kPi / (d.pme_alpha * d.pme_alpha);
         hp.grid_scale = hp.prec == kMixed ? 4294967296.0 : 1099511627776.0;
         hp.grid_scale_inv = 1.0 / hp.grid_scale;
-        const size_t K0 = hp.K[0], K1 = hp.K[1], K2 = hp.K[2], Kh = hp.Kh;
-        const size_t nt = K0 * K1 * K2, nh = K0 * K1 * Kh;
+        const size_t K0 = hp.K[0], K1 = hp.K[1], K2 = hp.K[2], Khp = hp.Khp;
+        const size_t nt = K0 * K1 * K2, nh = K0 * K1 * Khp;
         const size_t rs = hp.prec == kMixed ? 4 : 8;
         hp.fp4 = (double4*)dalloc((size_t)n * sizeof(double4));
         hp.grid_fix = (unsigned long long*)dalloc(nt * 8);
@@ -938,6 +939,24 @@ FftCfg Engine::fft_items(const std::vector<int>& pme) {
     f.cz = fft_lines_per_block(f.nz, f.kz, mixed);
     f.cy = fft_lines_per_block(f.ny, f.ny, mixed);
     f.cx = fft_lines_per_block(f.nx, f.nx, mixed);
+    // the register forms where every system has the same line length on
+    // the axis (z: an even K2, the line K2 / 2)
+    bool same_z = true, same_y = true, same_x = true;
+    for (int id : pme) {
+        const SysParams& P = slots_[id]->hp;
+        same_z = same_z && P.K[2] % 2 == 0 && P.K[2] / 2 == f.nz;
+        same_y = same_y && P.K[1] == f.ny;
+        same_x = same_x && P.K[0] == f.nx;
+    }
+    f.rz = same_z ? fft_reg_index(f.nz) : -1;
+    f.ry = same_y ? fft_reg_index(f.ny) : -1;
+    f.rx = same_x ? fft_reg_index(f.nx) : -1;
+    if (f.rz >= 0)
+        f.cz = fft_reg_lines(f.rz, mixed);
+    if (f.ry >= 0)
+        f.cy = fft_reg_cols(mixed);
+    if (f.rx >= 0)
+        f.cx = fft_reg_cols(mixed);
     std::vector<Item> z, y, x;
     for (int id : pme) {
         const SysParams& P = slots_[id]->hp;
@@ -949,10 +968,10 @@ FftCfg Engine::fft_items(const std::vector<int>& pme) {
         for (int q = 0; q < P.K[1] * bx; ++q)
             x.push_back({id, q});
     }
-    const int g = num_sms_ * 8;
-    f.z = make_list(list_allocs_, z, g, mem_);
-    f.y = make_list(list_allocs_, y, g, mem_);
-    f.x = make_list(list_allocs_, x, g, mem_);
+    const int g = num_sms_ * 8, gr = num_sms_ * 16;
+    f.z = make_list(list_allocs_, z, f.rz >= 0 ? gr : g, mem_);
+    f.y = make_list(list_allocs_, y, f.ry >= 0 ? gr : g, mem_);
+    f.x = make_list(list_allocs_, x, f.rx >= 0 ? gr : g, mem_);
     return f;
 }
 

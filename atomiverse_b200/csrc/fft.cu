@@ -6,7 +6,8 @@
 // 203-210) or cuFFT (src/cuda/longrange/pme.cu:293,330,334), unnormalised
 // in both directions, between its spread and its gather.  The same
 // transform here, on the half-complex grid K0 x K1 x (K2/2 + 1) (index
-// m2 + Kh (m1 + K1 m0)), with the stages of the PME step folded in:
+// m2 + Khp (m1 + K1 m0), rows padded to Khp, a multiple of 16), with the
+// stages of the PME step folded in:
 //   1. z forward (one block per line group): the 64-bit fixed-point charge
 //      grid read, converted and cleared, real-to-complex along z;
 //   2. y forward: complex FFT along y (tiles of a few m2 columns, loaded
@@ -256,13 +257,13 @@ __global__ void __launch_bounds__(kFftBlock, 3)
         const SysParams& P = sp[item.sys];
         if (!P.has_pme || P.prec != (MIXED ? kMixed : kFP64))
             continue;
-        const int K0 = P.K[0], K1 = P.K[1], K2 = P.K[2], Kh = P.Kh;
+        const int K0 = P.K[0], K1 = P.K[1], K2 = P.K[2], Kh = P.Kh, Khp = P.Khp;
         const bool even = (K2 & 1) == 0;
         const int n = even ? K2 / 2 : K2, ls = line_stride(n);
         const int l0 = item.begin, nl = min(C, K0 * K1 - l0);
         const double gsi = P.grid_scale_inv;
         unsigned long long* __restrict__ gf = P.grid_fix + (size_t)l0 * K2;
-        T2* __restrict__ out = reinterpret_cast<T2*>(P.grid_cplx) + (size_t)l0 * Kh;
+        T2* __restrict__ out = reinterpret_cast<T2*>(P.grid_cplx) + (size_t)l0 * Khp;
         int nf;
         load_fac(P, 2, s_fac, nf);
         T2* a = reinterpret_cast<T2*>(fsh_raw);
@@ -306,7 +307,7 @@ __global__ void __launch_bounds__(kFftBlock, 3)
             } else {
                 X = r[c * ls + k];
             }
-            out[(size_t)c * Kh + k] = X;
+            out[(size_t)c * Khp + k] = X;
         }
         __syncthreads();
     }
@@ -325,23 +326,23 @@ __global__ void __launch_bounds__(kFftBlock, 3)
         const SysParams& P = sp[item.sys];
         if (!P.has_pme || P.prec != (MIXED ? kMixed : kFP64))
             continue;
-        const int K1 = P.K[1], Kh = P.Kh;
+        const int K1 = P.K[1], Kh = P.Kh, Khp = P.Khp;
         const int nb2 = (Kh + C - 1) / C;
         const int k0 = item.begin / nb2, m2a = (item.begin - k0 * nb2) * C;
         const int nc = min(C, Kh - m2a);
         const int ls = line_stride(K1);
-        T2* __restrict__ g = reinterpret_cast<T2*>(P.grid_cplx) + (size_t)k0 * K1 * Kh + m2a;
+        T2* __restrict__ g = reinterpret_cast<T2*>(P.grid_cplx) + (size_t)k0 * K1 * Khp + m2a;
         int nf;
         load_fac(P, 1, s_fac, nf);
         T2* a = reinterpret_cast<T2*>(fsh_raw);
         T2* b = a + C * ls;
         const T2* roots = stage_roots(b + C * ls, reinterpret_cast<const T2*>(P.fft_root[1]), K1);
         for (Walk2 w(threadIdx.x, nc, blockDim.x); w.r < K1; w.next())
-            a[w.c * ls + w.r] = g[(size_t)w.r * Kh + w.c];
+            a[w.c * ls + w.r] = g[(size_t)w.r * Khp + w.c];
         __syncthreads();
         T2* r = fft_lines<T, T2>(a, b, nc, K1, ls, s_fac, nf, roots, 1, INV);
         for (Walk2 w(threadIdx.x, nc, blockDim.x); w.r < K1; w.next())
-            g[(size_t)w.r * Kh + w.c] = r[w.c * ls + w.r];
+            g[(size_t)w.r * Khp + w.c] = r[w.c * ls + w.r];
         __syncthreads();
     }
 }
@@ -365,8 +366,8 @@ __global__ void __launch_bounds__(kFftBlock, 3)
         const int m1 = item.begin / nb2, m2a = (item.begin - m1 * nb2) * C;
         const int nc = min(C, Kh - m2a);
         const int ls = line_stride(K0);
-        const size_t sx = (size_t)K1 * Kh; // stride along x
-        T2* __restrict__ g = reinterpret_cast<T2*>(P.grid_cplx) + (size_t)m1 * Kh + m2a;
+        const size_t sx = (size_t)K1 * P.Khp; // stride along x
+        T2* __restrict__ g = reinterpret_cast<T2*>(P.grid_cplx) + (size_t)m1 * P.Khp + m2a;
         const double* __restrict__ bm = P.bmod;
         const double ilx = P.invL[0], ily = P.invL[1], ilz = P.invL[2];
         const double a2pi2 = P.pme_alpha2_pi2, escale = P.pme_escale;
@@ -458,7 +459,8 @@ __global__ void __launch_bounds__(kFftBlock, 3)
         const bool even = (K2 & 1) == 0;
         const int n = even ? K2 / 2 : K2, ls = line_stride(n);
         const int l0 = item.begin, nl = min(C, K0 * K1 - l0);
-        const T2* __restrict__ in = reinterpret_cast<const T2*>(P.grid_cplx) + (size_t)l0 * Kh;
+        const int Khp = P.Khp;
+        const T2* __restrict__ in = reinterpret_cast<const T2*>(P.grid_cplx) + (size_t)l0 * Khp;
         T* __restrict__ out = reinterpret_cast<T*>(P.grid_real) + (size_t)l0 * K2;
         int nf;
         load_fac(P, 2, s_fac, nf);
@@ -470,7 +472,7 @@ __global__ void __launch_bounds__(kFftBlock, 3)
             // Z'[k] = (X[k] + conj X[n-k]) + i (X[k] - conj X[n-k]) e^{2 pi i k / K2}
             for (Walk2 w(threadIdx.x, n, blockDim.x); w.r < nl; w.next()) {
                 const int c = w.r, k = w.c;
-                const size_t row = (size_t)c * Kh;
+                const size_t row = (size_t)c * Khp;
                 const T2 Xk = in[row + k];
                 const T2 Xc = cconj(in[row + (n - k)]);
                 const T2 E = cadd(Xk, Xc);
@@ -484,7 +486,7 @@ __global__ void __launch_bounds__(kFftBlock, 3)
             // the full Hermitian spectrum
             for (Walk2 w(threadIdx.x, K2, blockDim.x); w.r < nl; w.next()) {
                 const int c = w.r, k = w.c;
-                const size_t row = (size_t)c * Kh;
+                const size_t row = (size_t)c * Khp;
                 a[c * ls + k] = k < Kh ? in[row + k] : cconj(in[row + (K2 - k)]);
             }
         }
@@ -510,17 +512,34 @@ static size_t fft_smem(int C, int n, int K, bool mixed) {
     return ((size_t)2 * C * (n + 1) + K) * (mixed ? sizeof(float2) : sizeof(double2));
 }
 
+// Each pass runs its register form (fft_reg.cuh) when the launch has one
+// for that axis, else the generic Stockham kernel above.
 template <bool MIXED>
 static void fft_all(const LaunchCfg& lc, cudaStream_t s) {
     const FftCfg& f = lc.fft;
     if (f.z.n) {
         const size_t sz = fft_smem(f.cz, f.nz, f.kz, MIXED), sy = fft_smem(f.cy, f.ny, f.ny, MIXED),
                      sx = fft_smem(f.cx, f.nx, f.nx, MIXED);
-        k_fft_zf<MIXED><<<f.z.grid, kFftBlock, sz, s>>>(f.z.d, f.z.n, lc.sp, f.cz);
-        k_fft_y<MIXED, false><<<f.y.grid, kFftBlock, sy, s>>>(f.y.d, f.y.n, lc.sp, f.cy);
-        k_fft_x_infl<MIXED><<<f.x.grid, kFftBlock, sx, s>>>(f.x.d, f.x.n, lc.sp, f.cx);
-        k_fft_y<MIXED, true><<<f.y.grid, kFftBlock, sy, s>>>(f.y.d, f.y.n, lc.sp, f.cy);
-        k_fft_zi<MIXED><<<f.z.grid, kFftBlock, sz, s>>>(f.z.d, f.z.n, lc.sp, f.cz);
+        if (f.rz >= 0)
+            launch_fft_reg(0, f.rz, MIXED, f.z, lc.sp, s);
+        else
+            k_fft_zf<MIXED><<<f.z.grid, kFftBlock, sz, s>>>(f.z.d, f.z.n, lc.sp, f.cz);
+        if (f.ry >= 0)
+            launch_fft_reg(1, f.ry, MIXED, f.y, lc.sp, s);
+        else
+            k_fft_y<MIXED, false><<<f.y.grid, kFftBlock, sy, s>>>(f.y.d, f.y.n, lc.sp, f.cy);
+        if (f.rx >= 0)
+            launch_fft_reg(2, f.rx, MIXED, f.x, lc.sp, s);
+        else
+            k_fft_x_infl<MIXED><<<f.x.grid, kFftBlock, sx, s>>>(f.x.d, f.x.n, lc.sp, f.cx);
+        if (f.ry >= 0)
+            launch_fft_reg(3, f.ry, MIXED, f.y, lc.sp, s);
+        else
+            k_fft_y<MIXED, true><<<f.y.grid, kFftBlock, sy, s>>>(f.y.d, f.y.n, lc.sp, f.cy);
+        if (f.rz >= 0)
+            launch_fft_reg(4, f.rz, MIXED, f.z, lc.sp, s);
+        else
+            k_fft_zi<MIXED><<<f.z.grid, kFftBlock, sz, s>>>(f.z.d, f.z.n, lc.sp, f.cz);
     }
 }
 
