@@ -2,6 +2,8 @@
 // and the engine that captures them into the per-step CUDA graph.
 #pragma once
 
+#include <vector>
+
 #include "atvb_common.cuh"
 
 namespace atvb {
@@ -19,21 +21,24 @@ struct ItemList {
     int grid = 0;            // blocks to launch (persistent loop covers n)
 };
 
-// The PME transforms of a launch (fft.cu): items of the z passes (first
-// line of a group), the y passes (k0 x column block) and the x pass
-// (m1 x column block); lines per block and the longest line, for the
-// shared-memory size.
+// The PME transforms of a launch (fft.cu): per pass, one group of items
+// per line length (the z passes: first line of a group of lines; the y
+// passes: k0 x column block; the x pass: m1 x column block), so that each
+// system's transform depends on its own mesh alone, whatever it is batched
+// with.
 constexpr int kFftBlock = 256;          // threads per FFT block
 constexpr int kFftSmem = 56 * 1024;     // shared memory an FFT block may use
 constexpr int kFftMaxLines = 16;        // lines per FFT block
+struct FftGroup {
+    ItemList items;
+    int n = 0;    // line length (z: K2 / 2 for an even K2, else K2)
+    int k = 0;    // roots of unity of the axis (z: K2)
+    int reg = -1; // register form (fft_reg*.cu), -1 for the generic kernels
+    int c = 1;    // lines (z) or columns (y, x) per item
+};
 struct FftCfg {
-    ItemList z, y, x;
-    int cz = 1, cy = 1, cx = 1;
-    int nz = 0, ny = 0, nx = 0;
-    int kz = 0; // longest root table of the z passes (K2; the line is K2/2 when even)
-    // register forms (fft_reg.cu) per pass, -1 for the generic kernels: used
-    // when every system of the launch has the same line length on that axis
-    int rz = -1, ry = -1, rx = -1;
+    std::vector<FftGroup> z, y, x;
+    int launches() const { return (int)(2 * z.size() + 2 * y.size() + x.size()); }
 };
 
 struct LaunchCfg {

@@ -920,58 +920,56 @@ void Engine::build_lists() {
     single_.clear();
 }
 
-// The PME transforms' work items over the systems in `pme` (fft.cu): lines
-// per block from the longest line of each pass, then the z items (groups of
-// x-y lines), the y items (k0 x a block of m2 columns) and the x items (m1 x
-// a block of columns).
+// The PME transforms' work items over the systems in `pme` (fft.cu): per
+// pass one group per line length, in the register form of that length
+// where there is one (fft_reg*.cu), else the generic kernels; the z items
+// are groups of x-y lines, the y items k0 x a block of m2 columns and the x
+// items m1 x a block of columns.
 FftCfg Engine::fft_items(const std::vector<int>& pme) {
     FftCfg f;
     if (pme.empty())
         return f;
     const bool mixed = slots_[pme[0]]->hp.prec == kMixed;
-    for (int id : pme) {
-        const SysParams& P = slots_[id]->hp;
-        f.nz = std::max(f.nz, (P.K[2] % 2 == 0) ? P.K[2] / 2 : P.K[2]);
-        f.kz = std::max(f.kz, P.K[2]);
-        f.ny = std::max(f.ny, P.K[1]);
-        f.nx = std::max(f.nx, P.K[0]);
-    }
-    f.cz = fft_lines_per_block(f.nz, f.kz, mixed);
-    f.cy = fft_lines_per_block(f.ny, f.ny, mixed);
-    f.cx = fft_lines_per_block(f.nx, f.nx, mixed);
-    // the register forms where every system has the same line length on
-    // the axis (z: an even K2, the line K2 / 2)
-    bool same_z = true, same_y = true, same_x = true;
-    for (int id : pme) {
-        const SysParams& P = slots_[id]->hp;
-        same_z = same_z && P.K[2] % 2 == 0 && P.K[2] / 2 == f.nz;
-        same_y = same_y && P.K[1] == f.ny;
-        same_x = same_x && P.K[0] == f.nx;
-    }
-    f.rz = same_z ? fft_reg_index(f.nz) : -1;
-    f.ry = same_y ? fft_reg_index(f.ny) : -1;
-    f.rx = same_x ? fft_reg_index(f.nx) : -1;
-    if (f.rz >= 0)
-        f.cz = fft_reg_lines(f.rz, mixed);
-    if (f.ry >= 0)
-        f.cy = fft_reg_cols(mixed);
-    if (f.rx >= 0)
-        f.cx = fft_reg_cols(mixed);
-    std::vector<Item> z, y, x;
-    for (int id : pme) {
-        const SysParams& P = slots_[id]->hp;
-        for (int l = 0; l < P.K[0] * P.K[1]; l += f.cz)
-            z.push_back({id, l});
-        const int by = (P.Kh + f.cy - 1) / f.cy, bx = (P.Kh + f.cx - 1) / f.cx;
-        for (int q = 0; q < P.K[0] * by; ++q)
-            y.push_back({id, q});
-        for (int q = 0; q < P.K[1] * bx; ++q)
-            x.push_back({id, q});
-    }
     const int g = num_sms_ * 8, gr = num_sms_ * 16;
-    f.z = make_list(list_allocs_, z, f.rz >= 0 ? gr : g, mem_);
-    f.y = make_list(list_allocs_, y, f.ry >= 0 ? gr : g, mem_);
-    f.x = make_list(list_allocs_, x, f.rx >= 0 ? gr : g, mem_);
+    // axis 2: z, 1: y, 0: x
+    for (int axis = 2; axis >= 0; --axis) {
+        std::vector<FftGroup>& out = axis == 2 ? f.z : axis == 1 ? f.y : f.x;
+        std::vector<std::vector<Item>> items;
+        for (int id : pme) {
+            const SysParams& P = slots_[id]->hp;
+            const int K = P.K[axis];
+            const int n = (axis == 2 && K % 2 == 0) ? K / 2 : K;
+            size_t gi = 0;
+            while (gi < out.size() && !(out[gi].n == n && out[gi].k == K))
+                ++gi;
+            if (gi == out.size()) {
+                FftGroup grp;
+                grp.n = n;
+                grp.k = K;
+                // the z register forms take an even K2 (lines of K2 / 2)
+                grp.reg = (axis != 2 || K % 2 == 0) ? fft_reg_index(n) : -1;
+                if (grp.reg >= 0)
+                    grp.c = axis == 2 ? fft_reg_lines(grp.reg, mixed) : fft_reg_cols(mixed);
+                else
+                    grp.c = fft_lines_per_block(n, K, mixed);
+                out.push_back(grp);
+                items.emplace_back();
+            }
+            const int c = out[gi].c;
+            std::vector<Item>& v = items[gi];
+            if (axis == 2) {
+                for (int l = 0; l < P.K[0] * P.K[1]; l += c)
+                    v.push_back({id, l});
+            } else {
+                const int nb = (P.Kh + c - 1) / c;
+                const int lines = axis == 1 ? P.K[0] : P.K[1];
+                for (int q = 0; q < lines * nb; ++q)
+                    v.push_back({id, q});
+            }
+        }
+        for (size_t gi = 0; gi < out.size(); ++gi)
+            out[gi].items = make_list(list_allocs_, items[gi], out[gi].reg >= 0 ? gr : g, mem_);
+    }
     return f;
 }
 
@@ -986,7 +984,7 @@ int64_t Engine::kernels_per_step() const {
     k += lc_.any_near ? 1 : 0;                // near-cutoff fix-up (mixed LJ)
     k += (lc_.pair_gen[0].n ? 1 : 0) + (lc_.pair_gen[1].n ? 1 : 0); // general pair
     if (!pme_slots_.empty())
-        k += 7;                               // spread, 5 transform passes, gather
+        k += 2 + lc_.fft.launches();          // spread, gather, the transform passes
     k += 2;                                   // integrate_b, sys_b
     k += lc_.any_snap ? 3 : 0;                // trajectory snapshots
     k += lc_.any_baro ? 1 : 0;                // Berendsen position scaling

@@ -512,35 +512,38 @@ static size_t fft_smem(int C, int n, int K, bool mixed) {
     return ((size_t)2 * C * (n + 1) + K) * (mixed ? sizeof(float2) : sizeof(double2));
 }
 
-// Each pass runs its register form (fft_reg.cuh) when the launch has one
-// for that axis, else the generic Stockham kernel above.
+// Each pass runs, per line length, its register form (fft_reg.cuh) where
+// there is one, else the generic Stockham kernel above.
+template <bool MIXED>
+static void fft_pass(int pass, const std::vector<FftGroup>& gs, const SysParams* sp,
+                     cudaStream_t s) {
+    for (const FftGroup& g : gs) {
+        if (g.items.n == 0)
+            continue;
+        if (g.reg >= 0) {
+            launch_fft_reg(pass, g.reg, MIXED, g.items, sp, s);
+            continue;
+        }
+        const size_t sm = fft_smem(g.c, g.n, g.k, MIXED);
+        const ItemList& il = g.items;
+        switch (pass) {
+        case 0: k_fft_zf<MIXED><<<il.grid, kFftBlock, sm, s>>>(il.d, il.n, sp, g.c); break;
+        case 1: k_fft_y<MIXED, false><<<il.grid, kFftBlock, sm, s>>>(il.d, il.n, sp, g.c); break;
+        case 2: k_fft_x_infl<MIXED><<<il.grid, kFftBlock, sm, s>>>(il.d, il.n, sp, g.c); break;
+        case 3: k_fft_y<MIXED, true><<<il.grid, kFftBlock, sm, s>>>(il.d, il.n, sp, g.c); break;
+        default: k_fft_zi<MIXED><<<il.grid, kFftBlock, sm, s>>>(il.d, il.n, sp, g.c); break;
+        }
+    }
+}
+
 template <bool MIXED>
 static void fft_all(const LaunchCfg& lc, cudaStream_t s) {
     const FftCfg& f = lc.fft;
-    if (f.z.n) {
-        const size_t sz = fft_smem(f.cz, f.nz, f.kz, MIXED), sy = fft_smem(f.cy, f.ny, f.ny, MIXED),
-                     sx = fft_smem(f.cx, f.nx, f.nx, MIXED);
-        if (f.rz >= 0)
-            launch_fft_reg(0, f.rz, MIXED, f.z, lc.sp, s);
-        else
-            k_fft_zf<MIXED><<<f.z.grid, kFftBlock, sz, s>>>(f.z.d, f.z.n, lc.sp, f.cz);
-        if (f.ry >= 0)
-            launch_fft_reg(1, f.ry, MIXED, f.y, lc.sp, s);
-        else
-            k_fft_y<MIXED, false><<<f.y.grid, kFftBlock, sy, s>>>(f.y.d, f.y.n, lc.sp, f.cy);
-        if (f.rx >= 0)
-            launch_fft_reg(2, f.rx, MIXED, f.x, lc.sp, s);
-        else
-            k_fft_x_infl<MIXED><<<f.x.grid, kFftBlock, sx, s>>>(f.x.d, f.x.n, lc.sp, f.cx);
-        if (f.ry >= 0)
-            launch_fft_reg(3, f.ry, MIXED, f.y, lc.sp, s);
-        else
-            k_fft_y<MIXED, true><<<f.y.grid, kFftBlock, sy, s>>>(f.y.d, f.y.n, lc.sp, f.cy);
-        if (f.rz >= 0)
-            launch_fft_reg(4, f.rz, MIXED, f.z, lc.sp, s);
-        else
-            k_fft_zi<MIXED><<<f.z.grid, kFftBlock, sz, s>>>(f.z.d, f.z.n, lc.sp, f.cz);
-    }
+    fft_pass<MIXED>(0, f.z, lc.sp, s);
+    fft_pass<MIXED>(1, f.y, lc.sp, s);
+    fft_pass<MIXED>(2, f.x, lc.sp, s);
+    fft_pass<MIXED>(3, f.y, lc.sp, s);
+    fft_pass<MIXED>(4, f.z, lc.sp, s);
 }
 
 void launch_pme_fft(const LaunchCfg& lc, cudaStream_t s) {

@@ -224,6 +224,15 @@ ATVB_DEV void twiddle(T2 (&v)[N], const T2* roots, int step) {
 template <bool MIXED>
 __host__ __device__ constexpr int cols() { return MIXED ? 16 : 8; }
 
+// Blocks per SM the compiler must fit: a register budget per thread
+// (measured on the 192^3 mesh: 128 for the x pass, 96 for y (64 in FP32,
+// where a looser budget only buys registers the pass does not need), 80
+// for z; tighter budgets spill and run slower).
+__host__ __device__ constexpr int min_blocks(int threads, int regs) {
+    return 65536 / (threads * regs) < 1 ? 1 : 65536 / (threads * regs) > 16 ? 16
+                                                                          : 65536 / (threads * regs);
+}
+
 template <int N1, int N2>
 struct Shape {
     static constexpr int n = N1 * N2;
@@ -261,7 +270,8 @@ ATVB_DEV void stage_roots(T2* sr, const void* roots, int K) {
 // Lines of K2 = 2 n real points as n complex points; the real spectrum from
 // the even/odd split X[k] = E[k] + e^{-2 pi i k / K2} O[k].
 template <int N1, int N2, bool MIXED>
-__global__ void __launch_bounds__(Shape<N1, N2>::template z_threads<MIXED>())
+__global__ void __launch_bounds__(Shape<N1, N2>::template z_threads<MIXED>(),
+                                  min_blocks(Shape<N1, N2>::template z_threads<MIXED>(), 80))
     k_fftr_zf(const Item* items, int nitems, const SysParams* sp) {
     using T = typename std::conditional<MIXED, float, double>::type;
     using T2 = typename C2<T>::type;
@@ -331,7 +341,9 @@ __global__ void __launch_bounds__(Shape<N1, N2>::template z_threads<MIXED>())
 
 // ---- passes 2 and 4: y forward / inverse -------------------------------------
 template <int N1, int N2, bool MIXED, bool INV>
-__global__ void __launch_bounds__(Shape<N1, N2>::template col_threads<MIXED>())
+__global__ void __launch_bounds__(Shape<N1, N2>::template col_threads<MIXED>(),
+                                  min_blocks(Shape<N1, N2>::template col_threads<MIXED>(),
+                                             MIXED ? 64 : 96))
     k_fftr_y(const Item* items, int nitems, const SysParams* sp) {
     using T = typename std::conditional<MIXED, float, double>::type;
     using T2 = typename C2<T>::type;
@@ -381,7 +393,8 @@ __global__ void __launch_bounds__(Shape<N1, N2>::template col_threads<MIXED>())
 // k1 holds m0 = k1 + N1 e', which is the four-step load of the (N2, N1)
 // split, so the second transform needs one more exchange and no reload.
 template <int N1, int N2, bool MIXED>
-__global__ void __launch_bounds__(Shape<N1, N2>::template col_threads<MIXED>())
+__global__ void __launch_bounds__(Shape<N1, N2>::template col_threads<MIXED>(),
+                                  min_blocks(Shape<N1, N2>::template col_threads<MIXED>(), 128))
     k_fftr_x(const Item* items, int nitems, const SysParams* sp) {
     using T = typename std::conditional<MIXED, float, double>::type;
     using T2 = typename C2<T>::type;
@@ -396,6 +409,7 @@ __global__ void __launch_bounds__(Shape<N1, N2>::template col_threads<MIXED>())
     stage_roots(sr, sp[items[blockIdx.x].sys].fft_root[0], n);
     __syncthreads();
     const int c = threadIdx.x % CW, q = threadIdx.x / CW;
+    int tab_sys = -1; // the system sx_tab was made for (one cell per step)
     for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
         const Item item = items[it];
         const SysParams& P = sp[item.sys];
@@ -415,10 +429,13 @@ __global__ void __launch_bounds__(Shape<N1, N2>::template col_threads<MIXED>())
         // H(m) = exp(-pi^2 m^2 / alpha^2) / m^2 B(m) (pme_influence.h:112-155),
         // the Gaussian and B(m) split per axis: a table along x, one factor
         // per thread for y and z
-        for (int j = threadIdx.x; j < n; j += blockDim.x) {
-            const int h0 = j <= n / 2 ? j : j - n;
-            const double mx = h0 * ilx;
-            sx_tab[j] = bm[j] * exp_neg64(a2pi2 * mx * mx);
+        if (item.sys != tab_sys) { // uniform across the block
+            for (int j = threadIdx.x; j < n; j += blockDim.x) {
+                const int h0 = j <= n / 2 ? j : j - n;
+                const double mx = h0 * ilx;
+                sx_tab[j] = bm[j] * exp_neg64(a2pi2 * mx * mx);
+            }
+            tab_sys = item.sys;
         }
         const int h1 = m1 <= K1 / 2 ? m1 : m1 - K1;
         const int h2 = m2 <= K2 / 2 ? m2 : m2 - K2;
@@ -500,7 +517,8 @@ __global__ void __launch_bounds__(Shape<N1, N2>::template col_threads<MIXED>())
 // Z'[j] = (X[j] + conj X[n-j]) + i (X[j] - conj X[n-j]) e^{2 pi i j / K2},
 // then the complex inverse of length n; z[j] = x[2j] + i x[2j+1].
 template <int N1, int N2, bool MIXED>
-__global__ void __launch_bounds__(Shape<N1, N2>::template z_threads<MIXED>())
+__global__ void __launch_bounds__(Shape<N1, N2>::template z_threads<MIXED>(),
+                                  min_blocks(Shape<N1, N2>::template z_threads<MIXED>(), 80))
     k_fftr_zi(const Item* items, int nitems, const SysParams* sp) {
     using T = typename std::conditional<MIXED, float, double>::type;
     using T2 = typename C2<T>::type;
@@ -549,10 +567,27 @@ __global__ void __launch_bounds__(Shape<N1, N2>::template z_threads<MIXED>())
     }
 }
 
-// Line lengths with a register form, as (index, n, N1, N2): N1, N2 <= 16.
-#define ATVB_FFTR_SIZES(X)                                                              \
-    X(0, 10, 2, 5) X(1, 12, 3, 4) X(2, 15, 3, 5) X(3, 16, 4, 4) X(4, 24, 3, 8)           \
-    X(5, 30, 5, 6) X(6, 48, 6, 8) X(7, 96, 12, 8) X(8, 192, 12, 16)
+// Line lengths with a register form, as (index, n, N1, N2): every
+// 2,3,5,7-smooth n from 8 to 256 that splits into N1, N2 <= 16 (the most
+// balanced split, N2 a power of two on ties), in two halves compiled by
+// separate units.
+#define ATVB_FFTR_SIZES_A(X) \
+    X(0, 8, 2, 4) X(1, 9, 3, 3) X(2, 10, 5, 2) X(3, 12, 3, 4) X(4, 14, 7, 2)           \
+    X(5, 15, 3, 5) X(6, 16, 4, 4) X(7, 18, 3, 6) X(8, 20, 5, 4) X(9, 21, 3, 7)         \
+    X(10, 24, 6, 4) X(11, 25, 5, 5) X(12, 27, 3, 9) X(13, 28, 7, 4) X(14, 30, 5, 6)    \
+    X(15, 32, 4, 8) X(16, 35, 5, 7) X(17, 36, 6, 6) X(18, 40, 5, 8) X(19, 42, 6, 7)    \
+    X(20, 45, 5, 9) X(21, 48, 6, 8) X(22, 49, 7, 7) X(23, 50, 5, 10) X(24, 54, 6, 9)   \
+    X(25, 56, 7, 8) X(26, 60, 6, 10) X(27, 63, 7, 9) X(28, 64, 8, 8)
+#define ATVB_FFTR_SIZES_B(X) \
+    X(29, 70, 7, 10) X(30, 72, 9, 8) X(31, 75, 5, 15) X(32, 80, 10, 8)                 \
+    X(33, 81, 9, 9) X(34, 84, 7, 12) X(35, 90, 9, 10) X(36, 96, 12, 8)                 \
+    X(37, 98, 7, 14) X(38, 100, 10, 10) X(39, 105, 7, 15) X(40, 108, 9, 12)            \
+    X(41, 112, 14, 8) X(42, 120, 10, 12) X(43, 126, 9, 14) X(44, 128, 8, 16)           \
+    X(45, 135, 9, 15) X(46, 140, 10, 14) X(47, 144, 12, 12) X(48, 150, 10, 15)         \
+    X(49, 160, 10, 16) X(50, 168, 12, 14) X(51, 180, 12, 15) X(52, 192, 12, 16)        \
+    X(53, 196, 14, 14) X(54, 210, 14, 15) X(55, 224, 14, 16) X(56, 225, 15, 15)        \
+    X(57, 240, 15, 16) X(58, 256, 16, 16)
+#define ATVB_FFTR_SIZES(X) ATVB_FFTR_SIZES_A(X) ATVB_FFTR_SIZES_B(X)
 
 // One pass of the register form <N1, N2> over the items of `il`.
 template <int N1, int N2, bool MIXED>
@@ -568,16 +603,25 @@ void launch_pass(int pass, const ItemList& il, const SysParams* sp, cudaStream_t
     }
 }
 
-template <bool MIXED>
-void launch_any(int pass, int idx, const ItemList& il, const SysParams* sp, cudaStream_t s) {
-    switch (idx) {
 #define ATVB_FFTR_CASE(i, len, a, b)                                                    \
-    case i: launch_pass<a, b, MIXED>(pass, il, sp, s); break;
-        ATVB_FFTR_SIZES(ATVB_FFTR_CASE)
-#undef ATVB_FFTR_CASE
-    default: break;
+    case i: launch_pass<a, b, MIXED>(pass, il, sp, s); return true;
+
+// The launch of form `idx` if it is in the first (second) half of the table.
+template <bool MIXED>
+bool launch_half_a(int pass, int idx, const ItemList& il, const SysParams* sp, cudaStream_t s) {
+    switch (idx) {
+        ATVB_FFTR_SIZES_A(ATVB_FFTR_CASE)
+    default: return false;
     }
 }
+template <bool MIXED>
+bool launch_half_b(int pass, int idx, const ItemList& il, const SysParams* sp, cudaStream_t s) {
+    switch (idx) {
+        ATVB_FFTR_SIZES_B(ATVB_FFTR_CASE)
+    default: return false;
+    }
+}
+#undef ATVB_FFTR_CASE
 
 } // namespace fftr
 } // namespace atvb

@@ -1,0 +1,12 @@
+// fft_reg32b.cu -- the FP32 (mixed-precision) register forms of the PME line transforms
+// (fft_reg.cuh), second half of the size table.
+#include "fft_reg.cuh"
+
+namespace atvb {
+
+bool fftr_launch_32b(int pass, int idx, const ItemList& il, const SysParams* sp,
+                     cudaStream_t s) {
+    return fftr::launch_half_b<true>(pass, idx, il, sp, s);
+}
+
+} // namespace atvb

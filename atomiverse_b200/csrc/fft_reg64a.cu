@@ -1,11 +1,14 @@
-// fft_reg64.cu -- the FP64 register forms of the PME line transforms
-// (fft_reg.cuh), and the size table the engine consults.
+// fft_reg64a.cu -- the FP64 register forms of the PME line transforms
+// (fft_reg.cuh), first half of the size table; the table lookups and the
+// dispatch over the four units (two precisions x two halves, compiled in
+// parallel).
 #include "fft_reg.cuh"
 
 namespace atvb {
 
-void launch_fft_reg32(int pass, int idx, const ItemList& il, const SysParams* sp,
-                      cudaStream_t s);
+bool fftr_launch_64b(int pass, int idx, const ItemList& il, const SysParams* sp, cudaStream_t s);
+bool fftr_launch_32a(int pass, int idx, const ItemList& il, const SysParams* sp, cudaStream_t s);
+bool fftr_launch_32b(int pass, int idx, const ItemList& il, const SysParams* sp, cudaStream_t s);
 
 int fft_reg_index(int n) {
     switch (n) {
@@ -33,10 +36,12 @@ void launch_fft_reg(int pass, int idx, bool mixed, const ItemList& il, const Sys
                     cudaStream_t s) {
     if (il.n == 0)
         return;
-    if (mixed)
-        launch_fft_reg32(pass, idx, il, sp, s);
-    else
-        fftr::launch_any<false>(pass, idx, il, sp, s);
+    if (mixed) {
+        if (!fftr_launch_32a(pass, idx, il, sp, s))
+            fftr_launch_32b(pass, idx, il, sp, s);
+    } else if (!fftr::launch_half_a<false>(pass, idx, il, sp, s)) {
+        fftr_launch_64b(pass, idx, il, sp, s);
+    }
 }
 
 } // namespace atvb
