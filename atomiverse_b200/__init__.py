@@ -301,6 +301,12 @@ class System:
         """cuda::StopOnNaN: stop integrating at a non-finite state."""
         _abi.check(self.lib.atvb_system_set_stop_on_nan(self._h, 1 if on else 0))
 
+    def set_langevin_ramp(self, T_stop: float, nfirst: int, nlast: int):
+        """FixLangevin's setpoint ramp (fix_langevin.cpp:94-104): from the
+        descriptor's temperature to T_stop over steps [nfirst, nlast]."""
+        _abi.check(self.lib.atvb_system_set_langevin_ramp(self._h, float(T_stop), int(nfirst),
+                                                          int(nlast)))
+
     def set_capacity(self, row_capacity: int = 0, nearq_capacity: int = 0):
         """Pin the neighbour row length / size the near-cutoff queue (0: auto)."""
         _abi.check(self.lib.atvb_system_set_capacity(self._h, int(row_capacity),
@@ -430,6 +436,10 @@ class Batch:
 
     def set_stop_on_nan(self, k: int, on: bool = True):
         _abi.check(self.lib.atvb_batch_set_stop_on_nan(self._h, int(k), 1 if on else 0))
+
+    def set_langevin_ramp(self, k: int, T_stop: float, nfirst: int, nlast: int):
+        _abi.check(self.lib.atvb_batch_set_langevin_ramp(self._h, int(k), float(T_stop),
+                                                         int(nfirst), int(nlast)))
 
     def autotune(self) -> int:
         g = C.c_int32()
@@ -604,12 +614,21 @@ class NoseHoover:
 
 @dataclass
 class FixLangevin:
-    """FixLangevin(T_start, T_stop, damp, dt, seed) (fix_langevin.h)."""
+    """FixLangevin(T_start, T_stop, damp, dt, seed) + set_run_span(nfirst,
+    nlast) (fix_langevin.h; cuda/dynamics/fix_langevin.cuh:69-80): the
+    setpoint ramps linearly from T_start to T_stop over the span (T_stop < 0:
+    constant)."""
     T_start: float
     T_stop: float
     damp: float
     dt: float
     seed: int = 0
+    nfirst: int = 0
+    nlast: int = 0
+
+    def set_run_span(self, nfirst: int, nlast: int):
+        self.nfirst, self.nlast = int(nfirst), int(nlast)
+        return self
 
 
 @dataclass
@@ -795,8 +814,6 @@ class MD:
             if isinstance(th, NoseHoover):
                 kw.update(thermostat=NOSE_HOOVER, temperature=th.T, tau=th.tau)
             elif isinstance(th, FixLangevin):
-                if th.T_stop not in (th.T_start, -1.0):
-                    raise ValueError("temperature ramps are not supported")
                 kw.update(thermostat=LANGEVIN, temperature=th.T_start, damp=th.damp,
                           seed=th.seed)
             else:
@@ -817,6 +834,9 @@ class MD:
                                   deform=(dfm.axis, dfm.strain_rate) if dfm else None)
             if self._criteria:
                 self._system.set_stop_on_nan(True)
+            lang = next((t for t in self._thermostats if isinstance(t, FixLangevin)), None)
+            if lang is not None and lang.T_stop >= 0 and lang.T_stop != lang.T_start:
+                self._system.set_langevin_ramp(lang.T_stop, lang.nfirst, lang.nlast)
         if self._thermo is None:
             sc = self._system.run(frame, n_steps)
         else:

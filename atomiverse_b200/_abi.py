@@ -137,6 +137,23 @@ class RequestResult(C.Structure):
 
 # name -> (restype, argtypes); every function declared in include/atvb.h
 _vp = C.c_void_p
+
+
+class DeviceFrame(C.Structure):
+    """atvb_device_frame: the system's device arrays as a component sees them."""
+    _fields_ = [("n_atoms", C.c_int64)] + [(k, C.c_void_p) for k in (
+        "x", "y", "z", "vx", "vy", "vz", "mass", "charge", "tag", "fx", "fy", "fz",
+        "energy", "virial", "box")]
+
+
+class LaunchCtx(C.Structure):
+    """atvb_launch_ctx: stream, phase, cumulative step, device frame."""
+    _fields_ = [("stream", C.c_void_p), ("phase", C.c_int32), ("reserved", C.c_int32),
+                ("step", C.c_int64), ("frame", DeviceFrame)]
+
+
+# atvb_component_fn: int (*)(void* user, const atvb_launch_ctx* ctx)
+COMPONENT_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(LaunchCtx))
 SIGNATURES = {
     "atvb_abi_version": (C.c_int, []),
     "atvb_last_error": (C.c_char_p, []),
@@ -156,9 +173,14 @@ SIGNATURES = {
                                     C.c_int64, C.POINTER(C.c_int64)]),
     "atvb_system_clear_status": (C.c_int, [_vp]),
     "atvb_system_set_stop_on_nan": (C.c_int, [_vp, C.c_int32]),
+    "atvb_system_set_langevin_ramp": (C.c_int, [_vp, C.c_double, C.c_int64, C.c_int64]),
+    # build / launch / destroy are COMPONENT_FN callbacks (or None)
+    "atvb_system_add_component": (C.c_int, [_vp, C.c_int32, C.c_int32, _vp, _vp, _vp, _vp]),
     "atvb_system_set_capacity": (C.c_int, [_vp, C.c_int32, C.c_int32]),
     "atvb_batch_clear_status": (C.c_int, [_vp, C.c_int32]),
     "atvb_batch_set_stop_on_nan": (C.c_int, [_vp, C.c_int32, C.c_int32]),
+    "atvb_batch_set_langevin_ramp": (C.c_int, [_vp, C.c_int32, C.c_double, C.c_int64,
+                                               C.c_int64]),
     "atvb_system_profile": (C.c_int, [_vp, C.c_int32]),
     "atvb_system_profile_read": (C.c_int, [_vp, C.POINTER(KernelTime), C.c_int32,
                                            C.POINTER(C.c_int32)]),

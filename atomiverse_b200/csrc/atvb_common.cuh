@@ -188,6 +188,10 @@ struct SysParams {
     int thermostat;
     double T, Q, n_dof_kT, tau;
     double lang_g1, lang_g2pre; // -1/(damp ftm2v), sqrt(2 kT/(damp dt mvv2e))/ftm2v
+    // setpoint ramp T0 -> T1 over steps [lang_nfirst, lang_nlast] (none when
+    // lang_nlast <= lang_nfirst); lang_ddm = damp dt mvv2e
+    double lang_T0, lang_T1, lang_ddm;
+    long long lang_nfirst, lang_nlast;
     unsigned int seed;
     int need_virial;
     double e_const; // PME self + net-charge energy
@@ -227,6 +231,11 @@ struct SysParams {
     // per-atom master state (original order)
     double *x, *y, *z, *vx, *vy, *vz, *mass, *q;
     long long* tag;
+    // user components' accumulators (atvb_system_add_component), null when
+    // the system has none: forces in the caller's order (x block, y block,
+    // z block), energy + virial (7 doubles)
+    double* ext_f;
+    double* ext_ev;
     double *xr, *yr, *zr; // positions at the last neighbour build
     // sorted order
     void* pos4;      // FP64: 64-bit fixed-point x, y, z + q (pack_pos64); mixed: int4 fixed-point + float q

@@ -99,6 +99,14 @@ class Slot {
     void* nbr_alloc = nullptr;
 };
 
+// A user component's callbacks at one phase (atvb_system_add_component).
+struct UserComp {
+    int slot, phase, order, seq;
+    atvb_component_fn build, launch, destroy;
+    void* user;
+    bool built;
+};
+
 struct ProfEntry {
     std::string name;
     double ms;
@@ -138,6 +146,9 @@ class Engine {
     void check_halted(int id); // throws ATVB_ERR_PHYSICS if StopOnNaN stopped it
     void clear_status(int id);
     void set_stop_on_nan(int id, bool on);
+    void set_langevin_ramp(int id, double T_stop, long long nfirst, long long nlast);
+    void add_component(int id, int phase, int order, atvb_component_fn build,
+                       atvb_component_fn launch, atvb_component_fn destroy, void* user);
     void set_capacity(int id, int row_cap, int nearq_cap);
     void download(int id, atvb_soa_view* f, atvb_scalars* sc);
     void scalars(int id, atvb_scalars* out);
@@ -178,6 +189,11 @@ class Engine {
     void enqueue_forces(const LaunchCfg& lc, const std::vector<int>& pme,
                         bool profile, bool overlap, bool build_list = false);
     void prof_mark(bool profile, const char* next);
+    atvb_launch_ctx comp_ctx(const UserComp& c, int phase) const;
+    void build_components();
+    void run_components(int phase, bool before);
+    void zero_component_sums();
+    void enqueue_step_components();
     void collect_profile();
     void release_graph();
 
@@ -212,6 +228,8 @@ class Engine {
     size_t prof_used_ = 0;
     std::vector<std::string> prof_seq_;
     std::vector<ProfEntry> prof_acc_;
+    std::vector<UserComp> comps_; // sorted by (phase, order, seq)
+    long long comp_step_ = 0;     // cumulative index of the step being taken
 };
 
 } // namespace atvb

@@ -196,6 +196,23 @@ int atvb_system_clear_status(atvb_system* sys) {
     });
 }
 
+int atvb_system_add_component(atvb_system* sys, int32_t phase, int32_t order,
+                              atvb_component_fn build, atvb_component_fn launch,
+                              atvb_component_fn destroy, void* user) {
+    return guard([&] {
+        need(sys, "sys");
+        sys->eng->add_component(sys->id, phase, order, build, launch, destroy, user);
+    });
+}
+
+int atvb_system_set_langevin_ramp(atvb_system* sys, double T_stop, int64_t nfirst,
+                                  int64_t nlast) {
+    return guard([&] {
+        need(sys, "sys");
+        sys->eng->set_langevin_ramp(sys->id, T_stop, nfirst, nlast);
+    });
+}
+
 int atvb_system_set_stop_on_nan(atvb_system* sys, int32_t on) {
     return guard([&] {
         need(sys, "sys");
@@ -515,6 +532,14 @@ int atvb_batch_clear_status(atvb_batch* b, int32_t index) {
     return guard([&] {
         need(b, "batch");
         b->eng->clear_status(batch_id(b, index));
+    });
+}
+
+int atvb_batch_set_langevin_ramp(atvb_batch* b, int32_t index, double T_stop,
+                                 int64_t nfirst, int64_t nlast) {
+    return guard([&] {
+        need(b, "batch");
+        b->eng->set_langevin_ramp(batch_id(b, index), T_stop, nfirst, nlast);
     });
 }
 

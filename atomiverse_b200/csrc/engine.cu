@@ -475,6 +475,9 @@ Slot::Slot(const atvb_system_desc& d, const DevMem& mem) : desc(d), mem_(mem) {
         hp.lang_g2pre =
             std::sqrt(2.0 * kKB * d.temperature / (d.damp * d.dt * kMvv2e)) /
             kFtm2v;
+        hp.lang_T0 = hp.lang_T1 = d.temperature;
+        hp.lang_ddm = d.damp * d.dt * kMvv2e;
+        hp.lang_nfirst = hp.lang_nlast = 0;
         hp.seed = d.seed;
     } else if (d.thermostat != ATVB_NVE) {
         throw Error(ATVB_ERR_INVALID, "unknown thermostat");
@@ -632,6 +635,12 @@ Engine::Engine(int device) : device_(device) {
 
 Engine::~Engine() {
     cudaSetDevice(device_);
+    cudaStreamSynchronize(stream_);
+    for (auto it = comps_.rbegin(); it != comps_.rend(); ++it) // reverse plan order
+        if (const UserComp& c = *it; c.built && c.destroy && has(c.slot)) {
+            const atvb_launch_ctx ctx = comp_ctx(c, -1);
+            c.destroy(c.user, &ctx); // errors cannot be reported from here
+        }
     release_graph();
     slots_.clear();
     for (void* p : list_allocs_)
@@ -973,6 +982,135 @@ FftCfg Engine::fft_items(const std::vector<int>& pme) {
     return f;
 }
 
+// ---- user components (atvb_system_add_component) ---------------------------
+
+void Engine::add_component(int id, int phase, int order, atvb_component_fn build,
+                           atvb_component_fn launch, atvb_component_fn destroy, void* user) {
+    Slot* s = slot(id);
+    if (phase < ATVB_PHASE_INITIAL_INTEGRATE || phase > ATVB_PHASE_END_OF_STEP)
+        throw Error(ATVB_ERR_INVALID, "add_component: phase must be one of ATVB_PHASE_*");
+    if (!launch)
+        throw Error(ATVB_ERR_INVALID, "add_component: launch is required");
+    CK(cudaSetDevice(device_));
+    if (!s->hp.ext_f) {
+        const size_t n = (size_t)s->hp.n;
+        s->hp.ext_f = (double*)s->dalloc(3 * n * sizeof(double));
+        s->hp.ext_ev = (double*)s->dalloc(7 * sizeof(double));
+        CK(cudaMemsetAsync(s->hp.ext_f, 0, 3 * n * sizeof(double), stream_));
+        CK(cudaMemsetAsync(s->hp.ext_ev, 0, 7 * sizeof(double), stream_));
+        push_params(id);
+        CK(cudaStreamSynchronize(stream_));
+    }
+    UserComp c{id, phase, order, (int)comps_.size(), build, launch, destroy, user, false};
+    comps_.push_back(c);
+    std::stable_sort(comps_.begin(), comps_.end(), [](const UserComp& a, const UserComp& b) {
+        return a.phase != b.phase ? a.phase < b.phase
+                                  : (a.order != b.order ? a.order < b.order : a.seq < b.seq);
+    });
+    release_graph(); // steps of a system with components run as launches
+}
+
+atvb_launch_ctx Engine::comp_ctx(const UserComp& c, int phase) const {
+    const Slot& s = *slots_[c.slot];
+    const SysParams& P = s.hp;
+    atvb_launch_ctx x{};
+    x.stream = (void*)stream_;
+    x.phase = phase;
+    x.step = comp_step_;
+    atvb_device_frame& f = x.frame;
+    f.n_atoms = P.n;
+    f.x = P.x;
+    f.y = P.y;
+    f.z = P.z;
+    f.vx = P.vx;
+    f.vy = P.vy;
+    f.vz = P.vz;
+    f.mass = P.mass;
+    f.charge = P.q;
+    f.tag = reinterpret_cast<const int64_t*>(P.tag);
+    f.fx = P.ext_f;
+    f.fy = P.ext_f + P.n;
+    f.fz = P.ext_f + 2 * (size_t)P.n;
+    f.energy = P.ext_ev;
+    f.virial = P.ext_ev + 1;
+    // the device table entry's cell edges: the cell in force this step
+    f.box = reinterpret_cast<const double*>(reinterpret_cast<const char*>(d_sp_ + c.slot) +
+                                            offsetof(SysParams, L));
+    return x;
+}
+
+// build() of every component not built yet (the frame is on the device),
+// and the step index the next launches report.
+void Engine::build_components() {
+    CK(cudaStreamSynchronize(stream_));
+    for (UserComp& c : comps_) {
+        if (c.built)
+            continue;
+        if (c.build) {
+            const atvb_launch_ctx ctx = comp_ctx(c, -1);
+            const int rc = c.build(c.user, &ctx);
+            if (rc != 0)
+                throw Error(ATVB_ERR_STATE, "component build returned " + std::to_string(rc));
+        }
+        c.built = true;
+    }
+    SysState st;
+    CK(cudaMemcpy(&st, slots_[comps_.front().slot]->hp.st, sizeof(st), cudaMemcpyDeviceToHost));
+    comp_step_ = st.step;
+}
+
+void Engine::run_components(int phase, bool before) {
+    for (const UserComp& c : comps_) {
+        if (c.phase != phase || (c.order < 0) != before)
+            continue;
+        const atvb_launch_ctx ctx = comp_ctx(c, phase);
+        const int rc = c.launch(c.user, &ctx);
+        if (rc != 0)
+            throw Error(ATVB_ERR_STATE, "component launch returned " + std::to_string(rc) +
+                                            " at phase " + std::to_string(phase));
+    }
+}
+
+void Engine::zero_component_sums() {
+    for (const auto& up : slots_)
+        if (up && up->hp.ext_f) {
+            CK(cudaMemsetAsync(up->hp.ext_f, 0, 3 * (size_t)up->hp.n * sizeof(double), stream_));
+            CK(cudaMemsetAsync(up->hp.ext_ev, 0, 7 * sizeof(double), stream_));
+        }
+}
+
+// One step of a system with components: the kernels of enqueue_step as
+// launches, with the components' callbacks at their phases (stage.h:24-36).
+void Engine::enqueue_step_components() {
+    auto phase = [&](int p, auto&& own) {
+        run_components(p, true);
+        own();
+        run_components(p, false);
+    };
+    phase(ATVB_PHASE_INITIAL_INTEGRATE, [&] {
+        launch_integrate_a(lc_, stream_);
+        launch_sys_a(lc_, stream_);
+    });
+    phase(ATVB_PHASE_POST_INTEGRATE, [] {});
+    phase(ATVB_PHASE_PRE_EXCHANGE, [] {});
+    phase(ATVB_PHASE_PRE_NEIGHBOR, [] {});
+    phase(ATVB_PHASE_NEIGHBOR, [&] {
+        launch_sort_cells(lc_, stream_);
+        launch_build_list(lc_, stream_);
+    });
+    phase(ATVB_PHASE_PRE_FORCE, [&] { zero_component_sums(); });
+    phase(ATVB_PHASE_FORCE, [&] { enqueue_forces(lc_, pme_slots_, false, true, false); });
+    phase(ATVB_PHASE_POST_FORCE, [] {});
+    phase(ATVB_PHASE_FINAL_INTEGRATE, [&] { launch_integrate_b(lc_, stream_); });
+    phase(ATVB_PHASE_END_OF_STEP, [&] {
+        launch_sys_b(lc_, stream_);
+        if (lc_.any_snap)
+            launch_snapshots(lc_, stream_);
+    });
+    CK(cudaGetLastError());
+    ++comp_step_;
+}
+
 // Kernel launches of one step.
 int64_t Engine::kernels_per_step() const {
     int64_t k = 0;
@@ -1158,7 +1296,10 @@ void Engine::run_pieces(int n, double* step_ms, double* total_ms) {
         if (!timed) {
             run_steps(k);
         } else {
-            ensure_graph();
+            if (comps_.empty())
+                ensure_graph();
+            else
+                build_components();
             while ((int)ev.size() < k + 1) {
                 cudaEvent_t e;
                 CK(cudaEventCreate(&e));
@@ -1166,7 +1307,10 @@ void Engine::run_pieces(int n, double* step_ms, double* total_ms) {
             }
             CK(cudaEventRecord(ev[0], stream_));
             for (int j = 0; j < k; ++j) {
-                CK(cudaGraphLaunch(gexec_, stream_));
+                if (comps_.empty())
+                    CK(cudaGraphLaunch(gexec_, stream_));
+                else
+                    enqueue_step_components();
                 CK(cudaEventRecord(ev[j + 1], stream_));
             }
             CK(cudaEventSynchronize(ev[k]));
@@ -1208,6 +1352,12 @@ void Engine::ensure_graph() {
 }
 
 void Engine::run_steps(int n) {
+    if (!comps_.empty()) {
+        build_components();
+        for (int k = 0; k < n; ++k)
+            enqueue_step_components();
+        return;
+    }
     if (profiling_) {
         for (int k = 0; k < n; ++k) {
             enqueue_step(true);
@@ -1253,7 +1403,20 @@ void Engine::compute_forces() {
     CK(cudaSetDevice(device_));
     ensure_ready();
     sized_rebuild(lc_);
-    enqueue_forces(lc_, pme_slots_, false, false);
+    if (!comps_.empty()) {
+        // Verlet::setup: the force phases of the components too
+        build_components();
+        run_components(ATVB_PHASE_PRE_FORCE, true);
+        zero_component_sums();
+        run_components(ATVB_PHASE_PRE_FORCE, false);
+        run_components(ATVB_PHASE_FORCE, true);
+        enqueue_forces(lc_, pme_slots_, false, false);
+        run_components(ATVB_PHASE_FORCE, false);
+        run_components(ATVB_PHASE_POST_FORCE, true);
+        run_components(ATVB_PHASE_POST_FORCE, false);
+    } else {
+        enqueue_forces(lc_, pme_slots_, false, false);
+    }
     launch_force_combine(lc_, stream_);
     launch_sys_energy(lc_, stream_);
     launch_npt_prep(lc_, stream_);
@@ -1562,6 +1725,26 @@ void Engine::clear_status(int id) {
 }
 
 // cuda::StopOnNaN attached to (or detached from) one system.
+// FixLangevin(T_start, T_stop, ...).set_run_span(nfirst, nlast)
+// (fix_langevin.cpp:94-104): the setpoint moves linearly from the
+// descriptor's temperature to T_stop over the steps [nfirst, nlast] and holds
+// outside it; T_stop < 0 or nlast <= nfirst: the constant setpoint.
+void Engine::set_langevin_ramp(int id, double T_stop, long long nfirst, long long nlast) {
+    Slot* s = slot(id);
+    if (s->hp.thermostat != kLangevin)
+        throw Error(ATVB_ERR_INVALID, "set_langevin_ramp: the system has no FixLangevin");
+    if (T_stop >= 0.0 && nlast > nfirst) {
+        s->hp.lang_T1 = T_stop;
+        s->hp.lang_nfirst = nfirst;
+        s->hp.lang_nlast = nlast;
+    } else {
+        s->hp.lang_T1 = s->hp.lang_T0;
+        s->hp.lang_nfirst = s->hp.lang_nlast = 0;
+    }
+    push_params(id);
+    CK(cudaStreamSynchronize(stream_));
+}
+
 void Engine::set_stop_on_nan(int id, bool on) {
     Slot* s = slot(id);
     s->hp.stop_on_nan = on ? 1 : 0;

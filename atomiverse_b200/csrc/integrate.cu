@@ -250,6 +250,19 @@ __global__ void k_sys_a(const int* sys_list, int nsys, const SysParams* sp) {
     }
 }
 
+// sqrt(2 kB T / (damp dt mvv2e)) / ftm2v at the setpoint of `step`: the
+// linear ramp of fix_langevin.cpp:94-104 (delta clamped to [0, 1]), each
+// operation rounded separately, as the host and the reference compute it.
+ATVB_DEV double lang_g2pre(const SysParams& P, long long step) {
+    if (P.lang_nlast <= P.lang_nfirst)
+        return P.lang_g2pre;
+    double delta = __ddiv_rn((double)(step - P.lang_nfirst),
+                             (double)(P.lang_nlast - P.lang_nfirst));
+    delta = delta < 0.0 ? 0.0 : (delta > 1.0 ? 1.0 : delta);
+    const double T = __dadd_rn(P.lang_T0, __dmul_rn(delta, __dsub_rn(P.lang_T1, P.lang_T0)));
+    return __ddiv_rn(__dsqrt_rn(__ddiv_rn(__dmul_rn(2.0 * kKB, T), P.lang_ddm)), kFtm2v);
+}
+
 // Final half: initial-half thermostat scale, Langevin force, kick, KE.
 __global__ void __launch_bounds__(kChunk)
     k_integrate_b(const Item* items, int nitems, const SysParams* sp) {
@@ -276,9 +289,15 @@ __global__ void __launch_bounds__(kChunk)
                 f.x = __dadd_rn(f.x, g.x);
                 f.y = __dadd_rn(f.y, g.y);
                 f.z = __dadd_rn(f.z, g.z);
-                if (P.thermostat != kLangevin)
-                    P.f4[r] = f;
             }
+            if (P.ext_f) {
+                // the user components' forces (atvb_system_add_component)
+                f.x = __dadd_rn(f.x, P.ext_f[i]);
+                f.y = __dadd_rn(f.y, P.ext_f[P.n + i]);
+                f.z = __dadd_rn(f.z, P.ext_f[2 * P.n + i]);
+            }
+            if ((P.has_pme || P.ext_f) && P.thermostat != kLangevin)
+                P.f4[r] = f;
             if (P.thermostat == kLangevin) {
                 const unsigned long long base =
                     (unsigned long long)P.seed * 0x9E3779B97F4A7C15ull +
@@ -287,7 +306,7 @@ __global__ void __launch_bounds__(kChunk)
                                          0xD6E8FEB86659FD93ull,
                               false, 0.0};
                 const double g1 = -m * P.lang_g1;
-                const double g2 = P.lang_g2pre * sqrt(m);
+                const double g2 = lang_g2pre(P, P.st->step) * sqrt(m);
                 const double rx = g.next(), ry = g.next(), rz = g.next();
                 f.x += g1 * v[0] + g2 * rx;
                 f.y += g1 * v[1] + g2 * ry;
@@ -328,6 +347,11 @@ ATVB_DEV void finish_energy(const SysParams& P, SysState* st) {
     st->energy = st->e_lj + st->e_coul + st->e_recip + st->e_const;
     for (int k = 0; k < 6; ++k)
         st->virial[k] = fix_to_d(st->acc[kAccVir + k]);
+    if (P.ext_ev) { // the user components' energy and virial
+        st->energy += P.ext_ev[0];
+        for (int k = 0; k < 6; ++k)
+            st->virial[k] += P.ext_ev[1 + k];
+    }
     st->acc[kAccELJ] = st->acc[kAccECoul] = st->acc[kAccERecip] = 0ull;
     for (int k = 0; k < 6; ++k)
         st->acc[kAccVir + k] = 0ull;
@@ -805,14 +829,21 @@ __global__ void k_force_combine(const Item* items, int nitems, const SysParams* 
         const Item item = items[it];
         const SysParams& P = sp[item.sys];
         const int i = item.begin + threadIdx.x;
-        if (!P.has_pme || i >= P.n)
+        if (!(P.has_pme || P.ext_f) || i >= P.n)
             continue;
         const int r = P.rank[i];
         double4 f = P.f4[r];
-        const double4 g = P.fp4[r];
-        f.x = __dadd_rn(f.x, g.x);
-        f.y = __dadd_rn(f.y, g.y);
-        f.z = __dadd_rn(f.z, g.z);
+        if (P.has_pme) {
+            const double4 g = P.fp4[r];
+            f.x = __dadd_rn(f.x, g.x);
+            f.y = __dadd_rn(f.y, g.y);
+            f.z = __dadd_rn(f.z, g.z);
+        }
+        if (P.ext_f) {
+            f.x = __dadd_rn(f.x, P.ext_f[i]);
+            f.y = __dadd_rn(f.y, P.ext_f[P.n + i]);
+            f.z = __dadd_rn(f.z, P.ext_f[2 * P.n + i]);
+        }
         P.f4[r] = f;
     }
 }

@@ -15,14 +15,20 @@
 // set_thermostat and the continuable run(frame, n_steps)
 // (include/atomiverse/cuda/dynamics/md.cuh:118-385).  Errors surface as
 // std::invalid_argument (bad configuration) or std::runtime_error (CUDA),
-// as in the reference.  The components only record their parameters: the
-// device step is one fused, graph-captured sequence built by the library.
+// as in the reference.  The built-in components only record their
+// parameters: the device step is one fused, graph-captured sequence built by
+// the library.  User components (class Component, registered with
+// MD::on(phase).add(c, order), include/atomiverse/cuda/component/
+// component.cuh:94-203 and cuda/dynamics/md.cuh:115-126) run their own
+// launches at their phase of every step on the library's stream.
 #pragma once
 
 #include <atvb.h>
 
+#include <algorithm>
 #include <array>
 #include <cstdint>
+#include <memory>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -148,6 +154,77 @@ struct KSpacePME {
     }
 };
 
+// ---- user components --------------------------------------------------------
+
+namespace md {
+/// md::Phase (include/atomiverse/core/stage.h:24-36): the phases of a step.
+enum class Phase {
+    initial_integrate,
+    post_integrate,
+    pre_exchange,
+    pre_neighbor,
+    neighbor,
+    pre_force,
+    force,
+    post_force,
+    final_integrate,
+    end_of_step,
+    COUNT
+};
+} // namespace md
+
+/// A component's default phase slot (include/atomiverse/core/binding.h).
+struct DefaultBinding {
+    md::Phase phase;
+    int order;
+};
+
+/// What build / launch / destroy receive (component.cuh:22-49).  `stream` is
+/// the library's cudaStream_t (the reference's cuda::Context streams);
+/// `frame` the device arrays of the system (atvb_device_frame: positions,
+/// velocities, masses, charges, tags in the caller's atom order, and the
+/// components' own force / energy / virial accumulators).
+struct BuildContext {
+    void* stream;
+    const atvb_device_frame& frame;
+};
+struct LaunchContext {
+    void* stream;
+    const atvb_device_frame& frame;
+    int stage;    ///< the phase being walked (compare with at())
+    int64_t step; ///< cumulative step index (0-based)
+    template <typename PhaseEnum>
+    bool at(PhaseEnum phase) const {
+        return stage == static_cast<int>(phase);
+    }
+};
+struct DestroyContext {
+    void* stream;
+    const atvb_device_frame& frame;
+};
+
+/// cuda::Component (include/atomiverse/cuda/component/component.cuh:94-203):
+/// build once, launch every step at its phase (enqueue device work on
+/// ctx.stream only: no allocation, no synchronisation), destroy at the end.
+/// Forces, energy and virial a component adds to frame.fx / fy / fz /
+/// energy / virial join the step's totals.
+class Component {
+  public:
+    virtual ~Component() = default;
+    virtual std::string name() const = 0;
+    virtual bool requires_system_stress() const { return false; }
+    virtual bool provides_system_stress() const { return false; }
+    virtual bool provides_energy() const { return false; }
+    virtual bool provides_force() const { return false; }
+    /// Plan-level verdict, called once before the system is built: true iff
+    /// some part of the simulation consumes the virial (component.cuh:131).
+    virtual void set_stress_required(bool /*required*/) {}
+    virtual std::vector<DefaultBinding> default_bindings() const { return {}; }
+    virtual void build(const BuildContext& /*ctx*/) {}
+    virtual void launch(const LaunchContext& ctx) = 0;
+    virtual void destroy(const DestroyContext& /*ctx*/) {}
+};
+
 namespace md {
 struct VelocityVerlet {
     double dt;
@@ -157,11 +234,20 @@ struct NoseHoover {
     double T, tau, dt;
     NoseHoover(double T_, double tau_, double dt_) : T(T_), tau(tau_), dt(dt_) {}
 };
+/// FixLangevin (cuda/dynamics/fix_langevin.cuh:69-80): T_stop < 0 is the
+/// constant setpoint; set_run_span(nfirst, nlast) ramps it linearly from
+/// T_start to T_stop over those cumulative steps (fix_langevin.cpp:94-104).
 struct FixLangevin {
     double T_start, T_stop, damp, dt;
     uint32_t seed;
+    int64_t nfirst = 0, nlast = 0;
     FixLangevin(double t0, double t1, double damp_, double dt_, uint32_t seed_)
         : T_start(t0), T_stop(t1 < 0 ? t0 : t1), damp(damp_), dt(dt_), seed(seed_) {}
+    FixLangevin& set_run_span(int64_t first, int64_t last) {
+        nfirst = first;
+        nlast = last;
+        return *this;
+    }
 };
 /// md::NVELimit(dt, xmax) (cuda/dynamics/nve_limit.cuh): velocity Verlet
 /// with each half kick's speed capped at xmax / dt.  An integrator.
@@ -243,6 +329,39 @@ class MD {
     }
     MD(const MD&) = delete;
     MD& operator=(const MD&) = delete;
+
+    /// One phase of the plan: on(phase).add(component, order)
+    /// (md.cuh:17,70,115-126).  Components of a phase run by ascending
+    /// order; order < 0 before the library's own work of that phase.
+    class PhaseSlot {
+      public:
+        template <typename C>
+        MD& add(C&& c, int order = 0) {
+            return md_.add_component(std::make_shared<std::decay_t<C>>(std::forward<C>(c)),
+                                     {{phase_, order}});
+        }
+
+      private:
+        friend class MD;
+        PhaseSlot(MD& m, Phase p) : md_(m), phase_(p) {}
+        MD& md_;
+        Phase phase_;
+    };
+    PhaseSlot on(Phase p) { return PhaseSlot(*this, p); }
+
+    /// add(component) at its default_bindings() (the path of set_observer).
+    template <typename C>
+    MD& add(C&& c) {
+        auto sp = std::make_shared<std::decay_t<C>>(std::forward<C>(c));
+        const std::vector<DefaultBinding> b = sp->default_bindings();
+        if (b.empty())
+            throw std::invalid_argument("MD::add: component " + sp->name() +
+                                        " has no default binding; use on(phase).add");
+        std::vector<std::pair<Phase, int>> at;
+        for (const DefaultBinding& d : b)
+            at.emplace_back(d.phase, d.order);
+        return add_component(std::move(sp), at);
+    }
 
     MD& set_neighbor(const NeighborList& nl) {
         d_.nl_cutoff = nl.cutoff;
@@ -327,8 +446,9 @@ class MD {
         return *this;
     }
     MD& set_thermostat(const FixLangevin& t) {
-        if (t.T_stop != t.T_start)
-            throw std::invalid_argument("FixLangevin: temperature ramps are not supported");
+        ramp_T_stop_ = t.T_stop;
+        ramp_nfirst_ = t.nfirst;
+        ramp_nlast_ = t.nlast;
         d_.thermostat = ATVB_LANGEVIN;
         d_.temperature = t.T_start;
         d_.damp = t.damp;
@@ -479,6 +599,55 @@ class MD {
         }
     }
 
+    // a component and its slots; the first slot carries build and destroy
+    struct Bound {
+        std::shared_ptr<Component> c;
+        bool first;
+    };
+
+    static int comp_build(void* u, const atvb_launch_ctx* x) {
+        try {
+            static_cast<Bound*>(u)->c->build(BuildContext{x->stream, x->frame});
+            return 0;
+        } catch (...) {
+            return 1;
+        }
+    }
+    static int comp_launch(void* u, const atvb_launch_ctx* x) {
+        try {
+            static_cast<Bound*>(u)->c->launch(LaunchContext{x->stream, x->frame, x->phase, x->step});
+            return 0;
+        } catch (...) {
+            return 1;
+        }
+    }
+    static int comp_destroy(void* u, const atvb_launch_ctx* x) {
+        try {
+            static_cast<Bound*>(u)->c->destroy(DestroyContext{x->stream, x->frame});
+            return 0;
+        } catch (...) {
+            return 1;
+        }
+    }
+
+    MD& add_component(std::shared_ptr<Component> c, const std::vector<std::pair<Phase, int>>& at) {
+        for (size_t k = 0; k < at.size(); ++k) {
+            if (at[k].first == Phase::COUNT)
+                throw std::invalid_argument("MD::on: not a phase");
+            bound_.push_back(std::unique_ptr<Bound>(new Bound{c, k == 0}));
+            slots_.emplace_back(bound_.back().get(), at[k]);
+            if (sys_) // the system exists: the component joins from the next call
+                register_slot(slots_.back());
+        }
+        return *this;
+    }
+
+    void register_slot(const std::pair<Bound*, std::pair<Phase, int>>& s) {
+        check(atvb_system_add_component(sys_, (int32_t)s.second.first, s.second.second,
+                                        s.first->first ? comp_build : nullptr, comp_launch,
+                                        s.first->first ? comp_destroy : nullptr, s.first));
+    }
+
     void ensure_system(Frame& frame) {
         if (!sys_)
             create_system(frame);
@@ -498,6 +667,15 @@ class MD {
             d_.box[0] = frame.box[0];
             d_.box[4] = frame.box[1];
             d_.box[8] = frame.box[2];
+            // install_defaults: the plan-level stress verdict, to every
+            // component and to the library's own evaluators
+            bool needs = d_.stress_required != 0 || have_npt_ || have_baro_;
+            for (const auto& b : bound_)
+                needs = needs || b->c->requires_system_stress();
+            for (const auto& b : bound_)
+                if (b->first)
+                    b->c->set_stress_required(needs);
+            d_.stress_required = needs ? 1 : 0;
             check(atvb_system_create(ctx_, &d_, &sys_));
             if (have_npt_)
                 check(atvb_system_set_npt(sys_, &npt_));
@@ -508,6 +686,9 @@ class MD {
                 check(atvb_system_set_nve_limit(sys_, vlimit_));
             if (deform_axis_ >= 0)
                 check(atvb_system_set_deform(sys_, deform_axis_, deform_rate_));
+            if (d_.thermostat == ATVB_LANGEVIN && ramp_T_stop_ != d_.temperature)
+                check(atvb_system_set_langevin_ramp(sys_, ramp_T_stop_, ramp_nfirst_,
+                                                    ramp_nlast_));
             if (!lj_coeffs_.empty()) {
                 std::vector<int32_t> ti, tj;
                 std::vector<double> e, sg;
@@ -533,12 +714,18 @@ class MD {
             }
             if (snap_every_ > 0)
                 check(atvb_system_set_snapshots(sys_, snap_every_, snap_depth_));
+            for (const auto& s : slots_)
+                register_slot(s);
         }
     }
 
     atvb_ctx* ctx_ = nullptr;
     atvb_system* sys_ = nullptr;
     atvb_system_desc d_;
+    double ramp_T_stop_ = -1.0;
+    int64_t ramp_nfirst_ = 0, ramp_nlast_ = 0;
+    std::vector<std::unique_ptr<Bound>> bound_;
+    std::vector<std::pair<Bound*, std::pair<Phase, int>>> slots_;
     int precision_;
     bool have_nl_ = false, have_pair_ = false, have_integrator_ = false;
     std::vector<LJTypeCoeff> lj_coeffs_;

@@ -194,6 +194,78 @@ int atvb_system_download(atvb_system* sys, atvb_soa_view* frame,
 int atvb_system_scalars(atvb_system* sys, atvb_scalars* scalars);
 int atvb_system_run(atvb_system* sys, atvb_soa_view* frame, int32_t n_steps,
                     atvb_scalars* scalars);
+/* ---- user components (include/atomiverse/cuda/component/component.cuh:94-203,
+ * registration on(phase).add(c, order) of cuda/dynamics/md.cuh:115-126) ----
+ * The phases of one step, in order (include/atomiverse/core/stage.h:24-36). */
+#define ATVB_PHASE_INITIAL_INTEGRATE 0
+#define ATVB_PHASE_POST_INTEGRATE 1
+#define ATVB_PHASE_PRE_EXCHANGE 2
+#define ATVB_PHASE_PRE_NEIGHBOR 3
+#define ATVB_PHASE_NEIGHBOR 4
+#define ATVB_PHASE_PRE_FORCE 5
+#define ATVB_PHASE_FORCE 6
+#define ATVB_PHASE_POST_FORCE 7
+#define ATVB_PHASE_FINAL_INTEGRATE 8
+#define ATVB_PHASE_END_OF_STEP 9
+
+/* The system as a component sees it: device arrays in the caller's atom
+ * order (the order of atvb_soa_view).  Positions are wrapped into [0, L).
+ * fx/fy/fz, energy (1 double) and virial (6 doubles, xx yy zz xy xz yz, eV)
+ * are the components' own accumulators: the library zeroes them before the
+ * pre_force phase of every step (and of a force pass), adds the forces into
+ * the step's forces at final_integrate and the energy and virial into the
+ * step's scalars at end_of_step; downloads report the sums. */
+typedef struct atvb_device_frame {
+    int64_t n_atoms;
+    const double* x;
+    const double* y;
+    const double* z;
+    double* vx;
+    double* vy;
+    double* vz;
+    const double* mass;
+    const double* charge;
+    const int64_t* tag;
+    double* fx;
+    double* fy;
+    double* fz;
+    double* energy;
+    double* virial;
+    const double* box; /* device: the 3 cell edges [A] in force this step */
+} atvb_device_frame;
+
+/* What a component's callbacks get: the library's stream (a cudaStream_t),
+ * the phase (-1 for build and destroy), the cumulative step index of the
+ * step being taken (0-based, continued across calls; a force pass reports
+ * the index of the next step) and the frame. */
+typedef struct atvb_launch_ctx {
+    void* stream;
+    int32_t phase;
+    int32_t reserved;
+    int64_t step;
+    atvb_device_frame frame;
+} atvb_launch_ctx;
+
+/* A component callback; a non-zero return fails the library call that made
+ * it (ATVB_ERR_STATE). */
+typedef int (*atvb_component_fn)(void* user, const atvb_launch_ctx* ctx);
+
+/* cuda::Component build / launch / destroy registered at `phase`, `order`.
+ * build (may be NULL) runs once, on the first force pass or step call after
+ * registration, when the frame is on the device: it may allocate and
+ * synchronise.  launch runs at its phase of every step, and at the
+ * pre_force, force and post_force phases of atvb_system_compute_forces
+ * (Verlet::setup), on the calling thread; it must only enqueue device work
+ * on ctx->stream (no allocation, no synchronisation).  Within a phase
+ * components run by ascending order (ties: registration order); order < 0
+ * runs before the library's own work of that phase, order >= 0 after it.
+ * destroy (may be NULL) runs at atvb_system_destroy.  A system with
+ * components runs its steps as individual launches instead of one CUDA
+ * graph per step. */
+int atvb_system_add_component(atvb_system* sys, int32_t phase, int32_t order,
+                              atvb_component_fn build, atvb_component_fn launch,
+                              atvb_component_fn destroy, void* user);
+
 /* Energy history ring: 3 doubles per step (potential, kinetic, step).
  * Writes up to max_steps most recent entries, oldest first; *count gets the
  * number written. */
@@ -292,6 +364,15 @@ int atvb_system_clear_status(atvb_system* sys);
  * default (the reference stops only with the criterion attached); the
  * ATVB_STATUS_NONFINITE bit is raised either way. */
 int atvb_system_set_stop_on_nan(atvb_system* sys, int32_t on);
+/* FixLangevin(T_start, T_stop, damp, dt, seed).set_run_span(nfirst, nlast)
+ * (src/cpu/dynamics/fix_langevin.cpp:94-104,
+ * include/atomiverse/cuda/dynamics/fix_langevin.cuh:69-80): the Langevin
+ * setpoint moves linearly from the descriptor's temperature (T_start) to
+ * T_stop over the cumulative steps [nfirst, nlast] and holds at either end
+ * outside it.  T_stop < 0 or nlast <= nfirst: the constant setpoint.
+ * ATVB_ERR_INVALID unless the system's thermostat is ATVB_LANGEVIN. */
+int atvb_system_set_langevin_ramp(atvb_system* sys, double T_stop, int64_t nfirst,
+                                  int64_t nlast);
 /* Capacity overrides (0 = automatic sizing).  row_capacity pins the
  * neighbour row length (no automatic growth: a build that needs longer rows
  * fails with ATVB_ERR_OVERFLOW outside a step call, and raises
@@ -322,6 +403,9 @@ int atvb_batch_download(atvb_batch* b, int32_t index, atvb_soa_view* frame,
 /* atvb_system_clear_status / _set_stop_on_nan for system `index`. */
 int atvb_batch_clear_status(atvb_batch* b, int32_t index);
 int atvb_batch_set_stop_on_nan(atvb_batch* b, int32_t index, int32_t on);
+/* atvb_system_set_langevin_ramp for system `index`. */
+int atvb_batch_set_langevin_ramp(atvb_batch* b, int32_t index, double T_stop,
+                                 int64_t nfirst, int64_t nlast);
 /* atvb_system_set_lj_types / _set_special_bonds for system `index` of a
  * batch, before that system's first upload. */
 /* atvb_system_set_npt for system `index` of a batch, before its first upload. */

@@ -65,6 +65,12 @@ class OrcDesc(C.Structure):
         ("damp", C.c_double),
         ("seed", C.c_uint32),
         ("need_virial", C.c_int),
+        ("T_stop", C.c_double),
+        ("lang_nfirst", C.c_int64),
+        ("lang_nlast", C.c_int64),
+        ("wall_axis", C.c_int),
+        ("wall_pos", C.c_double),
+        ("wall_k", C.c_double),
     ]
 
 
@@ -178,6 +184,12 @@ def make_desc(n, L, **kw) -> OrcDesc:
     d.damp = kw.get("damp", 100.0)
     d.seed = int(kw.get("seed", 0))
     d.need_virial = int(kw.get("need_virial", 1))
+    d.T_stop = kw.get("T_stop", d.T)
+    d.lang_nfirst = int(kw.get("lang_nfirst", 0))
+    d.lang_nlast = int(kw.get("lang_nlast", 0))
+    d.wall_axis = int(kw.get("wall_axis", -1))
+    d.wall_pos = kw.get("wall_pos", 0.0)
+    d.wall_k = kw.get("wall_k", 0.0)
     return d
 
 

@@ -94,7 +94,7 @@ struct orc_sys {
     int32_t* nbr;
     int64_t nbr_cap;
     /* scalars */
-    double e_lj, e_coul, e_recip, e_const, ke, vir[6];
+    double e_lj, e_coul, e_recip, e_const, e_ext, ke, vir[6];
     double xi, Q;
     int64_t step;
     int n_dof;
@@ -229,7 +229,7 @@ void orc_get_state(const orc_sys* s, double* x, double* y, double* z,
 }
 
 void orc_scalars(const orc_sys* s, double* out) {
-    out[0] = s->e_lj + s->e_coul + s->e_recip + s->e_const;
+    out[0] = s->e_lj + s->e_coul + s->e_recip + s->e_const + s->e_ext;
     out[1] = s->e_lj;
     out[2] = s->e_coul;
     out[3] = s->e_recip;
@@ -1232,18 +1232,35 @@ void orc_ewald_recip(int n, const double* x, const double* y, const double* z,
 /* integrators and thermostats                                         */
 /* ------------------------------------------------------------------ */
 
+/* the test-only harmonic wall (orc_desc.wall_*) */
+static void wall_forces(orc_sys* s) {
+    double* c = s->d.wall_axis == 0 ? s->x : s->d.wall_axis == 1 ? s->y : s->z;
+    double* f = s->d.wall_axis == 0 ? s->fx : s->d.wall_axis == 1 ? s->fy : s->fz;
+    double e = 0.0;
+    for (int i = 0; i < s->n; ++i) {
+        const double d = c[i] - s->d.wall_pos;
+        if (d > 0.0) {
+            f[i] += -2.0 * s->d.wall_k * d;
+            e += s->d.wall_k * d * d;
+        }
+    }
+    s->e_ext = e;
+}
+
 void orc_compute_forces(orc_sys* s) {
     const int n = s->n;
     memset(s->fx, 0, sizeof(double) * (size_t)n);
     memset(s->fy, 0, sizeof(double) * (size_t)n);
     memset(s->fz, 0, sizeof(double) * (size_t)n);
-    s->e_lj = s->e_coul = s->e_recip = s->e_const = 0.0;
+    s->e_lj = s->e_coul = s->e_recip = s->e_const = s->e_ext = 0.0;
     for (int k = 0; k < 6; ++k)
         s->vir[k] = 0.0;
     if (s->d.has_lj || s->d.has_coul)
         pair_forces(s);
     if (s->d.has_pme)
         pme_forces(s);
+    if (s->d.wall_axis >= 0 && s->d.wall_axis < 3)
+        wall_forces(s);
 }
 
 /* init.cpp:29-45 */
@@ -1314,9 +1331,16 @@ void orc_gauss3(uint32_t seed, int64_t step, int64_t tag, double* out3) {
     out3[2] = gs_next(&g);
 }
 
-/* fix_langevin.cpp:79-155 (constant setpoint) */
+/* fix_langevin.cpp:79-155; the setpoint follows the linear ramp of
+ * :94-104, delta = (step - nfirst) / (nlast - nfirst) clamped to [0, 1] */
 static void langevin(orc_sys* s) {
-    const double T = s->d.T;
+    double T = s->d.T;
+    if (s->d.lang_nlast > s->d.lang_nfirst) {
+        double delta = (double)(s->step - s->d.lang_nfirst) /
+                       (double)(s->d.lang_nlast - s->d.lang_nfirst);
+        delta = delta < 0.0 ? 0.0 : (delta > 1.0 ? 1.0 : delta);
+        T = s->d.T + delta * (s->d.T_stop - s->d.T);
+    }
     const double inv_damp_ftm2v = 1.0 / (s->d.damp * ORC_FTM2V);
     const double g2pre =
         sqrt(2.0 * ORC_KB * T / (s->d.damp * s->d.dt * ORC_MVV2E)) /
@@ -1578,7 +1602,7 @@ static void npt_propagate(orc_sys* s) {
 
 /* extended_hamiltonian (nose_hoover_npt.cpp:770-805) */
 static double npt_hamiltonian(const orc_sys* s) {
-    double H = s->ke + (s->e_lj + s->e_coul + s->e_recip + s->e_const);
+    double H = s->ke + (s->e_lj + s->e_coul + s->e_recip + s->e_const + s->e_ext);
     const double Wa = s->W / 3.0;
     for (int a = 0; a < 3; ++a)
         if (s->np.couple[a])
@@ -1719,7 +1743,7 @@ int orc_run(orc_sys* s, int n_steps, double* hist) {
             npt_step(s);
             ++rebuilds;
             if (hist) {
-                hist[2 * st] = s->e_lj + s->e_coul + s->e_recip + s->e_const;
+                hist[2 * st] = s->e_lj + s->e_coul + s->e_recip + s->e_const + s->e_ext;
                 hist[2 * st + 1] = s->ke;
             }
             s->step++;
@@ -1779,7 +1803,7 @@ int orc_run(orc_sys* s, int n_steps, double* hist) {
         if (s->baro_on)
             berendsen(s);
         if (hist) {
-            hist[2 * st] = s->e_lj + s->e_coul + s->e_recip + s->e_const;
+            hist[2 * st] = s->e_lj + s->e_coul + s->e_recip + s->e_const + s->e_ext;
             hist[2 * st + 1] = s->ke;
         }
         s->step++;

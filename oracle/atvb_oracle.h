@@ -57,6 +57,15 @@ typedef struct orc_desc {
     double T, tau, damp;   /* K, fs (NH tau), fs (Langevin damp) */
     uint32_t seed;         /* Langevin seed */
     int need_virial;
+    /* Langevin setpoint ramp T -> T_stop over steps [lang_nfirst,
+     * lang_nlast] (fix_langevin.cpp:94-104; no ramp when nlast <= nfirst) */
+    double T_stop;
+    int64_t lang_nfirst, lang_nlast;
+    /* test-only external term, the same one a user component adds on the
+     * GPU: a harmonic wall E = k d^2, F = -2 k d along `wall_axis` for
+     * d = coordinate - wall_pos > 0 (wall_axis < 0: none) */
+    int wall_axis;
+    double wall_pos, wall_k;
 } orc_desc;
 
 typedef struct orc_sys orc_sys;

@@ -54,7 +54,11 @@ def oracle_system(orc, desc: dict, frame: dict, **over):
               dt=d.get("dt", 1.0), thermostat=d.get("thermostat", 0),
               T=d.get("temperature", 0.0), tau=d.get("tau", 100.0),
               damp=d.get("damp", 100.0), seed=d.get("seed", 0),
-              need_virial=d.get("stress_required", 1))
+              need_virial=d.get("stress_required", 1),
+              T_stop=d.get("lang_T_stop", d.get("temperature", 0.0)),
+              lang_nfirst=d.get("lang_nfirst", 0), lang_nlast=d.get("lang_nlast", 0),
+              wall_axis=d.get("wall_axis", -1), wall_pos=d.get("wall_pos", 0.0),
+              wall_k=d.get("wall_k", 0.0))
     s = orc.OracleSystem(orc.make_desc(d["n_atoms"], box, **kw))
     s.set_state(frame["x"], frame["y"], frame["z"], frame.get("vx"), frame.get("vy"),
                 frame.get("vz"), frame.get("fx"), frame.get("fy"), frame.get("fz"),

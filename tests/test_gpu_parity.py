@@ -134,12 +134,14 @@ def test_madelung_nacl(atvb, ctx):
     assert abs(e / e_exp - 1.0) < 5e-4
 
 
-def _traj_compare(atvb, ctx, orc, desc, frame, steps, tol_x):
+def _traj_compare(atvb, ctx, orc, desc, frame, steps, tol_x, setup=None, oracle_over=None):
     sys = atvb.System(ctx, desc, frame)
+    if setup is not None:
+        setup(sys)
     sys.compute_forces()
     sys.step(steps)
     out, sc = sys.download()
-    s = oracle_system(orc, desc, frame)
+    s = oracle_system(orc, desc, frame, **(oracle_over or {}))
     s.build_list()
     s.compute_forces()
     s.run(steps)
@@ -175,6 +177,37 @@ def test_trajectory_nose_hoover_rocksalt_fp64(atvb, ctx, orc):
 def test_trajectory_langevin_fp64(atvb, ctx, orc):
     desc, frame = W.lj_fcc(ncell=5, thermostat=2, seed=9)
     _traj_compare(atvb, ctx, orc, desc, frame, 40, 1e-8)
+
+
+def test_trajectory_langevin_ramp_fp64(atvb, ctx, orc):
+    """FixLangevin(T, 3 T).set_run_span(5, 35) (fix_langevin.cpp:94-104):
+    the setpoint ramps over steps 5-35 and holds after them; the trajectory
+    follows the oracle's, which ramps the same way."""
+    desc, frame = W.lj_fcc(ncell=5, thermostat=2, seed=9)
+    T0 = desc["temperature"]
+    ramp = dict(lang_T_stop=3.0 * T0, lang_nfirst=5, lang_nlast=35)
+    _traj_compare(atvb, ctx, orc, desc, frame, 45, 1e-8,
+                  setup=lambda s: s.set_langevin_ramp(3.0 * T0, 5, 35), oracle_over=ramp)
+
+
+def test_langevin_ramp_heats(atvb, ctx):
+    """A ramp T -> 3 T over 400 steps ends clearly hotter than the
+    constant setpoint from the same state (damping time 0.1 tau)."""
+    desc, frame = W.lj_fcc(ncell=6, thermostat=2, seed=4, damp_tau=0.1)
+    T0 = desc["temperature"]
+    kin = []
+    for ramp in (False, True):
+        s = atvb.System(ctx, desc, frame)
+        if ramp:
+            s.set_langevin_ramp(3.0 * T0, 0, 400)
+        s.compute_forces()
+        s.step(600)
+        kin.append(s.scalars()["kinetic"])
+        s.close()
+    assert kin[1] > 2.0 * kin[0], kin
+    with pytest.raises(atvb.AtvbError):
+        d2, f2 = W.lj_fcc(ncell=4)                 # NVE: no Langevin to ramp
+        atvb.System(ctx, d2, f2).set_langevin_ramp(2.0, 0, 10)
 
 
 def test_bitwise_reproducible_mixed(atvb, ctx):
