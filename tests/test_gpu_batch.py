@@ -145,6 +145,46 @@ def test_served_result_equals_alone(atvb, ctx, tight):
 
 
 @pytest.mark.gpu
+def test_served_arrivals_while_running_equal_alone(atvb, ctx):
+    """Continuous batching with arrivals: requests submitted while others are
+    already on the GPU join the running batch at the next tick, run beside
+    them, and each result is still the one it gets alone, bit for bit."""
+    from atomiverse_b200 import workloads as W
+    mix = _mix(W, 1)
+    reqs = [(mix[0][0], mix[0][1], 60), (mix[3][0], mix[3][1], 30),
+            (mix[2][0], mix[2][1], 25), (mix[1][0], mix[1][1], 20)]
+    budget = 2 * sum(atvb.request_bytes(d) for d, _, _ in reqs)
+    srv = atvb.Server(ctx, budget)
+    ids = [srv.submit(*reqs[0])]
+    srv.tick(5)                                  # the first request is running
+    assert srv.poll(ids[0])["state"] == 1
+    ids.append(srv.submit(*reqs[1]))             # arrives mid-run
+    srv.tick(5)
+    st = srv.stats()
+    assert st["running"] == 2                    # both on the device together
+    ids.append(srv.submit(*reqs[2]))
+    srv.tick(5)
+    ids.append(srv.submit(*reqs[3]))
+    peak = 0
+    for _ in range(200):
+        srv.tick(5)
+        st = srv.stats()
+        peak = max(peak, st["running"])
+        if st["queued"] == 0 and st["running"] == 0:
+            break
+    assert peak >= 2
+    outs = [srv.collect(r) for r in ids]
+    srv.close()
+    # the late arrivals started before the first request finished
+    assert outs[1][1]["t_start"] < outs[0][1]["t_done"]
+    for (d, f, n), (out, res) in zip(reqs, outs):
+        assert res["steps_done"] == n
+        alone, sa = _alone(atvb, ctx, d, f, n)
+        _same(out, alone)
+        assert res["scalars"]["energy"] == sa["energy"]
+
+
+@pytest.mark.gpu
 def test_server_admission_cancel_and_errors(atvb, ctx):
     from atomiverse_b200 import workloads as W
     d1, f1 = W.lj_fcc(ncell=5, seed=21, precision=1)
