@@ -189,6 +189,8 @@ class Engine {
     void enqueue_forces(const LaunchCfg& lc, const std::vector<int>& pme,
                         bool profile, bool overlap, bool build_list = false);
     void prof_mark(bool profile, const char* next);
+    template <typename F>
+    void capture_if(cudaGraphConditionalHandle h, F&& body);
     atvb_launch_ctx comp_ctx(const UserComp& c, int phase) const;
     void build_components();
     void run_components(int phase, bool before);
@@ -201,6 +203,11 @@ class Engine {
     cudaStream_t stream_ = nullptr;
     DevMem mem_;
     cudaStream_t pme_stream_ = nullptr; // the PME chain beside the pair kernel
+    // the list build as conditional nodes of the step graph: the handle of
+    // the graph being captured and the stream their bodies are captured on
+    cudaStream_t cond_stream_ = nullptr;
+    cudaGraphConditionalHandle cond_sort_ = 0, cond_rows_ = 0; // one per node
+    bool capturing_ = false;
     cudaEvent_t pme_fork_ = nullptr, pme_join_ = nullptr;
     bool any_npt_ = false; // an MTK NPT system exists (re-plan check per step call)
     int num_sms_ = 148;

@@ -9,6 +9,9 @@
 namespace atvb {
 
 constexpr int kChunk = 256;     // atoms per item of the per-atom kernels
+constexpr int kRebuildKernels = 6; // launches of one list build (cell sort + rows)
+constexpr long long kCondMinAtoms = 100000; // engines from this size skip them by
+                                            // conditional graph nodes
 constexpr int kListChunk = 8;   // cells per item of the list build (warp/cell)
 constexpr int kGridChunk = 4096; // grid points per item of the PME grid kernels
 constexpr int kLaneClasses = 6;  // pair lanes per atom: 1, 2, 4, 8, 16, 32
@@ -96,7 +99,11 @@ void launch_fft_reg(int pass, int idx, bool mixed, const ItemList& il, const Sys
                     cudaStream_t s);
 // integrate.cu
 void launch_integrate_a(const LaunchCfg& lc, cudaStream_t s);
-void launch_sys_a(const LaunchCfg& lc, cudaStream_t s);
+// cond_sort / cond_rows / use_cond: the step graph's conditional handles of
+// the list build (set when a system rebuilds), only while the step is being
+// captured
+void launch_sys_a(const LaunchCfg& lc, cudaStream_t s, cudaGraphConditionalHandle cond_sort = 0,
+                  cudaGraphConditionalHandle cond_rows = 0, bool use_cond = false);
 void launch_integrate_b(const LaunchCfg& lc, cudaStream_t s);
 void launch_sys_b(const LaunchCfg& lc, cudaStream_t s);
 void launch_sys_energy(const LaunchCfg& lc, cudaStream_t s);

@@ -610,6 +610,7 @@ Slot::Slot(const atvb_system_desc& d, const DevMem& mem) : desc(d), mem_(mem) {
 Engine::Engine(int device) : device_(device) {
     CK(cudaSetDevice(device));
     CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&cond_stream_, cudaStreamNonBlocking));
     CK(cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount,
                               device));
     cudaMemPoolProps props = {};
@@ -659,6 +660,8 @@ Engine::~Engine() {
         cudaMemPoolDestroy(mem_.pool);
     for (auto& e : prof_events_)
         cudaEventDestroy(e);
+    if (cond_stream_)
+        cudaStreamDestroy(cond_stream_);
     if (stream_)
         cudaStreamDestroy(stream_);
 }
@@ -1115,7 +1118,7 @@ void Engine::enqueue_step_components() {
 int64_t Engine::kernels_per_step() const {
     int64_t k = 0;
     k += 2;                                   // integrate_a, sys_a
-    k += 6;                                   // rebuild pipeline
+    k += kRebuildKernels;                     // list build (rebuild steps only)
     for (int p = 0; p < 2; ++p)                // pair: one per lane class used
         for (int c = 0; c < kLaneClasses; ++c)
             k += lc_.pair[p][c].n ? 1 : 0;
@@ -1146,8 +1149,12 @@ void Engine::enqueue_forces(const LaunchCfg& lc, const std::vector<int>& pme,
     // the cells are sorted, so on a rebuild step it also runs beside the
     // list build (issue-bound at low occupancy), not only beside the pair
     // kernel.
-    if (build_list)
-        launch_build_list(lc, stream_);
+    if (build_list) {
+        if (capturing_)
+            capture_if(cond_rows_, [&](cudaStream_t cs) { launch_build_list(lc, cs); });
+        else
+            launch_build_list(lc, stream_);
+    }
     if (!pme.empty()) {
         prof_mark(profile, "pme_spread");
         launch_pme_spread(lc, ps);
@@ -1168,12 +1175,64 @@ void Engine::enqueue_forces(const LaunchCfg& lc, const std::vector<int>& pme,
     }
 }
 
+// Inside the step graph being captured on stream_: an IF node on handle h
+// (a handle serves one node) whose body is what `body` launches (captured
+// on cond_stream_), with the capture continuing after the node.
+template <typename F>
+void Engine::capture_if(cudaGraphConditionalHandle h, F&& body) {
+    cudaStreamCaptureStatus st;
+    unsigned long long id = 0;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    CK(cudaStreamGetCaptureInfo(stream_, &st, &id, &g, &deps, &nd));
+    cudaGraphNodeParams p = {};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = h;
+    p.conditional.type = cudaGraphCondTypeIf;
+    p.conditional.size = 1;
+    cudaGraphNode_t node;
+    CK(cudaGraphAddNode(&node, g, deps, nd, &p));
+    CK(cudaStreamBeginCaptureToGraph(cond_stream_, p.conditional.phGraph_out[0], nullptr, nullptr,
+                                     0, cudaStreamCaptureModeThreadLocal));
+    body(cond_stream_);
+    cudaGraph_t out = nullptr;
+    CK(cudaStreamEndCapture(cond_stream_, &out));
+    CK(cudaStreamUpdateCaptureDependencies(stream_, &node, 1, cudaStreamSetCaptureDependencies));
+}
+
+// One step.  In the captured graph of an engine with at least
+// kCondMinAtoms atoms the list-build kernels sit in two IF nodes whose
+// handles k_sys_a sets when any system builds its list (reset at every
+// launch): the cell sort before the PME branch forks, the list build beside
+// it; on other steps they do not launch.  Measured on the B200: 262,144
+// ions +0.8 %, 1,000,188 LJ atoms +7 %; but 4,000 and 10,648 atoms -13 %
+// and -15 % (the conditional nodes cost more than the early-exit launches
+// of a small system), hence the threshold.
 void Engine::enqueue_step(bool profile) {
+    if (capturing_) {
+        long long atoms = 0;
+        for (const auto& up : slots_)
+            if (up)
+                atoms += up->hp.n;
+        capturing_ = atoms >= kCondMinAtoms;
+    }
+    if (capturing_) {
+        cudaStreamCaptureStatus st;
+        unsigned long long id = 0;
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamGetCaptureInfo(stream_, &st, &id, &g, nullptr, nullptr));
+        CK(cudaGraphConditionalHandleCreate(&cond_sort_, g, 0, cudaGraphCondAssignDefault));
+        CK(cudaGraphConditionalHandleCreate(&cond_rows_, g, 0, cudaGraphCondAssignDefault));
+    }
     prof_mark(profile, "integrate_a");
     launch_integrate_a(lc_, stream_);
-    launch_sys_a(lc_, stream_);
+    launch_sys_a(lc_, stream_, cond_sort_, cond_rows_, capturing_);
     prof_mark(profile, "neighbor");
-    launch_sort_cells(lc_, stream_);
+    if (capturing_)
+        capture_if(cond_sort_, [&](cudaStream_t cs) { launch_sort_cells(lc_, cs); });
+    else
+        launch_sort_cells(lc_, stream_);
     enqueue_forces(lc_, pme_slots_, profile, true, true);
     prof_mark(profile, "integrate_b");
     launch_integrate_b(lc_, stream_);
@@ -1338,15 +1397,26 @@ void Engine::ensure_graph() {
     if (gexec_)
         return;
     CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+    capturing_ = true;
     try {
         enqueue_step(false);
     } catch (...) {
+        capturing_ = false;
         cudaGraph_t g = nullptr;
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(cond_stream_, &cs) == cudaSuccess &&
+            cs != cudaStreamCaptureStatusNone) {
+            cudaStreamEndCapture(cond_stream_, &g); // a body capture left open
+            if (g)
+                cudaGraphDestroy(g);
+            g = nullptr;
+        }
         cudaStreamEndCapture(stream_, &g);
         if (g)
             cudaGraphDestroy(g);
         throw;
     }
+    capturing_ = false;
     CK(cudaStreamEndCapture(stream_, &graph_));
     CK(cudaGraphInstantiate(&gexec_, graph_, 0));
 }

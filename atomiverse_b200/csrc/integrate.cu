@@ -199,8 +199,13 @@ __global__ void __launch_bounds__(kChunk)
 }
 
 // One thread per system: thermostat scalar of the initial half, neighbour
-// decision (every / delay / check), step accumulators reset.
-__global__ void k_sys_a(const int* sys_list, int nsys, const SysParams* sp) {
+// decision (every / delay / check), step accumulators reset.  Inside the
+// step graph (use_cond), a system that builds its list sets the graph's
+// two conditional handles (one per conditional node: the cell sort and the
+// rows), which launch the list-build kernels of this step.
+__global__ void k_sys_a(const int* sys_list, int nsys, const SysParams* sp,
+                        cudaGraphConditionalHandle cond_sort,
+                        cudaGraphConditionalHandle cond_rows, int use_cond) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= nsys)
         return;
@@ -237,6 +242,10 @@ __global__ void k_sys_a(const int* sys_list, int nsys, const SysParams* sp) {
     const bool rebuild = forced || (st->ago >= P.nl_delay && (st->ago % P.nl_every) == 0 &&
                                     (!P.nl_check || disp));
     st->rebuild = rebuild ? 1 : 0;
+    if (rebuild && use_cond) {
+        cudaGraphSetConditional(cond_sort, 1u);
+        cudaGraphSetConditional(cond_rows, 1u);
+    }
     if (rebuild) {
         st->overflow = 0; // set again by the build if a row is cut
         for (int d = 0; d < 3; ++d) {
@@ -873,8 +882,10 @@ void launch_integrate_a(const LaunchCfg& lc, cudaStream_t s) {
     k_integrate_a<<<lc.atoms.grid, kChunk, 0, s>>>(lc.atoms.d, lc.atoms.n,
                                                     lc.sp);
 }
-void launch_sys_a(const LaunchCfg& lc, cudaStream_t s) {
-    k_sys_a<<<sys_blocks(lc.nsys), 128, 0, s>>>(lc.sys_list, lc.nsys, lc.sp);
+void launch_sys_a(const LaunchCfg& lc, cudaStream_t s, cudaGraphConditionalHandle cond_sort,
+                  cudaGraphConditionalHandle cond_rows, bool use_cond) {
+    k_sys_a<<<sys_blocks(lc.nsys), 128, 0, s>>>(lc.sys_list, lc.nsys, lc.sp, cond_sort,
+                                                 cond_rows, use_cond ? 1 : 0);
 }
 void launch_integrate_b(const LaunchCfg& lc, cudaStream_t s) {
     k_integrate_b<<<lc.atoms.grid, kChunk, 0, s>>>(lc.atoms.d, lc.atoms.n,

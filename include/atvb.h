@@ -386,7 +386,11 @@ int atvb_system_profile_read(atvb_system* sys, atvb_kernel_time* out,
                              int32_t capacity, int32_t* count);
 /* Lanes per atom in the pair kernel (1,2,4,8,16,32); 0 = autotune. */
 int atvb_system_set_pair_lanes(atvb_system* sys, int32_t lanes);
-/* Kernel launches this library made in the last step() call. */
+/* Kernel launches of the last step() call, counting the six list-build
+ * kernels on every step: in the step graph of a system (or batch) of at
+ * least 100,000 atoms they launch only on steps where a system rebuilds
+ * its list (conditional nodes), so the launches made there are this count
+ * less 6 per step without a rebuild. */
 int atvb_system_launch_count(atvb_system* sys, int64_t* launches);
 /* The system's CUDA stream (cudaStream_t) for event timing by callers. */
 void* atvb_system_stream(atvb_system* sys);
