@@ -942,7 +942,10 @@ FftCfg Engine::fft_items(const std::vector<int>& pme) {
     if (pme.empty())
         return f;
     const bool mixed = slots_[pme[0]]->hp.prec == kMixed;
-    const int g = num_sms_ * 8, gr = num_sms_ * 16;
+    // register forms: 4 blocks per SM looping over their tiles (measured at
+    // 192^3: 165 / 122 us FP64 / FP32 for the five passes, against 174 / 129
+    // with 16 per SM and 220 / 142 with 2)
+    const int g = num_sms_ * 8, gr = num_sms_ * 4;
     // axis 2: z, 1: y, 0: x
     for (int axis = 2; axis >= 0; --axis) {
         std::vector<FftGroup>& out = axis == 2 ? f.z : axis == 1 ? f.y : f.x;
