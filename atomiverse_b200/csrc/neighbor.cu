@@ -191,9 +191,8 @@ ATVB_DEV double exact_r2(const double4& a, const double4& b, const double* L,
 // wraps).  Offsets along an axis stay within one period of the cell index,
 // so one conditional add or subtract wraps them (also on an aliased axis,
 // whose offsets are absolute cell indices).
-ATVB_DEV void column_runs(const SysParams& P, const int* __restrict__ cstart, int4 col,
+ATVB_DEV void column_runs(int nc0, int nc1, int nc2, const int* __restrict__ cstart, int4 col,
                           int cx, int cy, int cz, int& a0, int& l0, int& a1, int& l1) {
-    const int nc0 = P.nc[0], nc1 = P.nc[1], nc2 = P.nc[2];
     int xx = cx + col.x;
     xx += xx < 0 ? nc0 : (xx >= nc0 ? -nc0 : 0);
     int yy = cy + col.y;
@@ -269,7 +268,12 @@ __global__ void __launch_bounds__(256)
         const int c = item.begin + warp;
         if (c >= P.ncell)
             continue; // warp-uniform
-        const int nc1 = P.nc[1], nc2 = P.nc[2];
+        // every field the loops use, read once: the row stores below could
+        // alias SysParams as far as the compiler knows, and would force a
+        // reload of any field read after them
+        const int nc0 = P.nc[0], nc1 = P.nc[1], nc2 = P.nc[2];
+        int* __restrict__ nbr = P.nbr;
+        const bool has_sp = P.has_special != 0;
         const double L[3] = {P.L[0], P.L[1], P.L[2]};
         const double hL[3] = {P.halfL[0], P.halfL[1], P.halfL[2]};
         const double rl2 = P.rlist2;
@@ -301,7 +305,8 @@ __global__ void __launch_bounds__(256)
             for (int c0 = 0; c0 < ncol; c0 += 32) {
                 int a0 = 0, l0 = 0, a1 = 0, l1 = 0;
                 if (c0 + lane < ncol)
-                    column_runs(P, cstart, cols[c0 + lane], cx, cy, cz, a0, l0, a1, l1);
+                    column_runs(nc0, nc1, nc2, cstart, cols[c0 + lane], cx, cy, cz, a0, l0,
+                                a1, l1);
                 const int tot = l0 + l1;
                 int incl = tot;
 #pragma unroll
@@ -368,18 +373,18 @@ __global__ void __launch_bounds__(256)
                                 if (ha) {
                                     const int wpos = basea + __popc(ma & lt);
                                     unsigned e = (unsigned)j;
-                                    if (P.has_special)
+                                    if (has_sp)
                                         e |= special_class(P, i0 + ii, j) << 30;
                                     if (wpos < cap)
-                                        P.nbr[(size_t)(i0 + ii) * cap + wpos] = (int)e;
+                                        nbr[(size_t)(i0 + ii) * cap + wpos] = (int)e;
                                 }
                                 if (hb) {
                                     const int wpos = baseb + __popc(mb & lt);
                                     unsigned e = (unsigned)j;
-                                    if (P.has_special)
+                                    if (has_sp)
                                         e |= special_class(P, i0 + i1, j) << 30;
                                     if (wpos < cap)
-                                        P.nbr[(size_t)(i0 + i1) * cap + wpos] = (int)e;
+                                        nbr[(size_t)(i0 + i1) * cap + wpos] = (int)e;
                                 }
                                 if (lane == ii)
                                     cnt += __popc(ma);
@@ -404,10 +409,10 @@ __global__ void __launch_bounds__(256)
                                 if (hit) {
                                     const int wpos = base + __popc(m & lt);
                                     unsigned e = (unsigned)j;
-                                    if (P.has_special)
+                                    if (has_sp)
                                         e |= special_class(P, i0 + ii, j) << 30;
                                     if (wpos < cap)
-                                        P.nbr[(size_t)(i0 + ii) * cap + wpos] = (int)e;
+                                        nbr[(size_t)(i0 + ii) * cap + wpos] = (int)e;
                                 }
                                 if (lane == ii)
                                     cnt += __popc(m);
@@ -434,10 +439,10 @@ __global__ void __launch_bounds__(256)
                                 if (hit) {
                                     const int wpos = base + __popc(m & lt);
                                     unsigned e = (unsigned)j;
-                                    if (P.has_special)
+                                    if (has_sp)
                                         e |= special_class(P, i0 + ii, j) << 30;
                                     if (wpos < cap)
-                                        P.nbr[(size_t)(i0 + ii) * cap + wpos] = (int)e;
+                                        nbr[(size_t)(i0 + ii) * cap + wpos] = (int)e;
                                 }
                                 if (lane == ii)
                                     cnt += __popc(m);
