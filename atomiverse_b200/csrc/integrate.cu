@@ -57,12 +57,12 @@ ATVB_DEV double fix_to_d(unsigned long long v) {
 
 // md::NVELimit (nve_limit.cu:20-30, LAMMPS fix nve/limit): after a half
 // kick, a speed above vmax = xmax / dt is scaled back to vmax.
-ATVB_DEV void speed_cap(const SysParams& P, double v[3]) {
-    if (!(P.vlimit2 > 0.0))
+ATVB_DEV void speed_cap(double vlimit, double vlimit2, double v[3]) {
+    if (!(vlimit2 > 0.0))
         return;
     const double vsq = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
-    if (vsq > P.vlimit2) {
-        const double s = P.vlimit / sqrt(vsq);
+    if (vsq > vlimit2) {
+        const double s = vlimit / sqrt(vsq);
         v[0] *= s;
         v[1] *= s;
         v[2] *= s;
@@ -99,7 +99,7 @@ ATVB_DEV double npt_drift_atom(const SysParams& P, int i) {
 #pragma unroll
     for (int d = 0; d < 3; ++d)
         v[d] = __dadd_rn(__dmul_rn(v[d], st->vs[d]), __dmul_rn(dtfm, fa[d]));
-    speed_cap(P, v);
+    speed_cap(P.vlimit, P.vlimit2, v);
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
         const double Ln = st->Lnext[d];
@@ -136,7 +136,7 @@ ATVB_DEV double npt_drift_atom(const SysParams& P, int i) {
 
 // Initial half: deferred scale, kick, drift, wrap, sorted repack,
 // displacement check, KE of the kicked velocities (for Nose-Hoover).
-__global__ void __launch_bounds__(kChunk)
+__global__ void __launch_bounds__(kChunk, 3)
     k_integrate_a(const Item* items, int nitems, const SysParams* sp) {
     __shared__ double sh[32];
     for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
@@ -149,19 +149,33 @@ __global__ void __launch_bounds__(kChunk)
         if (i < P.n && (P.thermostat == kNPT || P.generic_drift)) {
             ke = npt_drift_atom(P, i);
         } else if (i < P.n) {
+            // every load first (atom data, then the system fields read after
+            // the stores): a load placed after a store to global memory
+            // cannot be hoisted above it, and would add a round trip
             const double sc = P.st->vscale;
             const int r = P.rank[i];
             const double4 f = P.f4[r];
-            const double dtfm = P.dtf / P.mass[i];
+            const double m = P.mass[i];
+            const double q = P.q[i];
+            const double x0[3] = {P.x[i], P.y[i], P.z[i]};
+            const double xr[3] = {P.xr[i], P.yr[i], P.zr[i]};
             double v[3] = {P.vx[i], P.vy[i], P.vz[i]};
+            const double L[3] = {P.L[0], P.L[1], P.L[2]};
+            const double invL[3] = {P.invL[0], P.invL[1], P.invL[2]};
+            const double dt = P.dt, skin_half2 = P.skin_half2;
+            const bool mixed = P.prec == kMixed;
+            const double fs[3] = {mixed ? P.fix_scale[0] : P.fix64_scale[0],
+                                  mixed ? P.fix_scale[1] : P.fix64_scale[1],
+                                  mixed ? P.fix_scale[2] : P.fix64_scale[2]};
+            void* const pos4 = P.pos4;
+            const double dtfm = P.dtf / m;
             const double fa[3] = {f.x, f.y, f.z};
-            double* const xs[3] = {P.x, P.y, P.z};
             double x[3];
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
                 v[d] = __dadd_rn(__dmul_rn(v[d], sc), __dmul_rn(dtfm, fa[d]));
-                double xd = __dadd_rn(xs[d][i], __dmul_rn(P.dt, v[d]));
-                xd = __dadd_rn(xd, -__dmul_rn(P.L[d], floor(xd / P.L[d])));
+                double xd = __dadd_rn(x0[d], __dmul_rn(dt, v[d]));
+                xd = __dadd_rn(xd, -__dmul_rn(L[d], floor(xd / L[d])));
                 x[d] = xd;
             }
             P.vx[i] = v[0];
@@ -171,24 +185,23 @@ __global__ void __launch_bounds__(kChunk)
             P.y[i] = x[1];
             P.z[i] = x[2];
             check_finite(P, x, v);
-            const double q = P.q[i];
-            if (P.prec == kMixed) {
+            if (mixed) {
                 int4 p;
-                p.x = (int)pos_fix(x[0], P.fix_scale[0]);
-                p.y = (int)pos_fix(x[1], P.fix_scale[1]);
-                p.z = (int)pos_fix(x[2], P.fix_scale[2]);
+                p.x = (int)pos_fix(x[0], fs[0]);
+                p.y = (int)pos_fix(x[1], fs[1]);
+                p.z = (int)pos_fix(x[2], fs[2]);
                 p.w = __float_as_int((float)q);
-                reinterpret_cast<int4*>(P.pos4)[r] = p;
+                reinterpret_cast<int4*>(pos4)[r] = p;
             } else {
-                reinterpret_cast<double4*>(P.pos4)[r] = pack_pos64(x, P.fix64_scale, q);
+                reinterpret_cast<double4*>(pos4)[r] = pack_pos64(x, fs, q);
             }
             // cell_list.cpp:355-392 with min-image displacement
-            const double ddx = min_img(x[0] - P.xr[i], P.L[0], P.invL[0]);
-            const double ddy = min_img(x[1] - P.yr[i], P.L[1], P.invL[1]);
-            const double ddz = min_img(x[2] - P.zr[i], P.L[2], P.invL[2]);
-            if (ddx * ddx + ddy * ddy + ddz * ddz > P.skin_half2)
+            const double ddx = min_img(x[0] - xr[0], L[0], invL[0]);
+            const double ddy = min_img(x[1] - xr[1], L[1], invL[1]);
+            const double ddz = min_img(x[2] - xr[2], L[2], invL[2]);
+            if (ddx * ddx + ddy * ddy + ddz * ddz > skin_half2)
                 P.st->need_rebuild = 1;
-            ke = P.mass[i] * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+            ke = m * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
         }
         if (P.thermostat == kNoseHoover) {
             const double t = block_sum(ke, sh);
@@ -210,11 +223,16 @@ __global__ void k_sys_a(const int* sys_list, int nsys, const SysParams* sp,
     if (k >= nsys)
         return;
     const SysParams& P = sp[sys_list[k]];
-    SysState* st = P.st;
-    if (st->halted) {
-        st->rebuild = 0; // nothing of this system moves: no list build either
+    SysState* gst = P.st;
+    if (gst->halted) {
+        gst->rebuild = 0; // nothing of this system moves: no list build either
         return;
     }
+    // the state in local memory, written back once: each read below is then
+    // an L1 hit instead of a global round trip ordered behind the previous
+    // store (this thread is the state's only reader and writer meanwhile)
+    SysState loc = *gst;
+    SysState* st = &loc;
     if (P.thermostat == kNPT || P.deform_axis >= 0) {
         // commit the cell of this step's drift: every later kernel of the
         // step (neighbour build, forces, PME) reads it from SysParams
@@ -257,6 +275,7 @@ __global__ void k_sys_a(const int* sys_list, int nsys, const SysParams* sp,
         st->max_nnbr = 0;
         st->list_entries = 0ull;
     }
+    *gst = loc;
 }
 
 // sqrt(2 kB T / (damp dt mvv2e)) / ftm2v at the setpoint of `step`: the
@@ -285,6 +304,10 @@ __global__ void __launch_bounds__(kChunk)
         const int i = item.begin + threadIdx.x;
         double ke = 0.0;
         double kax[3] = {0.0, 0.0, 0.0};
+        // system fields read after the force store below, read before it
+        // (a load after a global store cannot be hoisted above it)
+        const double dtf = P.dtf, vlimit = P.vlimit, vlimit2 = P.vlimit2;
+        const int thermostat = P.thermostat;
         if (i < P.n) {
             const double sc = P.st->s_a;
             const int r = P.rank[i];
@@ -305,9 +328,9 @@ __global__ void __launch_bounds__(kChunk)
                 f.y = __dadd_rn(f.y, P.ext_f[P.n + i]);
                 f.z = __dadd_rn(f.z, P.ext_f[2 * P.n + i]);
             }
-            if ((P.has_pme || P.ext_f) && P.thermostat != kLangevin)
+            if ((P.has_pme || P.ext_f) && thermostat != kLangevin)
                 P.f4[r] = f;
-            if (P.thermostat == kLangevin) {
+            if (thermostat == kLangevin) {
                 const unsigned long long base =
                     (unsigned long long)P.seed * 0x9E3779B97F4A7C15ull +
                     (unsigned long long)P.st->step * 0xBF58476D1CE4E5B9ull;
@@ -322,11 +345,11 @@ __global__ void __launch_bounds__(kChunk)
                 f.z += g1 * v[2] + g2 * rz;
                 P.f4[r] = f;
             }
-            const double dtfm = P.dtf / m;
+            const double dtfm = dtf / m;
             v[0] = __dadd_rn(v[0], __dmul_rn(dtfm, f.x));
             v[1] = __dadd_rn(v[1], __dmul_rn(dtfm, f.y));
             v[2] = __dadd_rn(v[2], __dmul_rn(dtfm, f.z));
-            speed_cap(P, v);
+            speed_cap(vlimit, vlimit2, v);
             P.vx[i] = v[0];
             P.vy[i] = v[1];
             P.vz[i] = v[2];
@@ -335,7 +358,7 @@ __global__ void __launch_bounds__(kChunk)
             kax[1] = m * v[1] * v[1];
             kax[2] = m * v[2] * v[2];
         }
-        if (P.thermostat == kNPT) {
+        if (thermostat == kNPT) {
             block_sum_vec<3>(kax, sh3);
             if (threadIdx.x == 0)
                 for (int d = 0; d < 3; ++d)
@@ -529,11 +552,15 @@ __global__ void k_sys_b(const int* sys_list, int nsys, const SysParams* sp) {
     if (k >= nsys)
         return;
     const SysParams& P = sp[sys_list[k]];
-    SysState* st = P.st;
-    if (st->halted)
+    SysState* gst = P.st;
+    if (gst->halted)
         return;
+    // the state in local memory, written back once (as in k_sys_a)
+    SysState loc = *gst;
+    SysState* st = &loc;
     if (P.thermostat == kNPT) {
         npt_end_of_step(P, st);
+        *gst = loc;
         return;
     }
     const double ke = fix_to_d(st->acc[kAccKEB]);
@@ -567,6 +594,7 @@ __global__ void k_sys_b(const int* sys_list, int nsys, const SysParams* sp) {
         *(volatile int*)P.row_hint = st->max_nnbr;
     end_status(P, st);
     st->step += 1;
+    *gst = loc;
 }
 
 // Energies of a force-only evaluation (no step, no thermostat update).
