@@ -61,6 +61,9 @@ DT_FS = 2.0
 # launches of one neighbour-list build (cell sort + rows): in the step graph
 # they run only on steps that rebuild a list
 REBUILD_KERNELS = 6
+# FP64 instructions per evaluated list entry of k_pair<fp64> on this workload
+# (ncu: 250 M FP64 warp instructions for 108 M entries, one launch)
+FP64_PER_ENTRY = 74
 
 
 def _peaks():
@@ -674,6 +677,19 @@ def run_headline(args):
                 "frac": achieved / peak, "traffic": _traffic("k_pair_fp64_config1"),
                 "kernel": "k_pair<fp64>", "peak_kind": peak_kind,
                 "algorithmic_bytes": b_alg, "pair_launch_ms": pair_avg_s * 1e3}
+    # the pair kernel's own limit: the FP64 pipe (64 FP64 lanes per SM per
+    # clock on B200).  Every listed pair is evaluated from both of its rows,
+    # with FP64_PER_ENTRY FP64 instructions per evaluation (the ncu count of
+    # the current kernel); the clock is the SM clock sampled during the run
+    import torch
+    sms = torch.cuda.get_device_properties(local).multi_processor_count
+    fp64_peak = sms * 64 * clk["sm_mhz"] * 1e6 / 1e12 if clk.get("sm_mhz") else None
+    fp64_done = 2 * p_half * FP64_PER_ENTRY / pair_avg_s / 1e12
+    compute_roofline = {"bound": "fp64", "kernel": "k_pair<fp64>", "unit": "T FP64 instr/s",
+                        "achieved": fp64_done, "peak": fp64_peak,
+                        "frac": fp64_done / fp64_peak if fp64_peak else None,
+                        "fp64_instr_per_entry": FP64_PER_ENTRY, "entries": 2 * p_half,
+                        "peak_kind": "nominal 64 lanes/SM/clock x SMs x sampled SM clock"}
     kernels = {k: {"ms_per_launch": v[0] / v[1], "share": v[0] / sum(x[0] for x in prof.values())}
                for k, v in prof.items()}
 
@@ -771,6 +787,7 @@ def run_headline(args):
             "mixed_precision_value": mixed,
             "gpu_launches": launches,
             "roofline": roofline,
+            "compute_roofline": compute_roofline,
             "kernels": kernels,
             "cpu_baseline": cpu,
             "e2e": {"value": ws * e2e_steps / e2e_s, "unit": UNIT,
