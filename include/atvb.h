@@ -22,7 +22,7 @@ extern "C" {
 
 #define ATVB_OK 0
 #define ATVB_ERR_INVALID 1  /* bad argument (std::invalid_argument in the reference) */
-#define ATVB_ERR_CUDA 2     /* CUDA runtime / cuFFT failure (ATV_CUDA_CHECK) */
+#define ATVB_ERR_CUDA 2     /* CUDA runtime failure (ATV_CUDA_CHECK) */
 #define ATVB_ERR_OVERFLOW 3 /* neighbour row capacity exceeded during a step */
 #define ATVB_ERR_STATE 4    /* call out of order (e.g. step before upload) */
 #define ATVB_ERR_NOMEM 5    /* device memory budget exceeded */
