@@ -213,7 +213,9 @@ def cpu_baseline(budget_s: float = 20.0, max_steps: int = 5):
 
 
 def run_reference(args):
-    dist, rank, ws, local = _dist()
+    # host cores only: rank 0 runs it, the other ranks of a torchrun launch
+    # exit at once (no process group, no GPU work)
+    rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     steps = max(1, min(args.steps, 5))
