@@ -9,7 +9,9 @@
 - coordinates outside [0, L) and on the box faces: wrapped on upload
   (cpu/frame/pbc.h:48-50), so the forces are those of the wrapped frame;
 - neutral ions beside charged ones with real-space Ewald and PME (real-space
-  terms with q == 0 skipped, coul_long.cpp:146-222) and a net charge.
+  terms with q == 0 skipped, coul_long.cpp:146-222) and a net charge;
+- an empty system is refused when it is created, and a system or batch with
+  nothing uploaded refuses to step, each with an error the caller can read.
 """
 import numpy as np
 import pytest
@@ -158,3 +160,16 @@ def test_neutral_ions_and_net_charge(atvb, ctx, orc, precision, tol):
     assert sc["energy"] == pytest.approx(o.scalars()["energy"], rel=tol)
     vir = o.scalars()["virial"]
     assert np.allclose(sc["stress"], vir, rtol=1e-5, atol=1e-6 * np.abs(vir).max())
+
+
+def test_empty_and_unuploaded_systems_are_refused(atvb, ctx):
+    with pytest.raises(atvb.AtvbError, match="n_atoms"):
+        atvb.System(ctx, _lj_desc(0, (10.0, 10.0, 10.0)))
+    s = atvb.System(ctx, _lj_desc(4, (10.0, 10.0, 10.0)))
+    with pytest.raises(atvb.AtvbError, match="upload"):
+        s.step(1)
+    s.close()
+    b = atvb.Batch(ctx, [(_lj_desc(4, (10.0, 10.0, 10.0)), None)])
+    with pytest.raises(atvb.AtvbError, match="upload"):
+        b.step(1)
+    b.close()
